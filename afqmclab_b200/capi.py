@@ -1,0 +1,284 @@
+"""ctypes binding of the engine's C ABI (include/afqmc_b200.h).
+
+This is the host-side mirror used by the tests and bench.py: the same entry
+points a C++ or cgo/JNI caller binds.  The library is the in-tree
+libafqmc_b200.so built for sm_100a; importing this module on a machine
+without it raises immediately (there is no fallback path).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_lib = None
+
+AFQMC_FP64, AFQMC_MIXED = 0, 1
+DECOMP = {"densityCharge": 0, "densitySpin": 1, "hopCharge": 2, "hopSpin": 3}
+FORCE = {"dynamicForce": 0, "constForce": 1}
+
+SYMBOLS = [
+    "afqmc_last_error", "afqmc_version", "afqmc_cp_create", "afqmc_pl_create", "afqmc_destroy",
+    "afqmc_set_stream", "afqmc_synchronize", "afqmc_set_walkers", "afqmc_get_walkers",
+    "afqmc_set_rng", "afqmc_get_rng", "afqmc_set_ET", "afqmc_set_cadence",
+    "afqmc_project_one_step", "afqmc_project_half", "afqmc_modify_gm", "afqmc_pop_control",
+    "afqmc_reset_measurement", "afqmc_add_mixed_measurement", "afqmc_get_measurement",
+    "afqmc_get_cholesky_nums", "afqmc_pl_update_background", "afqmc_log_overlaps",
+    "afqmc_green_matrix", "afqmc_taylor_stats", "afqmc_status", "afqmc_pop_configuration_dev",
+    "afqmc_profile_enable", "afqmc_profile_get", "afqmc_launch_count",
+]
+
+PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
+          "popcontrol", "exchange", "measure"]
+
+
+class AfqmcError(RuntimeError):
+    pass
+
+
+def lib_path():
+    return _build.LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = lib_path()
+        if not os.path.exists(path):
+            raise AfqmcError(f"engine library {path} is missing: run python -m afqmclab_b200.build")
+        _lib = ctypes.CDLL(path)
+        _declare(_lib)
+    return _lib
+
+
+def _declare(L):
+    P, I, D, U64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong
+    PP = ctypes.POINTER(ctypes.c_void_p)
+    L.afqmc_last_error.restype = ctypes.c_char_p
+    L.afqmc_version.restype = ctypes.c_char_p
+    L.afqmc_cp_create.argtypes = [I, I, I, I, I, D, D, D, I, I, I, P, P, P, P, P, P, P, P, P, P,
+                                  P, D, D, U64, PP]
+    L.afqmc_pl_create.argtypes = [I, I, I, I, I, I, D, D, D, I, I, I, P, P, P, P, D, P, D, P, D,
+                                  P, D, P, P, P, D, D, U64, PP]
+    for name in ["afqmc_destroy", "afqmc_synchronize", "afqmc_modify_gm",
+                 "afqmc_reset_measurement", "afqmc_add_mixed_measurement"]:
+        getattr(L, name).argtypes = [P]
+    L.afqmc_set_stream.argtypes = [P, P]
+    L.afqmc_set_walkers.argtypes = [P, P, P, P]
+    L.afqmc_get_walkers.argtypes = [P, P, P, P]
+    L.afqmc_set_rng.argtypes = [P, U64, U64]
+    L.afqmc_get_rng.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64)]
+    L.afqmc_set_ET.argtypes = [P, D]
+    L.afqmc_set_cadence.argtypes = [P, I, I]
+    L.afqmc_project_one_step.argtypes = [P, I]
+    L.afqmc_project_half.argtypes = [P, I]
+    L.afqmc_pop_control.argtypes = [P, P, P]
+    L.afqmc_get_measurement.argtypes = [P, P]
+    L.afqmc_get_cholesky_nums.argtypes = [P, P, P]
+    L.afqmc_pl_update_background.argtypes = [P, P, P, D, P, D, P, D]
+    L.afqmc_log_overlaps.argtypes = [P, P]
+    L.afqmc_green_matrix.argtypes = [P, I, I, P]
+    L.afqmc_taylor_stats.argtypes = [P, ctypes.POINTER(ctypes.c_longlong),
+                                     ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(I),
+                                     ctypes.POINTER(I)]
+    L.afqmc_status.argtypes = [P, ctypes.POINTER(I)]
+    L.afqmc_pop_configuration_dev.argtypes = [I, P, P, P, P]
+    L.afqmc_profile_enable.argtypes = [P, I]
+    L.afqmc_profile_get.argtypes = [P, P, P]
+    L.afqmc_launch_count.argtypes = []
+    for name in SYMBOLS[2:]:
+        getattr(L, name).restype = I
+    L.afqmc_launch_count.restype = ctypes.c_longlong
+
+
+def _check(r):
+    if r != 0:
+        raise AfqmcError(f"afqmc error {r}: {lib().afqmc_last_error().decode()}")
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _z(a):
+    return None if a is None else np.asfortranarray(a, dtype=np.complex128)
+
+
+def _d(a):
+    return None if a is None else np.asfortranarray(a, dtype=np.float64)
+
+
+class Engine:
+    """A walker population resident on the GPU (one engine handle)."""
+
+    def __init__(self, handle, kind, n, ncol, W, G=0, nup=0, ndn=0, keep=()):
+        self.h = handle
+        self.kind, self.n, self.ncol, self.W, self.G = kind, n, ncol, W, G
+        self.nup, self.ndn = nup, ndn
+        self._keep = keep
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().afqmc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # population
+    def set_walkers(self, wf, logw, alive):
+        wf = np.asfortranarray(wf, dtype=np.complex128)
+        assert wf.shape == (self.n, self.ncol, self.W), wf.shape
+        lw = np.ascontiguousarray(logw, dtype=np.complex128)
+        al = np.ascontiguousarray(alive, dtype=np.int32)
+        _check(lib().afqmc_set_walkers(self.h, _p(wf), _p(lw), _p(al)))
+
+    def get_walkers(self):
+        wf = np.zeros((self.n, self.ncol, self.W), np.complex128, order="F")
+        lw = np.zeros(self.W, np.complex128)
+        al = np.zeros(self.W, np.int32)
+        _check(lib().afqmc_get_walkers(self.h, _p(wf), _p(lw), _p(al)))
+        return wf, lw, al
+
+    def set_rng(self, seed, counter=0):
+        _check(lib().afqmc_set_rng(self.h, seed, counter))
+
+    def rng_counter(self):
+        s, c = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        _check(lib().afqmc_get_rng(self.h, ctypes.byref(s), ctypes.byref(c)))
+        return c.value
+
+    def set_ET(self, ET):
+        _check(lib().afqmc_set_ET(self.h, ET))
+
+    def set_cadence(self, mgs_index, pop_index):
+        _check(lib().afqmc_set_cadence(self.h, mgs_index, pop_index))
+
+    def set_stream(self, stream_ptr):
+        _check(lib().afqmc_set_stream(self.h, stream_ptr))
+
+    def synchronize(self):
+        _check(lib().afqmc_synchronize(self.h))
+
+    # driver pieces
+    def step(self, nsteps=1):
+        _check(lib().afqmc_project_one_step(self.h, nsteps))
+
+    def project_half(self, which):
+        _check(lib().afqmc_project_half(self.h, which))
+
+    def modify_gm(self):
+        _check(lib().afqmc_modify_gm(self.h))
+
+    def pop_control(self):
+        table = np.zeros(self.W, np.int32)
+        weight = np.zeros(self.W)
+        _check(lib().afqmc_pop_control(self.h, _p(table), _p(weight)))
+        return table, weight
+
+    def reset_measurement(self):
+        _check(lib().afqmc_reset_measurement(self.h))
+
+    def add_mixed_measurement(self):
+        _check(lib().afqmc_add_mixed_measurement(self.h))
+
+    def measurement(self):
+        out = np.zeros(5, np.complex128)
+        _check(lib().afqmc_get_measurement(self.h, _p(out)))
+        return out
+
+    def cholesky_nums(self):
+        b = np.zeros(self.G, np.complex128)
+        e = np.zeros(self.G, np.complex128)
+        _check(lib().afqmc_get_cholesky_nums(self.h, _p(b), _p(e)))
+        return b, e
+
+    def update_background(self, m):
+        """m: MoleculeInputs after set_background()."""
+        a = [_d(m.bg), _z(m.expMinusDtK), _z(m.expHalfDtK), _z(m.expMinusHalfDtK)]
+        _check(lib().afqmc_pl_update_background(self.h, _p(a[0]), _p(a[1]), float(m.logwDt),
+                                                _p(a[2]), -float(m.logwHalf), _p(a[3]),
+                                                float(m.logwHalf)))
+
+    # diagnostics
+    def log_overlaps(self):
+        out = np.zeros(self.W, np.complex128)
+        _check(lib().afqmc_log_overlaps(self.h, _p(out)))
+        return out
+
+    def green(self, w, spin=0):
+        out = np.zeros((self.n, self.n), np.complex128, order="F")
+        _check(lib().afqmc_green_matrix(self.h, w, spin, _p(out)))
+        return out
+
+    def taylor_stats(self):
+        c, t = ctypes.c_longlong(), ctypes.c_longlong()
+        mn, mx = ctypes.c_int(), ctypes.c_int()
+        _check(lib().afqmc_taylor_stats(self.h, ctypes.byref(c), ctypes.byref(t),
+                                        ctypes.byref(mn), ctypes.byref(mx)))
+        return c.value, t.value, mn.value, mx.value
+
+    def profile(self, on=True):
+        _check(lib().afqmc_profile_enable(self.h, 1 if on else 0))
+
+    def profile_get(self):
+        ms = np.zeros(len(PHASES))
+        cnt = np.zeros(len(PHASES), np.int64)
+        _check(lib().afqmc_profile_get(self.h, _p(ms), _p(cnt)))
+        return {PHASES[i]: (float(ms[i]), int(cnt[i])) for i in range(len(PHASES))}
+
+    def status(self):
+        s = ctypes.c_int()
+        _check(lib().afqmc_status(self.h, ctypes.byref(s)))
+        return s.value
+
+
+def cp_engine(m, W, seed, mgs_step=10, pop_step=40, force_type="dynamicForce",
+              precision=AFQMC_FP64, const_force=None):
+    """Constrained-path Hubbard engine from a HubbardInputs bundle."""
+    keep = [_z(m.K), _z(m.expMinusDtK), _z(m.expHalfDtK), _z(m.expMinusHalfDtK), _d(m.U),
+            _d(m.mu), _d(m.hx), _d(m.hy), _d(m.hz), _d(const_force), _z(m.phiT)]
+    h = ctypes.c_void_p()
+    _check(lib().afqmc_cp_create(m.L, m.N, W, DECOMP[m.decomp], FORCE[force_type], m.dt, m.ET,
+                                 m.force_cap, mgs_step, pop_step, precision,
+                                 *[_p(a) for a in keep], float(np.real(m.logwT)),
+                                 float(np.imag(m.logwT)), seed, ctypes.byref(h)))
+    return Engine(h.value, "cp", 2 * m.L, m.N, W)
+
+
+def pl_engine(m, W, seed, mgs_step=10, pop_step=10, force_type="dynamicForce",
+              precision=AFQMC_FP64, log_one_body=False, const_force=None):
+    """Phaseless engine from a MoleculeInputs bundle."""
+    if log_one_body:
+        mats = [None, 0.0, _z(m.logExpHalfDtK), -float(m.logwHalf), _z(m.logExpMinusHalfDtK),
+                float(m.logwHalf), _z(m.logExpMinusDtK), float(m.logwDt)]
+    else:
+        mats = [_z(m.expMinusDtK), float(m.logwDt), _z(m.expHalfDtK), -float(m.logwHalf),
+                _z(m.expMinusHalfDtK), float(m.logwHalf), None, 0.0]
+    arrs = [_d(m.chol), _d(m.bg), _d(m.t)]
+    cf = _z(const_force)
+    tu, td = _z(m.phiTUp), _z(m.phiTDn)
+    keep = arrs + [mats[0], mats[2], mats[4], mats[6], cf, tu, td]
+    margs = [_p(mats[0]), mats[1], _p(mats[2]), mats[3], _p(mats[4]), mats[5], _p(mats[6]),
+             mats[7]]
+    h = ctypes.c_void_p()
+    _check(lib().afqmc_pl_create(m.n, m.nup, m.ndn, m.G, W, FORCE[force_type], m.dt, m.ET,
+                                 m.force_cap, mgs_step, pop_step, precision,
+                                 *[_p(a) for a in arrs], *margs, _p(cf), _p(tu), _p(td),
+                                 float(np.real(m.logwT)), float(np.imag(m.logwT)), seed,
+                                 ctypes.byref(h)))
+    return Engine(h.value, "pl", m.n, max(m.nup, m.ndn), W, G=m.G, nup=m.nup, ndn=m.ndn,
+                  keep=keep)
+
+
+def launch_count():
+    return int(lib().afqmc_launch_count())
+
+
+def pop_configuration_dev(weights_dev_ptr, uniforms_dev_ptr, table_dev_ptr, W, stream=None):
+    _check(lib().afqmc_pop_configuration_dev(W, weights_dev_ptr, uniforms_dev_ptr, table_dev_ptr,
+                                             stream))

@@ -1,0 +1,1016 @@
+// AFQMC walker-step engine: host-side sequencing of the sm_100a kernels and
+// the extern "C" entry points declared in include/afqmc_b200.h.
+//
+// The population (W walkers) lives in device memory as one strided batch:
+// walker w's n x ncol column-major matrix starts at w * n * ncol, its log
+// weight, alive flag and random-stream offset sit in per-walker arrays.
+// The step order is the reference drivers' per-walker loop body
+// (tutorials/afqmcConstraintPath/source/afqmcConstraintPathProjection.cpp:37-74,
+//  tutorials/afqmcPhaseless/source/afqmcPhaselessProjection.cpp:75-121),
+// executed population-wide, kernel by kernel.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/afqmc_b200.h"
+#include "common.cuh"
+#include "mixed.cuh"
+#include "walker_kernels.cuh"
+#include "zgemm.cuh"
+
+#include <atomic>
+extern std::atomic<long long> g_launch_count;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                        \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            return fail(AFQMC_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+#define TRY(expr)                   \
+    do {                            \
+        int _r = (expr);            \
+        if (_r != AFQMC_OK) return _r; \
+    } while (0)
+
+constexpr int TAYLOR_KMAX = 30;
+constexpr int TAYLOR_BASE = 3;          // baseTaylorOrder default (logHop2isSD2isOperation.h:31)
+constexpr double TAYLOR_ACC = 1e-10;    // accuracy default
+
+typedef std::complex<double> cd;
+
+// ------------------------------------------------ NiupNidn constants (host)
+// solveCoshxEqExpy / solveCosxEqExpy / exp2by2Matrix (common/mathHao/source/simple_fun.cpp:7-91)
+cd solve_cosh_eq_exp(double y)
+{
+    cd ey(std::exp(y), 0.0);
+    cd g = std::log(ey - std::sqrt(ey * ey - 1.0));
+    if (std::abs(g.real()) < std::abs(g.imag())) g = cd(0, g.imag());
+    else g = cd(g.real(), 0);
+    return g;
+}
+cd solve_cos_eq_exp(double y)
+{
+    cd ey(std::exp(y), 0.0);
+    cd g = std::acos(ey);
+    if (std::abs(g.real()) < std::abs(g.imag())) g = cd(0, g.imag());
+    else g = cd(g.real(), 0);
+    return g;
+}
+void exp2by2(double &a, double &b, cd &c)
+{
+    if (std::abs(c) < 1e-60) { a = std::exp(a); b = std::exp(b); c = 0.0; return; }
+    double abs_c = std::abs(c), arg_c = std::arg(c);
+    double d0, d1; cd v00, v01, v10, v11; cd im(0.0, 1.0);
+    if (std::abs(a - b) < 1e-60) {
+        double norm = 1.0 / std::sqrt(2.0);
+        d0 = std::exp(-abs_c + a); d1 = std::exp(abs_c + b);
+        v00 = -norm; v10 = norm * std::exp(im * arg_c); v01 = norm; v11 = norm * std::exp(im * arg_c);
+    } else {
+        double xi = 0.5 * std::atan(2.0 * abs_c / (a - b));
+        d0 = std::exp(0.5 * std::cos(2.0 * xi) * (a - b) + std::sin(2.0 * xi) * abs_c + (a + b) * 0.5);
+        d1 = std::exp(-0.5 * std::cos(2.0 * xi) * (a - b) - std::sin(2.0 * xi) * abs_c + (a + b) * 0.5);
+        v00 = std::exp(-im * arg_c * 0.5) * std::cos(xi);
+        v10 = std::exp(im * arg_c * 0.5) * std::sin(xi);
+        v01 = -std::exp(-im * arg_c * 0.5) * std::sin(xi);
+        v11 = std::exp(im * arg_c * 0.5) * std::cos(xi);
+    }
+    double na = (d0 * v00 * std::conj(v00) + d1 * v01 * std::conj(v01)).real();
+    double nb = (d0 * v10 * std::conj(v10) + d1 * v11 * std::conj(v11)).real();
+    c = d0 * v10 * std::conj(v00) + d1 * v11 * std::conj(v01);
+    a = na; b = nb;
+}
+
+zd tozd(cd z) { return make_double2(z.real(), z.imag()); }
+
+}  // namespace
+
+enum { KIND_CP = 0, KIND_PL = 1 };
+
+struct afqmc_engine {
+    int kind = 0;
+    int n = 0, ncol = 0, nup = 0, ndn = 0, W = 0, L = 0, G = 0;
+    int precision = AFQMC_FP64;
+    int decomp = 0, forceType = 0;
+    double dt = 0, ET = 0, forceCap = 0;
+    int mgsStep = 1, popStep = 1, mgsIndex = 0, popIndex = 0;
+    uint64_t seed = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    Blocks bl{};
+    long long wsize = 0;
+    zd logwT{0, 0};
+    zd *phiT[2] = {nullptr, nullptr};
+    // population and workspaces
+    zd *wf = nullptr, *wfTmp = nullptr, *term[2] = {nullptr, nullptr}, *logw = nullptr,
+       *logov = nullptr, *S = nullptr, *Sinv = nullptr, *thetaT = nullptr;
+    int *alive = nullptr, *surv = nullptr, *status = nullptr, *done = nullptr, *order = nullptr,
+        *table = nullptr, *number = nullptr;
+    unsigned long long *counter = nullptr, *offs = nullptr;
+    double *weight = nullptr;
+    long long *tstats = nullptr;
+    // one-body operators: 0 exp(-dt K), 1 exp(+dt/2 K), 2 exp(-dt/2 K)
+    zd *expK[3] = {nullptr, nullptr, nullptr};
+    zd expLogw[3] = {{0, 0}, {0, 0}, {0, 0}};
+    bool useLog = false;
+    zd *logK = nullptr;
+    zd logKLogw{0, 0};
+    // Hubbard
+    HubbardDev hd{};
+    zd *gamma = nullptr, *cdiag[4] = {nullptr, nullptr, nullptr, nullptr};
+    double *U = nullptr, *mu = nullptr, *hx = nullptr, *hy = nullptr, *hz = nullptr,
+           *constForceCP = nullptr, *forceCP = nullptr;
+    zd *wfDaggerK = nullptr;
+    // phaseless
+    CholDev cdv{};
+    double *chol = nullptr, *bg = nullptr;
+    zd *Aall = nullptr, *wfDaggerT = nullptr, *xbar = nullptr, *forcePL = nullptr, *aux = nullptr,
+       *M = nullptr, *ex = nullptr, *constForcePL = nullptr;
+    long long Ktot = 0;
+    // measurement
+    zd *acc = nullptr, *bgNum = nullptr, *exNum = nullptr, *eloc = nullptr, *den = nullptr,
+       *parts = nullptr;
+    // mixed-precision state
+    MixedState *mx = nullptr;
+    // phase profiler (CUDA events on the engine stream; off unless enabled)
+    bool prof = false;
+    struct Mark { int phase; cudaEvent_t a, b; };
+    std::vector<Mark> marks;
+    std::vector<cudaEvent_t> evpool;
+    double profMs[AFQMC_NPHASES] = {};
+    long long profCount[AFQMC_NPHASES] = {};
+    std::vector<void *> allocs;
+};
+
+// Phase timing: record an event pair around a phase when profiling is on.
+struct PhaseScope {
+    afqmc_engine *e; int phase; cudaEvent_t a = nullptr;
+    PhaseScope(afqmc_engine *e_, int p) : e(e_), phase(p)
+    {
+        if (!e->prof) return;
+        if (e->evpool.empty()) cudaEventCreate(&a); else { a = e->evpool.back(); e->evpool.pop_back(); }
+        cudaEventRecord(a, e->stream);
+    }
+    ~PhaseScope()
+    {
+        if (!e->prof) return;
+        cudaEvent_t b;
+        if (e->evpool.empty()) cudaEventCreate(&b); else { b = e->evpool.back(); e->evpool.pop_back(); }
+        cudaEventRecord(b, e->stream);
+        e->marks.push_back({phase, a, b});
+    }
+};
+#define PHASE(p) PhaseScope _ps_##p(e, p)
+
+static void prof_resolve(afqmc_engine *e)
+{
+    if (e->marks.empty()) return;
+    cudaStreamSynchronize(e->stream);
+    for (auto &m : e->marks) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, m.a, m.b);
+        e->profMs[m.phase] += ms;
+        e->profCount[m.phase] += 1;
+        e->evpool.push_back(m.a);
+        e->evpool.push_back(m.b);
+    }
+    e->marks.clear();
+}
+
+namespace {
+
+template <class T>
+int dalloc(afqmc_engine *e, T **p, size_t count)
+{
+    if (count == 0) count = 1;
+    void *q = nullptr;
+    cudaError_t r = cudaMalloc(&q, count * sizeof(T));
+    if (r != cudaSuccess)
+        return fail(AFQMC_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(r));
+    r = cudaMemset(q, 0, count * sizeof(T));
+    if (r != cudaSuccess) return fail(AFQMC_ERR_CUDA, cudaGetErrorString(r));
+    e->allocs.push_back(q);
+    *p = (T *)q;
+    return AFQMC_OK;
+}
+
+template <class T>
+int dupload(afqmc_engine *e, T **p, const void *host, size_t count)
+{
+    TRY(dalloc(e, p, count));
+    if (host) CUDA_TRY(cudaMemcpy(*p, host, count * sizeof(T), cudaMemcpyHostToDevice));
+    return AFQMC_OK;
+}
+
+int check_launch()
+{
+    cudaError_t r = cudaGetLastError();
+    if (r != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(r));
+    return AFQMC_OK;
+}
+
+int gemm(const ZGemmArgs &a, cudaStream_t s)
+{
+    cudaError_t r = zgemm_batched(a, s);
+    if (r != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("zgemm: ") + cudaGetErrorString(r));
+    return AFQMC_OK;
+}
+
+// common allocations for both engines
+int alloc_population(afqmc_engine *e)
+{
+    const int W = e->W;
+    e->wsize = (long long)e->n * e->ncol;
+    TRY(dalloc(e, &e->wf, (size_t)W * e->wsize));
+    TRY(dalloc(e, &e->wfTmp, (size_t)W * e->wsize));
+    TRY(dalloc(e, &e->term[0], (size_t)W * e->wsize));
+    TRY(dalloc(e, &e->term[1], (size_t)W * e->wsize));
+    TRY(dalloc(e, &e->logw, W));
+    TRY(dalloc(e, &e->logov, W));
+    TRY(dalloc(e, &e->S, (size_t)W * e->bl.sStride));
+    TRY(dalloc(e, &e->Sinv, (size_t)W * e->bl.sStride));
+    TRY(dalloc(e, &e->thetaT, (size_t)W * e->bl.tStride));
+    TRY(dalloc(e, &e->alive, W));
+    TRY(dalloc(e, &e->surv, W));
+    TRY(dalloc(e, &e->status, W + 1));
+    TRY(dalloc(e, &e->done, W));
+    TRY(dalloc(e, &e->order, W));
+    TRY(dalloc(e, &e->table, W));
+    TRY(dalloc(e, &e->number, W));
+    TRY(dalloc(e, &e->counter, 1));
+    TRY(dalloc(e, &e->offs, W));
+    TRY(dalloc(e, &e->weight, W));
+    TRY(dalloc(e, &e->tstats, 4));
+    long long init[4] = {0, 0, 1LL << 40, 0};
+    CUDA_TRY(cudaMemcpy(e->tstats, init, sizeof(init), cudaMemcpyHostToDevice));
+    TRY(dalloc(e, &e->acc, 8));
+    TRY(dalloc(e, &e->eloc, W));
+    TRY(dalloc(e, &e->den, W));
+    TRY(dalloc(e, &e->parts, (size_t)3 * W));
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->own, cudaStreamNonBlocking));
+    e->stream = e->own;
+    return AFQMC_OK;
+}
+
+void set_blocks(afqmc_engine *e)
+{
+    Blocks &b = e->bl;
+    if (e->kind == KIND_CP) {
+        b.nblk = 1; b.Ns[0] = e->ncol; b.Ns[1] = 0;
+        b.sOff[0] = 0; b.tOff[0] = 0; b.sOff[1] = 0; b.tOff[1] = 0;
+        b.sStride = (long long)e->ncol * e->ncol;
+        b.tStride = (long long)e->ncol * e->n;
+    } else {
+        b.nblk = e->ndn > 0 ? 2 : 1;
+        b.Ns[0] = e->nup; b.Ns[1] = e->ndn;
+        b.sOff[0] = 0; b.sOff[1] = (long long)e->nup * e->nup;
+        b.tOff[0] = 0; b.tOff[1] = (long long)e->nup * e->n;
+        b.sStride = (long long)e->nup * e->nup + (long long)e->ndn * e->ndn;
+        b.tStride = (long long)(e->nup + e->ndn) * e->n;
+    }
+}
+
+// ---------------------------------------------------------------- pieces
+// S_b = phiT_b^H phi (SDSDOperation.cpp:154-164, gmm 'C')
+int overlap_gemm(afqmc_engine *e, const zd *wf, const int *mask)
+{
+    for (int b = 0; b < e->bl.nblk; ++b) {
+        int Ns = e->bl.Ns[b];
+        if (Ns == 0) continue;
+        ZGemmArgs g;
+        g.m = Ns; g.n = Ns; g.k = e->n;
+        g.opA = OP_C; g.opB = OP_N;
+        g.A = e->phiT[b]; g.lda = e->n; g.strideA = 0;
+        g.B = wf; g.ldb = e->n; g.strideB = e->wsize;
+        g.C = e->S + e->bl.sOff[b]; g.ldc = Ns; g.strideC = e->bl.sStride;
+        g.batch = e->W; g.mask = mask;
+        TRY(gemm(g, e->stream));
+    }
+    return AFQMC_OK;
+}
+
+// thetaT_b = (S_b^{-1})^T phi_b^T  (zgetrs 'T', SDSDOperation.cpp:166-173)
+int theta_gemm(afqmc_engine *e, const zd *wf, const int *mask)
+{
+    for (int b = 0; b < e->bl.nblk; ++b) {
+        int Ns = e->bl.Ns[b];
+        if (Ns == 0) continue;
+        ZGemmArgs g;
+        g.m = Ns; g.n = e->n; g.k = Ns;
+        g.opA = OP_T; g.opB = OP_T;
+        g.A = e->Sinv + e->bl.sOff[b]; g.lda = Ns; g.strideA = e->bl.sStride;
+        g.B = wf; g.ldb = e->n; g.strideB = e->wsize;
+        g.C = e->thetaT + e->bl.tOff[b]; g.ldc = Ns; g.strideC = e->bl.tStride;
+        g.batch = e->W; g.mask = mask;
+        TRY(gemm(g, e->stream));
+    }
+    return AFQMC_OK;
+}
+
+// phaseless xbar = A^T thetaT for every walker (calculateCholeskyBg, :237-256)
+int xbar_gemm(afqmc_engine *e)
+{
+    ZGemmArgs g;
+    g.m = e->G; g.n = e->W; g.k = (int)e->Ktot;
+    g.opA = OP_T; g.opB = OP_N;
+    g.A = e->Aall; g.lda = e->Ktot;
+    g.B = e->thetaT; g.ldb = e->bl.tStride;
+    g.C = e->xbar; g.ldc = e->G;
+    g.batch = 1;
+    return gemm(g, e->stream);
+}
+
+// dst = exp(M) src via the dynamicOrder Taylor series
+// (LogHop2isSD2isOperation::applyToRight, logHop2isSD2isOperation.cpp:38-45,159-195).
+// Mstride = 0 for a shared matrix (one-body LogHop2is), n*n per walker otherwise.
+int taylor_apply(afqmc_engine *e, const zd *M, long long Mstride, const zd *src, zd *dst,
+                 const int *mask, bool stats)
+{
+    const int W = e->W;
+    launch_copy_masked(W, e->wsize, src, dst, mask, e->stream);
+    CUDA_TRY(cudaMemsetAsync(e->done, 0, sizeof(int) * W, e->stream));
+    const zd *old = src;
+    for (int k = 1; k <= TAYLOR_KMAX; ++k) {
+        zd *nw = e->term[(k - 1) & 1];
+        ZGemmArgs g;
+        g.m = e->n; g.n = e->ncol; g.k = e->n;
+        g.A = M; g.lda = e->n; g.strideA = Mstride;
+        g.B = old; g.ldb = e->n; g.strideB = e->wsize;
+        g.C = nw; g.ldc = e->n; g.strideC = e->wsize;
+        g.alpha = make_double2(1.0 / k, 0.0);
+        g.batch = W; g.mask = mask; g.skip = e->done;
+        TRY(gemm(g, e->stream));
+        launch_taylor_accum(W, e->wsize, nw, dst, mask, e->done, e->order, k, TAYLOR_BASE + 1,
+                            TAYLOR_ACC, k == TAYLOR_KMAX ? 1 : 0, e->status, e->stream);
+        old = nw;
+    }
+    if (stats) launch_taylor_stats(W, mask, e->order, e->tstats, e->stream);
+    return check_launch();
+}
+
+// one-body operator `which` applied to src -> dst for masked walkers
+int one_body(afqmc_engine *e, int which, const zd *src, zd *dst, const int *mask)
+{
+    if (e->useLog && e->kind == KIND_PL) {
+        const zd *Mx = which == 0 ? e->logK : e->expK[which];
+        return taylor_apply(e, Mx, 0, src, dst, mask, false);
+    }
+    ZGemmArgs g;
+    g.m = e->n; g.n = e->ncol; g.k = e->n;
+    g.A = e->expK[which]; g.lda = e->n; g.strideA = 0;
+    g.B = src; g.ldb = e->n; g.strideB = e->wsize;
+    g.C = dst; g.ldc = e->n; g.strideC = e->wsize;
+    g.batch = e->W; g.mask = mask;
+    return gemm(g, e->stream);
+}
+
+zd one_body_logw(afqmc_engine *e, int which)
+{
+    if (e->useLog && e->kind == KIND_PL && which == 0) return e->logKLogw;
+    return e->expLogw[which];
+}
+
+// --------------------------------------------------- projectExpMinusDtKExpMinusDtV
+int project_dtk_dtv(afqmc_engine *e)
+{
+    const int W = e->W;
+    cudaStream_t s = e->stream;
+    if (e->precision == AFQMC_MIXED) return mixed_project_dtk_dtv(e);
+    const bool needTheta = (e->forceType == AFQMC_DYNAMIC_FORCE);
+    // overlap, log-determinant, first cos projection
+    { PHASE(AFQMC_PH_OVERLAP); TRY(overlap_gemm(e, e->wf, e->alive)); }
+    {
+        PHASE(AFQMC_PH_LU);
+        launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, make_double2(0, 0),
+                                 e->logwT, e->logov, e->alive, e->surv, e->logw, nullptr, e->status,
+                                 LU_PROJECT, needTheta, s);
+        TRY(check_launch());
+    }
+    if (needTheta) { PHASE(AFQMC_PH_THETA); TRY(theta_gemm(e, e->wf, e->surv)); }
+    zd hop = one_body_logw(e, 0);
+    if (e->kind == KIND_CP) {
+        if (needTheta) {
+            PHASE(AFQMC_PH_FORCE);
+            launch_cp_force(W, e->hd, e->thetaT, e->bl.tStride, e->surv, e->forceCP, s);
+        }
+        {
+            PHASE(AFQMC_PH_SAMPLE);
+            launch_rng_scan(W, e->surv, e->L, e->counter, e->offs, s);
+            launch_cp_sample_apply(W, e->hd, e->forceCP, e->surv, e->offs, e->seed, e->wf, e->wfTmp,
+                                   e->logw, e->dt * e->ET, hop, nullptr, s);
+            TRY(check_launch());
+        }
+        { PHASE(AFQMC_PH_ONEBODY); TRY(one_body(e, 0, e->wfTmp, e->wf, e->surv)); }
+    } else {
+        if (needTheta) { PHASE(AFQMC_PH_FORCE); TRY(xbar_gemm(e)); }
+        {
+            PHASE(AFQMC_PH_SAMPLE);
+            launch_rng_scan(W, e->surv, 2 * e->G, e->counter, e->offs, s);
+            launch_pl_sample(W, e->cdv, e->xbar, e->surv, e->surv, e->alive, e->offs, e->seed,
+                             e->aux, e->forcePL, e->logw, e->dt * e->ET, hop, s);
+            TRY(check_launch());
+        }
+        {
+            // M = sqrt(-dt) sum_g aux_g L_g  (choleskyReal.cpp:160-169), all walkers in one GEMM
+            PHASE(AFQMC_PH_MBUILD);
+            ZGemmArgs g;
+            g.m = e->n * e->n; g.n = W; g.k = e->G;
+            g.a_real = 1;
+            g.A = e->chol; g.lda = (long long)e->n * e->n;
+            g.B = e->aux; g.ldb = e->G;
+            g.C = e->M; g.ldc = (long long)e->n * e->n;
+            g.alpha = make_double2(0.0, e->cdv.sqrtDt);
+            TRY(gemm(g, s));
+        }
+        {
+            PHASE(AFQMC_PH_TAYLOR);
+            TRY(taylor_apply(e, e->M, (long long)e->n * e->n, e->wf, e->wfTmp, e->surv, true));
+        }
+        { PHASE(AFQMC_PH_ONEBODY); TRY(one_body(e, 0, e->wfTmp, e->wf, e->surv)); }
+    }
+    return check_launch();
+}
+
+int modify_gm(afqmc_engine *e)
+{
+    PHASE(AFQMC_PH_STABILIZE);
+    if (e->precision == AFQMC_MIXED) return mixed_modify_gm(e);
+    launch_mgs(e->W, e->n, e->ncol, e->nup, e->ndn, e->kind == KIND_PL ? 1 : 0, e->wf, e->logw,
+               e->alive, e->status, e->stream);
+    return check_launch();
+}
+
+int pop_control(afqmc_engine *e)
+{
+    PHASE(AFQMC_PH_POPCONTROL);
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    TRY(overlap_gemm(e, e->wf, e->alive));
+    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
+                             e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
+                             LU_POPWEIGHT, false, e->stream);
+    launch_pop_comb(e->W, e->weight, nullptr, e->seed, e->counter, e->number, e->table,
+                    e->status + e->W, e->stream);
+    launch_pop_gather(e->W, e->wsize, e->table, e->wf, e->logw, e->stream);
+    TRY(check_launch());
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
+    return AFQMC_OK;
+}
+
+int project_one_step(afqmc_engine *e)
+{
+    TRY(project_dtk_dtv(e));
+    e->mgsIndex++;
+    if (e->mgsIndex == e->mgsStep) { TRY(modify_gm(e)); e->mgsIndex = 0; }
+    e->popIndex++;
+    if (e->popIndex == e->popStep) { TRY(pop_control(e)); e->popIndex = 0; }
+    return AFQMC_OK;
+}
+
+int add_mixed_measurement(afqmc_engine *e)
+{
+    if (e->precision == AFQMC_MIXED) return mixed_add_measurement(e);
+    const int W = e->W;
+    cudaStream_t s = e->stream;
+    {
+        PHASE(AFQMC_PH_MEASURE);
+        TRY(one_body(e, 1, e->wf, e->wfTmp, e->alive));
+        TRY(overlap_gemm(e, e->wfTmp, e->alive));
+        launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, one_body_logw(e, 1),
+                                 e->logwT, e->logov, e->alive, nullptr, nullptr, nullptr,
+                                 e->status, LU_PLAIN, true, s);
+        TRY(check_launch());
+        TRY(theta_gemm(e, e->wfTmp, e->alive));
+    }
+    if (e->kind == KIND_CP) {
+        PHASE(AFQMC_PH_MEASURE);
+        launch_cp_energy(W, e->hd, e->wfDaggerK, e->thetaT, e->bl.tStride, e->U, e->mu, e->hx,
+                         e->hy, e->hz, e->alive, e->logov, e->eloc, e->den, e->parts, s);
+        launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 3, e->acc, 0, nullptr,
+                              nullptr, nullptr, nullptr, s);
+    } else {
+        { PHASE(AFQMC_PH_MEASURE); TRY(xbar_gemm(e)); }
+        {
+            PHASE(AFQMC_PH_EXCHANGE);
+            if (launch_pl_exchange(W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex, s))
+                return fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
+        }
+        {
+            PHASE(AFQMC_PH_MEASURE);
+            launch_pl_energy(W, e->G, e->Ktot, e->wfDaggerT, e->thetaT, e->xbar, e->ex, e->alive,
+                             e->logov, e->eloc, e->den, e->parts, s);
+            launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 1, e->acc, e->G, e->xbar,
+                                  e->ex, e->bgNum, e->exNum, s);
+        }
+    }
+    return check_launch();
+}
+
+int create_common_checks(int W, int precision)
+{
+    if (W <= 0) return fail(AFQMC_ERR_ARG, "walker count must be positive");
+    if (precision != AFQMC_FP64 && precision != AFQMC_MIXED) return fail(AFQMC_ERR_ARG, "unknown precision");
+    int dev = 0;
+    cudaError_t r = cudaGetDevice(&dev);
+    if (r != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(r));
+    return AFQMC_OK;
+}
+
+void free_engine(afqmc_engine *e)
+{
+    if (!e) return;
+    if (e->mx) mixed_destroy(e);
+    prof_resolve(e);
+    for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
+    for (void *p : e->allocs) cudaFree(p);
+    if (e->own) cudaStreamDestroy(e->own);
+    delete e;
+}
+
+}  // namespace
+
+// =========================================================== C ABI
+extern "C" {
+
+const char *afqmc_last_error(void) { return g_err.c_str(); }
+const char *afqmc_version(void) { return "afqmclab_b200 0.1 (sm_100a)"; }
+
+int afqmc_cp_create(int L, int N, int W, int decomp, int force_type, double dt, double ET,
+                    double force_cap, int mgs_step, int pop_control_step, int precision,
+                    const double *K, const double *expMinusDtK, const double *expHalfDtK,
+                    const double *expMinusHalfDtK, const double *U, const double *mu,
+                    const double *hx, const double *hy, const double *hz,
+                    const double *const_force, const double *phiT, double logwT_re,
+                    double logwT_im, unsigned long long seed, afqmc_engine **out)
+{
+    if (!out) return fail(AFQMC_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    TRY(create_common_checks(W, precision));
+    if (L <= 0 || N <= 0 || N > 2 * L) return fail(AFQMC_ERR_ARG, "need 0 < N <= 2L");
+    if (decomp < 0 || decomp > 3) return fail(AFQMC_ERR_ARG, "unknown decomposition");
+    if (!K || !expMinusDtK || !expHalfDtK || !U || !mu || !hx || !hy || !hz || !phiT)
+        return fail(AFQMC_ERR_ARG, "missing model array");
+    if (mgs_step <= 0 || pop_control_step <= 0) return fail(AFQMC_ERR_ARG, "cadence must be positive");
+    afqmc_engine *e = new afqmc_engine();
+    e->kind = KIND_CP; e->L = L; e->n = 2 * L; e->ncol = N; e->nup = N; e->ndn = 0; e->W = W;
+    e->precision = precision; e->decomp = decomp; e->forceType = force_type;
+    e->dt = dt; e->ET = ET; e->forceCap = force_cap; e->mgsStep = mgs_step; e->popStep = pop_control_step;
+    e->seed = seed; e->logwT = make_double2(logwT_re, logwT_im);
+    set_blocks(e);
+    int r = alloc_population(e);
+    const int n = e->n;
+#define CK(x) do { r = (x); if (r != AFQMC_OK) { free_engine(e); return r; } } while (0)
+    CK(r);
+    CK(dupload(e, &e->phiT[0], phiT, (size_t)n * N));
+    CK(dupload(e, &e->expK[0], expMinusDtK, (size_t)n * n));
+    CK(dupload(e, &e->expK[1], expHalfDtK, (size_t)n * n));
+    CK(dupload(e, &e->expK[2], expMinusHalfDtK ? expMinusHalfDtK : expHalfDtK, (size_t)n * n));
+    CK(dupload(e, &e->U, U, L)); CK(dupload(e, &e->mu, mu, L)); CK(dupload(e, &e->hx, hx, L));
+    CK(dupload(e, &e->hy, hy, L)); CK(dupload(e, &e->hz, hz, L));
+    // NiupNidn constants (NiupNidn.cpp:12-26, setGamma :223-250, setConstDiag :252-270)
+    std::vector<zd> gam(L), c00(L), c01(L), c10(L), c11(L);
+    double usum = 0;
+    for (int i = 0; i < L; ++i) usum += U[i];
+    for (int i = 0; i < L; ++i) {
+        double dtU = dt * U[i];
+        cd g;
+        if (decomp == AFQMC_DENSITY_CHARGE) g = solve_cosh_eq_exp(-dtU * 0.5);
+        else if (decomp == AFQMC_HOP_SPIN) g = solve_cos_eq_exp(dtU * 0.5);
+        else g = solve_cosh_eq_exp(dtU * 0.5);
+        double a = -dt * (U[i] * 0.5 - mu[i] + hz[i] * 0.5);
+        double b = -dt * (U[i] * 0.5 - mu[i] - hz[i] * 0.5);
+        cd c = -dt * 0.5 * cd(hx[i], hy[i]);
+        exp2by2(a, b, c);
+        gam[i] = tozd(g); c00[i] = make_double2(a, 0); c01[i] = tozd(std::conj(c));
+        c10[i] = tozd(c); c11[i] = make_double2(b, 0);
+    }
+    CK(dupload(e, &e->gamma, gam.data(), L));
+    CK(dupload(e, &e->cdiag[0], c00.data(), L)); CK(dupload(e, &e->cdiag[1], c01.data(), L));
+    CK(dupload(e, &e->cdiag[2], c10.data(), L)); CK(dupload(e, &e->cdiag[3], c11.data(), L));
+    if (const_force) CK(dupload(e, &e->constForceCP, const_force, L));
+    CK(dalloc(e, &e->forceCP, (size_t)W * L));
+    e->hd.L = L; e->hd.N = N; e->hd.n = n; e->hd.decomp = decomp;
+    e->hd.gamma = e->gamma; e->hd.cd00 = e->cdiag[0]; e->hd.cd01 = e->cdiag[1];
+    e->hd.cd10 = e->cdiag[2]; e->hd.cd11 = e->cdiag[3];
+    e->hd.dtUSum = dt * usum; e->hd.forceCap = force_cap;
+    e->hd.constForce = (force_type == AFQMC_CONST_FORCE)
+                           ? (e->constForceCP ? e->constForceCP : nullptr) : nullptr;
+    if (force_type == AFQMC_CONST_FORCE && !e->constForceCP) {
+        CK(dalloc(e, &e->constForceCP, L));
+        e->hd.constForce = e->constForceCP;
+    }
+    e->hd.phiT = e->phiT[0];
+    // wfDaggerK = phiT^H K (HubbardSOCMeasureFixedSDSD::initWfDaggerK, :160-167)
+    zd *Kd = nullptr;
+    CK(dupload(e, &Kd, K, (size_t)n * n));
+    CK(dalloc(e, &e->wfDaggerK, (size_t)N * n));
+    {
+        ZGemmArgs g;
+        g.m = N; g.n = n; g.k = n; g.opA = OP_C;
+        g.A = e->phiT[0]; g.lda = n; g.B = Kd; g.ldb = n; g.C = e->wfDaggerK; g.ldc = N;
+        CK(gemm(g, e->stream));
+    }
+    if (precision == AFQMC_MIXED) CK(mixed_create(e));
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) { free_engine(e); return fail(AFQMC_ERR_CUDA, cudaGetErrorString(ce)); }
+#undef CK
+    *out = e;
+    return AFQMC_OK;
+}
+
+int afqmc_pl_create(int n, int Nup, int Ndn, int G, int W, int force_type, double dt, double ET,
+                    double force_cap, int mgs_step, int pop_control_step, int precision,
+                    const double *chol, const double *bg, const double *t,
+                    const double *expMinusDtK, double logwExpMinusDtK, const double *expHalfDtK,
+                    double logwExpHalfDtK, const double *expMinusHalfDtK,
+                    double logwExpMinusHalfDtK, const double *logExpMinusDtK,
+                    double logwLogExpMinusDtK, const double *const_force, const double *phiTUp,
+                    const double *phiTDn, double logwT_re, double logwT_im,
+                    unsigned long long seed, afqmc_engine **out)
+{
+    if (!out) return fail(AFQMC_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    TRY(create_common_checks(W, precision));
+    if (n <= 0 || Nup <= 0 || Ndn < 0 || Nup > n || Ndn > n || G <= 0)
+        return fail(AFQMC_ERR_ARG, "bad sizes");
+    if (!chol || !bg || !t || !phiTUp || (Ndn > 0 && !phiTDn) || !expHalfDtK)
+        return fail(AFQMC_ERR_ARG, "missing model array");
+    if (!expMinusDtK && !logExpMinusDtK) return fail(AFQMC_ERR_ARG, "need expMinusDtK or logExpMinusDtK");
+    if (mgs_step <= 0 || pop_control_step <= 0) return fail(AFQMC_ERR_ARG, "cadence must be positive");
+    afqmc_engine *e = new afqmc_engine();
+    e->kind = KIND_PL; e->n = n; e->nup = Nup; e->ndn = Ndn; e->ncol = std::max(Nup, Ndn);
+    e->G = G; e->W = W; e->precision = precision; e->forceType = force_type;
+    e->dt = dt; e->ET = ET; e->forceCap = force_cap; e->mgsStep = mgs_step; e->popStep = pop_control_step;
+    e->seed = seed; e->logwT = make_double2(logwT_re, logwT_im);
+    set_blocks(e);
+    int r = alloc_population(e);
+#define CK(x) do { r = (x); if (r != AFQMC_OK) { free_engine(e); return r; } } while (0)
+    CK(r);
+    const size_t n2 = (size_t)n * n;
+    CK(dupload(e, &e->phiT[0], phiTUp, (size_t)n * Nup));
+    if (Ndn > 0) CK(dupload(e, &e->phiT[1], phiTDn, (size_t)n * Ndn));
+    e->useLog = (expMinusDtK == nullptr);
+    if (!e->useLog) CK(dupload(e, &e->expK[0], expMinusDtK, n2));
+    else CK(dupload(e, &e->logK, logExpMinusDtK, n2));
+    CK(dupload(e, &e->expK[1], expHalfDtK, n2));
+    CK(dupload(e, &e->expK[2], expMinusHalfDtK ? expMinusHalfDtK : expHalfDtK, n2));
+    e->expLogw[0] = make_double2(logwExpMinusDtK, 0);
+    e->expLogw[1] = make_double2(logwExpHalfDtK, 0);
+    e->expLogw[2] = make_double2(logwExpMinusHalfDtK, 0);
+    e->logKLogw = make_double2(logwLogExpMinusDtK, 0);
+    CK(dupload(e, &e->chol, chol, n2 * G));
+    CK(dupload(e, &e->bg, bg, G));
+    if (const_force) CK(dupload(e, &e->constForcePL, const_force, G));
+    else if (force_type == AFQMC_CONST_FORCE) CK(dalloc(e, &e->constForcePL, G));
+    e->Ktot = (long long)(Nup + Ndn) * n;
+    CK(dalloc(e, &e->Aall, (size_t)e->Ktot * G));
+    CK(dalloc(e, &e->wfDaggerT, (size_t)e->Ktot));
+    double *td = nullptr;
+    CK(dupload(e, &td, t, n2));
+    // A_g,sigma = phiT_sigma^H L_g (initWfDaggerCholeskyVecs, :165-186) and
+    // wfDaggerT = phiT_sigma^H t (initWfDaggerT, :148-163), stacked up/down
+    for (int b = 0; b < e->bl.nblk; ++b) {
+        int Ns = e->bl.Ns[b];
+        ZGemmArgs g;
+        g.m = Ns; g.n = n; g.k = n; g.opA = OP_C; g.b_real = 1;
+        g.A = e->phiT[b]; g.lda = n; g.strideA = 0;
+        g.B = e->chol; g.ldb = n; g.strideB = (long long)n2;
+        g.C = e->Aall + e->bl.tOff[b]; g.ldc = Ns; g.strideC = e->Ktot;
+        g.batch = G;
+        CK(gemm(g, e->stream));
+        ZGemmArgs h = g;
+        h.B = td; h.strideB = 0; h.C = e->wfDaggerT + e->bl.tOff[b]; h.strideC = 0; h.batch = 1;
+        CK(gemm(h, e->stream));
+    }
+    CK(dalloc(e, &e->xbar, (size_t)G * W));
+    CK(dalloc(e, &e->forcePL, (size_t)G * W));
+    CK(dalloc(e, &e->aux, (size_t)G * W));
+    CK(dalloc(e, &e->ex, (size_t)G * W));
+    CK(dalloc(e, &e->bgNum, G));
+    CK(dalloc(e, &e->exNum, G));
+    if (precision == AFQMC_FP64) CK(dalloc(e, &e->M, n2 * W));
+    e->cdv.n = n; e->cdv.G = G; e->cdv.bg = e->bg; e->cdv.forceCap = force_cap;
+    e->cdv.sqrtDt = std::sqrt(dt);
+    e->cdv.constForce = (force_type == AFQMC_CONST_FORCE) ? e->constForcePL : nullptr;
+    if (precision == AFQMC_MIXED) CK(mixed_create(e));
+    cudaError_t ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) { free_engine(e); return fail(AFQMC_ERR_CUDA, cudaGetErrorString(ce)); }
+#undef CK
+    *out = e;
+    return AFQMC_OK;
+}
+
+int afqmc_destroy(afqmc_engine *e)
+{
+    if (!e) return AFQMC_OK;
+    cudaStreamSynchronize(e->stream);
+    free_engine(e);
+    return AFQMC_OK;
+}
+
+int afqmc_set_stream(afqmc_engine *e, void *cuda_stream)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    e->stream = cuda_stream ? (cudaStream_t)cuda_stream : e->own;
+    return AFQMC_OK;
+}
+
+int afqmc_synchronize(afqmc_engine *e)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_set_walkers(afqmc_engine *e, const double *wf, const double *logw, const int *alive)
+{
+    if (!e || !wf || !logw || !alive) return fail(AFQMC_ERR_ARG, "null argument");
+    CUDA_TRY(cudaMemcpyAsync(e->wf, wf, sizeof(zd) * e->wsize * e->W, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->logw, logw, sizeof(zd) * e->W, cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->alive, alive, sizeof(int) * e->W, cudaMemcpyHostToDevice, e->stream));
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_get_walkers(afqmc_engine *e, double *wf, double *logw, int *alive)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    if (wf) CUDA_TRY(cudaMemcpyAsync(wf, e->wf, sizeof(zd) * e->wsize * e->W, cudaMemcpyDeviceToHost, e->stream));
+    if (logw) CUDA_TRY(cudaMemcpyAsync(logw, e->logw, sizeof(zd) * e->W, cudaMemcpyDeviceToHost, e->stream));
+    if (alive) CUDA_TRY(cudaMemcpyAsync(alive, e->alive, sizeof(int) * e->W, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_set_rng(afqmc_engine *e, unsigned long long seed, unsigned long long counter)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    e->seed = seed;
+    CUDA_TRY(cudaMemcpyAsync(e->counter, &counter, sizeof(counter), cudaMemcpyHostToDevice, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_get_rng(afqmc_engine *e, unsigned long long *seed, unsigned long long *counter)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    if (seed) *seed = e->seed;
+    if (counter) {
+        CUDA_TRY(cudaMemcpyAsync(counter, e->counter, sizeof(*counter), cudaMemcpyDeviceToHost, e->stream));
+        CUDA_TRY(cudaStreamSynchronize(e->stream));
+    }
+    return AFQMC_OK;
+}
+
+int afqmc_set_ET(afqmc_engine *e, double ET)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    e->ET = ET;
+    return AFQMC_OK;
+}
+
+int afqmc_set_cadence(afqmc_engine *e, int mgs_index, int pop_control_index)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    e->mgsIndex = mgs_index;
+    e->popIndex = pop_control_index;
+    return AFQMC_OK;
+}
+
+int afqmc_project_one_step(afqmc_engine *e, int nsteps)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    for (int i = 0; i < nsteps; ++i) TRY(project_one_step(e));
+    return AFQMC_OK;
+}
+
+int afqmc_project_half(afqmc_engine *e, int which)
+{
+    if (!e || (which != -1 && which != 1)) return fail(AFQMC_ERR_ARG, "which must be -1 or +1");
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    int idx = which < 0 ? 2 : 1;
+    TRY(one_body(e, idx, e->wf, e->wfTmp, e->alive));
+    launch_copy_masked(e->W, e->wsize, e->wfTmp, e->wf, e->alive, e->stream);
+    TRY(check_launch());
+    // walkerNew.logw = oneBody.logw + walker.logw for alive walkers
+    std::vector<zd> lw(e->W);
+    std::vector<int> al(e->W);
+    CUDA_TRY(cudaMemcpyAsync(lw.data(), e->logw, sizeof(zd) * e->W, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(al.data(), e->alive, sizeof(int) * e->W, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    zd add = one_body_logw(e, idx);
+    for (int w = 0; w < e->W; ++w)
+        if (al[w]) lw[w] = zadd(add, lw[w]);
+    CUDA_TRY(cudaMemcpyAsync(e->logw, lw.data(), sizeof(zd) * e->W, cudaMemcpyHostToDevice, e->stream));
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_modify_gm(afqmc_engine *e)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    return modify_gm(e);
+}
+
+int afqmc_pop_control(afqmc_engine *e, int *table_out, double *weight_out)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    TRY(pop_control(e));
+    if (table_out) CUDA_TRY(cudaMemcpyAsync(table_out, e->table, sizeof(int) * e->W, cudaMemcpyDeviceToHost, e->stream));
+    if (weight_out) CUDA_TRY(cudaMemcpyAsync(weight_out, e->weight, sizeof(double) * e->W, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_reset_measurement(afqmc_engine *e)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    CUDA_TRY(cudaMemsetAsync(e->acc, 0, sizeof(zd) * 8, e->stream));
+    if (e->bgNum) CUDA_TRY(cudaMemsetAsync(e->bgNum, 0, sizeof(zd) * e->G, e->stream));
+    if (e->exNum) CUDA_TRY(cudaMemsetAsync(e->exNum, 0, sizeof(zd) * e->G, e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_add_mixed_measurement(afqmc_engine *e)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    return add_mixed_measurement(e);
+}
+
+int afqmc_get_measurement(afqmc_engine *e, double *out)
+{
+    if (!e || !out) return fail(AFQMC_ERR_ARG, "null argument");
+    zd a[8];
+    CUDA_TRY(cudaMemcpyAsync(a, e->acc, sizeof(a), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (int i = 0; i < 5; ++i) { out[2 * i] = a[i].x; out[2 * i + 1] = a[i].y; }
+    if (e->kind == KIND_PL) { out[6] = out[7] = out[8] = out[9] = 0.0; }
+    return AFQMC_OK;
+}
+
+int afqmc_get_cholesky_nums(afqmc_engine *e, double *bgNum, double *exNum)
+{
+    if (!e || e->kind != KIND_PL) return fail(AFQMC_ERR_ARG, "phaseless engine required");
+    if (bgNum) CUDA_TRY(cudaMemcpyAsync(bgNum, e->bgNum, sizeof(zd) * e->G, cudaMemcpyDeviceToHost, e->stream));
+    if (exNum) CUDA_TRY(cudaMemcpyAsync(exNum, e->exNum, sizeof(zd) * e->G, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_pl_update_background(afqmc_engine *e, const double *bg, const double *expMinusDtK,
+                               double logwExpMinusDtK, const double *expHalfDtK,
+                               double logwExpHalfDtK, const double *expMinusHalfDtK,
+                               double logwExpMinusHalfDtK)
+{
+    if (!e || e->kind != KIND_PL || !bg) return fail(AFQMC_ERR_ARG, "phaseless engine and bg required");
+    const size_t n2 = (size_t)e->n * e->n;
+    CUDA_TRY(cudaMemcpyAsync(e->bg, bg, sizeof(double) * e->G, cudaMemcpyHostToDevice, e->stream));
+    if (expMinusDtK) {
+        if (!e->expK[0]) TRY(dalloc(e, &e->expK[0], n2));
+        CUDA_TRY(cudaMemcpyAsync(e->expK[0], expMinusDtK, sizeof(zd) * n2, cudaMemcpyHostToDevice, e->stream));
+        e->expLogw[0] = make_double2(logwExpMinusDtK, 0);
+        e->useLog = false;
+    }
+    if (expHalfDtK) {
+        CUDA_TRY(cudaMemcpyAsync(e->expK[1], expHalfDtK, sizeof(zd) * n2, cudaMemcpyHostToDevice, e->stream));
+        e->expLogw[1] = make_double2(logwExpHalfDtK, 0);
+    }
+    if (expMinusHalfDtK) {
+        CUDA_TRY(cudaMemcpyAsync(e->expK[2], expMinusHalfDtK, sizeof(zd) * n2, cudaMemcpyHostToDevice, e->stream));
+        e->expLogw[2] = make_double2(logwExpMinusHalfDtK, 0);
+    }
+    if (e->precision == AFQMC_MIXED) TRY(mixed_update_operators(e));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_log_overlaps(afqmc_engine *e, double *out)
+{
+    if (!e || !out) return fail(AFQMC_ERR_ARG, "null argument");
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    TRY(overlap_gemm(e, e->wf, nullptr));
+    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, nullptr, e->logw, make_double2(0, 0),
+                             e->logwT, e->logov, nullptr, nullptr, nullptr, nullptr, nullptr,
+                             LU_PLAIN, false, e->stream);
+    TRY(check_launch());
+    CUDA_TRY(cudaMemcpyAsync(out, e->logov, sizeof(zd) * e->W, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_green_matrix(afqmc_engine *e, int walker, int spin, double *out)
+{
+    if (!e || !out || walker < 0 || walker >= e->W) return fail(AFQMC_ERR_ARG, "bad argument");
+    if (spin < 0 || spin >= e->bl.nblk) return fail(AFQMC_ERR_ARG, "bad spin");
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    TRY(overlap_gemm(e, e->wf, nullptr));
+    launch_lu_logdet_inverse(e->W, e->bl, e->S, e->Sinv, nullptr, e->logw, make_double2(0, 0),
+                             e->logwT, e->logov, nullptr, nullptr, nullptr, nullptr, nullptr,
+                             LU_PLAIN, true, e->stream);
+    TRY(check_launch());
+    TRY(theta_gemm(e, e->wf, nullptr));
+    // G^T = thetaT^T phiT^H, i.e. G = conj(phiT) thetaT transposed back on the host
+    const int n = e->n, Ns = e->bl.Ns[spin];
+    std::vector<zd> h((size_t)n * n);
+    zd *scratch = nullptr;
+    TRY(dalloc(e, &scratch, (size_t)n * n));
+    ZGemmArgs g;
+    g.m = n; g.n = n; g.k = Ns; g.opA = OP_T; g.opB = OP_C;
+    g.A = e->thetaT + (size_t)walker * e->bl.tStride + e->bl.tOff[spin]; g.lda = Ns;
+    g.B = e->phiT[spin]; g.ldb = n;
+    g.C = scratch; g.ldc = n;
+    TRY(gemm(g, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(h.data(), scratch, sizeof(zd) * n * n, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    cudaFree(scratch);
+    e->allocs.pop_back();
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            zd v = h[j + (size_t)n * i];
+            out[2 * (i + (size_t)n * j)] = v.x;
+            out[2 * (i + (size_t)n * j) + 1] = v.y;
+        }
+    return AFQMC_OK;
+}
+
+int afqmc_taylor_stats(afqmc_engine *e, long long *calls, long long *total, int *min_order,
+                       int *max_order)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    long long s[4];
+    CUDA_TRY(cudaMemcpyAsync(s, e->tstats, sizeof(s), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    if (calls) *calls = s[0];
+    if (total) *total = s[1];
+    if (min_order) *min_order = (int)std::min<long long>(s[2], 1 << 30);
+    if (max_order) *max_order = (int)s[3];
+    return AFQMC_OK;
+}
+
+int afqmc_status(afqmc_engine *e, int *status_or)
+{
+    if (!e || !status_or) return fail(AFQMC_ERR_ARG, "null argument");
+    std::vector<int> st(e->W + 1);
+    CUDA_TRY(cudaMemcpyAsync(st.data(), e->status, sizeof(int) * (e->W + 1), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    int o = 0;
+    for (int v : st) o |= v;
+    if (e->mx) o |= mixed_status(e);
+    *status_or = o;
+    return AFQMC_OK;
+}
+
+long long afqmc_launch_count(void) { return g_launch_count.load(); }
+
+int afqmc_profile_enable(afqmc_engine *e, int on)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    prof_resolve(e);
+    e->prof = on != 0;
+    for (int i = 0; i < AFQMC_NPHASES; ++i) { e->profMs[i] = 0.0; e->profCount[i] = 0; }
+    return AFQMC_OK;
+}
+
+int afqmc_profile_get(afqmc_engine *e, double *ms, long long *counts)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    prof_resolve(e);
+    for (int i = 0; i < AFQMC_NPHASES; ++i) {
+        if (ms) ms[i] = e->profMs[i];
+        if (counts) counts[i] = e->profCount[i];
+    }
+    return AFQMC_OK;
+}
+
+int afqmc_pop_configuration_dev(int W, const double *weights, const double *uniforms, int *table,
+                                void *stream)
+{
+    if (W <= 0 || !weights || !uniforms || !table) return fail(AFQMC_ERR_ARG, "bad argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    int *number = nullptr;
+    CUDA_TRY(cudaMallocAsync(&number, sizeof(int) * W, s));
+    launch_pop_comb(W, weights, uniforms, 0, nullptr, number, table, nullptr, s);
+    int r = check_launch();
+    CUDA_TRY(cudaFreeAsync(number, s));
+    return r;
+}
+
+}  // extern "C"

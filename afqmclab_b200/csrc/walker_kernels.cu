@@ -1,0 +1,974 @@
+// AFQMC walker-step kernels other than the GEMMs (plain FP64 form).
+// Each kernel cites the reference function it replaces.
+#include "walker_kernels.cuh"
+
+#include <atomic>
+
+std::atomic<long long> g_launch_count{0};
+
+#include <stdio.h>
+
+namespace {
+
+constexpr int LU_SMEM_MAX_NS = 64;
+
+// ---------------------------------------------------------------------------
+// LU with partial pivoting + log-determinant (+ inverse) of every overlap
+// block of a walker; one CTA per walker.
+// Replaces SDSDOperation::calculateLUOverlap/returnLogOverlap
+// (SDSDOperation.cpp:65-72,154-164), SD2sSD2isOperation (:84-94,187-198),
+// LUconstruct_cpu (tensor_2d_bl_cpu.cpp:145-167, zgetrf) and
+// logDeterminant (tensor_2d_common_fun.cpp:75-105).  Pivoting follows
+// zgetf2: first row of maximal |re|+|im|, reciprocal scaling of the column.
+// The first cos projection of the driver step
+// (afqmcConstraintPathProjection.cpp:45-48, afqmcPhaselessProjection.cpp:85-88)
+// and the population-control weights (afqmcConstraintPathProjection.cpp:108-122)
+// are fused into the epilogue.
+// ---------------------------------------------------------------------------
+template <bool SMEM>
+__global__ void __launch_bounds__(256)
+lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, zd logwAdd,
+          zd logwT, zd *logov, int *alive, int *surv, zd *logwOut, double *weight, int *status,
+          int mode, int wantInverse, int maxNs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int w = blockIdx.x;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    zd *sA = (zd *)smem_raw;
+    zd *sX = sA + (SMEM ? maxNs * maxNs : 0);
+    int *piv = (int *)(sX + (SMEM ? maxNs * maxNs : 0));
+    __shared__ int sFlag;
+
+    const bool act = (active == nullptr) || active[w] != 0;
+    if (!act) {
+        if (tid == 0) {
+            if (mode == LU_PROJECT) surv[w] = 0;
+            if (mode == LU_POPWEIGHT) { weight[w] = 0.0; alive[w] = 1; }
+        }
+        return;
+    }
+    if (tid == 0) sFlag = 0;
+    zd logdetSum = make_double2(0.0, 0.0);
+
+    for (int b = 0; b < bl.nblk; ++b) {
+        const int Ns = bl.Ns[b];
+        if (Ns == 0) continue;
+        zd *Sg = S + (size_t)w * bl.sStride + bl.sOff[b];
+        zd *Xg = Sinv ? Sinv + (size_t)w * bl.sStride + bl.sOff[b] : nullptr;
+        zd *A = SMEM ? sA : Sg;
+        zd *X = SMEM ? sX : Xg;
+        if (SMEM)
+            for (int e = tid; e < Ns * Ns; e += nt) A[e] = Sg[e];
+        __syncthreads();
+        for (int j = 0; j < Ns; ++j) {
+            if (tid < 32) {
+                double best = -1.0; int bi = Ns;
+                for (int i = j + tid; i < Ns; i += 32) {
+                    double v = zcabs1(A[i + (size_t)j * Ns]);
+                    if (v > best) { best = v; bi = i; }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    double ov = __shfl_xor_sync(0xffffffffu, best, o);
+                    int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+                }
+                if (tid == 0) piv[j] = bi;
+            }
+            __syncthreads();
+            const int p = piv[j];
+            if (p != j)
+                for (int c = tid; c < Ns; c += nt) {
+                    zd t = A[j + (size_t)c * Ns];
+                    A[j + (size_t)c * Ns] = A[p + (size_t)c * Ns];
+                    A[p + (size_t)c * Ns] = t;
+                }
+            __syncthreads();
+            const zd d = A[j + (size_t)j * Ns];
+            if (!zeq0(d)) {
+                zd inv = zdiv(make_double2(1.0, 0.0), d);
+                for (int i = j + 1 + tid; i < Ns; i += nt) A[i + (size_t)j * Ns] = zmul(A[i + (size_t)j * Ns], inv);
+            } else if (tid == 0) {
+                sFlag = 1;
+            }
+            __syncthreads();
+            const int r = Ns - j - 1;
+            for (int e = tid; e < r * r; e += nt) {
+                int i = j + 1 + e % r, c = j + 1 + e / r;
+                zd u = A[j + (size_t)c * Ns];
+                zd l = A[i + (size_t)j * Ns];
+                zd v = A[i + (size_t)c * Ns];
+                v.x -= l.x * u.x - l.y * u.y;
+                v.y -= l.x * u.y + l.y * u.x;
+                A[i + (size_t)c * Ns] = v;
+            }
+            __syncthreads();
+        }
+        // log determinant with pivot signs
+        if (tid == 0) {
+            if (sFlag) {
+                logdetSum = make_double2(-1e300, 0.0);
+            } else {
+                double lognorm = 0.0; zd phase = make_double2(1.0, 0.0);
+                for (int j = 0; j < Ns; ++j) {
+                    zd u = A[j + (size_t)j * Ns];
+                    double a = zabs(u);
+                    lognorm += log(a);
+                    zd f = (piv[j] != j) ? zneg(u) : u;
+                    phase = zmul(phase, make_double2(f.x / a, f.y / a));
+                }
+                zd ld = zadd(make_double2(lognorm, 0.0), zlog(phase));
+                if (logdetSum.x > -1e299) logdetSum = zadd(logdetSum, ld);
+            }
+        }
+        // inverse: X = A^{-1} column by column (P, unit-L forward, U backward)
+        if (wantInverse && Xg) {
+            for (int c = tid; c < Ns; c += nt) {
+                zd *x = X + (size_t)c * Ns;
+                for (int i = 0; i < Ns; ++i) x[i] = make_double2(i == c ? 1.0 : 0.0, 0.0);
+                for (int i = 0; i < Ns; ++i) {
+                    int pi = piv[i];
+                    if (pi != i) { zd t = x[i]; x[i] = x[pi]; x[pi] = t; }
+                }
+                for (int i = 0; i < Ns; ++i) {
+                    zd s = x[i];
+                    for (int k = 0; k < i; ++k) {
+                        zd l = A[i + (size_t)k * Ns], xk = x[k];
+                        s.x -= l.x * xk.x - l.y * xk.y;
+                        s.y -= l.x * xk.y + l.y * xk.x;
+                    }
+                    x[i] = s;
+                }
+                for (int i = Ns - 1; i >= 0; --i) {
+                    zd s = x[i];
+                    for (int k = i + 1; k < Ns; ++k) {
+                        zd u = A[i + (size_t)k * Ns], xk = x[k];
+                        s.x -= u.x * xk.x - u.y * xk.y;
+                        s.y -= u.x * xk.y + u.y * xk.x;
+                    }
+                    x[i] = zdiv(s, A[i + (size_t)i * Ns]);
+                }
+            }
+            __syncthreads();
+            if (SMEM)
+                for (int e = tid; e < Ns * Ns; e += nt) Xg[e] = X[e];
+        }
+        __syncthreads();
+    }
+
+    if (tid == 0) {
+        zd lwR = zadd(logwAdd, logw[w]);
+        zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
+        logov[w] = lo;
+        if (sFlag && status) atomicOr(status + w, (int)ST_SINGULAR);
+        if (!(isfinite(lo.x) && isfinite(lo.y)) && status && !sFlag) atomicOr(status + w, (int)ST_NONFINITE);
+        if (mode == LU_PROJECT) {
+            double phase = lo.y;
+            double c = cos(phase);
+            if (c <= 0.0) {
+                alive[w] = 0; surv[w] = 0;
+            } else {
+                zd lw = logw[w];
+                lw = zadd(lw, make_double2(log(c), -phase));
+                logwOut[w] = lw;
+                surv[w] = 1;
+            }
+        } else if (mode == LU_POPWEIGHT) {
+            zd e = zexp(lo);
+            double ov = e.x;
+            if (ov <= 0.0) {
+                weight[w] = 0.0;
+            } else {
+                weight[w] = ov;
+                logwOut[w] = zsub(logw[w], lo);
+            }
+            alive[w] = 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exclusive scan of survivors x draws -> per-walker offset into the random
+// stream; reproduces the reference's sequential walker-major draw order
+// (afqmcPhaselessProjection.cpp:80-101, NiupNidn.cpp:66-84).
+// ---------------------------------------------------------------------------
+__global__ void rng_scan_kernel(int W, const int *surv, int draws, unsigned long long *counter,
+                                unsigned long long *offs)
+{
+    __shared__ unsigned long long warpSums[32];
+    __shared__ unsigned long long carry;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    if (tid == 0) carry = *counter;
+    __syncthreads();
+    for (int base = 0; base < W; base += blockDim.x) {
+        int w = base + tid;
+        unsigned long long v = (w < W && surv[w]) ? (unsigned long long)draws : 0ULL;
+        unsigned long long x = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warpSums[wid] = x;
+        __syncthreads();
+        if (wid == 0) {
+            int nw = blockDim.x >> 5;
+            unsigned long long s = lane < nw ? warpSums[lane] : 0ULL;
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned long long y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            if (lane < nw) warpSums[lane] = s;  // inclusive prefix of warp totals
+        }
+        __syncthreads();
+        unsigned long long prefix = carry + (wid > 0 ? warpSums[wid - 1] : 0ULL) + x - v;
+        if (w < W) offs[w] = prefix;
+        __syncthreads();
+        if (tid == blockDim.x - 1) carry = prefix + v;
+        __syncthreads();
+    }
+    if (tid == 0) *counter = carry;
+}
+
+// ---------------------------------------------------------------------------
+// Hubbard force: HubbardSOCMeasureFixedSDSD::getForce (:73-116) with the
+// Green's function diagonal / off-diagonal of SDSDOperation (:91-141).
+// ---------------------------------------------------------------------------
+__global__ void cp_force_kernel(int W, HubbardDev h, const zd *thetaT, long long tStride,
+                                const int *surv, double *force)
+{
+    const int w = blockIdx.x;
+    if (!surv[w]) return;
+    const int L = h.L, N = h.N, n = h.n;
+    const zd *th = thetaT + (size_t)w * tStride;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        double f;
+        if (h.constForce) {
+            f = h.constForce[i];
+        } else {
+            zd a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+            if (h.decomp <= 1) {
+                for (int j = 0; j < N; ++j) {
+                    zfma(a, zconj(h.phiT[i + (size_t)n * j]), th[j + (size_t)N * i]);
+                    zfma(b, zconj(h.phiT[i + L + (size_t)n * j]), th[j + (size_t)N * (i + L)]);
+                }
+            } else {
+                for (int j = 0; j < N; ++j) {
+                    zfma(a, zconj(h.phiT[i + (size_t)n * j]), th[j + (size_t)N * (i + L)]);
+                    zfma(b, zconj(h.phiT[i + L + (size_t)n * j]), th[j + (size_t)N * i]);
+                }
+            }
+            zd bgv;
+            if (h.decomp == 0) bgv = make_double2(a.x + b.x - 1.0, a.y + b.y);
+            else if (h.decomp == 1) bgv = zsub(a, b);
+            else if (h.decomp == 2) bgv = zadd(a, b);
+            else bgv = zsub(a, b);
+            f = zmul(h.gamma[i], bgv).x;
+            if (f > h.forceCap) f = h.forceCap;
+            if (f < -h.forceCap) f = -h.forceCap;
+        }
+        force[(size_t)w * L + i] = f;
+    }
+}
+
+__device__ __forceinline__ zd zcosh(zd z)
+{
+    zd e = zexp(z), ei = zexp(zneg(z));
+    return zscale(zadd(e, ei), 0.5);
+}
+__device__ __forceinline__ zd zsinh(zd z)
+{
+    zd e = zexp(z), ei = zexp(zneg(z));
+    return zscale(zsub(e, ei), 0.5);
+}
+__device__ __forceinline__ zd zcos(zd z)
+{
+    double s, c;
+    sincos(z.x, &s, &c);
+    return make_double2(c * cosh(z.y), -s * sinh(z.y));
+}
+__device__ __forceinline__ zd zsin(zd z)
+{
+    double s, c;
+    sincos(z.x, &s, &c);
+    return make_double2(s * cosh(z.y), c * sinh(z.y));
+}
+
+// ---------------------------------------------------------------------------
+// Hubbard aux-field sampling + two-body sample + its application:
+// NiupNidn::sampleAuxFromForce (NiupNidn.cpp:66-84),
+// getTwoBodySampleFromAuxForce (:100-142, setTwoBodySampleMatrix :252-322),
+// NiupNidnSampleSDOperation::applyToRight (NiupNidnSDOperation.cpp:15-41),
+// and the walker log-weight bookkeeping of the driver step
+// (afqmcConstraintPathProjection.cpp:63-72).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+cp_sample_apply_kernel(int W, HubbardDev h, const double *force, const int *surv,
+                       const unsigned long long *offs, uint64_t seed, const zd *wf, zd *wfTmp,
+                       zd *logw, double dtET, zd hopLogw, int *auxOut)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int w = blockIdx.x;
+    if (!surv[w]) return;
+    const int L = h.L, N = h.N, n = h.n;
+    zd *d00 = (zd *)smem_raw, *d01 = d00 + L, *d10 = d00 + 2 * L, *d11 = d00 + 3 * L;
+    int *aux = (int *)(d00 + 4 * L);
+    double *fs = (double *)(aux + L + (L & 1));
+    const double *fw = h.constForce ? h.constForce : force + (size_t)w * L;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        double f = fw[i];
+        fs[i] = f;
+        double em = exp(-f), ep = exp(f);
+        double prob = em / (em + ep);
+        int x = (rng_uniform(seed, offs[w] + (unsigned long long)i) < prob) ? -1 : 1;
+        aux[i] = x;
+        if (auxOut) auxOut[(size_t)w * L + i] = x;
+        zd ga = zscale(h.gamma[i], (double)x);
+        zd a00, a01, a10, a11;
+        if (h.decomp == 0) {
+            zd e = zexp(ga);
+            a00 = zmul(e, h.cd00[i]); a10 = zmul(e, h.cd10[i]); a01 = zmul(e, h.cd01[i]); a11 = zmul(e, h.cd11[i]);
+        } else if (h.decomp == 1) {
+            zd e = zexp(ga), ei = zdiv(make_double2(1.0, 0.0), e);
+            a00 = zmul(e, h.cd00[i]); a10 = zmul(ei, h.cd10[i]); a01 = zmul(e, h.cd01[i]); a11 = zmul(ei, h.cd11[i]);
+        } else if (h.decomp == 2) {
+            zd c = zcosh(ga), s = zsinh(ga);
+            a00 = zadd(zmul(c, h.cd00[i]), zmul(s, h.cd10[i]));
+            a10 = zadd(zmul(s, h.cd00[i]), zmul(c, h.cd10[i]));
+            a01 = zadd(zmul(c, h.cd01[i]), zmul(s, h.cd11[i]));
+            a11 = zadd(zmul(s, h.cd01[i]), zmul(c, h.cd11[i]));
+        } else {
+            zd c = zcos(ga), s = zsin(ga);
+            a00 = zadd(zmul(c, h.cd00[i]), zmul(s, h.cd10[i]));
+            a10 = zadd(zmul(zneg(s), h.cd00[i]), zmul(c, h.cd10[i]));
+            a01 = zadd(zmul(c, h.cd01[i]), zmul(s, h.cd11[i]));
+            a11 = zadd(zmul(zneg(s), h.cd01[i]), zmul(c, h.cd11[i]));
+        }
+        d00[i] = a00; d01[i] = a01; d10[i] = a10; d11[i] = a11;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        zd lw;
+        if (h.decomp == 0) {
+            // KahanData<complex<double>> sum of aux*gamma (erroranalysisHao/include/kahan.h)
+            zd sum = make_double2(0.0, 0.0), comp = make_double2(0.0, 0.0);
+            for (int i = 0; i < L; ++i) {
+                zd y = zsub(zscale(h.gamma[i], (double)aux[i]), comp);
+                zd t = zadd(sum, y);
+                comp = zsub(zsub(t, sum), y);
+                sum = t;
+            }
+            lw = zsub(make_double2(log(0.5) * L + h.dtUSum * 0.5, 0.0), sum);
+        } else {
+            lw = make_double2(log(0.5) * L, 0.0);
+        }
+        double lp = 0.0;
+        for (int i = 0; i < L; ++i) lp += aux[i] * fs[i] - log(exp(fs[i]) + exp(-fs[i]));
+        lw.x -= lp;
+        zd t = zadd(lw, logw[w]);
+        t.x += dtET;
+        logw[w] = zadd(hopLogw, t);
+    }
+    const zd *src = wf + (size_t)w * n * N;
+    zd *dst = wfTmp + (size_t)w * n * N;
+    for (int e = threadIdx.x; e < L * N; e += blockDim.x) {
+        int i = e % L, j = e / L;
+        zd a = src[i + (size_t)n * j], b = src[i + L + (size_t)n * j];
+        zd r0 = zmul(d00[i], a), r1 = zmul(d10[i], a);
+        zfma(r0, d01[i], b);
+        zfma(r1, d11[i], b);
+        dst[i + (size_t)n * j] = r0;
+        dst[i + L + (size_t)n * j] = r1;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phaseless force + aux sampling + sample log-weight + second cos projection:
+// RealMaterialMoleculeMeasureFixedSD2sSD2is::getForce (:93-116),
+// CholeskyReal::sampleAuxFromForce (choleskyReal.cpp:57-65),
+// getTwoBodySampleFromAuxForce (:104-124) and
+// afqmcPhaselessProjection.cpp:89-118.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+pl_sample_kernel(int W, CholDev c, const zd *xbar, int *surv, int *alive,
+                 const unsigned long long *offs, uint64_t seed, zd *aux, zd *force, zd *logw,
+                 double dtET, zd hopLogw)
+{
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (!surv[w]) return;
+    const int G = c.G;
+    zd f2 = make_double2(0, 0), xf = make_double2(0, 0), xb = make_double2(0, 0);
+    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        zd f;
+        if (c.constForce) {
+            f = c.constForce[g];
+        } else {
+            zd x = xbar[g + (size_t)G * w];
+            double a = x.x - c.bg[g], b = x.y;
+            f = make_double2(-b * c.sqrtDt, a * c.sqrtDt);
+            double af = zabs(f);
+            if (af > c.forceCap) f = make_double2(f.x * c.forceCap / af, f.y * c.forceCap / af);
+        }
+        double gs = rng_gaussian(seed, offs[w] + 2ULL * g);
+        zd x = make_double2(gs + f.x, f.y);
+        aux[g + (size_t)G * w] = x;
+        force[g + (size_t)G * w] = f;
+        zfma(f2, f, f);
+        zfma(xf, x, f);
+        zfma(xb, x, make_double2(c.bg[g], 0.0));
+    }
+    f2 = block_zsum(f2, red);
+    xf = block_zsum(xf, red);
+    xb = block_zsum(xb, red);
+    if (threadIdx.x == 0) {
+        double phase = xf.y;
+        double cs = cos(phase);
+        if (cs <= 0.0) {
+            alive[w] = 0; surv[w] = 0;
+        } else {
+            zd lw = logw[w];
+            lw.x += log(cs);
+            // sample logw = 0.5 f.f - x.f - sqrt(-dt) x.bg, sqrt(-dt) = i sqrtDt
+            zd smp = zsub(zscale(f2, 0.5), xf);
+            smp = zsub(smp, make_double2(-c.sqrtDt * xb.y, c.sqrtDt * xb.x));
+            zd t = zadd(smp, lw);
+            t.x += dtET;
+            logw[w] = zadd(hopLogw, t);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Taylor series step of LogHop2isSD2isOperation (logHop2isSD2isOperation.cpp:
+// 159-195): walkerNew += term_k, then the dynamicOrder convergence test
+// max|term_k| <= accuracy from order checkFrom on.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+taylor_accum_kernel(int W, long long wsize, const zd *term, zd *wfNew, const int *surv, int *done,
+                    int *order, int k, int checkFrom, double acc, int isLast, int *status)
+{
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (!surv[w] || done[w]) return;
+    const zd *t = term + (size_t)w * wsize;
+    zd *o = wfNew + (size_t)w * wsize;
+    double mx = 0.0;
+    for (long long e = threadIdx.x; e < wsize; e += blockDim.x) {
+        zd v = t[e];
+        zd a = o[e];
+        o[e] = zadd(a, v);
+        mx = fmax(mx, zabs(v));
+    }
+    if (k >= checkFrom) {
+        mx = block_max(mx, red);
+        if (threadIdx.x == 0) {
+            if (mx <= acc) { done[w] = 1; order[w] = k; }
+            else if (isLast) { done[w] = 1; order[w] = k; atomicOr(status + w, (int)ST_TAYLOR_CAP); }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Modified Gram-Schmidt orthonormalisation of a walker, replacing the
+// Householder QR of SD::stabilize / SD2is::stabilize (SD.cpp:42-56,
+// SD2is.cpp:48-76, QRMatrix_cpu tensor_2d_bl_cpu.cpp:263-315).  R's diagonal
+// is positive, so logw += sum log R_jj (+ the first Nmin again for SD2is);
+// the determinant-invariant quantities (overlaps, G, E_L) equal the
+// reference's, whose Q differs by a +-1 column gauge.
+// ---------------------------------------------------------------------------
+template <bool SMEM>
+__global__ void __launch_bounds__(256)
+mgs_kernel(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, zd *logw,
+           const int *alive, int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (alive && !alive[w]) return;
+    zd *g = wf + (size_t)w * n * ncol;
+    zd *A = SMEM ? (zd *)smem_raw : g;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    if (SMEM) {
+        for (int e = tid; e < n * ncol; e += nt) A[e] = g[e];
+        __syncthreads();
+    }
+    const int nmin = nup < ndn ? nup : ndn;
+    double logR = 0.0, logRmin = 0.0;
+    int bad = 0;
+    for (int j = 0; j < ncol; ++j) {
+        double s = 0.0;
+        for (int i = tid; i < n; i += nt) { zd v = A[i + (size_t)n * j]; s += v.x * v.x + v.y * v.y; }
+        s = block_sum(s, red);
+        double r = sqrt(s);
+        if (r == 0.0) bad = 1;
+        double inv = r > 0.0 ? 1.0 / r : 0.0;
+        for (int i = tid; i < n; i += nt) A[i + (size_t)n * j] = zscale(A[i + (size_t)n * j], inv);
+        if (tid == 0) {
+            double lr = log(r);
+            logR += lr;
+            if (j < nmin) logRmin += lr;
+        }
+        __syncthreads();
+        for (int c = j + 1 + wid; c < ncol; c += nw) {
+            zd d = make_double2(0.0, 0.0);
+            for (int i = lane; i < n; i += 32) zfma(d, zconj(A[i + (size_t)n * j]), A[i + (size_t)n * c]);
+            d.x = warp_sum(d.x);
+            d.y = warp_sum(d.y);
+            for (int i = lane; i < n; i += 32) {
+                zd q = A[i + (size_t)n * j];
+                zd v = A[i + (size_t)n * c];
+                v.x -= d.x * q.x - d.y * q.y;
+                v.y -= d.x * q.y + d.y * q.x;
+                A[i + (size_t)n * c] = v;
+            }
+        }
+        __syncthreads();
+    }
+    if (SMEM)
+        for (int e = tid; e < n * ncol; e += nt) g[e] = A[e];
+    if (tid == 0) {
+        zd lw = logw[w];
+        if (!isSD2is) lw.x += logR;
+        else if (nup == ndn) lw.x += 2.0 * logR;
+        else lw.x += logR + logRmin;
+        logw[w] = lw;
+        if (bad && status) atomicOr(status + w, (int)ST_ZERO_NORM);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// popConfiguration (populationControlConfiguration.cpp:24-101) for one
+// process: W uniforms from the stream, the comb over the normalised weights
+// accumulated in the reference's serial order (bit-exact tables), then the
+// slot filling.  The `number[zero_i]` read is bounds-checked first.
+// ---------------------------------------------------------------------------
+__global__ void pop_comb_kernel(int W, const double *weight, const double *uniforms, uint64_t seed,
+                                unsigned long long *counter, int *number, int *table, int *status)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long c0 = counter ? *counter : 0ULL;
+    double sum = 0.0;
+    for (int i = 0; i < W; ++i) sum += weight[i];
+    for (int i = 0; i < W; ++i) number[i] = 0;
+    int index_old = 0;
+    double prob_sum_old = weight[0] / sum;
+    for (int i = 0; i < W; ++i) {
+        double u = uniforms ? uniforms[i] : rng_uniform(seed, c0 + (unsigned long long)i);
+        double prob_sum_new = (i + u) / (W * 1.0);
+        while (prob_sum_new > prob_sum_old && index_old < W - 1) {
+            index_old++;
+            prob_sum_old += weight[index_old] / sum;
+        }
+        number[index_old]++;
+    }
+    if (counter) *counter = c0 + (unsigned long long)W;
+    for (int i = 0; i < W; ++i) table[i] = (number[i] != 0) ? i : -1;
+    int zero_i = 0, one_i = 0, max_i = W;
+    while (zero_i < max_i && number[zero_i] != 0) zero_i++;
+    while (one_i < max_i && number[one_i] <= 1) one_i++;
+    while (zero_i < max_i && one_i < max_i) {
+        table[zero_i] = one_i;
+        number[zero_i]++;
+        number[one_i]--;
+        while (zero_i < max_i && number[zero_i] != 0) zero_i++;
+        while (one_i < max_i && number[one_i] <= 1) one_i++;
+    }
+    int bad = 0;
+    for (int i = 0; i < W; ++i) if (number[i] != 1) bad = 1;
+    if (bad && status) status[0] |= 16;
+}
+
+// populationControl<T> serial branch (populationControl.h:110-117): parents
+// keep their own slot, so the copies can run in parallel in place.
+__global__ void pop_gather_kernel(int W, long long wsize, const int *table, zd *wf, zd *logw)
+{
+    const int i = blockIdx.x;
+    const int j = table[i];
+    if (j == i || j < 0) return;
+    const zd *src = wf + (size_t)j * wsize;
+    zd *dst = wf + (size_t)i * wsize;
+    for (long long e = threadIdx.x; e < wsize; e += blockDim.x) dst[e] = src[e];
+    if (threadIdx.x == 0) logw[i] = logw[j];
+}
+
+__global__ void set_int_kernel(int *p, int v, int count)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) p[i] = v;
+}
+
+__global__ void copy_masked_kernel(int W, long long wsize, const zd *src, zd *dst, const int *mask)
+{
+    const int w = blockIdx.x;
+    if (mask && !mask[w]) return;
+    const zd *s = src + (size_t)w * wsize;
+    zd *d = dst + (size_t)w * wsize;
+    for (long long e = threadIdx.x; e < wsize; e += blockDim.x) d[e] = s[e];
+}
+
+// ---------------------------------------------------------------------------
+// Hubbard local energy: HubbardSOCMeasureFixedSDSD::addEnergy (:178-218).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+cp_energy_kernel(int W, HubbardDev h, const zd *wfDaggerK, const zd *thetaT, long long tStride,
+                 const double *U, const double *mu, const double *hx, const double *hy,
+                 const double *hz, const int *alive, const zd *logov, zd *eloc, zd *den,
+                 zd *parts)
+{
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (!alive[w]) return;
+    const int L = h.L, N = h.N, n = h.n;
+    const zd *th = thetaT + (size_t)w * tStride;
+    zd K = make_double2(0, 0), V = make_double2(0, 0), R = make_double2(0, 0);
+    for (int e = threadIdx.x; e < N * n; e += blockDim.x) zfma(K, wfDaggerK[e], th[e]);
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        zd gi = make_double2(0, 0), gL = make_double2(0, 0), oi = make_double2(0, 0), oL = make_double2(0, 0);
+        for (int j = 0; j < N; ++j) {
+            zd pi = zconj(h.phiT[i + (size_t)n * j]), pL = zconj(h.phiT[i + L + (size_t)n * j]);
+            zfma(gi, pi, th[j + (size_t)N * i]);
+            zfma(gL, pL, th[j + (size_t)N * (i + L)]);
+            zfma(oi, pi, th[j + (size_t)N * (i + L)]);
+            zfma(oL, pL, th[j + (size_t)N * i]);
+        }
+        zd t = zsub(zmul(gi, gL), zmul(oi, oL));
+        V = zadd(V, zscale(t, U[i]));
+        R = zadd(R, zscale(gi, -mu[i] + hz[i] * 0.5));
+        R = zadd(R, zscale(gL, -mu[i] - hz[i] * 0.5));
+        R = zadd(R, zmul(make_double2(hx[i] * 0.5, -hy[i] * 0.5), oi));
+        R = zadd(R, zmul(make_double2(hx[i] * 0.5, hy[i] * 0.5), oL));
+    }
+    K = block_zsum(K, red);
+    V = block_zsum(V, red);
+    R = block_zsum(R, red);
+    if (threadIdx.x == 0) {
+        eloc[w] = zadd(zadd(K, V), R);
+        den[w] = zexp(logov[w]);
+        parts[3 * (size_t)w + 0] = K;
+        parts[3 * (size_t)w + 1] = V;
+        parts[3 * (size_t)w + 2] = R;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Exchange term ex_g = sum_sigma tr(D D), D = A_g,sigma theta_sigma
+// (RealMaterialMoleculeMeasureFixedSD2sSD2is::calculateCholeskyEx :258-284);
+// grid (walker, g-chunk), operand chunks of 32 orbitals staged in smem.
+// ---------------------------------------------------------------------------
+constexpr int EX_KC = 32;
+constexpr int EX_GCH = 16;
+
+// dynamic smem: As[Ns*EX_KC], Ts[Ns*EX_KC], Ds[Ns*Ns] for the largest block
+__global__ void __launch_bounds__(256)
+pl_exchange_kernel(int W, int n, int G, Blocks bl, const zd *Aall, long long Ktot,
+                   const zd *thetaT, const int *alive, zd *ex, int maxNs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    zd *As = (zd *)smem_raw;
+    zd *Ts = As + maxNs * EX_KC;
+    zd *Ds = Ts + maxNs * EX_KC;
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (!alive[w]) return;
+    const int g0 = blockIdx.y * EX_GCH;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int g = g0; g < G && g < g0 + EX_GCH; ++g) {
+        zd exg = make_double2(0.0, 0.0);
+        for (int b = 0; b < bl.nblk; ++b) {
+            const int Ns = bl.Ns[b];
+            if (Ns == 0) continue;
+            const zd *A = Aall + (size_t)g * Ktot + bl.tOff[b];
+            const zd *T = thetaT + (size_t)w * bl.tStride + bl.tOff[b];
+            const int ne = Ns * Ns;
+            zd acc[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) acc[q] = make_double2(0.0, 0.0);
+            for (int i0 = 0; i0 < n; i0 += EX_KC) {
+                int kc = min(EX_KC, n - i0);
+                for (int e = tid; e < Ns * kc; e += nt) {
+                    As[e] = A[(size_t)Ns * i0 + e];
+                    Ts[e] = T[(size_t)Ns * i0 + e];
+                }
+                __syncthreads();
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    int e = tid + q * nt;
+                    if (e < ne) {
+                        int a = e % Ns, bb = e / Ns;
+                        zd s = acc[q];
+                        for (int ii = 0; ii < kc; ++ii) zfma(s, As[a + Ns * ii], Ts[bb + Ns * ii]);
+                        acc[q] = s;
+                    }
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                int e = tid + q * nt;
+                if (e < ne) Ds[e] = acc[q];
+            }
+            __syncthreads();
+            zd part = make_double2(0.0, 0.0);
+            for (int e = tid; e < ne; e += nt) {
+                int a = e % Ns, bb = e / Ns;
+                zfma(part, Ds[a + Ns * bb], Ds[bb + Ns * a]);
+            }
+            part = block_zsum(part, red);
+            exg = zadd(exg, part);
+        }
+        if (tid == 0) ex[g + (size_t)G * w] = exg;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Phaseless local energy: addEnergy (:197-220) with calculateTenergy
+// (:222-235); T is an elementwise product in the stacked thetaT layout.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+pl_energy_kernel(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
+                 const zd *xbar, const zd *ex, const int *alive, const zd *logov, zd *eloc, zd *den,
+                 zd *tloc)
+{
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (!alive[w]) return;
+    const zd *th = thetaT + (size_t)w * Ktot;
+    zd T = make_double2(0, 0), H = make_double2(0, 0);
+    for (long long e = threadIdx.x; e < Ktot; e += blockDim.x) zfma(T, wfDaggerT[e], th[e]);
+    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        zd x = xbar[g + (size_t)G * w];
+        zd t = zmul(x, x);
+        H = zadd(H, zsub(t, ex[g + (size_t)G * w]));
+    }
+    T = block_zsum(T, red);
+    H = block_zsum(H, red);
+    if (threadIdx.x == 0) {
+        zd e = zadd(zscale(H, 0.5), T);
+        eloc[w] = e;
+        den[w] = zexp(logov[w]);
+        if (tloc) tloc[w] = T;
+    }
+}
+
+// Accumulate the estimator numerators/denominator over alive walkers in a
+// fixed order (writeThreadSum / MPISum of the reference become plain sums).
+__global__ void measure_reduce_kernel(int W, const int *alive, const zd *eloc, const zd *den,
+                                      const zd *parts, int nparts, zd *acc, int G, const zd *xbar,
+                                      const zd *ex, zd *bgNum, zd *exNum)
+{
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid == 0) {
+        zd sd = make_double2(0, 0), sh = make_double2(0, 0);
+        zd sp[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
+        for (int w = 0; w < W; ++w) {
+            if (!alive[w]) continue;
+            zd d = den[w];
+            sd = zadd(sd, d);
+            sh = zadd(sh, zmul(eloc[w], d));
+            for (int k = 0; k < nparts; ++k) sp[k] = zadd(sp[k], zmul(parts[(size_t)nparts * w + k], d));
+        }
+        acc[0] = zadd(acc[0], sd);
+        acc[1] = zadd(acc[1], sh);
+        for (int k = 0; k < nparts; ++k) acc[2 + k] = zadd(acc[2 + k], sp[k]);
+    }
+    if (xbar && tid < G) {
+        zd sb = make_double2(0, 0), se = make_double2(0, 0);
+        for (int w = 0; w < W; ++w) {
+            if (!alive[w]) continue;
+            zd d = den[w];
+            sb = zadd(sb, zmul(xbar[tid + (size_t)G * w], d));
+            se = zadd(se, zmul(ex[tid + (size_t)G * w], d));
+        }
+        bgNum[tid] = zadd(bgNum[tid], sb);
+        exNum[tid] = zadd(exNum[tid], se);
+    }
+}
+
+}  // namespace
+
+// ============================================================== launchers
+void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const int *active,
+                              const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive,
+                              int *surv, zd *logwOut, double *weight, int *status, int mode,
+                              bool wantInverse, cudaStream_t s)
+{
+    g_launch_count++;
+    int maxNs = 0;
+    for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
+    if (maxNs <= LU_SMEM_MAX_NS) {
+        size_t smem = (size_t)2 * maxNs * maxNs * sizeof(zd) + (size_t)(maxNs + 4) * sizeof(int);
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(lu_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+            attr = true;
+        }
+        lu_kernel<true><<<W, 256, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
+                                              alive, surv, logwOut, weight, status, mode,
+                                              wantInverse ? 1 : 0, maxNs);
+    } else {
+        size_t smem = (size_t)(maxNs + 4) * sizeof(int);
+        lu_kernel<false><<<W, 256, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
+                                               alive, surv, logwOut, weight, status, mode,
+                                               wantInverse ? 1 : 0, maxNs);
+    }
+}
+
+void launch_rng_scan(int W, const int *surv, int draws, unsigned long long *counter,
+                     unsigned long long *offs, cudaStream_t s)
+{
+    g_launch_count++;
+    rng_scan_kernel<<<1, 1024, 0, s>>>(W, surv, draws, counter, offs);
+}
+
+void launch_cp_force(int W, const HubbardDev &h, const zd *thetaT, long long tStride,
+                     const int *surv, double *force, cudaStream_t s)
+{
+    g_launch_count++;
+    cp_force_kernel<<<W, 128, 0, s>>>(W, h, thetaT, tStride, surv, force);
+}
+
+void launch_cp_sample_apply(int W, const HubbardDev &h, const double *force, const int *surv,
+                            const unsigned long long *offs, uint64_t seed, const zd *wf,
+                            zd *wfTmp, zd *logw, double dtET, zd hopLogw, int *auxOut,
+                            cudaStream_t s)
+{
+    g_launch_count++;
+    size_t smem = (size_t)4 * h.L * sizeof(zd) + (size_t)(h.L + 1) * sizeof(int) + (size_t)h.L * sizeof(double) + 16;
+    cp_sample_apply_kernel<<<W, 256, smem, s>>>(W, h, force, surv, offs, seed, wf, wfTmp, logw,
+                                                 dtET, hopLogw, auxOut);
+}
+
+void launch_pl_sample(int W, const CholDev &c, const zd *xbar, const int *surv_in, int *surv,
+                      int *alive, const unsigned long long *offs, uint64_t seed, zd *aux,
+                      zd *force, zd *logw, double dtET, zd hopLogw, cudaStream_t s)
+{
+    g_launch_count++;
+    (void)surv_in;
+    pl_sample_kernel<<<W, 256, 0, s>>>(W, c, xbar, surv, alive, offs, seed, aux, force, logw, dtET,
+                                        hopLogw);
+}
+
+void launch_taylor_accum(int W, long long wsize, const zd *term, zd *wfNew, const int *surv,
+                         int *done, int *order, int k, int checkFrom, double acc, int isLast,
+                         int *status, cudaStream_t s)
+{
+    g_launch_count++;
+    taylor_accum_kernel<<<W, 256, 0, s>>>(W, wsize, term, wfNew, surv, done, order, k, checkFrom,
+                                           acc, isLast, status);
+}
+
+void launch_mgs(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, zd *logw,
+                const int *alive, int *status, cudaStream_t s)
+{
+    g_launch_count++;
+    size_t bytes = (size_t)n * ncol * sizeof(zd);
+    if (bytes <= 160 * 1024) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(mgs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+            attr = true;
+        }
+        mgs_kernel<true><<<W, 256, bytes, s>>>(W, n, ncol, nup, ndn, isSD2is, wf, logw, alive, status);
+    } else {
+        mgs_kernel<false><<<W, 256, 0, s>>>(W, n, ncol, nup, ndn, isSD2is, wf, logw, alive, status);
+    }
+}
+
+void launch_pop_comb(int W, const double *weight, const double *uniforms, uint64_t seed,
+                     unsigned long long *counter, int *number, int *table, int *status,
+                     cudaStream_t s)
+{
+    g_launch_count++;
+    pop_comb_kernel<<<1, 32, 0, s>>>(W, weight, uniforms, seed, counter, number, table, status);
+}
+
+void launch_pop_gather(int W, long long wsize, const int *table, zd *wf, zd *logw, cudaStream_t s)
+{
+    g_launch_count++;
+    pop_gather_kernel<<<W, 256, 0, s>>>(W, wsize, table, wf, logw);
+}
+
+void launch_set_int(int *p, int v, int count, cudaStream_t s)
+{
+    g_launch_count++;
+    set_int_kernel<<<(count + 255) / 256, 256, 0, s>>>(p, v, count);
+}
+
+void launch_copy_masked(int W, long long wsize, const zd *src, zd *dst, const int *mask,
+                        cudaStream_t s)
+{
+    g_launch_count++;
+    copy_masked_kernel<<<W, 256, 0, s>>>(W, wsize, src, dst, mask);
+}
+
+void launch_cp_energy(int W, const HubbardDev &h, const zd *wfDaggerK, const zd *thetaT,
+                      long long tStride, const double *U, const double *mu, const double *hx,
+                      const double *hy, const double *hz, const int *alive, const zd *logov,
+                      zd *eloc, zd *den, zd *parts, cudaStream_t s)
+{
+    g_launch_count++;
+    cp_energy_kernel<<<W, 256, 0, s>>>(W, h, wfDaggerK, thetaT, tStride, U, mu, hx, hy, hz, alive,
+                                        logov, eloc, den, parts);
+}
+
+int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, long long Ktot,
+                       const zd *thetaT, const int *alive, zd *ex, cudaStream_t s)
+{
+    g_launch_count++;
+    int maxNs = 0;
+    for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
+    if (maxNs > 64) return -1;
+    size_t smem = ((size_t)2 * maxNs * EX_KC + (size_t)maxNs * maxNs) * sizeof(zd);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(pl_exchange_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        attr = true;
+    }
+    dim3 grid(W, (G + EX_GCH - 1) / EX_GCH);
+    pl_exchange_kernel<<<grid, 256, smem, s>>>(W, n, G, bl, Aall, Ktot, thetaT, alive, ex, maxNs);
+    return 0;
+}
+
+void launch_pl_energy(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
+                      const zd *xbar, const zd *ex, const int *alive, const zd *logov, zd *eloc,
+                      zd *den, zd *tloc, cudaStream_t s)
+{
+    g_launch_count++;
+    pl_energy_kernel<<<W, 256, 0, s>>>(W, G, Ktot, wfDaggerT, thetaT, xbar, ex, alive, logov, eloc,
+                                        den, tloc);
+}
+
+void launch_measure_reduce(int W, const int *alive, const zd *eloc, const zd *den, const zd *parts,
+                           int nparts, zd *acc, int G, const zd *xbar, const zd *ex, zd *bgNum,
+                           zd *exNum, cudaStream_t s)
+{
+    g_launch_count++;
+    int threads = 256;
+    int blocks = xbar ? (G + threads - 1) / threads : 1;
+    if (blocks < 1) blocks = 1;
+    measure_reduce_kernel<<<blocks, threads, 0, s>>>(W, alive, eloc, den, parts, nparts, acc, G,
+                                                      xbar, ex, bgNum, exNum);
+}
+
+namespace {
+// LogHop2isSD2isOperation order statistics (logHop2isSD2isOperation.cpp:146-157):
+// stats[0] calls, [1] total order, [2] min, [3] max.
+__global__ void taylor_stats_kernel(int W, const int *mask, const int *order, long long *stats)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    long long calls = stats[0], total = stats[1], mn = stats[2], mx = stats[3];
+    for (int w = 0; w < W; ++w) {
+        if (!mask[w]) continue;
+        long long o = order[w];
+        calls++; total += o;
+        if (o < mn) mn = o;
+        if (o > mx) mx = o;
+    }
+    stats[0] = calls; stats[1] = total; stats[2] = mn; stats[3] = mx;
+}
+}  // namespace
+
+void launch_taylor_stats(int W, const int *mask, const int *order, long long *stats, cudaStream_t s)
+{
+    g_launch_count++;
+    taylor_stats_kernel<<<1, 32, 0, s>>>(W, mask, order, stats);
+}

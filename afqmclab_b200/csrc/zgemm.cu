@@ -1,0 +1,155 @@
+// Batched complex FP64 GEMM (plain form).  B200 has no FP64 tcgen05 path, and
+// its FP64 DMMA rate equals its DFMA rate, so this kernel register-tiles the
+// complex multiply-adds on the FP64 pipe: each thread owns a TMxTN block of
+// the output, operand tiles are staged through shared memory (double
+// buffered), and column-major stores are coalesced along the row index.
+#include "zgemm.cuh"
+
+#include <atomic>
+
+extern std::atomic<long long> g_launch_count;
+
+namespace {
+
+constexpr int BK = 8;
+
+template <int OP, bool REAL>
+__device__ __forceinline__ zd load_op(const void *P, long long ld, int i, int l)
+{
+    // element (i, l) of op(P) where P is column-major with leading dimension ld
+    long long idx = (OP == OP_N) ? (long long)i + (long long)l * ld : (long long)l + (long long)i * ld;
+    zd v;
+    if (REAL) v = make_double2(__ldg((const double *)P + idx), 0.0);
+    else v = __ldg((const zd *)P + idx);
+    if (OP == OP_C) v.y = -v.y;
+    return v;
+}
+
+template <int BM, int BN, int TM, int TN, int OPA, int OPB, bool AR, bool BR>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+zgemm_kernel(ZGemmArgs a)
+{
+    constexpr int NTX = BM / TM;           // threads along rows
+    constexpr int NT = (BM / TM) * (BN / TN);
+    const int b = blockIdx.z;
+    if (a.mask && a.mask[b] == 0) return;
+    if (a.skip && a.skip[b] != 0) return;
+    const int tileM = blockIdx.x * BM, tileN = blockIdx.y * BN;
+    if (tileM >= a.m || tileN >= a.n) return;
+
+    const char *Ab = (const char *)a.A + (size_t)b * a.strideA * (AR ? sizeof(double) : sizeof(zd));
+    const char *Bb = (const char *)a.B + (size_t)b * a.strideB * (BR ? sizeof(double) : sizeof(zd));
+    zd *Cb = a.C + (size_t)b * a.strideC;
+
+    __shared__ zd As[2][BK][BM];
+    __shared__ zd Bs[2][BK][BN];
+
+    const int tid = threadIdx.x;
+    const int tx = tid % NTX, ty = tid / NTX;
+
+    zd acc[TM][TN];
+#pragma unroll
+    for (int i = 0; i < TM; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = make_double2(0.0, 0.0);
+
+    auto load_tiles = [&](int buf, int k0) {
+        for (int e = tid; e < BM * BK; e += NT) {
+            int i, l;
+            if (OPA == OP_N) { i = e % BM; l = e / BM; } else { l = e % BK; i = e / BK; }
+            int gi = tileM + i, gl = k0 + l;
+            zd v = make_double2(0.0, 0.0);
+            if (gi < a.m && gl < a.k) v = load_op<OPA, AR>(Ab, a.lda, gi, gl);
+            As[buf][l][i] = v;
+        }
+        for (int e = tid; e < BN * BK; e += NT) {
+            int l, j;
+            if (OPB == OP_N) { l = e % BK; j = e / BK; } else { j = e % BN; l = e / BN; }
+            int gl = k0 + l, gj = tileN + j;
+            zd v = make_double2(0.0, 0.0);
+            if (gl < a.k && gj < a.n) v = load_op<OPB, BR>(Bb, a.ldb, gl, gj);
+            Bs[buf][l][j] = v;
+        }
+    };
+
+    int buf = 0;
+    load_tiles(0, 0);
+    __syncthreads();
+    for (int k0 = 0; k0 < a.k; k0 += BK) {
+        if (k0 + BK < a.k) load_tiles(buf ^ 1, k0 + BK);
+#pragma unroll
+        for (int l = 0; l < BK; ++l) {
+            zd ra[TM], rb[TN];
+#pragma unroll
+            for (int i = 0; i < TM; ++i) ra[i] = As[buf][l][tx + i * NTX];
+#pragma unroll
+            for (int j = 0; j < TN; ++j) rb[j] = Bs[buf][l][ty + j * (BN / TN)];
+#pragma unroll
+            for (int i = 0; i < TM; ++i)
+#pragma unroll
+                for (int j = 0; j < TN; ++j) zfma(acc[i][j], ra[i], rb[j]);
+        }
+        __syncthreads();
+        buf ^= 1;
+    }
+
+    const bool beta0 = (a.beta.x == 0.0 && a.beta.y == 0.0);
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+        int gj = tileN + ty + j * (BN / TN);
+        if (gj >= a.n) continue;
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            int gi = tileM + tx + i * NTX;
+            if (gi >= a.m) continue;
+            zd *c = Cb + gi + (size_t)gj * a.ldc;
+            zd v = zmul(a.alpha, acc[i][j]);
+            if (!beta0) zfma(v, a.beta, *c);
+            *c = v;
+        }
+    }
+}
+
+template <int BM, int BN, int TM, int TN, int OPA, int OPB, bool AR, bool BR>
+cudaError_t launch4(const ZGemmArgs &a, cudaStream_t s)
+{
+    dim3 grid((a.m + BM - 1) / BM, (a.n + BN - 1) / BN, a.batch);
+    dim3 block((BM / TM) * (BN / TN));
+    zgemm_kernel<BM, BN, TM, TN, OPA, OPB, AR, BR><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int BM, int BN, int TM, int TN, int OPA, int OPB>
+cudaError_t launch3(const ZGemmArgs &a, cudaStream_t s)
+{
+    if (a.a_real && !a.b_real) return launch4<BM, BN, TM, TN, OPA, OPB, true, false>(a, s);
+    if (!a.a_real && a.b_real) return launch4<BM, BN, TM, TN, OPA, OPB, false, true>(a, s);
+    if (a.a_real && a.b_real) return launch4<BM, BN, TM, TN, OPA, OPB, true, true>(a, s);
+    return launch4<BM, BN, TM, TN, OPA, OPB, false, false>(a, s);
+}
+
+template <int BM, int BN, int TM, int TN>
+cudaError_t launch2(const ZGemmArgs &a, cudaStream_t s)
+{
+#define ZG_CASE(OA, OB) \
+    if (a.opA == OA && a.opB == OB) return launch3<BM, BN, TM, TN, OA, OB>(a, s);
+    ZG_CASE(OP_N, OP_N) ZG_CASE(OP_N, OP_T) ZG_CASE(OP_N, OP_C)
+    ZG_CASE(OP_T, OP_N) ZG_CASE(OP_T, OP_T) ZG_CASE(OP_T, OP_C)
+    ZG_CASE(OP_C, OP_N) ZG_CASE(OP_C, OP_T) ZG_CASE(OP_C, OP_C)
+#undef ZG_CASE
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+cudaError_t zgemm_batched(const ZGemmArgs &a, cudaStream_t stream)
+{
+    g_launch_count++;
+    if (a.m <= 0 || a.n <= 0 || a.batch <= 0) return cudaSuccess;
+    if (a.k <= 0) return cudaErrorInvalidValue;
+    // Tile choice: 64x64 (4x4 per thread) for large outputs, 32x32 (2x2) for
+    // the small per-walker overlap matrices.
+    if (a.m <= 32 && a.n <= 32) return launch2<32, 32, 2, 2>(a, stream);
+    if (a.m <= 32) return launch2<32, 64, 2, 4>(a, stream);
+    return launch2<64, 64, 4, 4>(a, stream);
+}

@@ -1,0 +1,26 @@
+// Batched complex FP64 GEMM used by the plain (FP64) form of the walker step.
+// C_b = alpha * op(A_b) * op(B_b) + beta * C_b for every batch entry b,
+// column-major operands, op in {N, T, C}; A or B may be real (double).
+// This is the B200 replacement for the reference's gmm_cpu/zgemm calls
+// (common/tensorHao/source/tensor_2d_bl_cpu.cpp:61-75) and its zgemv
+// (tensor_1d_bl_cpu.cpp:50-107), batched over the walker population.
+#pragma once
+#include "common.cuh"
+
+enum { OP_N = 0, OP_T = 1, OP_C = 2 };
+
+struct ZGemmArgs {
+    int m = 0, n = 0, k = 0;
+    int opA = OP_N, opB = OP_N;
+    int a_real = 0, b_real = 0;   // operand stored as double instead of double2
+    zd alpha = {1.0, 0.0}, beta = {0.0, 0.0};
+    const void *A = nullptr; long long lda = 0, strideA = 0;
+    const void *B = nullptr; long long ldb = 0, strideB = 0;
+    zd *C = nullptr; long long ldc = 0, strideC = 0;
+    int batch = 1;
+    const int *mask = nullptr;     // skip batch b when mask[b] == 0
+    const int *skip = nullptr;     // skip batch b when skip[b] != 0
+};
+
+// Launches on `stream`; returns cudaGetLastError().
+cudaError_t zgemm_batched(const ZGemmArgs &a, cudaStream_t stream);

@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Walker-step throughput of the B200 AFQMC engine (one JSON line on stdout).
+
+A step is one projectOneStep of the whole population (force, sampling,
+two-body Taylor propagation, one-body propagation, with modifyGM and
+popControl at the drivers' cadence) plus the mixed measurement every
+`measure_skip` steps (measureSkipStep = 5, the reference default).  The
+default workload is the synthetic phaseless molecule n=128, 32+32 electrons,
+G=640 Cholesky vectors, 2048 walkers, dt=0.005.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload molecule128|hubbard8x8|...] [--precision mixed|fp64]
+
+Under torchrun (N > 1) every rank advances its own population of the same
+size (walkers are independent between population controls: weak scaling);
+the timed region is bracketed by a barrier and the maximum over ranks is
+reported.  `--impl reference` times the CPU oracle port of the reference's
+algorithm on the host cores (rank 0 only).
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "walker-steps/s on 1 B200: mixed-precision vs FP64 form at |ΔE|≤0.5 mHa"
+UNIT = "walker-steps/s"
+
+
+# ------------------------------------------------------------------ helpers
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-i", str(self.gpu), "-lms", "100"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------- algorithmic counts
+def phase_flops(c, m, taylor_avg):
+    """Algorithmic real FLOPs of one launch of each timed phase (complex MAC = 8,
+    real x complex MAC = 4), for the phaseless workload."""
+    n, nup, ndn, G, W = m.n, m.nup, m.ndn, m.G, c["W"]
+    K = (nup + ndn) * n
+    f = {
+        "mbuild": 4.0 * n * n * G * W,
+        "force": 8.0 * G * K * W,
+        "taylor": 8.0 * n * n * max(nup, ndn) * W * taylor_avg,
+        "exchange": 8.0 * (nup * nup + ndn * ndn) * n * G * W + 8.0 * (nup * nup + ndn * ndn) * G * W,
+        "overlap": 8.0 * (nup * nup + ndn * ndn) * n * W,
+        "onebody": 8.0 * n * n * max(nup, ndn) * W,
+    }
+    return f
+
+
+def build_engine(capi, inputs, name, precision, seed):
+    m, c = inputs.make_config(name)
+    prec = capi.AFQMC_MIXED if precision == "mixed" else capi.AFQMC_FP64
+    if c["kind"] == "pl":
+        eng = capi.pl_engine(m, c["W"], seed, c["mgs"], c["pop"], precision=prec)
+        wf, lw, al = inputs.initial_walkers(m.phiTUp, c["W"])
+    else:
+        eng = capi.cp_engine(m, c["W"], seed, c["mgs"], c["pop"], precision=prec)
+        wf, lw, al = inputs.initial_walkers(m.phiT, c["W"])
+    eng.set_walkers(wf, lw, al)
+    # initialMgsAndPopControl (afqmcPhaselessSetWalker.cpp:140-144)
+    eng.modify_gm()
+    eng.pop_control()
+    return eng, m, c, (wf, lw, al)
+
+
+def run_steps(eng, k, start, measure_skip):
+    for i in range(k):
+        if (start + i) % measure_skip == 0:
+            eng.add_mixed_measurement()
+        eng.step(1)
+
+
+# ---------------------------------------------------------------- CPU arm
+def _cpu_worker(args):
+    name, nwalk, steps, seed, measure_skip = args
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    from afqmclab_b200 import inputs
+    from oracle import oracle as O
+    m, c = inputs.make_config(name)
+    if c["kind"] == "pl":
+        eng = O.pl_engine(m, nwalk, seed, c["mgs"], c["pop"])
+        wf, lw, al = inputs.initial_walkers(m.phiTUp, nwalk)
+    else:
+        eng = O.cp_engine(m, nwalk, seed, c["mgs"], c["pop"])
+        wf, lw, al = inputs.initial_walkers(m.phiT, nwalk)
+    eng.set_walkers(wf, lw, al)
+    t0 = time.perf_counter()
+    for i in range(steps):
+        if i % measure_skip == 0:
+            eng.add_mixed_measurement()
+        eng.step(1)
+    return nwalk * steps, time.perf_counter() - t0
+
+
+def cpu_measure(name, steps, measure_skip, max_procs=None, walkers_per_proc=None):
+    """Oracle port on the host cores: P single-threaded processes, each with
+    its own small population (the reference's MPI walker parallelism)."""
+    from afqmclab_b200 import inputs
+    c = inputs.CONFIGS[name]
+    cores = os.cpu_count() or 1
+    P = min(cores, max_procs or 64)
+    if walkers_per_proc is None:
+        walkers_per_proc = 2 if c["kind"] == "pl" else max(1, min(16, c["W"] // P))
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(P) as pool:
+        res = pool.map(_cpu_worker, [(name, walkers_per_proc, steps, 1000 + i, measure_skip)
+                                     for i in range(P)])
+    total = sum(r[0] for r in res)
+    wall = max(r[1] for r in res)
+    sample = (f"{P} processes x {walkers_per_proc} walkers x {steps} steps of {name} "
+              f"(measurement every {measure_skip} steps), slowest process timed")
+    return total / wall, P, sample
+
+
+# ------------------------------------------------------------------ main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="molecule128")
+    ap.add_argument("--precision", default="auto", choices=["auto", "mixed", "fp64"])
+    ap.add_argument("--measure-skip", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=5)
+    args = ap.parse_args()
+    rank, world, local = dist_info()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        t0 = time.perf_counter()
+        steps = max(args.cpu_steps, args.steps // 4 if args.steps >= 4 else 1)
+        v, P, sample = cpu_measure(args.workload, steps, args.measure_skip)
+        line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference",
+                "n_gpus": args.gpus, "steps": steps, "warmup": 0, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": P, "kind": "port",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "wall_s": time.perf_counter() - t0}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    from afqmclab_b200 import capi, inputs
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    precision = args.precision
+    if precision == "auto":
+        precision = "mixed" if os.environ.get("AFQMC_BENCH_FP64") is None else "fp64"
+    try:
+        eng, m, c, init = build_engine(capi, inputs, args.workload, precision, 77 + rank)
+    except capi.AfqmcError:
+        if args.precision != "auto":
+            raise
+        precision = "fp64"
+        eng, m, c, init = build_engine(capi, inputs, args.workload, precision, 77 + rank)
+    W = c["W"]
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+
+    # warm-up
+    run_steps(eng, args.warmup, 0, args.measure_skip)
+    eng.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # timed region: K steps, inputs resident in HBM (population + model
+    # tensors exceed the 126 MB L2 at this size)
+    eng.profile(True)
+    launches0 = capi.launch_count()
+    clocks = ClockSampler(dev)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    run_steps(eng, args.steps, args.warmup, args.measure_skip)
+    ev1.record(stream)
+    ev1.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = capi.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    prof = eng.profile_get()
+    eng.profile(False)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = W * args.steps * world / (ms / 1e3)
+
+    # e2e: the same steps through the C ABI with host buffers: each step
+    # uploads the population from pinned host memory and reads back the
+    # estimator sums.
+    wf0, lw0, al0 = init
+    h_wf = torch.from_numpy(np.ascontiguousarray(wf0.reshape(-1, order="F").view(np.float64))).pin_memory()
+    h_lw = torch.from_numpy(np.ascontiguousarray(lw0.view(np.float64))).pin_memory()
+    h_al = torch.from_numpy(np.ascontiguousarray(al0)).pin_memory()
+    meas = np.zeros(5, np.complex128)
+    lib = capi.lib()
+    e2e_steps = max(3, args.steps // 2)
+    eng.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        capi._check(lib.afqmc_set_walkers(eng.h, h_wf.data_ptr(), h_lw.data_ptr(), h_al.data_ptr()))
+        run_steps(eng, 1, i, args.measure_skip)
+        capi._check(lib.afqmc_get_measurement(eng.h, meas.ctypes.data))
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": W * e2e_steps * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int(h_wf.numel() * 8 + h_lw.numel() * 8 + h_al.numel() * 4),
+           "d2h_bytes_per_step": int(meas.nbytes)}
+
+    # roofline of the dominant phase
+    calls, total, mn, mx = eng.taylor_stats()
+    tavg = total / calls if calls else 0.0
+    roof = None
+    if c["kind"] == "pl":
+        fl = phase_flops(c, m, tavg)
+        cand = {k: v for k, v in prof.items() if k in fl and v[1] > 0}
+        top = max(cand, key=lambda k: cand[k][0])
+        t_launch = prof[top][0] / prof[top][1] / 1e3
+        achieved = fl[top] / t_launch / 1e12
+        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if precision == "mixed":
+            peak = json.load(open(peaks_path))["bf16_tflops_sustained"] if os.path.exists(peaks_path) else 1400.0
+            bound, psrc = "tensor", "measured bf16 sustained" if os.path.exists(peaks_path) else "fallback"
+        else:
+            peak, bound, psrc = 37.2, "fp64", "nominal FP64 (148 SM x 64 DFMA x 1.965 GHz); not in MEASURED_PEAKS.json"
+        roof = {"bound": bound, "kernel": top, "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "flops_per_launch": fl[top], "launch_ms": t_launch * 1e3, "peak_source": psrc}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, P, sample = cpu_measure(args.workload, args.cpu_steps, args.measure_skip)
+        cpu = {"value": v, "unit": UNIT, "cores": P, "kind": "port", "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16/f32 tensor + f64" if precision == "mixed" else "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "precision": precision, "n_orbitals": m.n if c["kind"] == "pl" else 2 * m.L,
+                       "electrons": [c.get("nup"), c.get("ndn")], "cholesky": c.get("G"),
+                       "walkers_per_gpu": W, "dt": c["dt"], "mgs_step": c["mgs"],
+                       "pop_control_step": c["pop"], "measure_skip": args.measure_skip,
+                       "parallelism": f"walker-dp{world}",
+                       "l2": "inputs larger than L2 (no flush)"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk,
+            "phases_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1] > 0},
+            "taylor_order": {"avg": tavg, "min": mn, "max": mx},
+            "status": eng.status(),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

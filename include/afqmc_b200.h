@@ -1,0 +1,210 @@
+/*
+ * afqmc_b200.h -- C ABI of the B200 AFQMC walker-step engine.
+ *
+ * The engine keeps a whole walker population resident in GPU memory as one
+ * strided batch and advances it with hand-written sm_100a kernels.  Each
+ * entry point below replaces one member (or loop) of the reference's
+ * compile-time plugin API for this path (hshi/AFQMCLAB); the reference
+ * interface is cited beside every declaration (file:line, relative to the
+ * AFQMCLAB project root).
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 = OK, otherwise an AFQMC_ERR_*
+ *    code; afqmc_last_error() gives a message.  Nothing here calls exit().
+ *  - Host buffers use the reference's storage: complex<double> interleaved
+ *    (re, im), column-major (TensorHao, tensor_core.h:83-91); a population is
+ *    W walker matrices stacked one after the other (walker w at w*n*ncol).
+ *  - "complex" scalars are passed as two doubles (re, im).
+ *  - All device work is issued on the engine's stream (afqmc_set_stream); the
+ *    get_* calls synchronise that stream before returning host data.
+ */
+#ifndef AFQMC_B200_H
+#define AFQMC_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AFQMC_OK 0
+#define AFQMC_ERR_ARG 1
+#define AFQMC_ERR_CUDA 2
+#define AFQMC_ERR_STATE 3
+#define AFQMC_ERR_UNSUPPORTED 4
+
+/* precision forms */
+#define AFQMC_FP64 0   /* plain form: every contraction in FP64 */
+#define AFQMC_MIXED 1  /* tensor-core contractions, FP64 LU/log-det/weights/QR */
+
+/* NiupNidn decompositions (NiupNidn.h:16) */
+#define AFQMC_DENSITY_CHARGE 0
+#define AFQMC_DENSITY_SPIN 1
+#define AFQMC_HOP_CHARGE 2
+#define AFQMC_HOP_SPIN 3
+
+/* force types (afqmcConstraintPathMethod.h / afqmcPhaselessMethod.h forceType) */
+#define AFQMC_DYNAMIC_FORCE 0
+#define AFQMC_CONST_FORCE 1
+
+typedef struct afqmc_engine afqmc_engine;
+
+/* Last error message of the calling thread (empty when none). */
+const char *afqmc_last_error(void);
+
+/* Library version string. */
+const char *afqmc_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Constrained-path Hubbard engine: SD walkers (2L x N), HubbardSOC model,
+ * NiupNidn two-body, HubbardSOCMeasureFixedSDSD mixed estimator.
+ * Replaces AfqmcConstraintPath::initialParameters/initialMeasure
+ * (tutorials/afqmcConstraintPath/source/afqmcConstraintPath.cpp:20-38):
+ *   K                 2L x 2L complex   HubbardSOC::K (HubbardSOC.cpp:39-59)
+ *   expMinusDtK, expHalfDtK, expMinusHalfDtK
+ *                     2L x 2L complex   Hop matrices from returnExpMinusAlphaK
+ *                                       (HubbardSOC.cpp:109-118); Hop::logw = 0
+ *   U, mu, hx, hy, hz L doubles each    (NiupNidn ctor, NiupNidn.cpp:12-26)
+ *   const_force       L doubles or NULL (readForce, NiupNidn.cpp:58-64)
+ *   phiT              2L x N complex    trial SD (phiT.dat)
+ * ------------------------------------------------------------------------- */
+int afqmc_cp_create(int L, int N, int W, int decomp, int force_type, double dt, double ET,
+                    double force_cap, int mgs_step, int pop_control_step, int precision,
+                    const double *K, const double *expMinusDtK, const double *expHalfDtK,
+                    const double *expMinusHalfDtK, const double *U, const double *mu,
+                    const double *hx, const double *hy, const double *hz,
+                    const double *const_force, const double *phiT, double logwT_re,
+                    double logwT_im, unsigned long long seed, afqmc_engine **out);
+
+/* ---------------------------------------------------------------------------
+ * Phaseless real-material engine: SD2is right walkers (n x max(Nup,Ndn)),
+ * SD2s trial, RealMaterialMolecule + CholeskyReal, mixed estimator
+ * RealMaterialMoleculeMeasureFixedSD2sSD2is.
+ * Replaces AfqmcPhaseless::initialParameters/initialMeasure
+ * (tutorials/afqmcPhaseless/source/afqmcPhaseless.cpp:32-72):
+ *   chol   n x n x G real   RealMaterialMolecule::choleskyVecs (realMaterialMolecule.cpp:41-60)
+ *   bg     G real           choleskyBg
+ *   t      n x n real       one-body matrix of the T energy (initWfDaggerT, :148-163)
+ *   expMinusDtK/expHalfDtK/expMinusHalfDtK (n x n complex) with their logw:
+ *          Hop2is operators of returnExpMinusAlphaK (realMaterialMolecule.cpp:117-132);
+ *          pass NULL for all three to use the Taylor (LogHop2is) form instead:
+ *   logExpMinusDtK (n x n complex) + logw: returnLogExpMinusAlphaK (:134-146);
+ *          in that case expHalfDtK/expMinusHalfDtK slots hold the LogHop2is
+ *          matrices of +-dt/2 (as in the oracle).
+ *   const_force  G complex or NULL
+ *   phiTUp (n x Nup), phiTDn (n x Ndn) complex: SD2s trial
+ * ------------------------------------------------------------------------- */
+int afqmc_pl_create(int n, int Nup, int Ndn, int G, int W, int force_type, double dt, double ET,
+                    double force_cap, int mgs_step, int pop_control_step, int precision,
+                    const double *chol, const double *bg, const double *t,
+                    const double *expMinusDtK, double logwExpMinusDtK, const double *expHalfDtK,
+                    double logwExpHalfDtK, const double *expMinusHalfDtK,
+                    double logwExpMinusHalfDtK, const double *logExpMinusDtK,
+                    double logwLogExpMinusDtK, const double *const_force, const double *phiTUp,
+                    const double *phiTDn, double logwT_re, double logwT_im,
+                    unsigned long long seed, afqmc_engine **out);
+
+int afqmc_destroy(afqmc_engine *e);
+
+/* Work stream (a cudaStream_t); NULL restores the engine's own stream. */
+int afqmc_set_stream(afqmc_engine *e, void *cuda_stream);
+int afqmc_synchronize(afqmc_engine *e);
+
+/* Population upload/download in the reference layout.
+ * Walker data: SD::wfRef/logwRef (SD.h:17-62), SD2is (SD2is.h:17-64);
+ * alive: the driver's walkerIsAlive vector. */
+int afqmc_set_walkers(afqmc_engine *e, const double *wf, const double *logw, const int *alive);
+int afqmc_get_walkers(afqmc_engine *e, double *wf, double *logw, int *alive);
+
+/* Counter-based random stream: replaces randomHaoInit/randomHaoSave/Read
+ * (common/randomHao/source/random_hao.cpp:10-71).  The stream is the
+ * SplitMix64 sequence of `seed`; `counter` is the next draw's position. */
+int afqmc_set_rng(afqmc_engine *e, unsigned long long seed, unsigned long long counter);
+int afqmc_get_rng(afqmc_engine *e, unsigned long long *seed, unsigned long long *counter);
+
+/* method.ET (afqmcConstraintPathMethod.h ET) */
+int afqmc_set_ET(afqmc_engine *e, double ET);
+/* mgsIndex / popControlIndex of projectOneStep */
+int afqmc_set_cadence(afqmc_engine *e, int mgs_index, int pop_control_index);
+
+/* projectOneStep x nsteps (afqmcConstraintPathProjection.cpp:76-93,
+ * afqmcPhaselessProjection.cpp:123-140): projectExpMinusDtKExpMinusDtV, then
+ * modifyGM every mgs_step and popControl every pop_control_step. */
+int afqmc_project_one_step(afqmc_engine *e, int nsteps);
+
+/* projectExpMinusHalfDtK (which = -1) / projectExpHalfDtK (which = +1)
+ * (afqmcConstraintPathProjection.cpp:11-29, afqmcPhaselessProjection.cpp:11-73) */
+int afqmc_project_half(afqmc_engine *e, int which);
+
+/* modifyGM: stabilize() every alive walker (SD.cpp:42-56, SD2is.cpp:48-76) */
+int afqmc_modify_gm(afqmc_engine *e);
+
+/* popControl (afqmcConstraintPathProjection.cpp:103-156): weights, comb
+ * (popConfiguration, populationControlConfiguration.cpp:24-101) and copies
+ * (populationControl<T>, populationControl.h:110-117).  table_out (W ints)
+ * and weight_out (W doubles) are optional host outputs. */
+int afqmc_pop_control(afqmc_engine *e, int *table_out, double *weight_out);
+
+/* Mixed estimator: addMixedMeasurement (afqmcConstraintPathMeasure.cpp:9-23,
+ * afqmcPhaselessMeasure.cpp:9-28), reSet, and the accumulated sums.
+ * afqmc_get_measurement writes 5 complex numbers:
+ *   CP: den, HNum, KNum, VNum, RNum   PL: den, HNum, TNum, 0, 0 */
+int afqmc_reset_measurement(afqmc_engine *e);
+int afqmc_add_mixed_measurement(afqmc_engine *e);
+int afqmc_get_measurement(afqmc_engine *e, double *out);
+/* choleskyBgNum / choleskyExNum (G complex each), PL only */
+int afqmc_get_cholesky_nums(afqmc_engine *e, double *bgNum, double *exNum);
+
+/* Background update + propagator replacement: RealMaterialMolecule::
+ * updateBackGround (realMaterialMolecule.cpp:103-115) and the rebuild in
+ * afqmcPhaseless.cpp:151-177.  Matrices as in afqmc_pl_create (NULL keeps). */
+int afqmc_pl_update_background(afqmc_engine *e, const double *bg, const double *expMinusDtK,
+                               double logwExpMinusDtK, const double *expHalfDtK,
+                               double logwExpHalfDtK, const double *expMinusHalfDtK,
+                               double logwExpMinusHalfDtK);
+
+/* Diagnostics (gauge-invariant quantities for parity checks) */
+/* log <phiT|phi_w> of every walker: SDSDOperation::returnLogOverlap (SDSDOperation.cpp:65-72) */
+int afqmc_log_overlaps(afqmc_engine *e, double *out);
+/* G = conj(phiT) thetaT of one walker (SDSDOperation.cpp:74-89; spin for SD2is) */
+int afqmc_green_matrix(afqmc_engine *e, int walker, int spin, double *out);
+/* dynamicOrder statistics of LogHop2isSD2isOperation::print (logHop2isSD2isOperation.cpp:56-88) */
+int afqmc_taylor_stats(afqmc_engine *e, long long *calls, long long *total, int *min_order,
+                       int *max_order);
+/* OR of the per-walker status bits since creation (1 singular overlap,
+ * 2 non-finite value, 4 Taylor order cap, 8 zero column norm, 16 comb) */
+int afqmc_status(afqmc_engine *e, int *status_or);
+
+/* Phase profiler: CUDA events around each phase of the step on the engine's
+ * stream (replaces the reference's 1-second TimerHao, common/timeHao/include/
+ * time_hao.h:16-41).  Enabling resets the totals; afqmc_profile_get writes
+ * AFQMC_NPHASES milliseconds totals and launch counts. */
+#define AFQMC_NPHASES 12
+#define AFQMC_PH_OVERLAP 0     /* S = phiT^H phi */
+#define AFQMC_PH_LU 1          /* LU, log-det, inverse, first cos projection */
+#define AFQMC_PH_THETA 2       /* thetaT = S^-T phi^T */
+#define AFQMC_PH_FORCE 3       /* force (Hubbard G diagonal / Cholesky xbar) */
+#define AFQMC_PH_SAMPLE 4      /* aux-field sampling (+ Hubbard 2x2 apply) */
+#define AFQMC_PH_MBUILD 5      /* M = sqrt(-dt) sum_g x_g L_g */
+#define AFQMC_PH_TAYLOR 6      /* exp(M) phi */
+#define AFQMC_PH_ONEBODY 7     /* exp(-dt K) phi */
+#define AFQMC_PH_STABILIZE 8   /* modifyGM */
+#define AFQMC_PH_POPCONTROL 9  /* popControl */
+#define AFQMC_PH_EXCHANGE 10   /* exchange term of the measurement */
+#define AFQMC_PH_MEASURE 11    /* rest of the measurement */
+int afqmc_profile_enable(afqmc_engine *e, int on);
+/* Number of kernels this library has launched since it was loaded. */
+long long afqmc_launch_count(void);
+int afqmc_profile_get(afqmc_engine *e, double *ms, long long *counts);
+
+/* ---------------------------------------------------------------------------
+ * Stand-alone batched operations on device pointers (same layouts).
+ * ------------------------------------------------------------------------- */
+/* popConfiguration for one process (populationControlConfiguration.cpp:24-101)
+ * with explicit uniforms: weights, uniforms (W doubles each), table (W ints).
+ * stream is a cudaStream_t (may be NULL). */
+int afqmc_pop_configuration_dev(int W, const double *weights, const double *uniforms, int *table,
+                                void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFQMC_B200_H */
