@@ -26,7 +26,7 @@ SYMBOLS = [
     "afqmc_reset_measurement", "afqmc_add_mixed_measurement", "afqmc_get_measurement",
     "afqmc_get_cholesky_nums", "afqmc_pl_update_background", "afqmc_log_overlaps",
     "afqmc_green_matrix", "afqmc_taylor_stats", "afqmc_status", "afqmc_pop_configuration_dev",
-    "afqmc_profile_enable", "afqmc_profile_get", "afqmc_launch_count",
+    "afqmc_profile_enable", "afqmc_profile_get", "afqmc_launch_count", "afqmc_gemm_bf16_dev",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -87,6 +87,8 @@ def _declare(L):
     L.afqmc_profile_enable.argtypes = [P, I]
     L.afqmc_profile_get.argtypes = [P, P, P]
     L.afqmc_launch_count.argtypes = []
+    LL = ctypes.c_longlong
+    L.afqmc_gemm_bf16_dev.argtypes = [I, I, I, P, LL, P, LL, P, LL, I, I, LL, ctypes.c_float, P]
     for name in SYMBOLS[2:]:
         getattr(L, name).restype = I
     L.afqmc_launch_count.restype = ctypes.c_longlong
@@ -273,6 +275,13 @@ def pl_engine(m, W, seed, mgs_step=10, pop_step=10, force_type="dynamicForce",
                                  ctypes.byref(h)))
     return Engine(h.value, "pl", m.n, max(m.nup, m.ndn), W, G=m.G, nup=m.nup, ndn=m.ndn,
                   keep=keep)
+
+
+def gemm_bf16_dev(M, N, K, A, lda, B, ldb, C, ldc, out_bf16=False, splits=1, split_stride=0,
+                  alpha=1.0, stream=None):
+    """Device-pointer tcgen05 GEMM (see afqmc_gemm_bf16_dev)."""
+    _check(lib().afqmc_gemm_bf16_dev(M, N, K, A, lda, B, ldb, C, ldc, 1 if out_bf16 else 0, splits,
+                                     split_stride, alpha, stream))
 
 
 def launch_count():

@@ -22,6 +22,7 @@
 #include "common.cuh"
 #include "mixed.cuh"
 #include "walker_kernels.cuh"
+#include "tc_gemm.cuh"
 #include "zgemm.cuh"
 
 #include <atomic>
@@ -997,6 +998,31 @@ int afqmc_profile_get(afqmc_engine *e, double *ms, long long *counts)
         if (ms) ms[i] = e->profMs[i];
         if (counts) counts[i] = e->profCount[i];
     }
+    return AFQMC_OK;
+}
+
+int afqmc_gemm_bf16_dev(int M, int N, int K, const void *A, long long lda, const void *B,
+                        long long ldb, void *C, long long ldc, int out_bf16, int splits,
+                        long long split_stride, float alpha, void *stream)
+{
+    if (M < 0 || N < 0 || K <= 0 || !A || !B || !C || splits < 1) return fail(AFQMC_ERR_ARG, "bad argument");
+    if (splits > 1 && (K % (64 * splits)) != 0) return fail(AFQMC_ERR_ARG, "K must split into multiples of 64");
+    static int *derr = nullptr;
+    if (!derr) CUDA_TRY(cudaMalloc(&derr, sizeof(int)));
+    cudaStream_t s = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(int), s));
+    TcGemmArgs a;
+    a.M = M; a.N = N; a.K = K;
+    a.A = (const __nv_bfloat16 *)A; a.lda = lda;
+    a.B = (const __nv_bfloat16 *)B; a.ldb = ldb;
+    a.C = C; a.ldc = ldc; a.outType = out_bf16 ? TC_OUT_BF16 : TC_OUT_F32;
+    a.splits = splits; a.splitStride = split_stride; a.alpha = alpha; a.err = derr;
+    int r = tc_gemm_bf16(a, s);
+    if (r) return fail(AFQMC_ERR_CUDA, "tcgen05 gemm launch failed: " + std::to_string(r));
+    int h = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (h) return fail(AFQMC_ERR_CUDA, "tcgen05 gemm: barrier wait timed out");
     return AFQMC_OK;
 }
 

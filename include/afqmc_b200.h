@@ -204,6 +204,16 @@ int afqmc_profile_get(afqmc_engine *e, double *ms, long long *counts);
 int afqmc_pop_configuration_dev(int W, const double *weights, const double *uniforms, int *table,
                                 void *stream);
 
+/* Tensor-core (tcgen05) bf16 GEMM used by the mixed-precision form, the
+ * batched counterpart of gmm_cpu (tensor_2d_bl_cpu.cpp:61-75):
+ * C[m + n*ldc] = alpha * sum_k A[m*lda + k] * B[n*ldb + k]  (A, B bf16
+ * K-major; C fp32, or bf16 with out_bf16 != 0).  With splits > 1, K is cut
+ * into `splits` equal parts (multiples of 64) and part s is written at
+ * C + s*split_stride.  Synchronises `stream` before returning. */
+int afqmc_gemm_bf16_dev(int M, int N, int K, const void *A, long long lda, const void *B,
+                        long long ldb, void *C, long long ldc, int out_bf16, int splits,
+                        long long split_stride, float alpha, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
