@@ -20,9 +20,10 @@
 
 #include "../../include/afqmc_b200.h"
 #include "common.cuh"
+#include "engine_internal.cuh"
 #include "mixed.cuh"
-#include "walker_kernels.cuh"
 #include "tc_gemm.cuh"
+#include "walker_kernels.cuh"
 #include "zgemm.cuh"
 
 #include <atomic>
@@ -102,97 +103,6 @@ void exp2by2(double &a, double &b, cd &c)
 zd tozd(cd z) { return make_double2(z.real(), z.imag()); }
 
 }  // namespace
-
-enum { KIND_CP = 0, KIND_PL = 1 };
-
-struct afqmc_engine {
-    int kind = 0;
-    int n = 0, ncol = 0, nup = 0, ndn = 0, W = 0, L = 0, G = 0;
-    int precision = AFQMC_FP64;
-    int decomp = 0, forceType = 0;
-    double dt = 0, ET = 0, forceCap = 0;
-    int mgsStep = 1, popStep = 1, mgsIndex = 0, popIndex = 0;
-    uint64_t seed = 0;
-    cudaStream_t own = nullptr, stream = nullptr;
-    Blocks bl{};
-    long long wsize = 0;
-    zd logwT{0, 0};
-    zd *phiT[2] = {nullptr, nullptr};
-    // population and workspaces
-    zd *wf = nullptr, *wfTmp = nullptr, *term[2] = {nullptr, nullptr}, *logw = nullptr,
-       *logov = nullptr, *S = nullptr, *Sinv = nullptr, *thetaT = nullptr;
-    int *alive = nullptr, *surv = nullptr, *status = nullptr, *done = nullptr, *order = nullptr,
-        *table = nullptr, *number = nullptr;
-    unsigned long long *counter = nullptr, *offs = nullptr;
-    double *weight = nullptr;
-    long long *tstats = nullptr;
-    // one-body operators: 0 exp(-dt K), 1 exp(+dt/2 K), 2 exp(-dt/2 K)
-    zd *expK[3] = {nullptr, nullptr, nullptr};
-    zd expLogw[3] = {{0, 0}, {0, 0}, {0, 0}};
-    bool useLog = false;
-    zd *logK = nullptr;
-    zd logKLogw{0, 0};
-    // Hubbard
-    HubbardDev hd{};
-    zd *gamma = nullptr, *cdiag[4] = {nullptr, nullptr, nullptr, nullptr};
-    double *U = nullptr, *mu = nullptr, *hx = nullptr, *hy = nullptr, *hz = nullptr,
-           *constForceCP = nullptr, *forceCP = nullptr;
-    zd *wfDaggerK = nullptr;
-    // phaseless
-    CholDev cdv{};
-    double *chol = nullptr, *bg = nullptr;
-    zd *Aall = nullptr, *wfDaggerT = nullptr, *xbar = nullptr, *forcePL = nullptr, *aux = nullptr,
-       *M = nullptr, *ex = nullptr, *constForcePL = nullptr;
-    long long Ktot = 0;
-    // measurement
-    zd *acc = nullptr, *bgNum = nullptr, *exNum = nullptr, *eloc = nullptr, *den = nullptr,
-       *parts = nullptr;
-    // mixed-precision state
-    MixedState *mx = nullptr;
-    // phase profiler (CUDA events on the engine stream; off unless enabled)
-    bool prof = false;
-    struct Mark { int phase; cudaEvent_t a, b; };
-    std::vector<Mark> marks;
-    std::vector<cudaEvent_t> evpool;
-    double profMs[AFQMC_NPHASES] = {};
-    long long profCount[AFQMC_NPHASES] = {};
-    std::vector<void *> allocs;
-};
-
-// Phase timing: record an event pair around a phase when profiling is on.
-struct PhaseScope {
-    afqmc_engine *e; int phase; cudaEvent_t a = nullptr;
-    PhaseScope(afqmc_engine *e_, int p) : e(e_), phase(p)
-    {
-        if (!e->prof) return;
-        if (e->evpool.empty()) cudaEventCreate(&a); else { a = e->evpool.back(); e->evpool.pop_back(); }
-        cudaEventRecord(a, e->stream);
-    }
-    ~PhaseScope()
-    {
-        if (!e->prof) return;
-        cudaEvent_t b;
-        if (e->evpool.empty()) cudaEventCreate(&b); else { b = e->evpool.back(); e->evpool.pop_back(); }
-        cudaEventRecord(b, e->stream);
-        e->marks.push_back({phase, a, b});
-    }
-};
-#define PHASE(p) PhaseScope _ps_##p(e, p)
-
-static void prof_resolve(afqmc_engine *e)
-{
-    if (e->marks.empty()) return;
-    cudaStreamSynchronize(e->stream);
-    for (auto &m : e->marks) {
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, m.a, m.b);
-        e->profMs[m.phase] += ms;
-        e->profCount[m.phase] += 1;
-        e->evpool.push_back(m.a);
-        e->evpool.push_back(m.b);
-    }
-    e->marks.clear();
-}
 
 namespace {
 
@@ -460,7 +370,7 @@ int modify_gm(afqmc_engine *e)
 int pop_control(afqmc_engine *e)
 {
     PHASE(AFQMC_PH_POPCONTROL);
-    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    if (e->precision == AFQMC_MIXED) return mixed_pop_control(e);
     TRY(overlap_gemm(e, e->wf, e->alive));
     launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
                              e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
@@ -468,9 +378,7 @@ int pop_control(afqmc_engine *e)
     launch_pop_comb(e->W, e->weight, nullptr, e->seed, e->counter, e->number, e->table,
                     e->status + e->W, e->stream);
     launch_pop_gather(e->W, e->wsize, e->table, e->wf, e->logw, e->stream);
-    TRY(check_launch());
-    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
-    return AFQMC_OK;
+    return check_launch();
 }
 
 int project_one_step(afqmc_engine *e)
@@ -544,6 +452,17 @@ void free_engine(afqmc_engine *e)
 }
 
 }  // namespace
+
+int engine_fail(int code, const std::string &msg) { return fail(code, msg); }
+int engine_check_launch() { return check_launch(); }
+int engine_gemm(const ZGemmArgs &a, cudaStream_t s) { return gemm(a, s); }
+template <class T> int engine_dalloc(afqmc_engine *e, T **p, size_t count) { return dalloc(e, p, count); }
+template int engine_dalloc<float>(afqmc_engine *, float **, size_t);
+template int engine_dalloc<int>(afqmc_engine *, int **, size_t);
+template int engine_dalloc<zd>(afqmc_engine *, zd **, size_t);
+template int engine_dalloc<double>(afqmc_engine *, double **, size_t);
+template int engine_dalloc<unsigned short>(afqmc_engine *, unsigned short **, size_t);
+zd engine_one_body_logw(afqmc_engine *e, int which) { return one_body_logw(e, which); }
 
 // =========================================================== C ABI
 extern "C" {

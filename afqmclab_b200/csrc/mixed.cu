@@ -1,15 +1,762 @@
-// Mixed-precision form (work in progress): not yet constructible.
-#include <string>
+// Mixed-precision form of the phaseless walker step.
+//
+// Walkers are stored as complex fp32 (planar: real plane then imaginary
+// plane, each n x ncol column-major).  The dense contractions run on the
+// tcgen05 tensor cores in bf16 with fp32 accumulation:
+//   force      xbar = A^T Theta            (calculateCholeskyBg, :237-256)
+//   two-body   M = sqrt(-dt) sum_g x_g L_g (CholeskyReal::setTwoBodySampleMatrix)
+//   Taylor     exp(M) phi, all orders in one kernel (LogHop2isSD2isOperation)
+//   one-body   exp(-dt K) phi = phi + (exp(-dt K) - 1) phi
+// while the overlap matrices, their LU / log-determinant / inverse, the phase
+// and cos projections, the weights, population control and the Gram-Schmidt
+// re-orthonormalisation stay in FP64 (FP64 arithmetic on the fp32 walker).
+#include <cuda_bf16.h>
 
-#include "../../include/afqmc_b200.h"
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "engine_internal.cuh"
 #include "mixed.cuh"
+#include "tc_common.cuh"
+#include "tc_gemm.cuh"
 
-int mixed_create(afqmc_engine *) { return AFQMC_ERR_UNSUPPORTED; }
-void mixed_destroy(afqmc_engine *) {}
-int mixed_project_dtk_dtv(afqmc_engine *) { return AFQMC_ERR_UNSUPPORTED; }
-int mixed_modify_gm(afqmc_engine *) { return AFQMC_ERR_UNSUPPORTED; }
-int mixed_add_measurement(afqmc_engine *) { return AFQMC_ERR_UNSUPPORTED; }
-int mixed_update_operators(afqmc_engine *) { return AFQMC_ERR_UNSUPPORTED; }
-int mixed_sync_to_fp64(afqmc_engine *) { return AFQMC_OK; }
-int mixed_sync_from_fp64(afqmc_engine *) { return AFQMC_OK; }
-int mixed_status(afqmc_engine *) { return 0; }
+struct MixedState {
+    float *wf32 = nullptr, *tmp32 = nullptr;
+    __nv_bfloat16 *Theta = nullptr, *Abig = nullptr, *Y = nullptr, *Lt = nullptr, *Mbuf = nullptr,
+                  *Et = nullptr;
+    float *xbarp = nullptr;
+    zd *wfDaggerTm = nullptr;
+    int *err = nullptr;
+    int splits = 1;
+    long long ws32 = 0;  // floats per walker (2 n ncol)
+    bool ready = false;
+};
+
+namespace {
+
+#define MTRY(expr)                   \
+    do {                             \
+        int _r = (expr);             \
+        if (_r != AFQMC_OK) return _r; \
+    } while (0)
+
+int cuda_check(cudaError_t r, const char *what)
+{
+    if (r != cudaSuccess) return engine_fail(AFQMC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(r));
+    return AFQMC_OK;
+}
+
+// ------------------------------------------------------------ setup kernels
+// Force operand, K-major rows: [Re; Im] outputs x [Re; Im] inputs of the
+// complex product xbar_g = sum_k A_gk Theta_k with Theta stored per spin as
+// theta(i, b) at tOff + i + n b (b = electron, i = orbital).
+__global__ void build_abig_kernel(int G, long long Ktot, int n, Blocks bl, const zd *Aall,
+                                  __nv_bfloat16 *Abig)
+{
+    const long long K2 = 2 * Ktot;
+    const long long total = (long long)G * Ktot;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        int g = (int)(e / Ktot);
+        long long kap = e % Ktot;
+        int b = bl.nblk > 1 && kap >= bl.tOff[1] ? 1 : 0;
+        long long r = kap - bl.tOff[b];
+        int Ns = bl.Ns[b];
+        int i = (int)(r % n), bb = (int)(r / n);
+        zd a = Aall[(size_t)g * Ktot + bl.tOff[b] + bb + (size_t)Ns * i];
+        Abig[(size_t)g * K2 + kap] = __double2bfloat16(a.x);
+        Abig[(size_t)g * K2 + Ktot + kap] = __double2bfloat16(-a.y);
+        Abig[(size_t)(G + g) * K2 + kap] = __double2bfloat16(a.y);
+        Abig[(size_t)(G + g) * K2 + Ktot + kap] = __double2bfloat16(a.x);
+    }
+}
+
+// L_g transposed to K-major rows: Lt[m * G + g] = chol[m + n^2 g]
+__global__ void build_lt_kernel(long long n2, int G, const double *chol, __nv_bfloat16 *Lt)
+{
+    const long long total = n2 * G;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long m = e / G;
+        int g = (int)(e % G);
+        Lt[e] = __double2bfloat16(chol[m + n2 * g]);
+    }
+}
+
+// (exp(-dt K) - 1) as a K-major bf16 operand: Et[i n + j] = E(i, j) - delta_ij
+__global__ void build_et_kernel(int n, const zd *E, __nv_bfloat16 *Et)
+{
+    const int total = n * n;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        int i = e / n, j = e % n;
+        double v = E[i + (size_t)n * j].x - (i == j ? 1.0 : 0.0);
+        Et[e] = __double2bfloat16(v);
+    }
+}
+
+// wfDaggerT permuted from the (b + Ns i) to the (i + n b) layout of each block
+__global__ void permute_wdt_kernel(int n, Blocks bl, const zd *src, zd *dst)
+{
+    for (int b = 0; b < bl.nblk; ++b) {
+        int Ns = bl.Ns[b];
+        for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Ns * n; e += gridDim.x * blockDim.x) {
+            int i = e % n, bb = e / n;
+            dst[bl.tOff[b] + e] = src[bl.tOff[b] + bb + (size_t)Ns * i];
+        }
+    }
+}
+
+// ---------------------------------------------------------- walker storage
+__global__ void wf_to_f32p_kernel(int W, long long wsize, const zd *wf, float *w32, const int *mask)
+{
+    const int w = blockIdx.x;
+    if (mask && !mask[w]) return;
+    for (long long e = threadIdx.x; e < wsize; e += blockDim.x) {
+        zd v = wf[(size_t)w * wsize + e];
+        w32[(size_t)w * 2 * wsize + e] = (float)v.x;
+        w32[(size_t)w * 2 * wsize + wsize + e] = (float)v.y;
+    }
+}
+__global__ void f32p_to_wf_kernel(int W, long long wsize, const float *w32, zd *wf, const int *mask)
+{
+    const int w = blockIdx.x;
+    if (mask && !mask[w]) return;
+    for (long long e = threadIdx.x; e < wsize; e += blockDim.x)
+        wf[(size_t)w * wsize + e] = make_double2(w32[(size_t)w * 2 * wsize + e],
+                                                 w32[(size_t)w * 2 * wsize + wsize + e]);
+}
+
+// populationControl<T> in-place copies of fp32 walkers (populationControl.h:110-117)
+__global__ void gather32_kernel(int W, long long ws32, const int *table, float *w32, zd *logw)
+{
+    const int i = blockIdx.x;
+    const int j = table[i];
+    if (j == i || j < 0) return;
+    const float4 *src = (const float4 *)(w32 + (size_t)j * ws32);
+    float4 *dst = (float4 *)(w32 + (size_t)i * ws32);
+    for (long long e = threadIdx.x; e < ws32 / 4; e += blockDim.x) dst[e] = src[e];
+    if (threadIdx.x == 0) logw[i] = logw[j];
+}
+
+// Gram-Schmidt (SD2is::stabilize, SD2is.cpp:48-76) in FP64 on an fp32 walker
+__global__ void __launch_bounds__(256)
+mgs32_kernel(int W, int n, int ncol, int nup, int ndn, float *w32, zd *logw, const int *alive,
+             int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (alive && !alive[w]) return;
+    zd *A = (zd *)smem_raw;
+    float *g = w32 + (size_t)w * 2 * n * ncol;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    const long long ws = (long long)n * ncol;
+    for (long long e = tid; e < ws; e += nt) A[e] = make_double2(g[e], g[ws + e]);
+    __syncthreads();
+    const int nmin = nup < ndn ? nup : ndn;
+    double logR = 0.0, logRmin = 0.0;
+    int bad = 0;
+    for (int j = 0; j < ncol; ++j) {
+        double s = 0.0;
+        for (int i = tid; i < n; i += nt) { zd v = A[i + (size_t)n * j]; s += v.x * v.x + v.y * v.y; }
+        s = block_sum(s, red);
+        double r = sqrt(s);
+        if (r == 0.0) bad = 1;
+        double inv = r > 0.0 ? 1.0 / r : 0.0;
+        for (int i = tid; i < n; i += nt) A[i + (size_t)n * j] = zscale(A[i + (size_t)n * j], inv);
+        if (tid == 0) {
+            double lr = log(r);
+            logR += lr;
+            if (j < nmin) logRmin += lr;
+        }
+        __syncthreads();
+        for (int c = j + 1 + wid; c < ncol; c += nw) {
+            zd d = make_double2(0.0, 0.0);
+            for (int i = lane; i < n; i += 32) zfma(d, zconj(A[i + (size_t)n * j]), A[i + (size_t)n * c]);
+            d.x = warp_sum(d.x);
+            d.y = warp_sum(d.y);
+            for (int i = lane; i < n; i += 32) {
+                zd q = A[i + (size_t)n * j], v = A[i + (size_t)n * c];
+                v.x -= d.x * q.x - d.y * q.y;
+                v.y -= d.x * q.y + d.y * q.x;
+                A[i + (size_t)n * c] = v;
+            }
+        }
+        __syncthreads();
+    }
+    for (long long e = tid; e < ws; e += nt) { g[e] = (float)A[e].x; g[ws + e] = (float)A[e].y; }
+    if (tid == 0) {
+        zd lw = logw[w];
+        if (nup == ndn) lw.x += 2.0 * logR;
+        else lw.x += logR + logRmin;
+        logw[w] = lw;
+        if (bad && status) atomicOr(status + w, (int)ST_ZERO_NORM);
+    }
+}
+
+// Phaseless force from the tensor-core xbar partials, aux sampling, sample
+// log-weight and second cos projection (same arithmetic as the FP64 form),
+// writing y = sqrt(-dt) x as the bf16 operand of the two-body GEMM.
+__global__ void __launch_bounds__(256)
+mixed_sample_kernel(int W, CholDev c, const float *xbarp, int splits, long long splitStride,
+                    int *surv, int *alive, const unsigned long long *offs, uint64_t seed,
+                    __nv_bfloat16 *Y, zd *logw, double dtET, zd hopLogw)
+{
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (!surv[w]) return;
+    const int G = c.G;
+    zd f2 = make_double2(0, 0), xf = make_double2(0, 0), xb = make_double2(0, 0);
+    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+        zd f;
+        if (c.constForce) {
+            f = c.constForce[g];
+        } else {
+            double xr = 0.0, xi = 0.0;
+            for (int s = 0; s < splits; ++s) {
+                xr += xbarp[s * splitStride + g + (size_t)2 * G * w];
+                xi += xbarp[s * splitStride + G + g + (size_t)2 * G * w];
+            }
+            double a = xr - c.bg[g], b = xi;
+            f = make_double2(-b * c.sqrtDt, a * c.sqrtDt);
+            double af = zabs(f);
+            if (af > c.forceCap) f = make_double2(f.x * c.forceCap / af, f.y * c.forceCap / af);
+        }
+        double gs = rng_gaussian(seed, offs[w] + 2ULL * g);
+        zd x = make_double2(gs + f.x, f.y);
+        Y[(size_t)(2 * w) * G + g] = __double2bfloat16(-c.sqrtDt * x.y);
+        Y[(size_t)(2 * w + 1) * G + g] = __double2bfloat16(c.sqrtDt * x.x);
+        zfma(f2, f, f);
+        zfma(xf, x, f);
+        zfma(xb, x, make_double2(c.bg[g], 0.0));
+    }
+    f2 = block_zsum(f2, red);
+    xf = block_zsum(xf, red);
+    xb = block_zsum(xb, red);
+    if (threadIdx.x == 0) {
+        double phase = xf.y;
+        double cs = cos(phase);
+        if (cs <= 0.0) {
+            alive[w] = 0; surv[w] = 0;
+        } else {
+            zd lw = logw[w];
+            lw.x += log(cs);
+            zd smp = zsub(zscale(f2, 0.5), xf);
+            smp = zsub(smp, make_double2(-c.sqrtDt * xb.y, c.sqrtDt * xb.x));
+            zd t = zadd(smp, lw);
+            t.x += dtET;
+            logw[w] = zadd(hopLogw, t);
+        }
+    }
+}
+
+// sum of the xbar partials -> FP64 complex xbar (G x W), for the measurement
+__global__ void xbar_combine_kernel(int G, int W, const float *xbarp, int splits,
+                                    long long splitStride, zd *xbar)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < (long long)G * W;
+         e += (long long)gridDim.x * blockDim.x) {
+        int g = (int)(e % G), w = (int)(e / G);
+        double xr = 0.0, xi = 0.0;
+        for (int s = 0; s < splits; ++s) {
+            xr += xbarp[s * splitStride + g + (size_t)2 * G * w];
+            xi += xbarp[s * splitStride + G + g + (size_t)2 * G * w];
+        }
+        xbar[e] = make_double2(xr, xi);
+    }
+}
+
+// ------------------------------------------------------------ Taylor kernel
+// One walker at a time per CTA (persistent over walkers).  The walker's
+// row i lives in thread i (fp32 accumulators); the current Taylor term is
+// the bf16 B operand in shared memory (K-major core matrices), M (bf16
+// planes, 128B-swizzled by TMA) the A operand; the complex product uses two
+// TMEM accumulators (real / imaginary rows) and the descriptor's A-negate
+// bit for -Im(M) Im(term).  After the series converges the one-body
+// operator (exp(-dt K) - 1, real) is applied the same way and the walker is
+// written back in place.  Rows beyond n (n = 64) are padding.
+template <int NC>
+struct TaylorSmem {
+    static constexpr size_t b_plane(int n) { return (size_t)NC * n * 2; }
+    static constexpr size_t bytes(int n)
+    {
+        return 1024 + (size_t)2 * (n / 64) * 16384 + 2 * b_plane(n) + 64;
+    }
+};
+
+__device__ __forceinline__ void store_b_bf16(uint8_t *sB, int n, int a, int i, float v)
+{
+    const uint32_t off = (uint32_t)(a >> 3) * (uint32_t)(n * 16) + (uint32_t)(i >> 3) * 128u +
+                         (uint32_t)(a & 7) * 16u + (uint32_t)(i & 7) * 2u;
+    *(__nv_bfloat16 *)(sB + off) = __float2bfloat16_rn(v);
+}
+
+template <int NC>
+__global__ void __launch_bounds__(128, 1)
+taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmE,
+                      int W, int n, float *w32, const int *surv, int *order, int kmax, float acc,
+                      int checkFrom, int doOneBody, int *status, int *err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const int KB = n / 64;
+    uint8_t *sMr = base;
+    uint8_t *sMi = base + KB * 16384;
+    uint8_t *sBr = base + 2 * KB * 16384;
+    uint8_t *sBi = sBr + (size_t)NC * n * 2;
+    uint64_t *bars = (uint64_t *)(sBi + (size_t)NC * n * 2);
+    uint32_t *tslot = (uint32_t *)(bars + 2);
+    __shared__ float red[4];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int row = tid;
+    const bool rowOK = row < n;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+        tma_prefetch_desc(&tmM);
+        tma_prefetch_desc(&tmE);
+    }
+    if (warp == 0) { tmem_alloc(tslot, 128); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tm = *tslot;
+    const uint32_t tCr = tm, tCi = tm + 64;
+    const uint32_t lanebase = (uint32_t)(warp * 32) << 16;
+    constexpr uint32_t IDESC = idesc_bf16(128, NC);
+    constexpr uint32_t IDESCN = idesc_bf16(128, NC, true);
+    const uint32_t LBO = 128, SBO = (uint32_t)n * 16;
+    uint32_t phL = 0, phD = 0;
+    bool ok = true;
+
+    auto issue = [&](bool complexA) {
+        // C_r (+)= Ar Br - Ai Bi ; C_i (+)= Ai Br + Ar Bi  (Ai absent for the real one-body)
+        tc_fence_after();
+        for (int kk = 0; kk < n / 16; ++kk) {
+            const uint32_t kb = kk >> 2, ko = (kk & 3) * 32;
+            const uint64_t aR = desc_k_sw128(smem_u32(sMr + kb * 16384) + ko);
+            const uint64_t aI = desc_k_sw128(smem_u32(sMi + kb * 16384) + ko);
+            const uint64_t bR = desc_k_noswz(smem_u32(sBr) + kk * 256, LBO, SBO);
+            const uint64_t bI = desc_k_noswz(smem_u32(sBi) + kk * 256, LBO, SBO);
+            umma_bf16(tCr, aR, bR, IDESC, kk > 0 ? 1u : 0u);
+            umma_bf16(tCi, aR, bI, IDESC, kk > 0 ? 1u : 0u);
+            if (complexA) {
+                umma_bf16(tCr, aI, bI, IDESCN, 1u);
+                umma_bf16(tCi, aI, bR, IDESC, 1u);
+            }
+        }
+        umma_commit(&bars[1]);
+    };
+
+    float pr[NC], pi[NC];
+    for (int w = blockIdx.x; w < W && ok; w += gridDim.x) {
+        if (!surv[w]) continue;
+        if (tid == 0) {
+            mbar_arrive_expect_tx(&bars[0], (uint32_t)(2 * KB * 16384));
+            for (int kb = 0; kb < KB; ++kb) {
+                tma_load_2d(sMr + kb * 16384, &tmM, &bars[0], kb * 64, (2 * w) * n);
+                tma_load_2d(sMi + kb * 16384, &tmM, &bars[0], kb * 64, (2 * w + 1) * n);
+            }
+        }
+        float *gw = w32 + (size_t)w * 2 * n * NC;
+#pragma unroll
+        for (int a = 0; a < NC; ++a) {
+            pr[a] = rowOK ? gw[row + (size_t)n * a] : 0.f;
+            pi[a] = rowOK ? gw[(size_t)n * NC + row + (size_t)n * a] : 0.f;
+            if (rowOK) { store_b_bf16(sBr, n, a, row, pr[a]); store_b_bf16(sBi, n, a, row, pi[a]); }
+        }
+        fence_proxy_async();
+        tc_fence_before();
+        __syncthreads();
+        ok = __syncthreads_and(mbar_wait(&bars[0], phL)) != 0;
+        phL ^= 1;
+        if (!ok) break;
+        int k = 0;
+        while (true) {
+            ++k;
+            if (tid == 0) issue(true);
+            ok = __syncthreads_and(mbar_wait(&bars[1], phD)) != 0;
+            phD ^= 1;
+            if (!ok) break;
+            tc_fence_after();
+            const float inv = 1.0f / (float)k;
+            float mx = 0.f;
+#pragma unroll
+            for (int c0 = 0; c0 < NC; c0 += 32) {
+                float vr[32], vi[32];
+                tmem_ld32(tCr + lanebase + c0, vr);
+                tmem_ld32(tCi + lanebase + c0, vi);
+#pragma unroll
+                for (int a = 0; a < 32; ++a) {
+                    if (c0 + a < NC) {
+                        const float tr = vr[a] * inv, ti = vi[a] * inv;
+                        pr[c0 + a] += tr;
+                        pi[c0 + a] += ti;
+                        if (rowOK) {
+                            mx = fmaxf(mx, tr * tr + ti * ti);
+                            store_b_bf16(sBr, n, c0 + a, row, tr);
+                            store_b_bf16(sBi, n, c0 + a, row, ti);
+                        }
+                    }
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            if (lane == 0) red[warp] = mx;
+            fence_proxy_async();
+            tc_fence_before();
+            __syncthreads();
+            const float m4 = fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]));
+            const bool conv = (k >= checkFrom) && (sqrtf(m4) <= acc);
+            if (conv || k >= kmax) {
+                if (!conv && tid == 0 && status) atomicOr(status + w, (int)ST_TAYLOR_CAP);
+                break;
+            }
+            __syncthreads();  // red[] is rewritten by the next order
+        }
+        if (!ok) break;
+        if (doOneBody) {
+            // one-body operator into the M buffer, current walker as operand
+            if (tid == 0) {
+                mbar_arrive_expect_tx(&bars[0], (uint32_t)(KB * 16384));
+                for (int kb = 0; kb < KB; ++kb) tma_load_2d(sMr + kb * 16384, &tmE, &bars[0], kb * 64, 0);
+            }
+#pragma unroll
+            for (int a = 0; a < NC; ++a)
+                if (rowOK) { store_b_bf16(sBr, n, a, row, pr[a]); store_b_bf16(sBi, n, a, row, pi[a]); }
+            fence_proxy_async();
+            tc_fence_before();
+            __syncthreads();
+            ok = __syncthreads_and(mbar_wait(&bars[0], phL)) != 0;
+            phL ^= 1;
+            if (!ok) break;
+            if (tid == 0) issue(false);
+            ok = __syncthreads_and(mbar_wait(&bars[1], phD)) != 0;
+            phD ^= 1;
+            if (!ok) break;
+            tc_fence_after();
+#pragma unroll
+            for (int c0 = 0; c0 < NC; c0 += 32) {
+                float vr[32], vi[32];
+                tmem_ld32(tCr + lanebase + c0, vr);
+                tmem_ld32(tCi + lanebase + c0, vi);
+#pragma unroll
+                for (int a = 0; a < 32; ++a)
+                    if (c0 + a < NC) { pr[c0 + a] += vr[a]; pi[c0 + a] += vi[a]; }
+            }
+        }
+        if (rowOK) {
+#pragma unroll
+            for (int a = 0; a < NC; ++a) {
+                gw[row + (size_t)n * a] = pr[a];
+                gw[(size_t)n * NC + row + (size_t)n * a] = pi[a];
+            }
+        }
+        if (tid == 0) order[w] = k;
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (!ok && err) atomicExch(err, 2);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tm, 128);
+}
+
+template <int NC>
+int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE, int doOneBody)
+{
+    const size_t smem = TaylorSmem<NC>::bytes(e->n);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(taylor_onebody_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TaylorSmem<NC>::bytes(128));
+        attr = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int grid = std::min(e->W, 2 * sms);
+    taylor_onebody_kernel<NC><<<grid, 128, smem, e->stream>>>(
+        mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, 30, 1e-10f, 4, doOneBody, e->status,
+        e->mx->err);
+    return engine_check_launch();
+}
+
+int run_taylor(afqmc_engine *e)
+{
+    MixedState *m = e->mx;
+    CUtensorMap mM, mE;
+    int r = tc_make_map_bf16(&mM, m->Mbuf, e->n, (long long)2 * e->W * e->n, e->n, 128);
+    if (r) return engine_fail(AFQMC_ERR_CUDA, "tensor map (M): " + std::to_string(r));
+    r = tc_make_map_bf16(&mE, m->Et, e->n, e->n, e->n, 128);
+    if (r) return engine_fail(AFQMC_ERR_CUDA, "tensor map (E): " + std::to_string(r));
+    switch (e->ncol) {
+    case 16: return launch_taylor<16>(e, mM, mE, 1);
+    case 32: return launch_taylor<32>(e, mM, mE, 1);
+    case 48: return launch_taylor<48>(e, mM, mE, 1);
+    case 64: return launch_taylor<64>(e, mM, mE, 1);
+    default: return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed Taylor kernel needs 16, 32, 48 or 64 columns");
+    }
+}
+
+int tc(afqmc_engine *e, TcGemmArgs a)
+{
+    a.err = e->mx->err;
+    int r = tc_gemm_bf16(a, e->stream);
+    if (r) return engine_fail(AFQMC_ERR_CUDA, "tcgen05 gemm: " + std::to_string(r));
+    return AFQMC_OK;
+}
+
+// S_b = phiT_b^H phi_b in FP64 from the fp32 walkers
+int overlap32(afqmc_engine *e, const float *w32, const int *mask)
+{
+    for (int b = 0; b < e->bl.nblk; ++b) {
+        int Ns = e->bl.Ns[b];
+        if (Ns == 0) continue;
+        ZGemmArgs g;
+        g.m = Ns; g.n = Ns; g.k = e->n;
+        g.opA = OP_C; g.opB = OP_N;
+        g.A = e->phiT[b]; g.lda = e->n;
+        g.B = w32; g.ldb = e->n; g.strideB = e->mx->ws32; g.b_real = ST_C32P;
+        g.planeB = (long long)e->n * e->ncol;
+        g.C = e->S + e->bl.sOff[b]; g.ldc = Ns; g.strideC = e->bl.sStride;
+        g.batch = e->W; g.mask = mask;
+        MTRY(engine_gemm(g, e->stream));
+    }
+    return AFQMC_OK;
+}
+
+// theta_b = phi_b S_b^{-1} (n x Ns) -> bf16 planar Theta (+ FP64 copy when thetaZ)
+int theta32(afqmc_engine *e, const float *w32, const int *mask, zd *thetaZ)
+{
+    MixedState *m = e->mx;
+    for (int b = 0; b < e->bl.nblk; ++b) {
+        int Ns = e->bl.Ns[b];
+        if (Ns == 0) continue;
+        ZGemmArgs g;
+        g.m = e->n; g.n = Ns; g.k = Ns;
+        g.A = w32; g.lda = e->n; g.strideA = m->ws32; g.a_real = ST_C32P;
+        g.planeA = (long long)e->n * e->ncol;
+        g.B = e->Sinv + e->bl.sOff[b]; g.ldb = Ns; g.strideB = e->bl.sStride;
+        g.C = thetaZ ? thetaZ + e->bl.tOff[b] : nullptr; g.ldc = e->n; g.strideC = e->bl.tStride;
+        g.outMode = OUT_BF16P;
+        g.C2 = m->Theta + e->bl.tOff[b]; g.ldc2 = e->n; g.strideC2 = 2 * e->Ktot; g.plane2 = e->Ktot;
+        g.batch = e->W; g.mask = mask;
+        MTRY(engine_gemm(g, e->stream));
+    }
+    return AFQMC_OK;
+}
+
+int force_tc(afqmc_engine *e)
+{
+    MixedState *m = e->mx;
+    TcGemmArgs a;
+    a.M = 2 * e->G; a.N = e->W; a.K = (int)(2 * e->Ktot);
+    a.A = m->Abig; a.lda = 2 * e->Ktot;
+    a.B = m->Theta; a.ldb = 2 * e->Ktot;
+    a.C = m->xbarp; a.ldc = 2 * e->G; a.outType = TC_OUT_F32;
+    a.splits = m->splits; a.splitStride = (long long)2 * e->G * e->W;
+    return tc(e, a);
+}
+
+int check_err(afqmc_engine *e)
+{
+    (void)e;
+    return engine_check_launch();
+}
+
+}  // namespace
+
+int mixed_create(afqmc_engine *e)
+{
+    if (e->kind != KIND_PL) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form is built for the phaseless engine");
+    if (e->n != 64 && e->n != 128) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form needs n = 64 or 128");
+    if (e->ncol % 16 != 0 || e->ncol > 64) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form needs 16..64 columns in steps of 16");
+    if (e->G % 64 != 0) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form needs G a multiple of 64");
+    if (e->useLog || !e->expK[0]) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form needs the dense exp(-dt K) operator");
+    MixedState *m = new MixedState();
+    e->mx = m;
+    const int W = e->W, n = e->n, G = e->G;
+    m->ws32 = (long long)2 * n * e->ncol;
+    const long long Ktot = e->Ktot;
+    m->splits = (2 * Ktot) % (64 * 4) == 0 ? 4 : 1;
+    MTRY(engine_dalloc(e, &m->wf32, (size_t)W * m->ws32));
+    MTRY(engine_dalloc(e, &m->tmp32, (size_t)W * m->ws32));
+    MTRY(engine_dalloc(e, (unsigned short **)&m->Theta, (size_t)W * 2 * Ktot));
+    MTRY(engine_dalloc(e, (unsigned short **)&m->Abig, (size_t)2 * G * 2 * Ktot));
+    MTRY(engine_dalloc(e, (unsigned short **)&m->Y, (size_t)2 * W * G));
+    MTRY(engine_dalloc(e, (unsigned short **)&m->Lt, (size_t)n * n * G));
+    MTRY(engine_dalloc(e, (unsigned short **)&m->Mbuf, (size_t)2 * W * n * n));
+    MTRY(engine_dalloc(e, (unsigned short **)&m->Et, (size_t)n * n));
+    MTRY(engine_dalloc(e, &m->xbarp, (size_t)m->splits * 2 * G * W));
+    MTRY(engine_dalloc(e, &m->wfDaggerTm, (size_t)Ktot));
+    MTRY(engine_dalloc(e, &m->err, 1));
+    build_abig_kernel<<<1184, 256, 0, e->stream>>>(G, Ktot, n, e->bl, e->Aall, m->Abig);
+    build_lt_kernel<<<1184, 256, 0, e->stream>>>((long long)n * n, G, e->chol, m->Lt);
+    build_et_kernel<<<64, 256, 0, e->stream>>>(n, e->expK[0], m->Et);
+    permute_wdt_kernel<<<64, 256, 0, e->stream>>>(n, e->bl, e->wfDaggerT, m->wfDaggerTm);
+    MTRY(engine_check_launch());
+    // the dense one-body operator must be real for the bf16 one-body path
+    std::vector<zd> h((size_t)n * n);
+    MTRY(cuda_check(cudaMemcpyAsync(h.data(), e->expK[0], sizeof(zd) * n * n, cudaMemcpyDeviceToHost, e->stream), "copy"));
+    MTRY(cuda_check(cudaStreamSynchronize(e->stream), "sync"));
+    for (const zd &v : h)
+        if (v.y != 0.0) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision one-body needs a real exp(-dt K)");
+    m->ready = true;
+    return AFQMC_OK;
+}
+
+void mixed_destroy(afqmc_engine *e)
+{
+    delete e->mx;
+    e->mx = nullptr;
+}
+
+int mixed_update_operators(afqmc_engine *e)
+{
+    build_et_kernel<<<64, 256, 0, e->stream>>>(e->n, e->expK[0], e->mx->Et);
+    return engine_check_launch();
+}
+
+int mixed_sync_to_fp64(afqmc_engine *e)
+{
+    f32p_to_wf_kernel<<<e->W, 256, 0, e->stream>>>(e->W, e->wsize, e->mx->wf32, e->wf, nullptr);
+    return engine_check_launch();
+}
+
+int mixed_sync_from_fp64(afqmc_engine *e)
+{
+    wf_to_f32p_kernel<<<e->W, 256, 0, e->stream>>>(e->W, e->wsize, e->wf, e->mx->wf32, nullptr);
+    return engine_check_launch();
+}
+
+int mixed_status(afqmc_engine *e)
+{
+    int h = 0;
+    cudaMemcpy(&h, e->mx->err, sizeof(int), cudaMemcpyDeviceToHost);
+    return h ? 32 : 0;
+}
+
+int mixed_project_dtk_dtv(afqmc_engine *e)
+{
+    MixedState *m = e->mx;
+    const int W = e->W;
+    cudaStream_t s = e->stream;
+    const bool needTheta = (e->forceType == AFQMC_DYNAMIC_FORCE);
+    { PHASE(AFQMC_PH_OVERLAP); MTRY(overlap32(e, m->wf32, e->alive)); }
+    {
+        PHASE(AFQMC_PH_LU);
+        launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, make_double2(0, 0),
+                                 e->logwT, e->logov, e->alive, e->surv, e->logw, nullptr, e->status,
+                                 LU_PROJECT, needTheta, s);
+        MTRY(engine_check_launch());
+    }
+    if (needTheta) {
+        { PHASE(AFQMC_PH_THETA); MTRY(theta32(e, m->wf32, e->surv, nullptr)); }
+        { PHASE(AFQMC_PH_FORCE); MTRY(force_tc(e)); }
+    }
+    {
+        PHASE(AFQMC_PH_SAMPLE);
+        launch_rng_scan(W, e->surv, 2 * e->G, e->counter, e->offs, s);
+        mixed_sample_kernel<<<W, 256, 0, s>>>(W, e->cdv, m->xbarp, m->splits,
+                                             (long long)2 * e->G * W, e->surv, e->alive, e->offs,
+                                             e->seed, m->Y, e->logw, e->dt * e->ET,
+                                             engine_one_body_logw(e, 0));
+        MTRY(engine_check_launch());
+    }
+    {
+        PHASE(AFQMC_PH_MBUILD);
+        TcGemmArgs a;
+        a.M = e->n * e->n; a.N = 2 * W; a.K = e->G;
+        a.A = m->Lt; a.lda = e->G;
+        a.B = m->Y; a.ldb = e->G;
+        a.C = m->Mbuf; a.ldc = (long long)e->n * e->n; a.outType = TC_OUT_BF16;
+        MTRY(tc(e, a));
+    }
+    {
+        PHASE(AFQMC_PH_TAYLOR);
+        MTRY(run_taylor(e));
+        launch_taylor_stats(W, e->surv, e->order, e->tstats, s);
+    }
+    return check_err(e);
+}
+
+int mixed_modify_gm(afqmc_engine *e)
+{
+    const size_t bytes = (size_t)e->n * e->ncol * sizeof(zd);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(mgs32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        attr = true;
+    }
+    if (bytes > 160 * 1024) return engine_fail(AFQMC_ERR_UNSUPPORTED, "walker too large for the fp32 stabiliser");
+    mgs32_kernel<<<e->W, 256, bytes, e->stream>>>(e->W, e->n, e->ncol, e->nup, e->ndn, e->mx->wf32,
+                                                  e->logw, e->alive, e->status);
+    return engine_check_launch();
+}
+
+int mixed_pop_control(afqmc_engine *e)
+{
+    MixedState *m = e->mx;
+    MTRY(overlap32(e, m->wf32, e->alive));
+    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
+                             e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
+                             LU_POPWEIGHT, false, e->stream);
+    launch_pop_comb(e->W, e->weight, nullptr, e->seed, e->counter, e->number, e->table,
+                    e->status + e->W, e->stream);
+    gather32_kernel<<<e->W, 256, 0, e->stream>>>(e->W, m->ws32, e->table, m->wf32, e->logw);
+    return engine_check_launch();
+}
+
+// Exchange term of the mixed estimator from the FP64 theta (i + n b layout).
+int mixed_exchange(afqmc_engine *e)
+{
+    if (launch_pl_exchange(e->W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex,
+                           e->stream, 1))
+        return engine_fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
+    return engine_check_launch();
+}
+
+int mixed_add_measurement(afqmc_engine *e)
+{
+    MixedState *m = e->mx;
+    const int W = e->W;
+    cudaStream_t s = e->stream;
+    {
+        PHASE(AFQMC_PH_MEASURE);
+        // walkerTemp = exp(dt/2 K) walker (FP64 arithmetic, fp32 result)
+        ZGemmArgs g;
+        g.m = e->n; g.n = e->ncol; g.k = e->n;
+        g.A = e->expK[1]; g.lda = e->n; g.strideA = 0;
+        g.B = m->wf32; g.ldb = e->n; g.strideB = m->ws32; g.b_real = ST_C32P;
+        g.planeB = (long long)e->n * e->ncol;
+        g.C = nullptr; g.outMode = OUT_C32P;
+        g.C3 = m->tmp32; g.ldc3 = e->n; g.strideC3 = m->ws32; g.plane3 = (long long)e->n * e->ncol;
+        g.batch = W; g.mask = e->alive;
+        MTRY(engine_gemm(g, s));
+        MTRY(overlap32(e, m->tmp32, e->alive));
+        launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, engine_one_body_logw(e, 1),
+                                 e->logwT, e->logov, e->alive, nullptr, nullptr, nullptr,
+                                 e->status, LU_PLAIN, true, s);
+        MTRY(engine_check_launch());
+        MTRY(theta32(e, m->tmp32, e->alive, e->thetaT));
+        MTRY(force_tc(e));
+        xbar_combine_kernel<<<592, 256, 0, s>>>(e->G, W, m->xbarp, m->splits, (long long)2 * e->G * W, e->xbar);
+        MTRY(engine_check_launch());
+    }
+    {
+        PHASE(AFQMC_PH_EXCHANGE);
+        MTRY(mixed_exchange(e));
+    }
+    {
+        PHASE(AFQMC_PH_MEASURE);
+        launch_pl_energy(W, e->G, e->Ktot, m->wfDaggerTm, e->thetaT, e->xbar, e->ex, e->alive,
+                         e->logov, e->eloc, e->den, e->parts, s);
+        launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 1, e->acc, e->G, e->xbar,
+                              e->ex, e->bgNum, e->exNum, s);
+    }
+    return engine_check_launch();
+}

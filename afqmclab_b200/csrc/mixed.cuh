@@ -14,3 +14,5 @@ int mixed_update_operators(afqmc_engine *e);
 int mixed_sync_to_fp64(afqmc_engine *e);
 int mixed_sync_from_fp64(afqmc_engine *e);
 int mixed_status(afqmc_engine *e);
+int mixed_pop_control(afqmc_engine *e);
+int mixed_exchange(afqmc_engine *e);

@@ -21,10 +21,10 @@ constexpr int TC_BK = 64;
 constexpr int A_STAGE_BYTES = TC_BM * TC_BK * 2;
 
 template <int BN>
-constexpr int stages_for() { return BN >= 256 ? 4 : 6; }
+__host__ __device__ constexpr int stages_for() { return BN >= 256 ? 4 : 6; }
 
 template <int BN>
-constexpr size_t smem_bytes()
+__host__ __device__ constexpr size_t smem_bytes()
 {
     return 1024 + (size_t)stages_for<BN>() * (A_STAGE_BYTES + BN * TC_BK * 2) + 256;
 }

@@ -660,7 +660,7 @@ constexpr int EX_GCH = 16;
 // dynamic smem: As[Ns*EX_KC], Ts[Ns*EX_KC], Ds[Ns*Ns] for the largest block
 __global__ void __launch_bounds__(256)
 pl_exchange_kernel(int W, int n, int G, Blocks bl, const zd *Aall, long long Ktot,
-                   const zd *thetaT, const int *alive, zd *ex, int maxNs)
+                   const zd *thetaT, const int *alive, zd *ex, int maxNs, int thetaLayout)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     zd *As = (zd *)smem_raw;
@@ -686,7 +686,9 @@ pl_exchange_kernel(int W, int n, int G, Blocks bl, const zd *Aall, long long Kto
                 int kc = min(EX_KC, n - i0);
                 for (int e = tid; e < Ns * kc; e += nt) {
                     As[e] = A[(size_t)Ns * i0 + e];
-                    Ts[e] = T[(size_t)Ns * i0 + e];
+                    // thetaLayout 0: thetaT (b + Ns i); 1: theta (i + n b)
+                    Ts[e] = thetaLayout == 0 ? T[(size_t)Ns * i0 + e]
+                                             : T[(size_t)(i0 + e / Ns) + (size_t)n * (e % Ns)];
                 }
                 __syncthreads();
 #pragma unroll
@@ -911,7 +913,7 @@ void launch_cp_energy(int W, const HubbardDev &h, const zd *wfDaggerK, const zd 
 }
 
 int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, long long Ktot,
-                       const zd *thetaT, const int *alive, zd *ex, cudaStream_t s)
+                       const zd *thetaT, const int *alive, zd *ex, cudaStream_t s, int thetaLayout)
 {
     g_launch_count++;
     int maxNs = 0;
@@ -924,7 +926,8 @@ int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, lo
         attr = true;
     }
     dim3 grid(W, (G + EX_GCH - 1) / EX_GCH);
-    pl_exchange_kernel<<<grid, 256, smem, s>>>(W, n, G, bl, Aall, Ktot, thetaT, alive, ex, maxNs);
+    pl_exchange_kernel<<<grid, 256, smem, s>>>(W, n, G, bl, Aall, Ktot, thetaT, alive, ex, maxNs,
+                                                thetaLayout);
     return 0;
 }
 

@@ -78,7 +78,8 @@ void launch_cp_energy(int W, const HubbardDev &h, const zd *wfDaggerK, const zd 
 // Aall: column g = [A_g,up (Nup x n); A_g,dn (Ndn x n)] flattened (Ktot rows);
 // returns -1 when a block is wider than 64 columns.
 int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, long long Ktot,
-                       const zd *thetaT, const int *alive, zd *ex, cudaStream_t s);
+                       const zd *thetaT, const int *alive, zd *ex, cudaStream_t s,
+                       int thetaLayout = 0);
 void launch_pl_energy(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
                       const zd *xbar, const zd *ex, const int *alive, const zd *logov, zd *eloc,
                       zd *den, zd *tloc, cudaStream_t s);

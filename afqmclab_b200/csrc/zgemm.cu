@@ -5,6 +5,8 @@
 // buffered), and column-major stores are coalesced along the row index.
 #include "zgemm.cuh"
 
+#include <cuda_bf16.h>
+
 #include <atomic>
 
 extern std::atomic<long long> g_launch_count;
@@ -13,19 +15,22 @@ namespace {
 
 constexpr int BK = 8;
 
-template <int OP, bool REAL>
-__device__ __forceinline__ zd load_op(const void *P, long long ld, int i, int l)
+template <int OP>
+__device__ __forceinline__ zd load_op(const void *P, long long ld, int i, int l, int kind,
+                                      long long plane)
 {
     // element (i, l) of op(P) where P is column-major with leading dimension ld
     long long idx = (OP == OP_N) ? (long long)i + (long long)l * ld : (long long)l + (long long)i * ld;
     zd v;
-    if (REAL) v = make_double2(__ldg((const double *)P + idx), 0.0);
+    if (kind == ST_R64) v = make_double2(__ldg((const double *)P + idx), 0.0);
+    else if (kind == ST_C32P) v = make_double2((double)__ldg((const float *)P + idx),
+                                               (double)__ldg((const float *)P + plane + idx));
     else v = __ldg((const zd *)P + idx);
     if (OP == OP_C) v.y = -v.y;
     return v;
 }
 
-template <int BM, int BN, int TM, int TN, int OPA, int OPB, bool AR, bool BR>
+template <int BM, int BN, int TM, int TN, int OPA, int OPB>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN))
 zgemm_kernel(ZGemmArgs a)
 {
@@ -37,9 +42,11 @@ zgemm_kernel(ZGemmArgs a)
     const int tileM = blockIdx.x * BM, tileN = blockIdx.y * BN;
     if (tileM >= a.m || tileN >= a.n) return;
 
-    const char *Ab = (const char *)a.A + (size_t)b * a.strideA * (AR ? sizeof(double) : sizeof(zd));
-    const char *Bb = (const char *)a.B + (size_t)b * a.strideB * (BR ? sizeof(double) : sizeof(zd));
-    zd *Cb = a.C + (size_t)b * a.strideC;
+    const size_t esA = a.a_real == ST_R64 ? sizeof(double) : a.a_real == ST_C32P ? sizeof(float) : sizeof(zd);
+    const size_t esB = a.b_real == ST_R64 ? sizeof(double) : a.b_real == ST_C32P ? sizeof(float) : sizeof(zd);
+    const char *Ab = (const char *)a.A + (size_t)b * a.strideA * esA;
+    const char *Bb = (const char *)a.B + (size_t)b * a.strideB * esB;
+    zd *Cb = a.C ? a.C + (size_t)b * a.strideC : nullptr;
 
     __shared__ zd As[2][BK][BM];
     __shared__ zd Bs[2][BK][BN];
@@ -59,7 +66,7 @@ zgemm_kernel(ZGemmArgs a)
             if (OPA == OP_N) { i = e % BM; l = e / BM; } else { l = e % BK; i = e / BK; }
             int gi = tileM + i, gl = k0 + l;
             zd v = make_double2(0.0, 0.0);
-            if (gi < a.m && gl < a.k) v = load_op<OPA, AR>(Ab, a.lda, gi, gl);
+            if (gi < a.m && gl < a.k) v = load_op<OPA>(Ab, a.lda, gi, gl, a.a_real, a.planeA);
             As[buf][l][i] = v;
         }
         for (int e = tid; e < BN * BK; e += NT) {
@@ -67,7 +74,7 @@ zgemm_kernel(ZGemmArgs a)
             if (OPB == OP_N) { l = e % BK; j = e / BK; } else { j = e % BN; l = e / BN; }
             int gl = k0 + l, gj = tileN + j;
             zd v = make_double2(0.0, 0.0);
-            if (gl < a.k && gj < a.n) v = load_op<OPB, BR>(Bb, a.ldb, gl, gj);
+            if (gl < a.k && gj < a.n) v = load_op<OPB>(Bb, a.ldb, gl, gj, a.b_real, a.planeB);
             Bs[buf][l][j] = v;
         }
     };
@@ -102,30 +109,33 @@ zgemm_kernel(ZGemmArgs a)
         for (int i = 0; i < TM; ++i) {
             int gi = tileM + tx + i * NTX;
             if (gi >= a.m) continue;
-            zd *c = Cb + gi + (size_t)gj * a.ldc;
             zd v = zmul(a.alpha, acc[i][j]);
-            if (!beta0) zfma(v, a.beta, *c);
-            *c = v;
+            if (Cb) {
+                zd *c = Cb + gi + (size_t)gj * a.ldc;
+                if (!beta0) zfma(v, a.beta, *c);
+                *c = v;
+            }
+            if (a.outMode & OUT_BF16P) {
+                __nv_bfloat16 *c2 = (__nv_bfloat16 *)a.C2 + (size_t)b * a.strideC2 + gi + (size_t)gj * a.ldc2;
+                c2[0] = __double2bfloat16(v.x);
+                c2[a.plane2] = __double2bfloat16(v.y);
+            }
+            if (a.outMode & OUT_C32P) {
+                float *c3 = a.C3 + (size_t)b * a.strideC3 + gi + (size_t)gj * a.ldc3;
+                c3[0] = (float)v.x;
+                c3[a.plane3] = (float)v.y;
+            }
         }
     }
-}
-
-template <int BM, int BN, int TM, int TN, int OPA, int OPB, bool AR, bool BR>
-cudaError_t launch4(const ZGemmArgs &a, cudaStream_t s)
-{
-    dim3 grid((a.m + BM - 1) / BM, (a.n + BN - 1) / BN, a.batch);
-    dim3 block((BM / TM) * (BN / TN));
-    zgemm_kernel<BM, BN, TM, TN, OPA, OPB, AR, BR><<<grid, block, 0, s>>>(a);
-    return cudaGetLastError();
 }
 
 template <int BM, int BN, int TM, int TN, int OPA, int OPB>
 cudaError_t launch3(const ZGemmArgs &a, cudaStream_t s)
 {
-    if (a.a_real && !a.b_real) return launch4<BM, BN, TM, TN, OPA, OPB, true, false>(a, s);
-    if (!a.a_real && a.b_real) return launch4<BM, BN, TM, TN, OPA, OPB, false, true>(a, s);
-    if (a.a_real && a.b_real) return launch4<BM, BN, TM, TN, OPA, OPB, true, true>(a, s);
-    return launch4<BM, BN, TM, TN, OPA, OPB, false, false>(a, s);
+    dim3 grid((a.m + BM - 1) / BM, (a.n + BN - 1) / BN, a.batch);
+    dim3 block((BM / TM) * (BN / TN));
+    zgemm_kernel<BM, BN, TM, TN, OPA, OPB><<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
 }
 
 template <int BM, int BN, int TM, int TN>

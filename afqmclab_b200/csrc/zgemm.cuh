@@ -8,6 +8,10 @@
 #include "common.cuh"
 
 enum { OP_N = 0, OP_T = 1, OP_C = 2 };
+// operand storage kinds
+enum { ST_Z64 = 0, ST_R64 = 1, ST_C32P = 2 };  // complex f64 | real f64 | complex f32 planar
+// output modes
+enum { OUT_Z64 = 1, OUT_BF16P = 2, OUT_C32P = 4 };
 
 struct ZGemmArgs {
     int m = 0, n = 0, k = 0;
@@ -20,6 +24,15 @@ struct ZGemmArgs {
     int batch = 1;
     const int *mask = nullptr;     // skip batch b when mask[b] == 0
     const int *skip = nullptr;     // skip batch b when skip[b] != 0
+    // complex f32 planar operands: imaginary plane at +planeA/+planeB floats
+    // (set a_real/b_real = 2 to select them; 1 = real f64 as before)
+    long long planeA = 0, planeB = 0;
+    // extra outputs: bits of OUT_* besides the f64 complex C (OUT_Z64 is implied
+    // when C != nullptr); C2 receives bf16 planar (imag plane at +plane2),
+    // C3 complex f32 planar (imag plane at +plane3); same ldc / strideC.
+    int outMode = OUT_Z64;
+    void *C2 = nullptr; long long plane2 = 0, strideC2 = 0, ldc2 = 0;
+    float *C3 = nullptr; long long plane3 = 0, strideC3 = 0, ldc3 = 0;
 };
 
 // Launches on `stream`; returns cudaGetLastError().
