@@ -1,0 +1,295 @@
+// Exchange term of the phaseless mixed estimator on the tcgen05 tensor cores
+// (RealMaterialMoleculeMeasureFixedSD2sSD2is::calculateCholeskyEx, :258-284):
+//   D_{g,w} = A_g theta_w  (Ns x Ns, complex),  ex[g, w] += sum_ab D_ab D_ba
+// for one spin block per launch.  As a GEMM: rows (g, a) of A (K = orbital
+// i), columns (w, b) of theta (K = i), both bf16 K-major; the 128 x 128 output
+// tile holds 128/Ns vectors g times 128/Ns walkers w, and the epilogue reduces
+// each Ns x Ns block to its trace tr(D D) without writing D.
+//
+// Persistent, warp-specialised: warp 0 TMA producer, warp 1 UMMA issuer (and
+// TMEM owner, 512 columns = two accumulator pairs so the epilogue of one tile
+// overlaps the MMAs of the next), warps 2..5 epilogue.  A CTA takes a work
+// item = one A tile (kept in shared memory) x a chunk of walker tiles.  All
+// waits are bounded.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <atomic>
+
+#include "engine_internal.cuh"
+#include "mixed.cuh"
+#include "tc_common.cuh"
+#include "tc_gemm.cuh"
+
+extern std::atomic<long long> g_launch_count;
+
+namespace {
+
+constexpr int XS_STAGES = 3;          // B stages: one 64-wide K box, both planes
+constexpr int XS_NCHUNK = 32;         // walker tiles per work item
+constexpr int XS_TILE_BYTES = 16384;  // 128 rows x 128 B
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0,
+                                            int c1, int c2)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
+        : "memory");
+}
+
+struct XSmem {
+    // sA: 2 planes x 2 K boxes; sB: XS_STAGES x (2 planes); transpose: 4 warps x 32x33 float2
+    static constexpr size_t bytes()
+    {
+        return 1024 + 4 * XS_TILE_BYTES + (size_t)XS_STAGES * 2 * XS_TILE_BYTES + 4 * 32 * 33 * 8 + 256;
+    }
+};
+
+__global__ void __launch_bounds__(192, 1)
+exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_constant__ CUtensorMap tmAi,
+                   const __grid_constant__ CUtensorMap tmBr, const __grid_constant__ CUtensorMap tmBi,
+                   int G, int W, int Ns, int n, const int *alive, zd *ex, int *err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t *sA = base;                                   // [plane][kb] tiles
+    uint8_t *sB = base + 4 * XS_TILE_BYTES;               // [stage][plane] tiles
+    float2 *sT = (float2 *)(sB + (size_t)XS_STAGES * 2 * XS_TILE_BYTES);
+    uint64_t *bars = (uint64_t *)(sT + 4 * 32 * 33);
+    uint64_t *full = bars, *empty = bars + XS_STAGES;
+    uint64_t *aFull = bars + 2 * XS_STAGES, *aEmpty = aFull + 1;
+    uint64_t *accFull = aEmpty + 1, *accEmpty = accFull + 2;
+    uint32_t *tslot = (uint32_t *)(accEmpty + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rowsTotal = G * Ns;
+    const int MT = (rowsTotal + 127) / 128;
+    const int WB = 128 / Ns;                      // walkers per tile
+    const int NT = (W + WB - 1) / WB;             // walker tiles
+    const int NCH = (NT + XS_NCHUNK - 1) / XS_NCHUNK;
+    const int items = MT * NCH;
+    const int KB = n / 64;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < XS_STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        mbar_init(aFull, 1);
+        mbar_init(aEmpty, 1);
+        for (int b = 0; b < 2; ++b) { mbar_init(&accFull[b], 1); mbar_init(&accEmpty[b], 4); }
+        fence_mbar_init();
+        tma_prefetch_desc(&tmAr); tma_prefetch_desc(&tmAi);
+        tma_prefetch_desc(&tmBr); tma_prefetch_desc(&tmBi);
+    }
+    if (warp == 1) { tmem_alloc(tslot, 512); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int stage = 0, sphase = 0, itemCount = 0;
+            for (int it = blockIdx.x; it < items && ok; it += gridDim.x, ++itemCount) {
+                const int mt = it % MT, ch = it / MT;
+                if (itemCount > 0) ok = mbar_wait(aEmpty, (itemCount - 1) & 1);
+                if (!ok) break;
+                mbar_arrive_expect_tx(aFull, 2 * KB * XS_TILE_BYTES);
+                for (int kb = 0; kb < KB; ++kb) {
+                    tma_load_2d(sA + (0 * 2 + kb) * XS_TILE_BYTES, &tmAr, aFull, kb * 64, mt * 128);
+                    tma_load_2d(sA + (1 * 2 + kb) * XS_TILE_BYTES, &tmAi, aFull, kb * 64, mt * 128);
+                }
+                const int t0 = ch * XS_NCHUNK, t1 = min(NT, t0 + XS_NCHUNK);
+                for (int t = t0; t < t1 && ok; ++t) {
+                    for (int kb = 0; kb < KB && ok; ++kb) {
+                        ok = mbar_wait(&empty[stage], sphase ^ 1);
+                        if (!ok) break;
+                        mbar_arrive_expect_tx(&full[stage], 2 * XS_TILE_BYTES);
+                        tma_load_3d(sB + (stage * 2 + 0) * XS_TILE_BYTES, &tmBr, &full[stage], kb * 64, 0, t * WB);
+                        tma_load_3d(sB + (stage * 2 + 1) * XS_TILE_BYTES, &tmBi, &full[stage], kb * 64, 0, t * WB);
+                        if (++stage == XS_STAGES) { stage = 0; sphase ^= 1; }
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            constexpr uint32_t ID = idesc_bf16(128, 128), IDN = idesc_bf16(128, 128, true);
+            int stage = 0, sphase = 0, itemCount = 0, tileCount = 0;
+            for (int it = blockIdx.x; it < items && ok; it += gridDim.x, ++itemCount) {
+                const int ch = it / MT;
+                ok = mbar_wait(aFull, itemCount & 1);
+                if (!ok) break;
+                const int t0 = ch * XS_NCHUNK, t1 = min(NT, t0 + XS_NCHUNK);
+                for (int t = t0; t < t1 && ok; ++t, ++tileCount) {
+                    const int ab = tileCount & 1;
+                    if (tileCount >= 2) ok = mbar_wait(&accEmpty[ab], ((tileCount >> 1) - 1) & 1);
+                    if (!ok) break;
+                    tc_fence_after();
+                    const uint32_t dR = tmem + ab * 256, dI = tmem + ab * 256 + 128;
+                    for (int kb = 0; kb < KB && ok; ++kb) {
+                        ok = mbar_wait(&full[stage], sphase);
+                        if (!ok) break;
+                        tc_fence_after();
+                        const uint32_t ar = smem_u32(sA + (0 * 2 + kb) * XS_TILE_BYTES);
+                        const uint32_t ai = smem_u32(sA + (1 * 2 + kb) * XS_TILE_BYTES);
+                        const uint32_t br = smem_u32(sB + (stage * 2 + 0) * XS_TILE_BYTES);
+                        const uint32_t bi = smem_u32(sB + (stage * 2 + 1) * XS_TILE_BYTES);
+#pragma unroll
+                        for (int kk = 0; kk < 4; ++kk) {
+                            const uint32_t acc = (kb > 0 || kk > 0) ? 1u : 0u;
+                            const uint64_t dar = desc_k_sw128(ar + kk * 32), dai = desc_k_sw128(ai + kk * 32);
+                            const uint64_t dbr = desc_k_sw128(br + kk * 32), dbi = desc_k_sw128(bi + kk * 32);
+                            umma_bf16(dR, dar, dbr, ID, acc);
+                            umma_bf16(dI, dar, dbi, ID, acc);
+                            umma_bf16(dR, dai, dbi, IDN, 1u);
+                            umma_bf16(dI, dai, dbr, ID, 1u);
+                        }
+                        umma_commit(&empty[stage]);
+                        if (++stage == XS_STAGES) { stage = 0; sphase ^= 1; }
+                    }
+                    umma_commit(&accFull[ab]);
+                }
+                umma_commit(aEmpty);
+            }
+        }
+        __syncwarp();
+    } else {
+        const int q = warp & 3;
+        float2 *T = sT + q * 32 * 33;
+        const int gpw = 32 / Ns;                      // vectors g per warp quarter
+        int tileCount = 0;
+        for (int it = blockIdx.x; it < items && ok; it += gridDim.x) {
+            const int mt = it % MT, ch = it / MT;
+            const int t0 = ch * XS_NCHUNK, t1 = min(NT, t0 + XS_NCHUNK);
+            for (int t = t0; t < t1 && ok; ++t, ++tileCount) {
+                const int ab = tileCount & 1;
+                ok = mbar_wait(&accFull[ab], (tileCount >> 1) & 1);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t tR = tmem + ab * 256 + ((uint32_t)(q * 32) << 16);
+                const uint32_t tI = tR + 128;
+                const int r = q * 32 + lane;                   // tile row
+                const int gl = r / Ns, a = r % Ns;
+                const int g = mt * (128 / Ns) + gl;
+#pragma unroll 1
+                for (int c0 = 0; c0 < 128; c0 += 32) {
+                    float vr[32], vi[32];
+                    tmem_ld32(tR + c0, vr);
+                    tmem_ld32(tI + c0, vi);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) T[lane * 33 + j] = make_float2(vr[j], vi[j]);
+                    __syncwarp();
+                    // blocks (g_local, w_local) inside this 32-column chunk
+                    for (int wb = 0; wb < 32 / Ns; ++wb) {
+                        const int cb = wb * Ns;                 // first column of the block in the chunk
+                        float sr = 0.f, si = 0.f;
+                        for (int b = 0; b < Ns; ++b) {
+                            const float2 x = T[lane * 33 + cb + b];                // D[a][b]
+                            const float2 y = T[(lane - a + b) * 33 + cb + a];       // D[b][a]
+                            sr += x.x * y.x - x.y * y.y;
+                            si += x.x * y.y + x.y * y.x;
+                        }
+                        for (int o = Ns >> 1; o > 0; o >>= 1) {
+                            sr += __shfl_xor_sync(0xffffffffu, sr, o);
+                            si += __shfl_xor_sync(0xffffffffu, si, o);
+                        }
+                        const int w = t * WB + (c0 + cb) / Ns;
+                        if (a == 0 && g < G && w < W && alive[w]) {
+                            zd *p = ex + g + (size_t)G * w;
+                            zd v = *p;
+                            v.x += sr; v.y += si;
+                            *p = v;
+                        }
+                    }
+                    __syncwarp();
+                }
+                tc_fence_before();
+                if (lane == 0) mbar_arrive(&accEmpty[ab]);
+                (void)gpw;
+            }
+        }
+    }
+    if (!ok && err) atomicExch(err, 3);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, 512);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// theta of spin block b for every walker: dims {n (i), Ns (b), W (w)}
+int make_map_theta(CUtensorMap *map, const void *base, int n, int Ns, int W, long long walkerPitch)
+{
+    auto enc = encode_fn();
+    if (!enc) return -1;
+    cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)Ns, (cuuint64_t)W};
+    cuuint64_t strides[2] = {(cuuint64_t)n * 2, (cuuint64_t)walkerPitch * 2};
+    cuuint32_t box[3] = {64u, (cuuint32_t)Ns, (cuuint32_t)(128 / Ns)};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void *>(base), dims, strides, box,
+                     estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : (int)r + 10000;
+}
+
+}  // namespace
+
+// A2 operand of spin block b: rows (g, a) -> r = g Ns + a, K = i; two bf16 planes
+__global__ void build_a2_kernel(int G, int Ns, int n, long long Ktot, long long tOff, const zd *Aall,
+                                __nv_bfloat16 *A2r, __nv_bfloat16 *A2i)
+{
+    const long long total = (long long)G * Ns * n;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        long long r = e / n;
+        int i = (int)(e % n);
+        int g = (int)(r / Ns), a = (int)(r % Ns);
+        zd v = Aall[(size_t)g * Ktot + tOff + a + (size_t)Ns * i];
+        A2r[e] = __double2bfloat16(v.x);
+        A2i[e] = __double2bfloat16(v.y);
+    }
+}
+
+int exchange_tc_supported(int n, int Ns) { return (n == 64 || n == 128) && Ns > 0 && 32 % Ns == 0; }
+
+// ex (G x W, complex) += exchange of spin block with the given operands
+int exchange_tc_launch(cudaStream_t s, int G, int W, int Ns, int n, const __nv_bfloat16 *A2r,
+                       const __nv_bfloat16 *A2i, const __nv_bfloat16 *Theta, long long tOff,
+                       long long Ktot, const int *alive, zd *ex, int *err)
+{
+    g_launch_count++;
+    CUtensorMap ar, ai, br, bi;
+    int r = tc_make_map_bf16(&ar, A2r, n, (long long)G * Ns, n, 128);
+    if (!r) r = tc_make_map_bf16(&ai, A2i, n, (long long)G * Ns, n, 128);
+    if (!r) r = make_map_theta(&br, Theta + tOff, n, Ns, W, 2 * Ktot);
+    if (!r) r = make_map_theta(&bi, Theta + Ktot + tOff, n, Ns, W, 2 * Ktot);
+    if (r) return r;
+    const size_t smem = XSmem::bytes();
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(exchange_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int MT = (G * Ns + 127) / 128;
+    const int NT = (W + 128 / Ns - 1) / (128 / Ns);
+    const int items = MT * ((NT + XS_NCHUNK - 1) / XS_NCHUNK);
+    exchange_tc_kernel<<<std::min(items, sms), 192, smem, s>>>(ar, ai, br, bi, G, W, Ns, n, alive, ex, err);
+    return (int)cudaGetLastError();
+}

@@ -27,6 +27,7 @@ struct MixedState {
                   *Et = nullptr;
     float *xbarp = nullptr;
     zd *wfDaggerTm = nullptr;
+    __nv_bfloat16 *A2r[2] = {nullptr, nullptr}, *A2i[2] = {nullptr, nullptr};
     int *err = nullptr;
     int splits = 1;
     long long ws32 = 0;  // floats per walker (2 n ncol)
@@ -594,6 +595,14 @@ int mixed_create(afqmc_engine *e)
     MTRY(engine_dalloc(e, &m->xbarp, (size_t)m->splits * 2 * G * W));
     MTRY(engine_dalloc(e, &m->wfDaggerTm, (size_t)Ktot));
     MTRY(engine_dalloc(e, &m->err, 1));
+    for (int b = 0; b < e->bl.nblk; ++b) {
+        const int Ns = e->bl.Ns[b];
+        if (Ns == 0 || !exchange_tc_supported(n, Ns)) continue;
+        MTRY(engine_dalloc(e, (unsigned short **)&m->A2r[b], (size_t)G * Ns * n));
+        MTRY(engine_dalloc(e, (unsigned short **)&m->A2i[b], (size_t)G * Ns * n));
+        build_a2_kernel<<<1184, 256, 0, e->stream>>>(G, Ns, n, Ktot, e->bl.tOff[b], e->Aall, m->A2r[b],
+                                                     m->A2i[b]);
+    }
     build_abig_kernel<<<1184, 256, 0, e->stream>>>(G, Ktot, n, e->bl, e->Aall, m->Abig);
     build_lt_kernel<<<1184, 256, 0, e->stream>>>((long long)n * n, G, e->chol, m->Lt);
     build_et_kernel<<<64, 256, 0, e->stream>>>(n, e->expK[0], m->Et);
@@ -711,12 +720,28 @@ int mixed_pop_control(afqmc_engine *e)
     return engine_check_launch();
 }
 
-// Exchange term of the mixed estimator from the FP64 theta (i + n b layout).
+// Exchange term of the mixed estimator: tcgen05 kernel per spin block
+// (bf16 operands: A2 planes, Theta), FP64 CUDA-core kernel for block widths
+// that do not divide 32.
 int mixed_exchange(afqmc_engine *e)
 {
-    if (launch_pl_exchange(e->W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex,
-                           e->stream, 1))
-        return engine_fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
+    MixedState *m = e->mx;
+    bool allTc = true;
+    for (int b = 0; b < e->bl.nblk; ++b)
+        if (e->bl.Ns[b] > 0 && !exchange_tc_supported(e->n, e->bl.Ns[b])) allTc = false;
+    if (!allTc) {
+        if (launch_pl_exchange(e->W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex,
+                               e->stream, 1))
+            return engine_fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
+        return engine_check_launch();
+    }
+    MTRY(cuda_check(cudaMemsetAsync(e->ex, 0, sizeof(zd) * e->G * e->W, e->stream), "memset ex"));
+    for (int b = 0; b < e->bl.nblk; ++b) {
+        if (e->bl.Ns[b] == 0) continue;
+        int r = exchange_tc_launch(e->stream, e->G, e->W, e->bl.Ns[b], e->n, m->A2r[b], m->A2i[b],
+                                   m->Theta, e->bl.tOff[b], e->Ktot, e->alive, e->ex, m->err);
+        if (r) return engine_fail(AFQMC_ERR_CUDA, "exchange launch: " + std::to_string(r));
+    }
     return engine_check_launch();
 }
 

@@ -71,8 +71,9 @@ def test_mixed_energy_tracks_fp64():
     assert x.status() == 0
 
 
-def test_mixed_measurement_matches_fp64_on_same_walkers():
-    m = molecule()
+@pytest.mark.parametrize("n,nup,ndn,G", [(64, 16, 16, 128), (128, 32, 32, 128), (64, 16, 8, 64)])
+def test_mixed_measurement_matches_fp64_on_same_walkers(n, nup, ndn, G):
+    m = molecule(n, nup, ndn, G)
     W = 32
     f, x = pair(m, W, 31, noise=0.05)
     for e in (f, x):
