@@ -252,7 +252,23 @@ def molecule_inputs(n=128, nup=32, ndn=32, G=640, dt=0.005, decay=60.0, seed=202
                        K=np.asfortranarray(K), chol=chol, bg=np.zeros(G), phiTUp=phiTUp,
                        phiTDn=phiTDn, logwT=0j)
     m.set_background(np.zeros(G))
+    m.ET = variational_energy(m)
     return m
+
+
+def variational_energy(m):
+    """<phiT|H|phiT>/<phiT|phiT> of the real RHF/UHF trial for
+    H = sum t c^+c + 1/2 sum_g (sum L_g c^+c)^2 - 1/2 sum_g L_g L_g c^+c
+    (the reference's T + 1/2 sum_g (xbar_g^2 - ex_g) at the trial itself)."""
+    Pu = (m.phiTUp @ m.phiTUp.conj().T).real
+    Pd = (m.phiTDn @ m.phiTDn.conj().T).real
+    e = np.sum(m.t * (Pu + Pd))
+    for g in range(m.G):
+        Lg = m.chol[:, :, g]
+        a = np.sum(Lg * Pu) + np.sum(Lg * Pd)
+        ex = np.sum((Lg @ Pu) * (Lg @ Pu).T) + np.sum((Lg @ Pd) * (Lg @ Pd).T)
+        e += 0.5 * (a * a - ex)
+    return float(e)
 
 
 # ------------------------------------------------------------------ walkers

@@ -137,6 +137,32 @@ def run_steps(eng, k, start, measure_skip):
         eng.step(1)
 
 
+def energy_check(capi, inputs, name, steps, measure_skip, stream, seed):
+    """Mixed vs FP64 form from identical walkers and random stream: mixed
+    estimator E = HNum/den (one measurement = addMixedMeasurement over the
+    population, afqmcPhaselessMeasure.cpp:9-28) every measure_skip steps."""
+    out = {}
+    for prec in ("fp64", "mixed"):
+        eng, m, c, _ = build_engine(capi, inputs, name, prec, seed)
+        eng.set_stream(stream.cuda_stream)
+        es = []
+        for i in range(steps):
+            if i % measure_skip == 0:
+                eng.reset_measurement()
+                eng.add_mixed_measurement()
+                mm = eng.measurement()
+                es.append((mm[1] / mm[0]).real)
+            eng.step(1)
+        out[prec] = np.array(es)
+        eng.close()
+    d = (out["mixed"] - out["fp64"]) * 1e3
+    return {"steps": steps, "measurements": len(d), "E_fp64_Ha": out["fp64"].tolist(),
+            "E_mixed_Ha": out["mixed"].tolist(), "dE_mHa": d.tolist(),
+            "max_abs_dE_mHa": float(np.abs(d).max()), "mean_dE_mHa": float(d.mean()),
+            "criterion_mHa": 0.5, "pass": bool(np.abs(d).max() <= 0.5),
+            "method": "paired: same walkers, same random stream, measurement by measurement"}
+
+
 # ---------------------------------------------------------------- CPU arm
 def _cpu_worker(args):
     name, nwalk, steps, seed, measure_skip = args
@@ -192,6 +218,8 @@ def main():
     ap.add_argument("--measure-skip", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--no-fp64-side", action="store_true")
+    ap.add_argument("--energy-steps", type=int, default=60)
     args = ap.parse_args()
     rank, world, local = dist_info()
 
@@ -300,6 +328,7 @@ def main():
 
     # roofline of the dominant phase
     calls, total, mn, mx = eng.taylor_stats()
+    status = eng.status()
     tavg = total / calls if calls else 0.0
     roof = None
     if c["kind"] == "pl":
@@ -317,6 +346,33 @@ def main():
         roof = {"bound": bound, "kernel": top, "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                 "flops_per_launch": fl[top], "launch_ms": t_launch * 1e3, "peak_source": psrc}
+
+    # the plain FP64 form side by side, and the paired energy check: both
+    # forms from the same walkers and random stream, mixed estimator every
+    # measure_skip steps (energies compared measurement by measurement)
+    side = None
+    echeck = None
+    if precision == "mixed" and not args.no_fp64_side:
+        eng.close()
+        f64, _, _, _ = build_engine(capi, inputs, args.workload, "fp64", 77 + rank)
+        f64.set_stream(stream.cuda_stream)
+        run_steps(f64, 2, 0, args.measure_skip)
+        f64.synchronize()
+        k64 = max(5, min(args.steps, 10))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run_steps(f64, k64, 2, args.measure_skip)
+        e1.record(stream)
+        e1.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        side = {"value": W * k64 * world / (ms64 / 1e3), "ms_per_step": ms64 / k64, "steps": k64,
+                "speedup_mixed_over_fp64": (ms64 / k64) / (ms / args.steps)}
+        f64.close()
+        if args.energy_steps > 0:
+            echeck = energy_check(capi, inputs, args.workload, args.energy_steps, args.measure_skip,
+                                  stream, 4242 + rank)
+        eng = None
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -340,10 +396,13 @@ def main():
             "clocks": clk,
             "phases_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1] > 0},
             "taylor_order": {"avg": tavg, "min": mn, "max": mx},
-            "status": eng.status(),
+            "status": status,
+            "fp64_form": side,
+            "energy_check": echeck,
         }
         print(json.dumps(line), flush=True)
-    eng.close()
+    if eng is not None:
+        eng.close()
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
