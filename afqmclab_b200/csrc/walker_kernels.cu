@@ -187,6 +187,148 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
 }
 
 // ---------------------------------------------------------------------------
+// Same contract as lu_kernel for blocks of at most 32 columns, one warp per
+// walker: Gauss-Jordan elimination with the zgetf2 pivot choice (first row
+// of maximal |re|+|im| in the current column), in place in a padded shared
+// tile (lane i owns row i), then the column unscrambling of the recorded row
+// interchanges.  The pivots are the U diagonal of the LU factorisation, so
+// the log-determinant follows logDeterminant (tensor_2d_common_fun.cpp:75-105).
+// ---------------------------------------------------------------------------
+constexpr int GJ_WARPS = 4;
+constexpr int GJ_LD = 33;
+
+__global__ void __launch_bounds__(GJ_WARPS * 32)
+gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const zd *logw,
+               zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut, double *weight,
+               int *status, int mode, int wantInverse)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * GJ_WARPS + warp;
+    if (w >= W) return;
+    zd *A = (zd *)smem_raw + (size_t)warp * 32 * GJ_LD;
+    const bool act = (active == nullptr) || active[w] != 0;
+    if (!act) {
+        if (lane == 0) {
+            if (mode == LU_PROJECT) surv[w] = 0;
+            if (mode == LU_POPWEIGHT) { weight[w] = 0.0; alive[w] = 1; }
+        }
+        return;
+    }
+    bool singular = false;
+    zd logdetSum = make_double2(0.0, 0.0);
+    for (int b = 0; b < bl.nblk; ++b) {
+        const int Ns = bl.Ns[b];
+        if (Ns == 0) continue;
+        const zd *Sg = S + (size_t)w * bl.sStride + bl.sOff[b];
+        for (int e = lane; e < Ns * Ns; e += 32) A[(e % Ns) * GJ_LD + e / Ns] = Sg[e];
+        __syncwarp();
+        double lognorm = 0.0;
+        zd phase = make_double2(1.0, 0.0);
+        int myPartner = lane;  // lane k keeps the row interchanged at step k
+        bool sing = false;
+        for (int k = 0; k < Ns; ++k) {
+            double v = (lane >= k && lane < Ns) ? zcabs1(A[lane * GJ_LD + k]) : -1.0;
+            int idx = lane;
+            for (int o = 16; o > 0; o >>= 1) {
+                double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+                if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+            }
+            const int p = idx;
+            if (lane == k) myPartner = p;
+            if (p != k) {
+                for (int j = lane; j < Ns; j += 32) {
+                    zd t = A[k * GJ_LD + j];
+                    A[k * GJ_LD + j] = A[p * GJ_LD + j];
+                    A[p * GJ_LD + j] = t;
+                }
+                __syncwarp();
+            }
+            const zd piv = A[k * GJ_LD + k];
+            if (zeq0(piv)) {
+                sing = true;
+                __syncwarp();
+                continue;
+            }
+            const double a = zabs(piv);
+            lognorm += log(a);
+            const zd f = (p != k) ? zneg(piv) : piv;
+            phase = zmul(phase, make_double2(f.x / a, f.y / a));
+            const zd pinv = zdiv(make_double2(1.0, 0.0), piv);
+            __syncwarp();
+            // normalise the pivot row; its column-k entry becomes 1/piv
+            for (int j = lane; j < Ns; j += 32)
+                A[k * GJ_LD + j] = (j == k) ? pinv : zmul(A[k * GJ_LD + j], pinv);
+            __syncwarp();
+            // eliminate column k from every other row (lane i owns row i)
+            if (lane < Ns && lane != k) {
+                zd *row = A + lane * GJ_LD;
+                const zd *prow = A + k * GJ_LD;
+                const zd dum = row[k];
+                row[k] = make_double2(0.0, 0.0);
+                for (int j = 0; j < Ns; ++j) {
+                    const zd pv = prow[j];
+                    zd r = row[j];
+                    r.x -= pv.x * dum.x - pv.y * dum.y;
+                    r.y -= pv.x * dum.y + pv.y * dum.x;
+                    row[j] = r;
+                }
+            }
+            __syncwarp();
+        }
+        // undo the row interchanges as column swaps, last first
+        for (int k = Ns - 1; k >= 0; --k) {
+            const int p = __shfl_sync(0xffffffffu, myPartner, k);
+            if (p != k && lane < Ns) {
+                zd t = A[lane * GJ_LD + k];
+                A[lane * GJ_LD + k] = A[lane * GJ_LD + p];
+                A[lane * GJ_LD + p] = t;
+            }
+        }
+        __syncwarp();
+        if (sing) {
+            singular = true;
+        } else {
+            zd ld = zadd(make_double2(lognorm, 0.0), zlog(phase));
+            if (logdetSum.x > -1e299) logdetSum = zadd(logdetSum, ld);
+        }
+        if (wantInverse && Sinv) {
+            zd *Xg = Sinv + (size_t)w * bl.sStride + bl.sOff[b];
+            for (int e = lane; e < Ns * Ns; e += 32) Xg[e] = A[(e % Ns) * GJ_LD + e / Ns];
+        }
+        __syncwarp();
+    }
+    if (singular) logdetSum = make_double2(-1e300, 0.0);
+    if (lane == 0) {
+        zd lwR = zadd(logwAdd, logw[w]);
+        zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
+        logov[w] = lo;
+        if (singular && status) atomicOr(status + w, (int)ST_SINGULAR);
+        if (!(isfinite(lo.x) && isfinite(lo.y)) && status && !singular) atomicOr(status + w, (int)ST_NONFINITE);
+        if (mode == LU_PROJECT) {
+            double ph = lo.y;
+            double c = cos(ph);
+            if (c <= 0.0) {
+                alive[w] = 0; surv[w] = 0;
+            } else {
+                logwOut[w] = zadd(logw[w], make_double2(log(c), -ph));
+                surv[w] = 1;
+            }
+        } else if (mode == LU_POPWEIGHT) {
+            zd e = zexp(lo);
+            if (e.x <= 0.0) {
+                weight[w] = 0.0;
+            } else {
+                weight[w] = e.x;
+                logwOut[w] = zsub(logw[w], lo);
+            }
+            alive[w] = 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Exclusive scan of survivors x draws -> per-walker offset into the random
 // stream; reproduces the reference's sequential walker-major draw order
 // (afqmcPhaselessProjection.cpp:80-101, NiupNidn.cpp:66-84).
@@ -542,38 +684,56 @@ mgs_kernel(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, zd *lo
 // slot filling.  The `number[zero_i]` read is bounds-checked first.
 // ---------------------------------------------------------------------------
 __global__ void pop_comb_kernel(int W, const double *weight, const double *uniforms, uint64_t seed,
-                                unsigned long long *counter, int *number, int *table, int *status)
+                                unsigned long long *counter, int *number, int *table, int *status,
+                                int useSmem)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    unsigned long long c0 = counter ? *counter : 0ULL;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int tid = threadIdx.x;
+    const unsigned long long c0 = counter ? *counter : 0ULL;
+    // stage weights, uniforms and counts in shared memory (parallel), then the
+    // comb and the slot filling run serially in the reference's order
+    double *sw = useSmem ? (double *)smem_raw : nullptr;
+    double *su = useSmem ? sw + W : nullptr;
+    int *sn = useSmem ? (int *)(su + W) : number;
+    if (useSmem) {
+        for (int i = tid; i < W; i += blockDim.x) {
+            sw[i] = weight[i];
+            su[i] = uniforms ? uniforms[i] : rng_uniform(seed, c0 + (unsigned long long)i);
+            sn[i] = 0;
+        }
+    } else {
+        for (int i = tid; i < W; i += blockDim.x) sn[i] = 0;
+    }
+    __syncthreads();
+    if (tid != 0) return;
+    const double *wt = useSmem ? sw : weight;
     double sum = 0.0;
-    for (int i = 0; i < W; ++i) sum += weight[i];
-    for (int i = 0; i < W; ++i) number[i] = 0;
+    for (int i = 0; i < W; ++i) sum += wt[i];
     int index_old = 0;
-    double prob_sum_old = weight[0] / sum;
+    double prob_sum_old = wt[0] / sum;
     for (int i = 0; i < W; ++i) {
-        double u = uniforms ? uniforms[i] : rng_uniform(seed, c0 + (unsigned long long)i);
+        double u = useSmem ? su[i] : (uniforms ? uniforms[i] : rng_uniform(seed, c0 + (unsigned long long)i));
         double prob_sum_new = (i + u) / (W * 1.0);
         while (prob_sum_new > prob_sum_old && index_old < W - 1) {
             index_old++;
-            prob_sum_old += weight[index_old] / sum;
+            prob_sum_old += wt[index_old] / sum;
         }
-        number[index_old]++;
+        sn[index_old]++;
     }
     if (counter) *counter = c0 + (unsigned long long)W;
-    for (int i = 0; i < W; ++i) table[i] = (number[i] != 0) ? i : -1;
+    for (int i = 0; i < W; ++i) table[i] = (sn[i] != 0) ? i : -1;
     int zero_i = 0, one_i = 0, max_i = W;
-    while (zero_i < max_i && number[zero_i] != 0) zero_i++;
-    while (one_i < max_i && number[one_i] <= 1) one_i++;
+    while (zero_i < max_i && sn[zero_i] != 0) zero_i++;
+    while (one_i < max_i && sn[one_i] <= 1) one_i++;
     while (zero_i < max_i && one_i < max_i) {
         table[zero_i] = one_i;
-        number[zero_i]++;
-        number[one_i]--;
-        while (zero_i < max_i && number[zero_i] != 0) zero_i++;
-        while (one_i < max_i && number[one_i] <= 1) one_i++;
+        sn[zero_i]++;
+        sn[one_i]--;
+        while (zero_i < max_i && sn[zero_i] != 0) zero_i++;
+        while (one_i < max_i && sn[one_i] <= 1) one_i++;
     }
     int bad = 0;
-    for (int i = 0; i < W; ++i) if (number[i] != 1) bad = 1;
+    for (int i = 0; i < W; ++i) if (sn[i] != 1) bad = 1;
     if (bad && status) status[0] |= 16;
 }
 
@@ -751,37 +911,56 @@ pl_energy_kernel(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *th
     }
 }
 
-// Accumulate the estimator numerators/denominator over alive walkers in a
-// fixed order (writeThreadSum / MPISum of the reference become plain sums).
-__global__ void measure_reduce_kernel(int W, const int *alive, const zd *eloc, const zd *den,
-                                      const zd *parts, int nparts, zd *acc, int G, const zd *xbar,
-                                      const zd *ex, zd *bgNum, zd *exNum)
+// Accumulate the estimator numerators/denominator over alive walkers
+// (writeThreadSum / MPISum of the reference become plain sums).  Block 0
+// reduces the scalars, block 1+g the per-vector sums of g; each block sums a
+// fixed strided partition then a fixed tree, so the order is reproducible.
+__device__ __forceinline__ zd block_zsum_fixed(zd v, double *scratch)
 {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid == 0) {
+    return block_zsum(v, scratch);
+}
+
+__global__ void __launch_bounds__(256)
+measure_reduce_kernel(int W, const int *alive, const zd *eloc, const zd *den, const zd *parts,
+                      int nparts, zd *acc, int G, const zd *xbar, const zd *ex, zd *bgNum,
+                      zd *exNum)
+{
+    __shared__ double red[32];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    if (blockIdx.x == 0) {
         zd sd = make_double2(0, 0), sh = make_double2(0, 0);
         zd sp[3] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0)};
-        for (int w = 0; w < W; ++w) {
+        for (int w = tid; w < W; w += nt) {
             if (!alive[w]) continue;
             zd d = den[w];
             sd = zadd(sd, d);
             sh = zadd(sh, zmul(eloc[w], d));
             for (int k = 0; k < nparts; ++k) sp[k] = zadd(sp[k], zmul(parts[(size_t)nparts * w + k], d));
         }
-        acc[0] = zadd(acc[0], sd);
-        acc[1] = zadd(acc[1], sh);
-        for (int k = 0; k < nparts; ++k) acc[2 + k] = zadd(acc[2 + k], sp[k]);
-    }
-    if (xbar && tid < G) {
-        zd sb = make_double2(0, 0), se = make_double2(0, 0);
-        for (int w = 0; w < W; ++w) {
-            if (!alive[w]) continue;
-            zd d = den[w];
-            sb = zadd(sb, zmul(xbar[tid + (size_t)G * w], d));
-            se = zadd(se, zmul(ex[tid + (size_t)G * w], d));
+        sd = block_zsum_fixed(sd, red);
+        sh = block_zsum_fixed(sh, red);
+        for (int k = 0; k < nparts; ++k) sp[k] = block_zsum_fixed(sp[k], red);
+        if (tid == 0) {
+            acc[0] = zadd(acc[0], sd);
+            acc[1] = zadd(acc[1], sh);
+            for (int k = 0; k < nparts; ++k) acc[2 + k] = zadd(acc[2 + k], sp[k]);
         }
-        bgNum[tid] = zadd(bgNum[tid], sb);
-        exNum[tid] = zadd(exNum[tid], se);
+        return;
+    }
+    const int g = blockIdx.x - 1;
+    if (!xbar || g >= G) return;
+    zd sb = make_double2(0, 0), se = make_double2(0, 0);
+    for (int w = tid; w < W; w += nt) {
+        if (!alive[w]) continue;
+        zd d = den[w];
+        sb = zadd(sb, zmul(xbar[g + (size_t)G * w], d));
+        se = zadd(se, zmul(ex[g + (size_t)G * w], d));
+    }
+    sb = block_zsum_fixed(sb, red);
+    se = block_zsum_fixed(se, red);
+    if (tid == 0) {
+        bgNum[g] = zadd(bgNum[g], sb);
+        exNum[g] = zadd(exNum[g], se);
     }
 }
 
@@ -796,6 +975,18 @@ void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const in
     g_launch_count++;
     int maxNs = 0;
     for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
+    if (maxNs <= 32) {
+        const size_t smem = (size_t)GJ_WARPS * 32 * GJ_LD * sizeof(zd);
+        static bool gattr = false;
+        if (!gattr) {
+            cudaFuncSetAttribute(gj_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            gattr = true;
+        }
+        gj_warp_kernel<<<(W + GJ_WARPS - 1) / GJ_WARPS, GJ_WARPS * 32, smem, s>>>(
+            W, bl, S, Sinv, active, logw, logwAdd, logwT, logov, alive, surv, logwOut, weight, status,
+            mode, wantInverse ? 1 : 0);
+        return;
+    }
     if (maxNs <= LU_SMEM_MAX_NS) {
         size_t smem = (size_t)2 * maxNs * maxNs * sizeof(zd) + (size_t)(maxNs + 4) * sizeof(int);
         static bool attr = false;
@@ -880,7 +1071,15 @@ void launch_pop_comb(int W, const double *weight, const double *uniforms, uint64
                      cudaStream_t s)
 {
     g_launch_count++;
-    pop_comb_kernel<<<1, 32, 0, s>>>(W, weight, uniforms, seed, counter, number, table, status);
+    const size_t smem = (size_t)W * (2 * sizeof(double) + sizeof(int));
+    const int useSmem = smem <= 160 * 1024 ? 1 : 0;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(pop_comb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        attr = true;
+    }
+    pop_comb_kernel<<<1, 256, useSmem ? smem : 0, s>>>(W, weight, uniforms, seed, counter, number, table,
+                                                       status, useSmem);
 }
 
 void launch_pop_gather(int W, long long wsize, const int *table, zd *wf, zd *logw, cudaStream_t s)
@@ -945,33 +1144,41 @@ void launch_measure_reduce(int W, const int *alive, const zd *eloc, const zd *de
                            zd *exNum, cudaStream_t s)
 {
     g_launch_count++;
-    int threads = 256;
-    int blocks = xbar ? (G + threads - 1) / threads : 1;
-    if (blocks < 1) blocks = 1;
-    measure_reduce_kernel<<<blocks, threads, 0, s>>>(W, alive, eloc, den, parts, nparts, acc, G,
-                                                      xbar, ex, bgNum, exNum);
+    int blocks = 1 + (xbar ? G : 0);
+    measure_reduce_kernel<<<blocks, 256, 0, s>>>(W, alive, eloc, den, parts, nparts, acc, G, xbar, ex,
+                                                  bgNum, exNum);
 }
 
 namespace {
 // LogHop2isSD2isOperation order statistics (logHop2isSD2isOperation.cpp:146-157):
 // stats[0] calls, [1] total order, [2] min, [3] max.
-__global__ void taylor_stats_kernel(int W, const int *mask, const int *order, long long *stats)
+__global__ void __launch_bounds__(256) taylor_stats_kernel(int W, const int *mask, const int *order, long long *stats)
 {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    long long calls = stats[0], total = stats[1], mn = stats[2], mx = stats[3];
-    for (int w = 0; w < W; ++w) {
+    __shared__ double red[32];
+    double calls = 0, total = 0, mn = 1e30, mx = 0;
+    for (int w = threadIdx.x; w < W; w += blockDim.x) {
         if (!mask[w]) continue;
-        long long o = order[w];
-        calls++; total += o;
-        if (o < mn) mn = o;
-        if (o > mx) mx = o;
+        double o = order[w];
+        calls += 1; total += o;
+        mn = fmin(mn, o); mx = fmax(mx, o);
     }
-    stats[0] = calls; stats[1] = total; stats[2] = mn; stats[3] = mx;
+    calls = block_sum(calls, red);
+    total = block_sum(total, red);
+    mx = block_max(mx, red);
+    mn = -block_max(-mn, red);
+    if (threadIdx.x == 0) {
+        stats[0] += (long long)calls;
+        stats[1] += (long long)total;
+        if (calls > 0) {
+            if ((long long)mn < stats[2]) stats[2] = (long long)mn;
+            if ((long long)mx > stats[3]) stats[3] = (long long)mx;
+        }
+    }
 }
 }  // namespace
 
 void launch_taylor_stats(int W, const int *mask, const int *order, long long *stats, cudaStream_t s)
 {
     g_launch_count++;
-    taylor_stats_kernel<<<1, 32, 0, s>>>(W, mask, order, stats);
+    taylor_stats_kernel<<<1, 256, 0, s>>>(W, mask, order, stats);
 }
