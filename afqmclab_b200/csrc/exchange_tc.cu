@@ -196,12 +196,7 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
                             si += __shfl_xor_sync(0xffffffffu, si, o);
                         }
                         const int w = t * WB + (c0 + cb) / Ns;
-                        if (a == 0 && g < G && w < W && alive[w]) {
-                            zd *p = ex + g + (size_t)G * w;
-                            zd v = *p;
-                            v.x += sr; v.y += si;
-                            *p = v;
-                        }
+                        if (a == 0 && g < G && w < W) ex[g + (size_t)G * w] = make_double2(sr, si);
                     }
                     __syncwarp();
                 }
@@ -266,7 +261,7 @@ __global__ void build_a2_kernel(int G, int Ns, int n, long long Ktot, long long 
 
 int exchange_tc_supported(int n, int Ns) { return (n == 64 || n == 128) && Ns > 0 && 32 % Ns == 0; }
 
-// ex (G x W, complex) += exchange of spin block with the given operands
+// ex (G x W, complex) = exchange of one spin block (every (g, w) written once)
 int exchange_tc_launch(cudaStream_t s, int G, int W, int Ns, int n, const __nv_bfloat16 *A2r,
                        const __nv_bfloat16 *A2i, const __nv_bfloat16 *Theta, long long tOff,
                        long long Ktot, const int *alive, zd *ex, int *err)

@@ -28,6 +28,7 @@ struct MixedState {
     float *xbarp = nullptr;
     zd *wfDaggerTm = nullptr;
     __nv_bfloat16 *A2r[2] = {nullptr, nullptr}, *A2i[2] = {nullptr, nullptr};
+    zd *ex2 = nullptr;
     int *err = nullptr;
     int splits = 1;
     long long ws32 = 0;  // floats per walker (2 n ncol)
@@ -250,6 +251,14 @@ mixed_sample_kernel(int W, CholDev c, const float *xbarp, int splits, long long 
             logw[w] = zadd(hopLogw, t);
         }
     }
+}
+
+// ex += ex2 (the second spin block's exchange plane)
+__global__ void add_planes_kernel(long long count, const zd *src, zd *dst)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+         e += (long long)gridDim.x * blockDim.x)
+        dst[e] = zadd(dst[e], src[e]);
 }
 
 // sum of the xbar partials -> FP64 complex xbar (G x W), for the measurement
@@ -595,6 +604,7 @@ int mixed_create(afqmc_engine *e)
     MTRY(engine_dalloc(e, &m->xbarp, (size_t)m->splits * 2 * G * W));
     MTRY(engine_dalloc(e, &m->wfDaggerTm, (size_t)Ktot));
     MTRY(engine_dalloc(e, &m->err, 1));
+    MTRY(engine_dalloc(e, &m->ex2, (size_t)G * W));
     for (int b = 0; b < e->bl.nblk; ++b) {
         const int Ns = e->bl.Ns[b];
         if (Ns == 0 || !exchange_tc_supported(n, Ns)) continue;
@@ -735,13 +745,16 @@ int mixed_exchange(afqmc_engine *e)
             return engine_fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
         return engine_check_launch();
     }
-    MTRY(cuda_check(cudaMemsetAsync(e->ex, 0, sizeof(zd) * e->G * e->W, e->stream), "memset ex"));
+    int nb = 0;
     for (int b = 0; b < e->bl.nblk; ++b) {
         if (e->bl.Ns[b] == 0) continue;
+        zd *out = nb == 0 ? e->ex : m->ex2;
         int r = exchange_tc_launch(e->stream, e->G, e->W, e->bl.Ns[b], e->n, m->A2r[b], m->A2i[b],
-                                   m->Theta, e->bl.tOff[b], e->Ktot, e->alive, e->ex, m->err);
+                                   m->Theta, e->bl.tOff[b], e->Ktot, e->alive, out, m->err);
         if (r) return engine_fail(AFQMC_ERR_CUDA, "exchange launch: " + std::to_string(r));
+        ++nb;
     }
+    if (nb == 2) add_planes_kernel<<<592, 256, 0, e->stream>>>((long long)e->G * e->W, m->ex2, e->ex);
     return engine_check_launch();
 }
 
