@@ -157,11 +157,9 @@ cudaError_t zgemm_batched(const ZGemmArgs &a, cudaStream_t stream)
     g_launch_count++;
     if (a.m <= 0 || a.n <= 0 || a.batch <= 0) return cudaSuccess;
     if (a.k <= 0) return cudaErrorInvalidValue;
-    // Tile choice: 32x32 (4x4 per thread, 64 threads) for the per-walker
-    // overlap matrices, 128x32 (8x2, 256 threads) for tall-skinny products
-    // such as theta = phi S^-1, 64x64 (4x4) otherwise.
-    if (a.m <= 32 && a.n <= 32) return launch2<32, 32, 4, 4>(a, stream);
+    // Tile choice (measured on B200): 32x32 with 2x2 per thread for the
+    // per-walker overlap matrices, 64x64 with 4x4 otherwise.
+    if (a.m <= 32 && a.n <= 32) return launch2<32, 32, 2, 2>(a, stream);
     if (a.m <= 32) return launch2<32, 64, 2, 4>(a, stream);
-    if (a.n <= 32 && a.m >= 96) return launch2<128, 32, 8, 2>(a, stream);
     return launch2<64, 64, 4, 4>(a, stream);
 }
