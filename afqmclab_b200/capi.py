@@ -27,6 +27,7 @@ SYMBOLS = [
     "afqmc_get_cholesky_nums", "afqmc_pl_update_background", "afqmc_log_overlaps",
     "afqmc_green_matrix", "afqmc_taylor_stats", "afqmc_status", "afqmc_pop_configuration_dev",
     "afqmc_profile_enable", "afqmc_profile_get", "afqmc_launch_count", "afqmc_gemm_bf16_dev",
+    "afqmc_pop_configuration_noalloc_dev",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -84,6 +85,7 @@ def _declare(L):
                                      ctypes.POINTER(I)]
     L.afqmc_status.argtypes = [P, ctypes.POINTER(I)]
     L.afqmc_pop_configuration_dev.argtypes = [I, P, P, P, P]
+    L.afqmc_pop_configuration_noalloc_dev.argtypes = [I, P, P, P, P]
     L.afqmc_profile_enable.argtypes = [P, I]
     L.afqmc_profile_get.argtypes = [P, P, P]
     L.afqmc_launch_count.argtypes = []
@@ -282,6 +284,13 @@ def gemm_bf16_dev(M, N, K, A, lda, B, ldb, C, ldc, out_bf16=False, splits=1, spl
     """Device-pointer tcgen05 GEMM (see afqmc_gemm_bf16_dev)."""
     _check(lib().afqmc_gemm_bf16_dev(M, N, K, A, lda, B, ldb, C, ldc, 1 if out_bf16 else 0, splits,
                                      split_stride, alpha, stream))
+
+
+def pop_configuration_noalloc_dev(weights_dev_ptr, uniforms_dev_ptr, table_dev_ptr, W,
+                                  stream=None):
+    """popConfiguration that allocates nothing (see afqmc_pop_configuration_noalloc_dev)."""
+    _check(lib().afqmc_pop_configuration_noalloc_dev(W, weights_dev_ptr, uniforms_dev_ptr,
+                                                     table_dev_ptr, stream))
 
 
 def launch_count():

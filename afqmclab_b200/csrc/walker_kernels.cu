@@ -1182,3 +1182,13 @@ void launch_taylor_stats(int W, const int *mask, const int *order, long long *st
     g_launch_count++;
     taylor_stats_kernel<<<1, 256, 0, s>>>(W, mask, order, stats);
 }
+
+// popConfiguration with the count array in caller-provided global scratch
+// (W ints), used by the allocation-free entry point.  The kernel clears the
+// scratch before use.
+void launch_pop_comb_scratch(int W, const double *weight, const double *uniforms, int *number,
+                             int *table, cudaStream_t s)
+{
+    g_launch_count++;
+    pop_comb_kernel<<<1, 256, 0, s>>>(W, weight, uniforms, 0, nullptr, number, table, nullptr, 0);
+}

@@ -90,3 +90,5 @@ void launch_measure_reduce(int W, const int *alive, const zd *eloc, const zd *de
                            int nparts, zd *acc, int G, const zd *xbar, const zd *ex, zd *bgNum,
                            zd *exNum, cudaStream_t s);
 void launch_taylor_stats(int W, const int *mask, const int *order, long long *stats, cudaStream_t s);
+void launch_pop_comb_scratch(int W, const double *weight, const double *uniforms, int *number,
+                             int *table, cudaStream_t s);

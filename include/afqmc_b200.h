@@ -204,6 +204,24 @@ int afqmc_profile_get(afqmc_engine *e, double *ms, long long *counts);
 int afqmc_pop_configuration_dev(int W, const double *weights, const double *uniforms, int *table,
                                 void *stream);
 
+/* Allocation-free variant of afqmc_pop_configuration_dev, for callers that
+ * cannot allocate device memory where they need a population-control table
+ * (a host framework that owns the GPU memory through its own pool, a fixed
+ * start-up memory budget, or a loop that cannot afford an allocation's
+ * implicit synchronisation).  It has no counterpart in the reference.
+ * Same inputs, outputs and table as afqmc_pop_configuration_dev; its only
+ * scratch, the per-walker copy counts, is a file-scope device array of
+ * AFQMC_NOALLOC_MAX_WALKERS ints that every GPU loading the library holds
+ * until the process exits.  W above that limit is rejected with
+ * AFQMC_ERR_ARG.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first
+ * call before any stream capture.  The kernel clears the counts itself, but
+ * all calls share the one array: calls that overlap on the GPU (different
+ * streams, no ordering) race on it. */
+#define AFQMC_NOALLOC_MAX_WALKERS 65536
+int afqmc_pop_configuration_noalloc_dev(int W, const double *weights, const double *uniforms,
+                                        int *table, void *stream);
+
 /* Tensor-core (tcgen05) bf16 GEMM used by the mixed-precision form, the
  * batched counterpart of gmm_cpu (tensor_2d_bl_cpu.cpp:61-75):
  * C[m + n*ldc] = alpha * sum_k A[m*lda + k] * B[n*ldb + k]  (A, B bf16
