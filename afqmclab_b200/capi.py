@@ -27,7 +27,7 @@ SYMBOLS = [
     "afqmc_get_cholesky_nums", "afqmc_pl_update_background", "afqmc_log_overlaps",
     "afqmc_green_matrix", "afqmc_taylor_stats", "afqmc_status", "afqmc_pop_configuration_dev",
     "afqmc_profile_enable", "afqmc_profile_get", "afqmc_launch_count", "afqmc_gemm_bf16_dev",
-    "afqmc_pop_configuration_noalloc_dev",
+    "afqmc_pop_configuration_noalloc_dev", "afqmc_set_graphs",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -89,6 +89,7 @@ def _declare(L):
     L.afqmc_profile_enable.argtypes = [P, I]
     L.afqmc_profile_get.argtypes = [P, P, P]
     L.afqmc_launch_count.argtypes = []
+    L.afqmc_set_graphs.argtypes = [P, I]
     LL = ctypes.c_longlong
     L.afqmc_gemm_bf16_dev.argtypes = [I, I, I, P, LL, P, LL, P, LL, I, I, LL, ctypes.c_float, P]
     for name in SYMBOLS[2:]:
@@ -164,6 +165,9 @@ class Engine:
 
     def set_stream(self, stream_ptr):
         _check(lib().afqmc_set_stream(self.h, stream_ptr))
+
+    def set_graphs(self, enable=True):
+        _check(lib().afqmc_set_graphs(self.h, 1 if enable else 0))
 
     def synchronize(self):
         _check(lib().afqmc_synchronize(self.h))

@@ -381,7 +381,7 @@ int pop_control(afqmc_engine *e)
     return check_launch();
 }
 
-int project_one_step(afqmc_engine *e)
+int project_one_step_direct(afqmc_engine *e)
 {
     TRY(project_dtk_dtv(e));
     e->mgsIndex++;
@@ -391,7 +391,74 @@ int project_one_step(afqmc_engine *e)
     return AFQMC_OK;
 }
 
+void drop_graphs(afqmc_engine *e)
+{
+    for (auto &g : e->graphExec)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    e->graphWarm = false;
+    e->measWarm = false;
+}
+
+// Records the kernels that `body` issues on the engine stream into a graph.
+template <class F>
+int capture(afqmc_engine *e, cudaGraphExec_t *out, F body)
+{
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int r = body();
+    cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
+    if (r != AFQMC_OK) { if (g) cudaGraphDestroy(g); return r; }
+    if (ce != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+    return AFQMC_OK;
+}
+
+// projectOneStep: with graphs on, the step's kernels (and the cadence
+// operations due at this step) replay as one graph launch.  The first step
+// runs directly so that every launcher's one-time setup happens outside
+// capture; the profiler needs direct launches.
+int project_one_step(afqmc_engine *e)
+{
+    if (!e->useGraphs || e->prof || !e->graphWarm) {
+        int r = project_one_step_direct(e);
+        if (r == AFQMC_OK && e->useGraphs) e->graphWarm = true;
+        return r;
+    }
+    const bool doMgs = (e->mgsIndex + 1 == e->mgsStep);
+    const bool doPop = (e->popIndex + 1 == e->popStep);
+    const int key = (doMgs ? 1 : 0) | (doPop ? 2 : 0);
+    if (!e->graphExec[key]) {
+        TRY(capture(e, &e->graphExec[key], [&]() {
+            TRY(project_dtk_dtv(e));
+            if (doMgs) TRY(modify_gm(e));
+            if (doPop) TRY(pop_control(e));
+            return AFQMC_OK;
+        }));
+    }
+    CUDA_TRY(cudaGraphLaunch(e->graphExec[key], e->stream));
+    e->mgsIndex = doMgs ? 0 : e->mgsIndex + 1;
+    e->popIndex = doPop ? 0 : e->popIndex + 1;
+    return AFQMC_OK;
+}
+
+int add_mixed_measurement_direct(afqmc_engine *e);
+
 int add_mixed_measurement(afqmc_engine *e)
+{
+    if (!e->useGraphs || e->prof || !e->measWarm) {
+        int r = add_mixed_measurement_direct(e);
+        if (r == AFQMC_OK && e->useGraphs) e->measWarm = true;
+        return r;
+    }
+    if (!e->graphExec[4])
+        TRY(capture(e, &e->graphExec[4], [&]() { return add_mixed_measurement_direct(e); }));
+    CUDA_TRY(cudaGraphLaunch(e->graphExec[4], e->stream));
+    return AFQMC_OK;
+}
+
+int add_mixed_measurement_direct(afqmc_engine *e)
 {
     if (e->precision == AFQMC_MIXED) return mixed_add_measurement(e);
     const int W = e->W;
@@ -443,6 +510,7 @@ int create_common_checks(int W, int precision)
 void free_engine(afqmc_engine *e)
 {
     if (!e) return;
+    drop_graphs(e);
     if (e->mx) mixed_destroy(e);
     prof_resolve(e);
     for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
@@ -646,7 +714,9 @@ int afqmc_destroy(afqmc_engine *e)
 int afqmc_set_stream(afqmc_engine *e, void *cuda_stream)
 {
     if (!e) return fail(AFQMC_ERR_ARG, "null engine");
-    e->stream = cuda_stream ? (cudaStream_t)cuda_stream : e->own;
+    cudaStream_t ns = cuda_stream ? (cudaStream_t)cuda_stream : e->own;
+    if (ns != e->stream) drop_graphs(e);
+    e->stream = ns;
     return AFQMC_OK;
 }
 
@@ -682,6 +752,7 @@ int afqmc_get_walkers(afqmc_engine *e, double *wf, double *logw, int *alive)
 int afqmc_set_rng(afqmc_engine *e, unsigned long long seed, unsigned long long counter)
 {
     if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    if (seed != e->seed) drop_graphs(e);
     e->seed = seed;
     CUDA_TRY(cudaMemcpyAsync(e->counter, &counter, sizeof(counter), cudaMemcpyHostToDevice, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
@@ -702,6 +773,7 @@ int afqmc_get_rng(afqmc_engine *e, unsigned long long *seed, unsigned long long 
 int afqmc_set_ET(afqmc_engine *e, double ET)
 {
     if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    if (ET != e->ET) drop_graphs(e);
     e->ET = ET;
     return AFQMC_OK;
 }
@@ -802,6 +874,7 @@ int afqmc_pl_update_background(afqmc_engine *e, const double *bg, const double *
 {
     if (!e || e->kind != KIND_PL || !bg) return fail(AFQMC_ERR_ARG, "phaseless engine and bg required");
     const size_t n2 = (size_t)e->n * e->n;
+    drop_graphs(e);
     CUDA_TRY(cudaMemcpyAsync(e->bg, bg, sizeof(double) * e->G, cudaMemcpyHostToDevice, e->stream));
     if (expMinusDtK) {
         if (!e->expK[0]) TRY(dalloc(e, &e->expK[0], n2));
@@ -899,6 +972,14 @@ int afqmc_status(afqmc_engine *e, int *status_or)
 }
 
 long long afqmc_launch_count(void) { return g_launch_count.load(); }
+
+int afqmc_set_graphs(afqmc_engine *e, int enable)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    if (!enable) drop_graphs(e);
+    e->useGraphs = enable != 0;
+    return AFQMC_OK;
+}
 
 int afqmc_profile_enable(afqmc_engine *e, int on)
 {

@@ -65,6 +65,11 @@ struct afqmc_engine {
     std::vector<cudaEvent_t> evpool;
     double profMs[AFQMC_NPHASES] = {};
     long long profCount[AFQMC_NPHASES] = {};
+    // CUDA graphs of the step, one per cadence variant (bit 0: modifyGM,
+    // bit 1: popControl), and of the measurement (index 4)
+    bool useGraphs = false;
+    bool graphWarm = false, measWarm = false;
+    cudaGraphExec_t graphExec[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     std::vector<void *> allocs;
 };
 

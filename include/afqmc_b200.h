@@ -130,6 +130,13 @@ int afqmc_set_cadence(afqmc_engine *e, int mgs_index, int pop_control_index);
  * modifyGM every mgs_step and popControl every pop_control_step. */
 int afqmc_project_one_step(afqmc_engine *e, int nsteps);
 
+/* With enable != 0, afqmc_project_one_step and afqmc_add_mixed_measurement
+ * replay CUDA graphs of their kernel sequences (one per cadence variant),
+ * captured on first use after one direct step; changing E_T, the seed, the
+ * stream or the one-body operators re-captures.  No counterpart in the
+ * reference (it launches nothing). */
+int afqmc_set_graphs(afqmc_engine *e, int enable);
+
 /* projectExpMinusHalfDtK (which = -1) / projectExpHalfDtK (which = +1)
  * (afqmcConstraintPathProjection.cpp:11-29, afqmcPhaselessProjection.cpp:11-73) */
 int afqmc_project_half(afqmc_engine *e, int which);
