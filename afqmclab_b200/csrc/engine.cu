@@ -400,12 +400,17 @@ void drop_graphs(afqmc_engine *e)
 }
 
 // Records the kernels that `body` issues on the engine stream into a graph.
+// The launches issued while capturing are counted as the graph's kernel
+// nodes and credited to the launch counter each time the graph is replayed.
 template <class F>
-int capture(afqmc_engine *e, cudaGraphExec_t *out, F body)
+int capture(afqmc_engine *e, cudaGraphExec_t *out, long long *kernels, F body)
 {
     cudaGraph_t g = nullptr;
     CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    const long long c0 = g_launch_count.load();
     int r = body();
+    *kernels = g_launch_count.load() - c0;
+    g_launch_count -= *kernels;
     cudaError_t ce = cudaStreamEndCapture(e->stream, &g);
     if (r != AFQMC_OK) { if (g) cudaGraphDestroy(g); return r; }
     if (ce != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(ce));
@@ -430,7 +435,7 @@ int project_one_step(afqmc_engine *e)
     const bool doPop = (e->popIndex + 1 == e->popStep);
     const int key = (doMgs ? 1 : 0) | (doPop ? 2 : 0);
     if (!e->graphExec[key]) {
-        TRY(capture(e, &e->graphExec[key], [&]() {
+        TRY(capture(e, &e->graphExec[key], &e->graphKernels[key], [&]() {
             TRY(project_dtk_dtv(e));
             if (doMgs) TRY(modify_gm(e));
             if (doPop) TRY(pop_control(e));
@@ -438,6 +443,7 @@ int project_one_step(afqmc_engine *e)
         }));
     }
     CUDA_TRY(cudaGraphLaunch(e->graphExec[key], e->stream));
+    g_launch_count += e->graphKernels[key];
     e->mgsIndex = doMgs ? 0 : e->mgsIndex + 1;
     e->popIndex = doPop ? 0 : e->popIndex + 1;
     return AFQMC_OK;
@@ -453,8 +459,9 @@ int add_mixed_measurement(afqmc_engine *e)
         return r;
     }
     if (!e->graphExec[4])
-        TRY(capture(e, &e->graphExec[4], [&]() { return add_mixed_measurement_direct(e); }));
+        TRY(capture(e, &e->graphExec[4], &e->graphKernels[4], [&]() { return add_mixed_measurement_direct(e); }));
     CUDA_TRY(cudaGraphLaunch(e->graphExec[4], e->stream));
+    g_launch_count += e->graphKernels[4];
     return AFQMC_OK;
 }
 

@@ -70,6 +70,7 @@ struct afqmc_engine {
     bool useGraphs = false;
     bool graphWarm = false, measWarm = false;
     cudaGraphExec_t graphExec[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    long long graphKernels[5] = {0, 0, 0, 0, 0};  // kernel nodes per graph
     std::vector<void *> allocs;
 };
 

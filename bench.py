@@ -219,6 +219,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=5)
     ap.add_argument("--no-fp64-side", action="store_true")
+    ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--energy-steps", type=int, default=60)
     args = ap.parse_args()
     rank, world, local = dist_info()
@@ -264,6 +265,8 @@ def main():
     W = c["W"]
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
+    if not args.no_graphs:
+        eng.set_graphs(True)
 
     # warm-up
     run_steps(eng, args.warmup, 0, args.measure_skip)
@@ -273,9 +276,16 @@ def main():
         if world > 1:
             torch.distributed.barrier()
 
+    # per-phase CUDA-event times (direct launches) over K steps, then the
     # timed region: K steps, inputs resident in HBM (population + model
-    # tensors exceed the 126 MB L2 at this size)
+    # tensors exceed the 126 MB L2 at this size), graphs replayed
     eng.profile(True)
+    run_steps(eng, args.steps, args.warmup, args.measure_skip)
+    eng.synchronize()
+    prof = eng.profile_get()
+    eng.profile(False)
+    run_steps(eng, 2, args.warmup + args.steps, args.measure_skip)
+    eng.synchronize()
     launches0 = capi.launch_count()
     clocks = ClockSampler(dev)
     barrier()
@@ -284,7 +294,7 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    run_steps(eng, args.steps, args.warmup, args.measure_skip)
+    run_steps(eng, args.steps, args.warmup + 2 + args.steps, args.measure_skip)
     ev1.record(stream)
     ev1.synchronize()
     barrier()
@@ -292,8 +302,6 @@ def main():
     clk = clocks.stop()
     launches = capi.launch_count() - launches0
     ms = ev0.elapsed_time(ev1)
-    prof = eng.profile_get()
-    eng.profile(False)
     if world > 1:
         t = torch.tensor([ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -356,6 +364,8 @@ def main():
         eng.close()
         f64, _, _, _ = build_engine(capi, inputs, args.workload, "fp64", 77 + rank)
         f64.set_stream(stream.cuda_stream)
+        if not args.no_graphs:
+            f64.set_graphs(True)
         run_steps(f64, 2, 0, args.measure_skip)
         f64.synchronize()
         k64 = max(5, min(args.steps, 10))
@@ -391,7 +401,8 @@ def main():
                        "walkers_per_gpu": W, "dt": c["dt"], "mgs_step": c["mgs"],
                        "pop_control_step": c["pop"], "measure_skip": args.measure_skip,
                        "parallelism": f"walker-dp{world}",
-                       "l2": "inputs larger than L2 (no flush)"},
+                       "l2": "inputs larger than L2 (no flush)",
+                       "cuda_graphs": not args.no_graphs},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk,
             "phases_ms": {k: round(v[0], 3) for k, v in prof.items() if v[1] > 0},
