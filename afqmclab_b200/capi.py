@@ -27,7 +27,7 @@ SYMBOLS = [
     "afqmc_get_cholesky_nums", "afqmc_pl_update_background", "afqmc_log_overlaps",
     "afqmc_green_matrix", "afqmc_taylor_stats", "afqmc_status", "afqmc_pop_configuration_dev",
     "afqmc_profile_enable", "afqmc_profile_get", "afqmc_launch_count", "afqmc_gemm_bf16_dev",
-    "afqmc_pop_configuration_noalloc_dev", "afqmc_set_graphs",
+    "afqmc_pop_configuration_noalloc_dev", "afqmc_set_graphs", "afqmc_pl_adjoint",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -90,6 +90,7 @@ def _declare(L):
     L.afqmc_profile_get.argtypes = [P, P, P]
     L.afqmc_launch_count.argtypes = []
     L.afqmc_set_graphs.argtypes = [P, I]
+    L.afqmc_pl_adjoint.argtypes = [P, P, P, P, P, P, P, P, P]
     LL = ctypes.c_longlong
     L.afqmc_gemm_bf16_dev.argtypes = [I, I, I, P, LL, P, LL, P, LL, I, I, LL, ctypes.c_float, P]
     for name in SYMBOLS[2:]:
@@ -238,6 +239,22 @@ class Engine:
         cnt = np.zeros(len(PHASES), np.int64)
         _check(lib().afqmc_profile_get(self.h, _p(ms), _p(cnt)))
         return {PHASES[i]: (float(ms[i]), int(cnt[i])) for i in range(len(PHASES))}
+
+    def adjoint(self, want_chol=True):
+        """Mixed local energy, mean log-overlap and their gradients (afqmc_pl_adjoint)."""
+        n, G, nu, nd = self.n, self.G, self.nup, self.ndn
+        E = np.zeros(1, np.complex128)
+        L = np.zeros(1, np.complex128)
+        dt = np.zeros((n, n), np.complex128, order="F")
+        dc = np.zeros((n, n, G), np.complex128, order="F") if want_chol else None
+        du = np.zeros((n, nu), np.complex128, order="F")
+        dd = np.zeros((n, max(nd, 1)), np.complex128, order="F")
+        lu = np.zeros((n, nu), np.complex128, order="F")
+        ld = np.zeros((n, max(nd, 1)), np.complex128, order="F")
+        _check(lib().afqmc_pl_adjoint(self.h, _p(E), _p(L), _p(dt), _p(dc), _p(du),
+                                      _p(dd) if nd else None, _p(lu), _p(ld) if nd else None))
+        return {"E": E[0], "mean_logov": L[0], "dE_dt": dt, "dE_dchol": dc,
+                "dE_dconj_phiT": (du, dd[:, :nd]), "dlogov_dconj_phiT": (lu, ld[:, :nd])}
 
     def status(self):
         s = ctypes.c_int()

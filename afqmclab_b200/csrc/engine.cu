@@ -528,6 +528,29 @@ void free_engine(afqmc_engine *e)
 
 }  // namespace
 
+// Mixed-estimator ingredients at the current walkers, without the one-body
+// half step of addMixedMeasurement: logov, Sinv, thetaT, xbar, ex, eloc, den
+// (FP64 arithmetic; the mixed form's fp32 walkers are read through the FP64
+// copy).  Used by the adjoint.
+int engine_pl_local_energy(afqmc_engine *e)
+{
+    const int W = e->W;
+    cudaStream_t s = e->stream;
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    TRY(overlap_gemm(e, e->wf, e->alive));
+    launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, make_double2(0, 0),
+                             e->logwT, e->logov, e->alive, nullptr, nullptr, nullptr, e->status,
+                             LU_PLAIN, true, s);
+    TRY(check_launch());
+    TRY(theta_gemm(e, e->wf, e->alive));
+    TRY(xbar_gemm(e));
+    if (launch_pl_exchange(W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex, s))
+        return fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
+    launch_pl_energy(W, e->G, e->Ktot, e->wfDaggerT, e->thetaT, e->xbar, e->ex, e->alive, e->logov,
+                     e->eloc, e->den, e->parts, s);
+    return check_launch();
+}
+
 int engine_fail(int code, const std::string &msg) { return fail(code, msg); }
 int engine_check_launch() { return check_launch(); }
 int engine_gemm(const ZGemmArgs &a, cudaStream_t s) { return gemm(a, s); }
@@ -677,6 +700,7 @@ int afqmc_pl_create(int n, int Nup, int Ndn, int G, int W, int force_type, doubl
     CK(dalloc(e, &e->wfDaggerT, (size_t)e->Ktot));
     double *td = nullptr;
     CK(dupload(e, &td, t, n2));
+    e->tdev = td;
     // A_g,sigma = phiT_sigma^H L_g (initWfDaggerCholeskyVecs, :165-186) and
     // wfDaggerT = phiT_sigma^H t (initWfDaggerT, :148-163), stacked up/down
     for (int b = 0; b < e->bl.nblk; ++b) {

@@ -49,7 +49,7 @@ struct afqmc_engine {
     zd *wfDaggerK = nullptr;
     // phaseless
     CholDev cdv{};
-    double *chol = nullptr, *bg = nullptr;
+    double *chol = nullptr, *bg = nullptr, *tdev = nullptr;
     zd *Aall = nullptr, *wfDaggerT = nullptr, *xbar = nullptr, *forcePL = nullptr, *aux = nullptr,
        *M = nullptr, *ex = nullptr, *constForcePL = nullptr;
     long long Ktot = 0;

@@ -168,6 +168,21 @@ int afqmc_pl_update_background(afqmc_engine *e, const double *bg, const double *
                                double logwExpHalfDtK, const double *expMinusHalfDtK,
                                double logwExpMinusHalfDtK);
 
+/* Adjoint of the mixed local energy E = sum_w den_w E_w / sum_w den_w and of
+ * the mean log-overlap at the current walkers (no one-body half step), with
+ * respect to the one-body matrix t (RealMaterialMolecule::t), the Cholesky
+ * vectors (choleskyVecs) and the trial orbitals of the SD2s trial (E depends
+ * on conj(phiT) only; the orbital outputs are d/dconj(phiT)).  dE_dt is the
+ * mixed one-body density matrix (sum_s G_s of SD2sSD2isOperation::
+ * returnGreenMatrixUp/Dn, SD2sSD2isOperation.cpp:74-104, den-weighted).
+ * Outputs (host, complex, column-major, any may be NULL): energy (1),
+ * mean_logov (1), dE_dt (n x n), dE_dchol (n x n x G), dE_dconj_phiT_up
+ * (n x Nup), dE_dconj_phiT_dn (n x Ndn), dLogov_dconj_phiT_up/dn.
+ * FP64; determinants and D_g are recomputed per walker, nothing is stored. */
+int afqmc_pl_adjoint(afqmc_engine *e, double *energy, double *mean_logov, double *dE_dt,
+                     double *dE_dchol, double *dE_dconj_phiT_up, double *dE_dconj_phiT_dn,
+                     double *dLogov_dconj_phiT_up, double *dLogov_dconj_phiT_dn);
+
 /* Diagnostics (gauge-invariant quantities for parity checks) */
 /* log <phiT|phi_w> of every walker: SDSDOperation::returnLogOverlap (SDSDOperation.cpp:65-72) */
 int afqmc_log_overlaps(afqmc_engine *e, double *out);

@@ -1,0 +1,114 @@
+"""Adjoint of the mixed local energy and of the mean log-overlap
+(afqmc_pl_adjoint) on the phaseless shapes of the adjoint configuration
+(n=64, 16+16 electrons): the energy and the one-body derivative against the
+oracle (the den-weighted mixed Green's function of the reference's
+SD2sSD2isOperation), every derivative against central finite differences
+(step 1e-6, FP64) along random directions.
+
+Tolerances: 1e-10 relative against the oracle; 1e-6 relative against the
+finite differences."""
+import numpy as np
+import pytest
+import torch
+
+from afqmclab_b200 import adjoint, capi, inputs
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+FD_STEP = 1e-6
+FD_TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def setup():
+    m = inputs.molecule_inputs(64, 16, 16, 64, dt=0.005, decay=20.0, seed=11)
+    m.ET = -20.0
+    W = 48
+    eng = capi.pl_engine(m, W, 3, 1000, 1000)
+    eng.set_walkers(*inputs.initial_walkers(m.phiTUp, W, seed=5, noise=0.03))
+    eng.step(3)
+    walkers = eng.get_walkers()
+    eng.close()
+    return m, walkers, adjoint.AdjointContext(m, walkers)
+
+
+def test_energy_and_density_matrix_match_oracle(setup):
+    m, walkers, actx = setup
+    out = actx.evaluate(m.t, m.chol, m.phiTUp, m.phiTDn)
+    # oracle: mixed estimator with an identity half step = local energy at the walkers
+    ident = np.eye(m.n, dtype=np.complex128)
+    mo = inputs.MoleculeInputs(**{k: getattr(m, k) for k in ("n", "nup", "ndn", "G", "dt", "t", "K",
+                                                             "chol", "bg", "phiTUp", "phiTDn",
+                                                             "logwT")})
+    mo.set_background(m.bg)
+    mo.expHalfDtK = np.asfortranarray(ident)
+    mo.logwHalf = 0.0
+    o = O.pl_engine(mo, walkers[0].shape[2], 1)
+    o.set_walkers(*walkers)
+    el, den = o.add_mixed_measurement()
+    meas = o.measurement()
+    E_o = meas[1] / meas[0]
+    assert abs(out["E"] - E_o) < 1e-10 * abs(E_o)
+    # d E / d t = den-weighted mixed one-body density matrix sum_s G_s
+    rdm = np.zeros((m.n, m.n), np.complex128)
+    al = walkers[2].astype(bool)
+    for w in np.nonzero(al)[0]:
+        rdm += den[w] * (o.green(int(w), 0) + o.green(int(w), 1))
+    rdm /= den[al].sum()
+    assert np.abs(out["dE_dt"] - rdm).max() < 1e-10 * np.abs(rdm).max()
+
+
+def _fd(actx, base, which, direction):
+    args = [a.copy() for a in base]
+    plus = [a.copy() for a in base]
+    minus = [a.copy() for a in base]
+    plus[which] = plus[which] + FD_STEP * direction
+    minus[which] = minus[which] - FD_STEP * direction
+    ep = actx.evaluate(*plus, want_chol=False)
+    em = actx.evaluate(*minus, want_chol=False)
+    del args
+    return (ep["E"] - em["E"]) / (2 * FD_STEP), (ep["mean_logov"] - em["mean_logov"]) / (2 * FD_STEP)
+
+
+def test_adjoint_matches_central_differences(setup):
+    m, walkers, actx = setup
+    base = [m.t.copy(), m.chol.copy(), m.phiTUp.copy(), m.phiTDn.copy()]
+    out = actx.evaluate(*base)
+    rng = np.random.default_rng(99)
+    # one-body matrix t
+    d = rng.standard_normal(m.t.shape)
+    fd, _ = _fd(actx, base, 0, d)
+    an = np.sum(out["dE_dt"] * d)
+    assert abs(fd - an) <= FD_TOL * abs(an)
+    # Cholesky vectors
+    d = rng.standard_normal(m.chol.shape)
+    fd, _ = _fd(actx, base, 1, d)
+    an = np.sum(out["dE_dchol"] * d)
+    assert abs(fd - an) <= FD_TOL * abs(an)
+    # trial orbitals (E and log-overlap depend on conj(phiT): dE = sum dE/dconj * conj(delta))
+    for s in (0, 1):
+        d = rng.standard_normal(base[2 + s].shape) + 1j * rng.standard_normal(base[2 + s].shape)
+        fdE, fdL = _fd(actx, base, 2 + s, d)
+        anE = np.sum(out["dE_dconj_phiT"][s] * np.conj(d))
+        anL = np.sum(out["dlogov_dconj_phiT"][s] * np.conj(d))
+        assert abs(fdE - anE) <= FD_TOL * abs(anE)
+        assert abs(fdL - anL) <= FD_TOL * abs(anL)
+
+
+def test_autograd_wrapper_backward(setup):
+    m, walkers, actx = setup
+    t = torch.tensor(m.t, requires_grad=True)
+    c = torch.tensor(m.chol, requires_grad=True)
+    pu = torch.tensor(m.phiTUp, requires_grad=True)
+    pd = torch.tensor(m.phiTDn, requires_grad=True)
+    E = adjoint.MixedEnergy.apply(t, c, pu, pd, actx)
+    E.backward()
+    rng = np.random.default_rng(5)
+    d = rng.standard_normal(m.t.shape)
+    fd, _ = _fd(actx, [m.t, m.chol, m.phiTUp, m.phiTDn], 0, d)
+    assert abs(np.real(fd) - float((t.grad.numpy() * d).sum())) <= FD_TOL * abs(np.real(fd))
+    dz = rng.standard_normal(m.phiTUp.shape)  # real direction: d Re E = Re(<grad, dz>)
+    fdz, _ = _fd(actx, [m.t, m.chol, m.phiTUp, m.phiTDn], 2, dz)
+    got = float(np.real(np.sum(np.conj(pu.grad.numpy()) * dz)))
+    assert abs(np.real(fdz) - got) <= FD_TOL * abs(np.real(fdz))
