@@ -28,6 +28,8 @@ SYMBOLS = [
     "afqmc_green_matrix", "afqmc_taylor_stats", "afqmc_status", "afqmc_pop_configuration_dev",
     "afqmc_profile_enable", "afqmc_profile_get", "afqmc_launch_count", "afqmc_gemm_bf16_dev",
     "afqmc_pop_configuration_noalloc_dev", "afqmc_set_graphs", "afqmc_pl_adjoint",
+    "afqmc_pop_configuration_host", "afqmc_pop_weights", "afqmc_walker_bytes",
+    "afqmc_copy_walker_out", "afqmc_copy_walker_in", "afqmc_apply_table",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -91,11 +93,18 @@ def _declare(L):
     L.afqmc_launch_count.argtypes = []
     L.afqmc_set_graphs.argtypes = [P, I]
     L.afqmc_pl_adjoint.argtypes = [P, P, P, P, P, P, P, P, P]
+    L.afqmc_pop_configuration_host.argtypes = [I, I, P, P, P]
+    L.afqmc_pop_weights.argtypes = [P, P]
+    L.afqmc_walker_bytes.argtypes = [P]
+    L.afqmc_copy_walker_out.argtypes = [P, I, P]
+    L.afqmc_copy_walker_in.argtypes = [P, I, P]
+    L.afqmc_apply_table.argtypes = [P, P]
     LL = ctypes.c_longlong
     L.afqmc_gemm_bf16_dev.argtypes = [I, I, I, P, LL, P, LL, P, LL, I, I, LL, ctypes.c_float, P]
     for name in SYMBOLS[2:]:
         getattr(L, name).restype = I
     L.afqmc_launch_count.restype = ctypes.c_longlong
+    L.afqmc_walker_bytes.restype = ctypes.c_longlong
 
 
 def _check(r):
@@ -256,6 +265,24 @@ class Engine:
         return {"E": E[0], "mean_logov": L[0], "dE_dt": dt, "dE_dchol": dc,
                 "dE_dconj_phiT": (du, dd[:, :nd]), "dlogov_dconj_phiT": (lu, ld[:, :nd])}
 
+    def pop_weights(self):
+        w = np.zeros(self.W)
+        _check(lib().afqmc_pop_weights(self.h, _p(w)))
+        return w
+
+    def walker_bytes(self):
+        return int(lib().afqmc_walker_bytes(self.h))
+
+    def copy_walker_out(self, w, dst_ptr):
+        _check(lib().afqmc_copy_walker_out(self.h, w, dst_ptr))
+
+    def copy_walker_in(self, w, src_ptr):
+        _check(lib().afqmc_copy_walker_in(self.h, w, src_ptr))
+
+    def apply_table(self, table):
+        t = np.ascontiguousarray(table, dtype=np.int32)
+        _check(lib().afqmc_apply_table(self.h, _p(t)))
+
     def status(self):
         s = ctypes.c_int()
         _check(lib().afqmc_status(self.h, ctypes.byref(s)))
@@ -312,6 +339,15 @@ def pop_configuration_noalloc_dev(weights_dev_ptr, uniforms_dev_ptr, table_dev_p
     """popConfiguration that allocates nothing (see afqmc_pop_configuration_noalloc_dev)."""
     _check(lib().afqmc_pop_configuration_noalloc_dev(W, weights_dev_ptr, uniforms_dev_ptr,
                                                      table_dev_ptr, stream))
+
+
+def pop_configuration_host(weights, uniforms, size=1):
+    """popConfiguration(size, weight) with explicit uniforms (host)."""
+    w = np.ascontiguousarray(weights, dtype=np.float64)
+    u = np.ascontiguousarray(uniforms, dtype=np.float64)
+    table = np.zeros(len(w), np.int32)
+    _check(lib().afqmc_pop_configuration_host(len(w), size, _p(w), _p(u), _p(table)))
+    return table
 
 
 def launch_count():

@@ -1057,6 +1057,106 @@ int afqmc_gemm_bf16_dev(int M, int N, int K, const void *A, long long lda, const
     return AFQMC_OK;
 }
 
+int afqmc_pop_configuration_host(int L, int size, const double *weight, const double *uniforms,
+                                 int *table)
+{
+    if (L <= 0 || size <= 0 || L % size != 0 || !weight || !uniforms || !table)
+        return fail(AFQMC_ERR_ARG, "need L > 0 divisible by size and non-null arrays");
+    const int Lc = L / size;
+    double sum = 0.0;
+    for (int i = 0; i < L; ++i) sum += weight[i];
+    std::vector<int> number(L, 0);
+    int index_old = 0;
+    double prob_sum_old = weight[0] / sum;
+    for (int i = 0; i < L; ++i) {
+        double prob_sum_new = (i + uniforms[i]) / (L * 1.0);
+        while (prob_sum_new > prob_sum_old && index_old < L - 1) {
+            index_old++;
+            prob_sum_old += weight[index_old] / sum;
+        }
+        number[index_old]++;
+    }
+    for (int i = 0; i < L; ++i) table[i] = number[i] != 0 ? i : -1;
+    auto fill = [&](int lo, int hi) {
+        int zero_i = lo, one_i = lo;
+        while (zero_i < hi && number[zero_i] != 0) zero_i++;
+        while (one_i < hi && number[one_i] <= 1) one_i++;
+        while (zero_i < hi && one_i < hi) {
+            table[zero_i] = one_i; number[zero_i]++; number[one_i]--;
+            while (zero_i < hi && number[zero_i] != 0) zero_i++;
+            while (one_i < hi && number[one_i] <= 1) one_i++;
+        }
+    };
+    for (int c = 0; c < size; ++c) fill(Lc * c, Lc * (c + 1));
+    if (size > 1) fill(0, L);
+    for (int i = 0; i < L; ++i)
+        if (number[i] != 1) return fail(AFQMC_ERR_STATE, "population configuration left a slot unfilled");
+    return AFQMC_OK;
+}
+
+int afqmc_pop_weights(afqmc_engine *e, double *weight_out)
+{
+    if (!e || !weight_out) return fail(AFQMC_ERR_ARG, "null argument");
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    TRY(overlap_gemm(e, e->wf, e->alive));
+    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
+                             e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
+                             LU_POPWEIGHT, false, e->stream);
+    TRY(check_launch());
+    CUDA_TRY(cudaMemcpyAsync(weight_out, e->weight, sizeof(double) * e->W, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+long long afqmc_walker_bytes(afqmc_engine *e)
+{
+    if (!e) return -1;
+    return (long long)sizeof(zd) * (e->wsize + 1);
+}
+
+int afqmc_copy_walker_out(afqmc_engine *e, int w, void *dst_dev)
+{
+    if (!e || !dst_dev || w < 0 || w >= e->W) return fail(AFQMC_ERR_ARG, "bad argument");
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    CUDA_TRY(cudaMemcpyAsync(dst_dev, e->wf + (size_t)w * e->wsize, sizeof(zd) * e->wsize,
+                             cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync((zd *)dst_dev + e->wsize, e->logw + w, sizeof(zd), cudaMemcpyDeviceToDevice,
+                             e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_copy_walker_in(afqmc_engine *e, int w, const void *src_dev)
+{
+    if (!e || !src_dev || w < 0 || w >= e->W) return fail(AFQMC_ERR_ARG, "bad argument");
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    CUDA_TRY(cudaMemcpyAsync(e->wf + (size_t)w * e->wsize, src_dev, sizeof(zd) * e->wsize,
+                             cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->logw + w, (const zd *)src_dev + e->wsize, sizeof(zd), cudaMemcpyDeviceToDevice,
+                             e->stream));
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_apply_table(afqmc_engine *e, const int *table)
+{
+    if (!e || !table) return fail(AFQMC_ERR_ARG, "null argument");
+    for (int i = 0; i < e->W; ++i)
+        if (table[i] < 0 || table[i] >= e->W) return fail(AFQMC_ERR_ARG, "table entry out of range");
+    CUDA_TRY(cudaMemcpyAsync(e->table, table, sizeof(int) * e->W, cudaMemcpyHostToDevice, e->stream));
+    if (e->precision == AFQMC_MIXED) {
+        TRY(mixed_sync_to_fp64(e));
+        launch_pop_gather(e->W, e->wsize, e->table, e->wf, e->logw, e->stream);
+        TRY(mixed_sync_from_fp64(e));
+    } else {
+        launch_pop_gather(e->W, e->wsize, e->table, e->wf, e->logw, e->stream);
+    }
+    TRY(check_launch());
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
 int afqmc_pop_configuration_dev(int W, const double *weights, const double *uniforms, int *table,
                                 void *stream)
 {

@@ -226,6 +226,30 @@ int afqmc_profile_get(afqmc_engine *e, double *ms, long long *counts);
 int afqmc_pop_configuration_dev(int W, const double *weights, const double *uniforms, int *table,
                                 void *stream);
 
+/* ---- population control across processes (one population per GPU) ----
+ * The reference gathers the weights on rank 0, builds the table there and
+ * moves walkers with MPI (populationControl<T>, populationControl.h:20-109;
+ * popConfiguration(size, weight), populationControlConfiguration.cpp:24-101).
+ * Here every rank computes the same table from the gathered weights and a
+ * shared uniform stream, then walkers move point to point (NCCL / gloo),
+ * see afqmclab_b200/parallel.py. */
+/* popConfiguration(size, weight) on the host, with explicit uniforms
+ * (L = size * walkers per rank); table[i] is the global parent of slot i. */
+int afqmc_pop_configuration_host(int L, int size, const double *weight, const double *uniforms,
+                                 int *table);
+/* First half of popControl on this rank: weights Re<phiT|phi>, logw -= logOverlap,
+ * walkers revived (afqmcConstraintPathProjection.cpp:106-122). */
+int afqmc_pop_weights(afqmc_engine *e, double *weight_out);
+/* Bytes of one walker in the transfer format: its n x ncol complex128
+ * matrix followed by its complex128 logw. */
+long long afqmc_walker_bytes(afqmc_engine *e);
+/* Copy walker w to / from a device buffer of afqmc_walker_bytes bytes. */
+int afqmc_copy_walker_out(afqmc_engine *e, int w, void *dst_dev);
+int afqmc_copy_walker_in(afqmc_engine *e, int w, const void *src_dev);
+/* In-place copies walker[i] = walker[table[i]] within this rank (table in
+ * local indices; parents keep their own slot). */
+int afqmc_apply_table(afqmc_engine *e, const int *table);
+
 /* Allocation-free variant of afqmc_pop_configuration_dev, for callers that
  * cannot allocate device memory where they need a population-control table
  * (a host framework that owns the GPU memory through its own pool, a fixed
