@@ -30,6 +30,8 @@ SYMBOLS = [
     "afqmc_pop_configuration_noalloc_dev", "afqmc_set_graphs", "afqmc_pl_adjoint",
     "afqmc_pop_configuration_host", "afqmc_pop_weights", "afqmc_walker_bytes",
     "afqmc_copy_walker_out", "afqmc_copy_walker_in", "afqmc_apply_table",
+    "afqmc_batch_create", "afqmc_batch_step", "afqmc_batch_synchronize", "afqmc_batch_destroy",
+    "afqmc_set_autotune",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -99,6 +101,11 @@ def _declare(L):
     L.afqmc_copy_walker_out.argtypes = [P, I, P]
     L.afqmc_copy_walker_in.argtypes = [P, I, P]
     L.afqmc_apply_table.argtypes = [P, P]
+    L.afqmc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), I, PP]
+    L.afqmc_batch_step.argtypes = [P, I]
+    L.afqmc_batch_synchronize.argtypes = [P]
+    L.afqmc_batch_destroy.argtypes = [P]
+    L.afqmc_set_autotune.argtypes = [I]
     LL = ctypes.c_longlong
     L.afqmc_gemm_bf16_dev.argtypes = [I, I, I, P, LL, P, LL, P, LL, I, I, LL, ctypes.c_float, P]
     for name in SYMBOLS[2:]:
@@ -348,6 +355,38 @@ def pop_configuration_host(weights, uniforms, size=1):
     table = np.zeros(len(w), np.int32)
     _check(lib().afqmc_pop_configuration_host(len(w), size, _p(w), _p(u), _p(table)))
     return table
+
+
+def set_autotune(enable=True):
+    _check(lib().afqmc_set_autotune(1 if enable else 0))
+
+
+class Batch:
+    """Engines advanced together, one graph launch per step (afqmc_batch_*)."""
+
+    def __init__(self, engines):
+        self.engines = list(engines)
+        arr = (ctypes.c_void_p * len(self.engines))(*[e.h for e in self.engines])
+        h = ctypes.c_void_p()
+        _check(lib().afqmc_batch_create(arr, len(self.engines), ctypes.byref(h)))
+        self.h = h.value
+
+    def step(self, nsteps=1):
+        _check(lib().afqmc_batch_step(self.h, nsteps))
+
+    def synchronize(self):
+        _check(lib().afqmc_batch_synchronize(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().afqmc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def launch_count():

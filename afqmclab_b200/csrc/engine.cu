@@ -1057,6 +1057,132 @@ int afqmc_gemm_bf16_dev(int M, int N, int K, const void *A, long long lda, const
     return AFQMC_OK;
 }
 
+int afqmc_set_autotune(int enable)
+{
+    zgemm_set_autotune(enable);
+    return AFQMC_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batches
+// Several engines (e.g. lattices of different size and filling) advanced
+// together: each step is one graph with one branch per engine, each branch
+// on that engine's stream, forked from and joined to the batch stream.
+struct afqmc_batch {
+    std::vector<afqmc_engine *> engines;
+    std::vector<cudaEvent_t> joins;
+    cudaEvent_t fork = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long kernels[4] = {0, 0, 0, 0};
+    bool warm = false;
+};
+
+namespace {
+void batch_drop(afqmc_batch *b)
+{
+    for (auto &g : b->exec)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+    b->warm = false;
+}
+}  // namespace
+
+extern "C" {
+
+int afqmc_batch_create(afqmc_engine **engines, int count, afqmc_batch **out)
+{
+    if (!engines || count <= 0 || !out) return fail(AFQMC_ERR_ARG, "bad argument");
+    for (int i = 0; i < count; ++i) {
+        if (!engines[i]) return fail(AFQMC_ERR_ARG, "null engine in batch");
+        if (engines[i]->mgsStep != engines[0]->mgsStep || engines[i]->popStep != engines[0]->popStep ||
+            engines[i]->mgsIndex != engines[0]->mgsIndex || engines[i]->popIndex != engines[0]->popIndex)
+            return fail(AFQMC_ERR_ARG, "engines of a batch must share the stabilisation and population-control cadence");
+    }
+    afqmc_batch *b = new afqmc_batch();
+    b->engines.assign(engines, engines + count);
+    cudaError_t r = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (r == cudaSuccess) r = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    b->joins.resize(count, nullptr);
+    for (int i = 0; i < count && r == cudaSuccess; ++i)
+        r = cudaEventCreateWithFlags(&b->joins[i], cudaEventDisableTiming);
+    if (r != cudaSuccess) { delete b; return fail(AFQMC_ERR_CUDA, cudaGetErrorString(r)); }
+    *out = b;
+    return AFQMC_OK;
+}
+
+int afqmc_batch_destroy(afqmc_batch *b)
+{
+    if (!b) return AFQMC_OK;
+    cudaStreamSynchronize(b->stream);
+    batch_drop(b);
+    for (cudaEvent_t ev : b->joins) if (ev) cudaEventDestroy(ev);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return AFQMC_OK;
+}
+
+int afqmc_batch_step(afqmc_batch *b, int nsteps)
+{
+    if (!b) return fail(AFQMC_ERR_ARG, "null batch");
+    for (int s = 0; s < nsteps; ++s) {
+        afqmc_engine *e0 = b->engines[0];
+        const bool doMgs = (e0->mgsIndex + 1 == e0->mgsStep);
+        const bool doPop = (e0->popIndex + 1 == e0->popStep);
+        const int key = (doMgs ? 1 : 0) | (doPop ? 2 : 0);
+        bool profiling = false;
+        for (auto *e : b->engines) profiling |= e->prof;
+        if (!b->warm || profiling) {
+            // first step direct: one-time launcher setup and autotuning happen
+            // here; the profiler also needs direct launches
+            for (auto *e : b->engines) TRY(project_one_step_direct(e));
+            for (auto *e : b->engines) CUDA_TRY(cudaStreamSynchronize(e->stream));
+            b->warm = true;
+            continue;
+        }
+        if (!b->exec[key]) {
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            const long long c0 = g_launch_count.load();
+            int r = AFQMC_OK;
+            cudaEventRecord(b->fork, b->stream);
+            for (size_t i = 0; i < b->engines.size() && r == AFQMC_OK; ++i) {
+                afqmc_engine *e = b->engines[i];
+                cudaStreamWaitEvent(e->stream, b->fork, 0);
+                r = project_dtk_dtv(e);
+                if (r == AFQMC_OK && doMgs) r = modify_gm(e);
+                if (r == AFQMC_OK && doPop) r = pop_control(e);
+                cudaEventRecord(b->joins[i], e->stream);
+                cudaStreamWaitEvent(b->stream, b->joins[i], 0);
+            }
+            b->kernels[key] = g_launch_count.load() - c0;
+            g_launch_count -= b->kernels[key];
+            cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+            if (r != AFQMC_OK) { if (g) cudaGraphDestroy(g); return r; }
+            if (ce != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("batch capture: ") + cudaGetErrorString(ce));
+            ce = cudaGraphInstantiate(&b->exec[key], g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("batch instantiate: ") + cudaGetErrorString(ce));
+        }
+        CUDA_TRY(cudaGraphLaunch(b->exec[key], b->stream));
+        g_launch_count += b->kernels[key];
+        for (auto *e : b->engines) {
+            e->mgsIndex = doMgs ? 0 : e->mgsIndex + 1;
+            e->popIndex = doPop ? 0 : e->popIndex + 1;
+        }
+    }
+    return AFQMC_OK;
+}
+
+int afqmc_batch_synchronize(afqmc_batch *b)
+{
+    if (!b) return fail(AFQMC_ERR_ARG, "null batch");
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    for (auto *e : b->engines) CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
 int afqmc_pop_configuration_host(int L, int size, const double *weight, const double *uniforms,
                                  int *table)
 {

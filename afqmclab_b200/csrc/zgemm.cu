@@ -8,6 +8,9 @@
 #include <cuda_bf16.h>
 
 #include <atomic>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 extern std::atomic<long long> g_launch_count;
 
@@ -152,14 +155,84 @@ cudaError_t launch2(const ZGemmArgs &a, cudaStream_t s)
 
 }  // namespace
 
+// ----------------------------------------------------------- autotuner
+// Candidate tile shapes; the default rule picks one by size, the autotuner
+// (when enabled) times every candidate once per problem shape and keeps the
+// fastest.  Timing runs are synchronous, so shapes are tuned on first use
+// outside stream capture; captured launches reuse the cached choice.
+namespace {
+
+constexpr int NCAND = 4;
+
+cudaError_t launch_cand(int c, const ZGemmArgs &a, cudaStream_t s)
+{
+    switch (c) {
+    case 0: return launch2<32, 32, 2, 2>(a, s);
+    case 1: return launch2<32, 64, 2, 4>(a, s);
+    case 2: return launch2<64, 64, 4, 4>(a, s);
+    default: return launch2<128, 32, 8, 2>(a, s);
+    }
+}
+
+int default_cand(const ZGemmArgs &a)
+{
+    if (a.m <= 32 && a.n <= 32) return 0;
+    if (a.m <= 32) return 1;
+    return 2;
+}
+
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int, int, int, int, int>, int> g_tuned;
+std::atomic<int> g_autotune{0};
+
+}  // namespace
+
+void zgemm_set_autotune(int on) { g_autotune = on; }
+
+int zgemm_tuned_choice(const ZGemmArgs &a)
+{
+    auto key = std::make_tuple(a.m, a.n, a.k, a.opA, a.opB, a.a_real, a.b_real, a.batch);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tuned.find(key);
+    return it == g_tuned.end() ? -1 : it->second;
+}
+
 cudaError_t zgemm_batched(const ZGemmArgs &a, cudaStream_t stream)
 {
     g_launch_count++;
     if (a.m <= 0 || a.n <= 0 || a.batch <= 0) return cudaSuccess;
     if (a.k <= 0) return cudaErrorInvalidValue;
-    // Tile choice (measured on B200): 32x32 with 2x2 per thread for the
-    // per-walker overlap matrices, 64x64 with 4x4 otherwise.
-    if (a.m <= 32 && a.n <= 32) return launch2<32, 32, 2, 2>(a, stream);
-    if (a.m <= 32) return launch2<32, 64, 2, 4>(a, stream);
-    return launch2<64, 64, 4, 4>(a, stream);
+    const auto key = std::make_tuple(a.m, a.n, a.k, a.opA, a.opB, a.a_real, a.b_real, a.batch);
+    int choice = -1;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tuned.find(key);
+        if (it != g_tuned.end()) choice = it->second;
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(stream, &cs);
+    if (choice < 0 && g_autotune && cs == cudaStreamCaptureStatusNone && a.beta.x == 0.0 &&
+        a.beta.y == 0.0) {
+        // time every candidate (the output is simply rewritten each time)
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        float best = 1e30f;
+        for (int c = 0; c < NCAND; ++c) {
+            if (launch_cand(c, a, stream) != cudaSuccess) { cudaGetLastError(); continue; }
+            cudaEventRecord(e0, stream);
+            for (int r = 0; r < 3; ++r) launch_cand(c, a, stream);
+            cudaEventRecord(e1, stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best) { best = ms; choice = c; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tuned[key] = choice;
+    }
+    if (choice < 0) choice = default_cand(a);
+    return launch_cand(choice, a, stream);
 }

@@ -37,3 +37,7 @@ struct ZGemmArgs {
 
 // Launches on `stream`; returns cudaGetLastError().
 cudaError_t zgemm_batched(const ZGemmArgs &a, cudaStream_t stream);
+
+// Autotuner switch (process-wide) and the cached choice for a shape (-1: none).
+void zgemm_set_autotune(int on);
+int zgemm_tuned_choice(const ZGemmArgs &a);

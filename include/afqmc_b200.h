@@ -226,6 +226,23 @@ int afqmc_profile_get(afqmc_engine *e, double *ms, long long *counts);
 int afqmc_pop_configuration_dev(int W, const double *weights, const double *uniforms, int *table,
                                 void *stream);
 
+/* ---- uneven batches ----
+ * Engines of different lattice size and filling advanced together: each
+ * afqmc_batch_step is one CUDA-graph launch holding one branch per engine
+ * (each on its engine's stream).  The engines must share mgs_step,
+ * pop_control_step and their current cadence indices.  The first step runs
+ * directly (one-time setup, autotuning); the graphs are captured after it.
+ * No counterpart in the reference, which runs one lattice per process. */
+typedef struct afqmc_batch afqmc_batch;
+int afqmc_batch_create(afqmc_engine **engines, int count, afqmc_batch **out);
+int afqmc_batch_step(afqmc_batch *b, int nsteps);
+int afqmc_batch_synchronize(afqmc_batch *b);
+int afqmc_batch_destroy(afqmc_batch *b);
+/* Process-wide switch of the GEMM autotuner: with enable != 0 every new
+ * FP64 GEMM shape is timed once over the candidate tile shapes (outside
+ * stream capture) and the fastest is kept for that shape. */
+int afqmc_set_autotune(int enable);
+
 /* ---- population control across processes (one population per GPU) ----
  * The reference gathers the weights on rank 0, builds the table there and
  * moves walkers with MPI (populationControl<T>, populationControl.h:20-109;
