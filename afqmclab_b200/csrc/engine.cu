@@ -467,7 +467,9 @@ int add_mixed_measurement(afqmc_engine *e)
 
 int add_mixed_measurement_direct(afqmc_engine *e)
 {
-    if (e->precision == AFQMC_MIXED) return mixed_add_measurement(e);
+    if (e->precision == AFQMC_MIXED && e->kind == KIND_PL) return mixed_add_measurement(e);
+    // constrained-path mixed form: the measurement runs on an FP64 copy
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
     const int W = e->W;
     cudaStream_t s = e->stream;
     {
@@ -518,7 +520,7 @@ void free_engine(afqmc_engine *e)
 {
     if (!e) return;
     drop_graphs(e);
-    if (e->mx) mixed_destroy(e);
+    if (e->mx || e->cpm) mixed_destroy(e);
     prof_resolve(e);
     for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
     for (void *p : e->allocs) cudaFree(p);
@@ -997,7 +999,7 @@ int afqmc_status(afqmc_engine *e, int *status_or)
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     int o = 0;
     for (int v : st) o |= v;
-    if (e->mx) o |= mixed_status(e);
+    if (e->mx || e->cpm) o |= mixed_status(e);
     *status_or = o;
     return AFQMC_OK;
 }

@@ -11,6 +11,7 @@
 #include "zgemm.cuh"
 
 struct MixedState;
+struct CpMixedState;
 
 enum { KIND_CP = 0, KIND_PL = 1 };
 
@@ -58,6 +59,7 @@ struct afqmc_engine {
        *parts = nullptr;
     // mixed-precision state
     MixedState *mx = nullptr;
+    CpMixedState *cpm = nullptr;   // constrained-path mixed form
     // phase profiler (CUDA events on the engine stream; off unless enabled)
     bool prof = false;
     struct Mark { int phase; cudaEvent_t a, b; };

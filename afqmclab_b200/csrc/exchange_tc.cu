@@ -29,16 +29,6 @@ constexpr int XS_STAGES = 3;          // B stages: one 64-wide K box, both plane
 constexpr int XS_NCHUNK = 32;         // walker tiles per work item
 constexpr int XS_TILE_BYTES = 16384;  // 128 rows x 128 B
 
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0,
-                                            int c1, int c2)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(
-            smem_u32(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1), "r"(c2)
-        : "memory");
-}
-
 struct XSmem {
     // sA: 2 planes x 2 K boxes; sB: XS_STAGES x (2 planes); transpose: 4 warps x 32x33 float2
     static constexpr size_t bytes()

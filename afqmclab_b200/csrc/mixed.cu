@@ -18,6 +18,7 @@
 
 #include "engine_internal.cuh"
 #include "mixed.cuh"
+#include "cp_mixed.cuh"
 #include "tc_common.cuh"
 #include "tc_gemm.cuh"
 
@@ -582,7 +583,7 @@ int check_err(afqmc_engine *e)
 
 int mixed_create(afqmc_engine *e)
 {
-    if (e->kind != KIND_PL) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form is built for the phaseless engine");
+    if (e->kind == KIND_CP) return cp_mixed_create(e);
     if (e->n != 64 && e->n != 128) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form needs n = 64 or 128");
     if (e->ncol % 16 != 0 || e->ncol > 64) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form needs 16..64 columns in steps of 16");
     if (e->G % 64 != 0) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision form needs G a multiple of 64");
@@ -630,30 +631,35 @@ int mixed_create(afqmc_engine *e)
 
 void mixed_destroy(afqmc_engine *e)
 {
+    if (e->cpm) cp_mixed_destroy(e);
     delete e->mx;
     e->mx = nullptr;
 }
 
 int mixed_update_operators(afqmc_engine *e)
 {
+    if (e->kind == KIND_CP) return AFQMC_OK;
     build_et_kernel<<<64, 256, 0, e->stream>>>(e->n, e->expK[0], e->mx->Et);
     return engine_check_launch();
 }
 
 int mixed_sync_to_fp64(afqmc_engine *e)
 {
+    if (e->kind == KIND_CP) return cp_mixed_sync_to_fp64(e);
     f32p_to_wf_kernel<<<e->W, 256, 0, e->stream>>>(e->W, e->wsize, e->mx->wf32, e->wf, nullptr);
     return engine_check_launch();
 }
 
 int mixed_sync_from_fp64(afqmc_engine *e)
 {
+    if (e->kind == KIND_CP) return cp_mixed_sync_from_fp64(e);
     wf_to_f32p_kernel<<<e->W, 256, 0, e->stream>>>(e->W, e->wsize, e->wf, e->mx->wf32, nullptr);
     return engine_check_launch();
 }
 
 int mixed_status(afqmc_engine *e)
 {
+    if (e->kind == KIND_CP) return cp_mixed_status(e);
     int h = 0;
     cudaMemcpy(&h, e->mx->err, sizeof(int), cudaMemcpyDeviceToHost);
     return h ? 32 : 0;
@@ -661,6 +667,7 @@ int mixed_status(afqmc_engine *e)
 
 int mixed_project_dtk_dtv(afqmc_engine *e)
 {
+    if (e->kind == KIND_CP) return cp_mixed_project_dtk_dtv(e);
     MixedState *m = e->mx;
     const int W = e->W;
     cudaStream_t s = e->stream;
@@ -705,6 +712,7 @@ int mixed_project_dtk_dtv(afqmc_engine *e)
 
 int mixed_modify_gm(afqmc_engine *e)
 {
+    if (e->kind == KIND_CP) return cp_mixed_modify_gm(e);
     const size_t bytes = (size_t)e->n * e->ncol * sizeof(zd);
     static bool attr = false;
     if (!attr) {
@@ -719,6 +727,7 @@ int mixed_modify_gm(afqmc_engine *e)
 
 int mixed_pop_control(afqmc_engine *e)
 {
+    if (e->kind == KIND_CP) return cp_mixed_pop_control(e);
     MixedState *m = e->mx;
     MTRY(overlap32(e, m->wf32, e->alive));
     launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),

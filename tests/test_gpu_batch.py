@@ -12,11 +12,11 @@ LATTICES = [(4, 4, 7, 7, 4.0), (6, 6, 16, 16, 8.0), (8, 8, 28, 28, 4.0)]
 W = 48
 
 
-def _engines():
+def _engines(precision=capi.AFQMC_FP64):
     out = []
     for k, (nx, ny, nu, nd, U) in enumerate(LATTICES):
         m = inputs.hubbard_inputs(nx, ny, nu, nd, t=1.0, tp=0.0, U=U, dt=0.01)
-        e = capi.cp_engine(m, W, 100 + k, mgs_step=3, pop_step=5)
+        e = capi.cp_engine(m, W, 100 + k, mgs_step=3, pop_step=5, precision=precision)
         e.set_walkers(*inputs.initial_walkers(m.phiT, W, seed=7 + k, noise=0.05))
         out.append(e)
     return out
@@ -27,16 +27,17 @@ def _state(e):
     return wf, lw, al, e.rng_counter()
 
 
-def test_batch_matches_separate_engines():
+@pytest.mark.parametrize("precision", [capi.AFQMC_FP64, capi.AFQMC_MIXED])
+def test_batch_matches_separate_engines(precision):
     steps = 11
-    solo = _engines()
+    solo = _engines(precision)
     for e in solo:
         e.step(steps)
     ref = [_state(e) for e in solo]
     for e in solo:
         e.close()
 
-    engines = _engines()
+    engines = _engines(precision)
     b = capi.Batch(engines)
     b.step(steps)
     b.synchronize()

@@ -24,14 +24,15 @@ def _run(make, graphs, steps=13, measure_every=5):
     return out
 
 
-@pytest.mark.parametrize("kind", ["cp_fp64", "pl_fp64", "pl_mixed"])
+@pytest.mark.parametrize("kind", ["cp_fp64", "cp_mixed", "pl_fp64", "pl_mixed"])
 def test_graph_replay_matches_direct_launches(kind):
-    if kind == "cp_fp64":
+    if kind.startswith("cp"):
         m = inputs.hubbard_inputs(4, 4, 7, 7)
         m.ET = -12.0
+        prec = capi.AFQMC_MIXED if kind == "cp_mixed" else capi.AFQMC_FP64
 
         def make():
-            g = capi.cp_engine(m, 32, 5, 3, 4)
+            g = capi.cp_engine(m, 32, 5, 3, 4, precision=prec)
             g.set_walkers(*inputs.initial_walkers(m.phiT, 32, seed=1, noise=0.05))
             return g
     else:
