@@ -31,6 +31,7 @@ SYMBOLS = [
     "afqmc_pop_configuration_host", "afqmc_pop_weights", "afqmc_walker_bytes",
     "afqmc_copy_walker_out", "afqmc_copy_walker_in", "afqmc_apply_table",
     "afqmc_batch_create", "afqmc_batch_step", "afqmc_batch_synchronize", "afqmc_batch_destroy",
+    "afqmc_batch_set_stream",
     "afqmc_set_autotune",
 ]
 
@@ -105,6 +106,7 @@ def _declare(L):
     L.afqmc_batch_step.argtypes = [P, I]
     L.afqmc_batch_synchronize.argtypes = [P]
     L.afqmc_batch_destroy.argtypes = [P]
+    L.afqmc_batch_set_stream.argtypes = [P, P]
     L.afqmc_set_autotune.argtypes = [I]
     LL = ctypes.c_longlong
     L.afqmc_gemm_bf16_dev.argtypes = [I, I, I, P, LL, P, LL, P, LL, I, I, LL, ctypes.c_float, P]
@@ -376,6 +378,9 @@ class Batch:
 
     def synchronize(self):
         _check(lib().afqmc_batch_synchronize(self.h))
+
+    def set_stream(self, stream_ptr):
+        _check(lib().afqmc_batch_set_stream(self.h, stream_ptr))
 
     def close(self):
         if getattr(self, "h", None):

@@ -1075,7 +1075,7 @@ struct afqmc_batch {
     std::vector<afqmc_engine *> engines;
     std::vector<cudaEvent_t> joins;
     cudaEvent_t fork = nullptr;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr, own = nullptr;
     cudaGraphExec_t exec[4] = {nullptr, nullptr, nullptr, nullptr};
     long long kernels[4] = {0, 0, 0, 0};
     bool warm = false;
@@ -1103,7 +1103,8 @@ int afqmc_batch_create(afqmc_engine **engines, int count, afqmc_batch **out)
     }
     afqmc_batch *b = new afqmc_batch();
     b->engines.assign(engines, engines + count);
-    cudaError_t r = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    cudaError_t r = cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking);
+    b->stream = b->own;
     if (r == cudaSuccess) r = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     b->joins.resize(count, nullptr);
     for (int i = 0; i < count && r == cudaSuccess; ++i)
@@ -1120,7 +1121,7 @@ int afqmc_batch_destroy(afqmc_batch *b)
     batch_drop(b);
     for (cudaEvent_t ev : b->joins) if (ev) cudaEventDestroy(ev);
     if (b->fork) cudaEventDestroy(b->fork);
-    if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->own) cudaStreamDestroy(b->own);
     delete b;
     return AFQMC_OK;
 }
@@ -1138,8 +1139,16 @@ int afqmc_batch_step(afqmc_batch *b, int nsteps)
         if (!b->warm || profiling) {
             // first step direct: one-time launcher setup and autotuning happen
             // here; the profiler also needs direct launches
-            for (auto *e : b->engines) TRY(project_one_step_direct(e));
-            for (auto *e : b->engines) CUDA_TRY(cudaStreamSynchronize(e->stream));
+            for (size_t i = 0; i < b->engines.size(); ++i) {
+                afqmc_engine *e = b->engines[i];
+                CUDA_TRY(cudaEventRecord(b->fork, b->stream));
+                CUDA_TRY(cudaStreamWaitEvent(e->stream, b->fork, 0));
+                TRY(project_one_step_direct(e));
+                CUDA_TRY(cudaEventRecord(b->joins[i], e->stream));
+                CUDA_TRY(cudaStreamWaitEvent(b->stream, b->joins[i], 0));
+            }
+            if (!b->warm)
+                for (auto *e : b->engines) CUDA_TRY(cudaStreamSynchronize(e->stream));
             b->warm = true;
             continue;
         }
@@ -1167,13 +1176,31 @@ int afqmc_batch_step(afqmc_batch *b, int nsteps)
             cudaGraphDestroy(g);
             if (ce != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("batch instantiate: ") + cudaGetErrorString(ce));
         }
+        // order the graph after work already queued on the engines' streams,
+        // and later work on those streams after the graph
+        for (size_t i = 0; i < b->engines.size(); ++i) {
+            CUDA_TRY(cudaEventRecord(b->joins[i], b->engines[i]->stream));
+            CUDA_TRY(cudaStreamWaitEvent(b->stream, b->joins[i], 0));
+        }
         CUDA_TRY(cudaGraphLaunch(b->exec[key], b->stream));
         g_launch_count += b->kernels[key];
+        CUDA_TRY(cudaEventRecord(b->fork, b->stream));
+        for (auto *e : b->engines) CUDA_TRY(cudaStreamWaitEvent(e->stream, b->fork, 0));
         for (auto *e : b->engines) {
             e->mgsIndex = doMgs ? 0 : e->mgsIndex + 1;
             e->popIndex = doPop ? 0 : e->popIndex + 1;
         }
     }
+    return AFQMC_OK;
+}
+
+int afqmc_batch_set_stream(afqmc_batch *b, void *cuda_stream)
+{
+    if (!b) return fail(AFQMC_ERR_ARG, "null batch");
+    if (!cuda_stream) return fail(AFQMC_ERR_ARG, "null stream");
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    if (b->own) { cudaStreamDestroy(b->own); b->own = nullptr; }
+    b->stream = (cudaStream_t)cuda_stream;
     return AFQMC_OK;
 }
 

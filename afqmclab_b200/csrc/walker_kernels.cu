@@ -187,6 +187,179 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
 }
 
 // ---------------------------------------------------------------------------
+// Same contract as lu_kernel for blocks of 33..GJ_CTA_MAX_NS columns, one CTA
+// per walker, the block resident in shared memory (column-major, as in S).
+// With the inverse requested: Gauss-Jordan elimination in place (zgetf2 pivot
+// choice, row interchanges undone as column swaps at the end).  Without it:
+// the LU elimination of the trailing block only.  In both cases the pivots
+// are the U diagonal of zgetrf, so the log-determinant follows
+// logDeterminant (tensor_2d_common_fun.cpp:75-105).  Three barriers per
+// column: pivot search, interchange + row scaling, elimination.
+// ---------------------------------------------------------------------------
+constexpr int GJ_CTA_MAX_NS = 120;
+
+__host__ __device__ constexpr size_t gj_cta_smem(int ns)
+{
+    return (size_t)ns * ns * sizeof(zd) + (size_t)ns * sizeof(zd) + 4 * sizeof(int);
+}
+
+template <int NT>
+__global__ void __launch_bounds__(NT)
+gj_cta_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const zd *logw,
+              zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut, double *weight,
+              int *status, int mode, int wantInverse, int maxNs)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    zd *A = (zd *)smem_raw;
+    zd *col = A + (size_t)maxNs * maxNs;
+    int *sc = (int *)(col + maxNs);   // [0] pivot row of the current column
+    const int w = blockIdx.x, tid = threadIdx.x;
+    const bool act = (active == nullptr) || active[w] != 0;
+    if (!act) {
+        if (tid == 0) {
+            if (mode == LU_PROJECT) surv[w] = 0;
+            if (mode == LU_POPWEIGHT) { weight[w] = 0.0; alive[w] = 1; }
+        }
+        return;
+    }
+    bool singular = false;
+    zd logdetSum = make_double2(0.0, 0.0);
+    for (int b = 0; b < bl.nblk; ++b) {
+        const int Ns = bl.Ns[b];
+        if (Ns == 0) continue;
+        const zd *Sg = S + (size_t)w * bl.sStride + bl.sOff[b];
+        zd *Xg = (wantInverse && Sinv) ? Sinv + (size_t)w * bl.sStride + bl.sOff[b] : nullptr;
+        const bool inv = Xg != nullptr;
+        __syncthreads();
+        for (int e = tid; e < Ns * Ns; e += NT) A[e] = Sg[e];
+        __syncthreads();
+        double lognorm = 0.0;
+        zd phase = make_double2(1.0, 0.0);
+        int myPiv = tid;   // thread k keeps the pivot row of column k
+        bool sing = false;
+        for (int j = 0; j < Ns; ++j) {
+            if (tid < 32) {
+                double best = -1.0;
+                int bi = Ns;
+                for (int i = j + tid; i < Ns; i += 32) {
+                    const double v = zcabs1(A[i + (size_t)Ns * j]);
+                    if (v > best) { best = v; bi = i; }
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+                }
+                if (tid == 0) sc[0] = bi;
+            }
+            __syncthreads();
+            const int p = sc[0];
+            if (tid == j) myPiv = p;
+            const zd d = A[p + (size_t)Ns * j];
+            const bool zero = zeq0(d);
+            const zd dinv = zero ? make_double2(0.0, 0.0) : zdiv(make_double2(1.0, 0.0), d);
+            if (zero) {
+                sing = true;
+            } else if (tid == 0) {
+                const double a = zabs(d);
+                lognorm += log(a);
+                const zd f = (p != j) ? zneg(d) : d;
+                phase = zmul(phase, make_double2(f.x / a, f.y / a));
+            }
+            // interchange rows j and p, scale the new row j, gather column j
+            // of the other rows (col[p] is the old A[j][j])
+            for (int c = tid; c < Ns; c += NT) {
+                const zd a = A[j + (size_t)Ns * c], bq = A[p + (size_t)Ns * c];
+                A[j + (size_t)Ns * c] = (inv && c == j) ? dinv : zmul(bq, dinv);
+                if (p != j) A[p + (size_t)Ns * c] = a;
+                if (c == j && p != j) col[p] = a;
+            }
+            for (int i = tid; i < Ns; i += NT)
+                if (i != j && i != p) col[i] = A[i + (size_t)Ns * j];
+            __syncthreads();
+            if (inv) {
+                for (int e = tid; e < Ns * Ns; e += NT) {
+                    const int i = e % Ns, c = e / Ns;
+                    if (i == j) continue;
+                    const zd f = col[i];
+                    if (c == j) {
+                        A[e] = zneg(zmul(f, dinv));
+                    } else {
+                        const zd u = A[j + (size_t)Ns * c];
+                        zd v = A[e];
+                        v.x -= f.x * u.x - f.y * u.y;
+                        v.y -= f.x * u.y + f.y * u.x;
+                        A[e] = v;
+                    }
+                }
+            } else {
+                const int r = Ns - j - 1;
+                for (int e = tid; e < r * r; e += NT) {
+                    const int i = j + 1 + e % r, c = j + 1 + e / r;
+                    const zd f = col[i], u = A[j + (size_t)Ns * c];
+                    zd v = A[i + (size_t)Ns * c];
+                    v.x -= f.x * u.x - f.y * u.y;
+                    v.y -= f.x * u.y + f.y * u.x;
+                    A[i + (size_t)Ns * c] = v;
+                }
+            }
+            __syncthreads();
+        }
+        if (inv) {
+            // column permutation that undoes the row interchanges, last first
+            int *pv = (int *)col, *idx = pv + Ns;
+            if (tid < Ns) pv[tid] = myPiv;
+            __syncthreads();
+            if (tid == 0) {
+                for (int k = 0; k < Ns; ++k) idx[k] = k;
+                for (int k = Ns - 1; k >= 0; --k) {
+                    const int q = pv[k];
+                    const int t = idx[k]; idx[k] = idx[q]; idx[q] = t;
+                }
+            }
+            __syncthreads();
+            for (int e = tid; e < Ns * Ns; e += NT) {
+                const int i = e % Ns, k = e / Ns;
+                Xg[e] = A[i + (size_t)Ns * idx[k]];
+            }
+        }
+        if (sing) {
+            singular = true;
+        } else if (tid == 0) {
+            const zd ld = zadd(make_double2(lognorm, 0.0), zlog(phase));
+            if (logdetSum.x > -1e299) logdetSum = zadd(logdetSum, ld);
+        }
+    }
+    if (singular) logdetSum = make_double2(-1e300, 0.0);
+    if (tid == 0) {
+        const zd lwR = zadd(logwAdd, logw[w]);
+        const zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
+        logov[w] = lo;
+        if (singular && status) atomicOr(status + w, (int)ST_SINGULAR);
+        if (!(isfinite(lo.x) && isfinite(lo.y)) && status && !singular) atomicOr(status + w, (int)ST_NONFINITE);
+        if (mode == LU_PROJECT) {
+            const double ph = lo.y;
+            const double c = cos(ph);
+            if (c <= 0.0) {
+                alive[w] = 0; surv[w] = 0;
+            } else {
+                logwOut[w] = zadd(logw[w], make_double2(log(c), -ph));
+                surv[w] = 1;
+            }
+        } else if (mode == LU_POPWEIGHT) {
+            const zd e = zexp(lo);
+            if (e.x <= 0.0) {
+                weight[w] = 0.0;
+            } else {
+                weight[w] = e.x;
+                logwOut[w] = zsub(logw[w], lo);
+            }
+            alive[w] = 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Same contract as lu_kernel for blocks of at most 32 columns, one warp per
 // walker: Gauss-Jordan elimination with the zgetf2 pivot choice (first row
 // of maximal |re|+|im| in the current column), in place in a padded shared
@@ -985,6 +1158,26 @@ void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const in
         gj_warp_kernel<<<(W + GJ_WARPS - 1) / GJ_WARPS, GJ_WARPS * 32, smem, s>>>(
             W, bl, S, Sinv, active, logw, logwAdd, logwT, logov, alive, surv, logwOut, weight, status,
             mode, wantInverse ? 1 : 0);
+        return;
+    }
+    if (maxNs <= GJ_CTA_MAX_NS) {
+        const size_t smem = gj_cta_smem(maxNs);
+        static bool cattr = false;
+        if (!cattr) {
+            cudaFuncSetAttribute(gj_cta_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)gj_cta_smem(GJ_CTA_MAX_NS));
+            cudaFuncSetAttribute(gj_cta_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)gj_cta_smem(GJ_CTA_MAX_NS));
+            cattr = true;
+        }
+        if (maxNs <= 64)
+            gj_cta_kernel<256><<<W, 256, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
+                                                     alive, surv, logwOut, weight, status, mode,
+                                                     wantInverse ? 1 : 0, maxNs);
+        else
+            gj_cta_kernel<512><<<W, 512, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
+                                                     alive, surv, logwOut, weight, status, mode,
+                                                     wantInverse ? 1 : 0, maxNs);
         return;
     }
     if (maxNs <= LU_SMEM_MAX_NS) {

@@ -158,6 +158,18 @@ def hubbard_inputs(nx=4, ny=4, nup=7, ndn=7, t=1.0, tp=0.0, U=4.0, dt=0.01,
         expMinusHalfDtK=np.asfortranarray(exp_minus_alpha(K, 0.5 * dt)))
 
 
+def hubbard_trial_energy(m):
+    """<phiT|H|phiT> / <phiT|phiT> of the Hubbard model (hopping, on-site U,
+    spin-orbit basis); used as the energy shift E_T of the weights."""
+    T = m.phiT
+    G = T @ np.linalg.solve(T.conj().T @ T, T.conj().T)   # G[p, q] = <c_q^+ c_p>
+    L = m.L
+    e = np.trace(m.K @ G)
+    d = np.diag(G)
+    e += np.sum(m.U * (d[:L] * d[L:] - np.diag(G[L:, :L]) * np.diag(G[:L, L:])))
+    return float(e.real)
+
+
 # ---------------------------------------------------------------- molecule
 @dataclass
 class MoleculeInputs:
@@ -326,7 +338,19 @@ CONFIGS = {
     "molecule64": dict(kind="pl", n=64, nup=16, ndn=16, G=320, dt=0.005, W=512, mgs=10, pop=10),
     "molecule256": dict(kind="pl", n=256, nup=64, ndn=64, G=1280, dt=0.005, W=512, mgs=10,
                         pop=10),
+    # the uneven batch: four lattices of different size and filling, U = 4 and 8
+    "hubbard6x6": dict(kind="cp", nx=6, ny=6, nup=16, ndn=16, t=1.0, tp=0.0, U=4.0, dt=0.01,
+                       W=1024, decomp="densitySpin", trial="free", mgs=10, pop=40),
+    "hubbard8x8u8": dict(kind="cp", nx=8, ny=8, nup=28, ndn=28, t=1.0, tp=0.0, U=8.0, dt=0.01,
+                         W=1024, decomp="densitySpin", trial="free", mgs=10, pop=40),
+    "hubbard10x10": dict(kind="cp", nx=10, ny=10, nup=40, ndn=40, t=1.0, tp=0.0, U=4.0, dt=0.01,
+                         W=1024, decomp="densitySpin", trial="free", mgs=10, pop=40),
+    "hubbard12x12u8": dict(kind="cp", nx=12, ny=12, nup=60, ndn=60, t=1.0, tp=0.0, U=8.0,
+                           dt=0.01, W=1024, decomp="densitySpin", trial="free", mgs=10, pop=40),
 }
+
+# Lattices advanced together as one batch (one graph launch per step).
+UNEVEN_BATCH = ["hubbard6x6", "hubbard8x8u8", "hubbard10x10", "hubbard12x12u8"]
 
 
 def make_config(name, **over):
@@ -335,6 +359,7 @@ def make_config(name, **over):
     if c["kind"] == "cp":
         m = hubbard_inputs(c["nx"], c["ny"], c["nup"], c["ndn"], c["t"], c["tp"], c["U"], c["dt"],
                            c["decomp"], c["trial"])
+        m.ET = hubbard_trial_energy(m)
     else:
         m = molecule_inputs(c["n"], c["nup"], c["ndn"], c["G"], c["dt"])
     return m, c

@@ -114,6 +114,26 @@ def phase_flops(c, m, taylor_avg):
     return f
 
 
+def cp_phase_model(m, W, precision):
+    """Algorithmic work of one launch of each timed phase of the constrained-path
+    step: ("bytes", B) for the mixed form (HBM-bound: fp32 hi/lo walker planes
+    read and written once per phase), ("flops", F) for the FP64 form."""
+    n, N = 2 * m.L, m.N
+    if precision == "mixed":
+        walker = 16.0 * n * N            # hi + lo planes, re + im, fp32
+        return {
+            "overlap": ("bytes", W * (walker + 16.0 * N * N)),
+            "force": ("bytes", W * (16.0 * N * N + 2 * 16.0 * N * N + walker / 2 + 8.0 * n)),
+            "sample": ("bytes", W * 2 * walker),
+            "onebody": ("bytes", W * 2 * walker),
+        }
+    return {
+        "overlap": ("flops", 8.0 * N * N * n * W),
+        "theta": ("flops", 8.0 * N * N * n * W),
+        "onebody": ("flops", 8.0 * n * n * N * W),
+    }
+
+
 def build_engine(capi, inputs, name, precision, seed):
     m, c = inputs.make_config(name)
     prec = capi.AFQMC_MIXED if precision == "mixed" else capi.AFQMC_FP64
@@ -161,6 +181,97 @@ def energy_check(capi, inputs, name, steps, measure_skip, stream, seed):
             "max_abs_dE_mHa": float(np.abs(d).max()), "mean_dE_mHa": float(d.mean()),
             "criterion_mHa": 0.5, "pass": bool(np.abs(d).max() <= 0.5),
             "method": "paired: same walkers, same random stream, measurement by measurement"}
+
+
+def bench_uneven(args, capi, inputs, torch, rank, world):
+    """The uneven batch: four Hubbard lattices of different size and filling
+    (1024 walkers each) advanced as one graph launch per step, in the chosen
+    form, then the same batch in the plain FP64 form from the same walkers and
+    random streams; per-lattice mixed estimators are compared measurement by
+    measurement."""
+    precision = "fp64" if args.precision == "fp64" else "mixed"
+    stream = torch.cuda.Stream()
+
+    def make(prec, seed0):
+        engines, tot = [], 0
+        for k, name in enumerate(inputs.UNEVEN_BATCH):
+            e, m, c, _ = build_engine(capi, inputs, name, prec, seed0 + k)
+            engines.append(e)
+            tot += c["W"]
+        b = capi.Batch(engines)
+        b.set_stream(stream.cuda_stream)
+        return b, engines, tot
+
+    def run(b, engines, k, start, energies=None):
+        for i in range(k):
+            if (start + i) % args.measure_skip == 0:
+                for j, e in enumerate(engines):
+                    if energies is not None:
+                        e.reset_measurement()
+                    e.add_mixed_measurement()
+                    if energies is not None:
+                        mm = e.measurement()
+                        energies[j].append((mm[1] / mm[0]).real)
+            b.step(1)
+
+    out = {}
+    for prec in ([precision, "fp64"] if precision == "mixed" and not args.no_fp64_side else [precision]):
+        b, engines, tot = make(prec, 77 + 10 * rank)
+        run(b, engines, args.warmup, 0)
+        b.synchronize()
+        launches0 = capi.launch_count()
+        clocks = ClockSampler(torch.cuda.current_device())
+        torch.cuda.synchronize()
+        clocks.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run(b, engines, args.steps, args.warmup)
+        e1.record(stream)
+        e1.synchronize()
+        b.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1)
+        out[prec] = {"value": tot * args.steps / (ms / 1e3), "ms_per_step": ms / args.steps,
+                     "gpu_launches": int(capi.launch_count() - launches0), "clocks": clk}
+        b.close()
+        for e in engines:
+            e.close()
+    # paired energies: same walkers and random streams in both forms
+    energies = {}
+    if precision == "mixed" and args.energy_steps > 0:
+        for prec in ("fp64", "mixed"):
+            b, engines, _ = make(prec, 4242)
+            acc = [[] for _ in engines]
+            run(b, engines, args.energy_steps, 0, acc)
+            b.synchronize()
+            energies[prec] = acc
+            b.close()
+            for e in engines:
+                e.close()
+        per = {}
+        for j, name in enumerate(inputs.UNEVEN_BATCH):
+            ef, ex = np.array(energies["fp64"][j]), np.array(energies["mixed"][j])
+            per[name] = {"E_fp64": ef.tolist(), "E_mixed": ex.tolist(),
+                         "max_abs_dE": float(np.abs(ex - ef).max()),
+                         "max_rel_dE": float(np.abs((ex - ef) / ef).max())}
+        energies = per
+    main = out[precision]
+    line = {"metric": METRIC, "value": main["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": main["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "tf32/f32 tensor + f64" if precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": "uneven", "lattices": inputs.UNEVEN_BATCH,
+                       "walkers_per_lattice": 1024, "precision": precision,
+                       "measure_skip": args.measure_skip, "cuda_graphs": "one graph launch per step"},
+            "gpu_launches": main["gpu_launches"], "clocks": main["clocks"],
+            "fp64_form": out.get("fp64") if precision == "mixed" else None,
+            "speedup_mixed_over_fp64": (out["fp64"]["ms_per_step"] / main["ms_per_step"])
+            if precision == "mixed" and "fp64" in out else None,
+            "energy_check": energies or None}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
 
 
 # ---------------------------------------------------------------- CPU arm
@@ -251,6 +362,12 @@ def main():
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
+
+    if args.workload == "uneven":
+        r = bench_uneven(args, capi, inputs, torch, rank, world)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return r
 
     precision = args.precision
     if precision == "auto":
@@ -354,6 +471,27 @@ def main():
         roof = {"bound": bound, "kernel": top, "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                 "flops_per_launch": fl[top], "launch_ms": t_launch * 1e3, "peak_source": psrc}
+    else:
+        model = cp_phase_model(m, W, precision)
+        cand = {k: v for k, v in prof.items() if k in model and v[1] > 0}
+        top = max(cand, key=lambda k: cand[k][0])
+        t_launch = prof[top][0] / prof[top][1] / 1e3
+        kind, amount = model[top]
+        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        have = os.path.exists(peaks_path)
+        if kind == "bytes":
+            peak = json.load(open(peaks_path))["hbm_gbs"] if have else 6650.0
+            roof = {"bound": "hbm", "kernel": top, "achieved": amount / t_launch / 1e9, "peak": peak,
+                    "unit": "GB/s", "traffic": None, "bytes_per_launch": amount,
+                    "launch_ms": t_launch * 1e3,
+                    "peak_source": "measured copy bandwidth" if have else "fallback"}
+        else:
+            peak = 37.2
+            roof = {"bound": "fp64", "kernel": top, "achieved": amount / t_launch / 1e12, "peak": peak,
+                    "unit": "TFLOP/s", "traffic": None, "flops_per_launch": amount,
+                    "launch_ms": t_launch * 1e3,
+                    "peak_source": "nominal FP64 (148 SM x 64 DFMA x 1.965 GHz); not in MEASURED_PEAKS.json"}
+        roof["frac"] = roof["achieved"] / roof["peak"]
 
     # the plain FP64 form side by side, and the paired energy check: both
     # forms from the same walkers and random stream, mixed estimator every

@@ -237,6 +237,9 @@ typedef struct afqmc_batch afqmc_batch;
 int afqmc_batch_create(afqmc_engine **engines, int count, afqmc_batch **out);
 int afqmc_batch_step(afqmc_batch *b, int nsteps);
 int afqmc_batch_synchronize(afqmc_batch *b);
+/* Launch the batch's graphs on a caller-owned cudaStream_t (NULL is refused:
+ * the legacy default stream cannot be captured). */
+int afqmc_batch_set_stream(afqmc_batch *b, void *cuda_stream);
 int afqmc_batch_destroy(afqmc_batch *b);
 /* Process-wide switch of the GEMM autotuner: with enable != 0 every new
  * FP64 GEMM shape is timed once over the candidate tile shapes (outside

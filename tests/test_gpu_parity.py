@@ -267,3 +267,43 @@ def test_pop_configuration_dev_bit_exact():
         capi.pop_configuration_dev(tw.data_ptr(), tu.data_ptr(), tt.data_ptr(), W)
         torch.cuda.synchronize()
         assert (tt.cpu().numpy() == table_o).all()
+
+
+# ------------------------------------------- wider overlap blocks (33..120)
+@pytest.mark.parametrize("nx,ny,nup,ndn", [(6, 6, 20, 20), (8, 8, 28, 28), (10, 10, 40, 40)])
+def test_cp_wide_blocks_step_and_pop_control(nx, ny, nup, ndn):
+    """Blocks of 40, 56 and 80 columns take the shared-memory Gauss-Jordan
+    path (inverse) and its LU-only variant (population-control weights)."""
+    m = hubbard("densitySpin", True, nx=nx, ny=ny, nup=nup, ndn=ndn)
+    W = 6
+    g, o = pair_cp(m, W, 31, 1000, 2, noise=0.1)
+    err = logov_close(g.log_overlaps(), o.log_overlaps(), STEP_TOL)
+    assert err < STEP_TOL
+    for w in (0, 3):
+        assert rel_err(g.green(w), o.green(w)) < STEP_TOL
+    for step in range(2):
+        wf, lw, al = o.get_walkers()
+        g.set_walkers(wf, lw, al)
+        g.set_rng(31, o.rng_counter())
+        g.set_cadence(0, step)
+        o_before = o.rng_counter()
+        g.step(1)
+        o.step(1)
+        compare_state(g, o, STEP_TOL)
+    assert g.rng_counter() == o.rng_counter() and o.rng_counter() > o_before
+
+
+def test_pl_wide_blocks_step():
+    m = molecule(n=96, nup=40, ndn=36, G=48)
+    W = 4
+    g, o = pair_pl(m, W, 41, 1000, 1000)
+    err = logov_close(g.log_overlaps(), o.log_overlaps(), STEP_TOL)
+    assert err < STEP_TOL
+    wf, lw, al = o.get_walkers()
+    g.set_walkers(wf, lw, al)
+    g.step(1)
+    o.step(1)
+    compare_state(g, o, STEP_TOL)
+    for w in (0, 2):
+        for spin in (0, 1):
+            assert rel_err(g.green(w, spin), o.green(w, spin)) < STEP_TOL
