@@ -715,13 +715,20 @@ int cp_mixed_modify_gm(afqmc_engine *e)
     return cp_mixed_sync_from_fp64(e);
 }
 
-int cp_mixed_pop_control(afqmc_engine *e)
+int cp_mixed_pop_weights(afqmc_engine *e)
 {
     CpMixedState *m = e->cpm;
     CM(overlap_tc(e, m->hi, m->lo));
     launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
                              e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
                              LU_POPWEIGHT, false, e->stream);
+    return engine_check_launch();
+}
+
+int cp_mixed_pop_control(afqmc_engine *e)
+{
+    CpMixedState *m = e->cpm;
+    CM(cp_mixed_pop_weights(e));
     launch_pop_comb(e->W, e->weight, nullptr, e->seed, e->counter, e->number, e->table,
                     e->status + e->W, e->stream);
     g_launch_count++;

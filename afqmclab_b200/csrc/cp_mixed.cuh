@@ -13,6 +13,7 @@ void cp_mixed_destroy(afqmc_engine *e);
 int cp_mixed_project_dtk_dtv(afqmc_engine *e);
 int cp_mixed_modify_gm(afqmc_engine *e);
 int cp_mixed_pop_control(afqmc_engine *e);
+int cp_mixed_pop_weights(afqmc_engine *e);
 int cp_mixed_sync_to_fp64(afqmc_engine *e);
 int cp_mixed_sync_from_fp64(afqmc_engine *e);
 int cp_mixed_status(afqmc_engine *e);

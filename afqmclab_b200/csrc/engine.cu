@@ -1252,12 +1252,15 @@ int afqmc_pop_configuration_host(int L, int size, const double *weight, const do
 int afqmc_pop_weights(afqmc_engine *e, double *weight_out)
 {
     if (!e || !weight_out) return fail(AFQMC_ERR_ARG, "null argument");
-    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
-    TRY(overlap_gemm(e, e->wf, e->alive));
-    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
-                             e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
-                             LU_POPWEIGHT, false, e->stream);
-    TRY(check_launch());
+    if (e->precision == AFQMC_MIXED) {
+        TRY(mixed_pop_weights(e));
+    } else {
+        TRY(overlap_gemm(e, e->wf, e->alive));
+        launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
+                                 e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
+                                 LU_POPWEIGHT, false, e->stream);
+        TRY(check_launch());
+    }
     CUDA_TRY(cudaMemcpyAsync(weight_out, e->weight, sizeof(double) * e->W, cudaMemcpyDeviceToHost, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     return AFQMC_OK;

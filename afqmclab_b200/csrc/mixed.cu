@@ -19,6 +19,7 @@
 #include "engine_internal.cuh"
 #include "mixed.cuh"
 #include "cp_mixed.cuh"
+#include "overlap_tc.cuh"
 #include "tc_common.cuh"
 #include "tc_gemm.cuh"
 
@@ -30,6 +31,7 @@ struct MixedState {
     zd *wfDaggerTm = nullptr;
     __nv_bfloat16 *A2r[2] = {nullptr, nullptr}, *A2i[2] = {nullptr, nullptr};
     zd *ex2 = nullptr;
+    float *Ohi[2] = {nullptr, nullptr}, *Olo[2] = {nullptr, nullptr};   // overlap operators
     int *err = nullptr;
     int splits = 1;
     long long ws32 = 0;  // floats per walker (2 n ncol)
@@ -521,21 +523,18 @@ int tc(afqmc_engine *e, TcGemmArgs a)
     return AFQMC_OK;
 }
 
-// S_b = phiT_b^H phi_b in FP64 from the fp32 walkers
+// S_b = phiT_b^H phi_b from the fp32 walkers (compensated tf32 tensor-core
+// product, FP64 result); every walker's slot is written
 int overlap32(afqmc_engine *e, const float *w32, const int *mask)
 {
+    (void)mask;
+    MixedState *m = e->mx;
     for (int b = 0; b < e->bl.nblk; ++b) {
-        int Ns = e->bl.Ns[b];
+        const int Ns = e->bl.Ns[b];
         if (Ns == 0) continue;
-        ZGemmArgs g;
-        g.m = Ns; g.n = Ns; g.k = e->n;
-        g.opA = OP_C; g.opB = OP_N;
-        g.A = e->phiT[b]; g.lda = e->n;
-        g.B = w32; g.ldb = e->n; g.strideB = e->mx->ws32; g.b_real = ST_C32P;
-        g.planeB = (long long)e->n * e->ncol;
-        g.C = e->S + e->bl.sOff[b]; g.ldc = Ns; g.strideC = e->bl.sStride;
-        g.batch = e->W; g.mask = mask;
-        MTRY(engine_gemm(g, e->stream));
+        const int r = overlap_tc_launch(e->stream, e->n, e->ncol, Ns, e->W, m->Ohi[b], m->Olo[b], w32,
+                                        (double *)e->S, e->bl.sStride, e->bl.sOff[b], m->err);
+        if (r) return engine_fail(AFQMC_ERR_CUDA, "overlap launch: " + std::to_string(r));
     }
     return AFQMC_OK;
 }
@@ -625,6 +624,20 @@ int mixed_create(afqmc_engine *e)
     MTRY(cuda_check(cudaStreamSynchronize(e->stream), "sync"));
     for (const zd &v : h)
         if (v.y != 0.0) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision one-body needs a real exp(-dt K)");
+    // compensated tf32 overlap operators, one per spin block
+    for (int b = 0; b < e->bl.nblk; ++b) {
+        const int Ns = e->bl.Ns[b];
+        if (Ns == 0) continue;
+        if (!overlap_tc_supported(n, Ns)) return engine_fail(AFQMC_ERR_UNSUPPORTED, "overlap block too wide for the mixed form");
+        std::vector<zd> T((size_t)n * Ns);
+        MTRY(cuda_check(cudaMemcpy(T.data(), e->phiT[b], sizeof(zd) * T.size(), cudaMemcpyDeviceToHost), "copy"));
+        std::vector<float> oh, ol;
+        overlap_tc_build(T.data(), n, Ns, oh, ol);
+        MTRY(engine_dalloc(e, &m->Ohi[b], oh.size()));
+        MTRY(engine_dalloc(e, &m->Olo[b], ol.size()));
+        MTRY(cuda_check(cudaMemcpy(m->Ohi[b], oh.data(), 4 * oh.size(), cudaMemcpyHostToDevice), "upload"));
+        MTRY(cuda_check(cudaMemcpy(m->Olo[b], ol.data(), 4 * ol.size(), cudaMemcpyHostToDevice), "upload"));
+    }
     m->ready = true;
     return AFQMC_OK;
 }
@@ -725,14 +738,21 @@ int mixed_modify_gm(afqmc_engine *e)
     return engine_check_launch();
 }
 
+int mixed_pop_weights(afqmc_engine *e)
+{
+    if (e->kind == KIND_CP) return cp_mixed_pop_weights(e);
+    MTRY(overlap32(e, e->mx->wf32, e->alive));
+    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
+                             e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
+                             LU_POPWEIGHT, false, e->stream);
+    return engine_check_launch();
+}
+
 int mixed_pop_control(afqmc_engine *e)
 {
     if (e->kind == KIND_CP) return cp_mixed_pop_control(e);
     MixedState *m = e->mx;
-    MTRY(overlap32(e, m->wf32, e->alive));
-    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
-                             e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
-                             LU_POPWEIGHT, false, e->stream);
+    MTRY(mixed_pop_weights(e));
     launch_pop_comb(e->W, e->weight, nullptr, e->seed, e->counter, e->number, e->table,
                     e->status + e->W, e->stream);
     gather32_kernel<<<e->W, 256, 0, e->stream>>>(e->W, m->ws32, e->table, m->wf32, e->logw);

@@ -15,6 +15,9 @@ int mixed_sync_to_fp64(afqmc_engine *e);
 int mixed_sync_from_fp64(afqmc_engine *e);
 int mixed_status(afqmc_engine *e);
 int mixed_pop_control(afqmc_engine *e);
+// overlaps, population-control weights and the log-weight shift, as the
+// mixed form's population control computes them (no comb)
+int mixed_pop_weights(afqmc_engine *e);
 int mixed_exchange(afqmc_engine *e);
 
 // tcgen05 exchange kernel (exchange_tc.cu)

@@ -1,0 +1,273 @@
+// Overlap S_b = phiT_b^H phi of every walker on the tcgen05 tensor cores from
+// fp32 walkers (planar [re n x ncol | im n x ncol] per walker), compensated:
+// each fp32 walker tile is split in shared memory into a tf32 high part and
+// the fp32 remainder, and the trial operator into tf32 high and low parts, so
+//   S = O_hi phi_hi + O_lo phi_hi + O_hi phi_lo
+// carries about 22 significant bits (kind::tf32, fp32 accumulation); the
+// result is written in FP64 for the LU / log-determinant.
+// Replaces SDSDOperation / SD2sSD2isOperation's overlap gmm
+// (SDSDOperation.cpp:154-164, SD2sSD2isOperation.cpp:84-94) in the
+// mixed-precision form.
+//
+//   warp 0 lane 0 : TMA producer (O_hi, O_lo tiles; raw fp32 walker tiles)
+//   warp 1        : TMEM owner; lane 0 issues the UMMAs
+//   warps 2..5    : split each walker tile in place (hi) and beside it (lo),
+//                   then the epilogue (TMEM lane quarter = warp % 4)
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "engine_internal.cuh"
+#include "overlap_tc.cuh"
+#include "tc_common.cuh"
+
+extern std::atomic<long long> g_launch_count;
+
+namespace {
+
+constexpr int BM = 128, BK = 32, BN = 256, STAGES = 2;
+constexpr int A_BYTES = BM * BK * 4;
+constexpr int B_BYTES = BN * BK * 4;
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+constexpr size_t SMEM = 1024 + (size_t)STAGES * STAGE_BYTES + 256;
+
+struct OvArgs {
+    int n, Ns, W, kbA, bnw, wpt;
+    uint32_t idesc;
+    double *S;
+    long long sStride, sOff;
+    int *err;
+};
+
+__global__ void __launch_bounds__(192, 1)
+ov_split_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
+                const __grid_constant__ CUtensorMap tB, OvArgs p)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t *full = (uint64_t *)(base + STAGES * STAGE_BYTES);
+    uint64_t *split = full + STAGES;
+    uint64_t *empty = split + STAGES;
+    uint64_t *tmemFull = empty + STAGES;
+    uint32_t *tmemSlot = (uint32_t *)(tmemFull + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x;
+    const int KT = 2 * p.kbA;
+    const uint32_t bBytes = (uint32_t)(p.wpt * p.bnw * BK * 4);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&split[s], 128);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(tmemFull, 1);
+        fence_mbar_init();
+        tma_prefetch_desc(&tAh);
+        tma_prefetch_desc(&tB);
+    }
+    if (warp == 1) { tmem_alloc(tmemSlot, BN); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmemSlot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            for (int kt = 0; kt < KT && ok; ++kt) {
+                const int s = kt % STAGES;
+                if (kt >= STAGES) ok = mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1);
+                if (!ok) break;
+                const int plane = kt / p.kbA, kk = (kt % p.kbA) * BK;
+                uint8_t *st = base + s * STAGE_BYTES;
+                mbar_arrive_expect_tx(&full[s], 2 * A_BYTES + bBytes);
+                tma_load_2d(st, &tAh, &full[s], plane * p.n + kk, 0);
+                tma_load_2d(st + A_BYTES, &tAl, &full[s], plane * p.n + kk, 0);
+                for (int j = 0; j < p.wpt; ++j)
+                    tma_load_3d(st + 2 * A_BYTES + j * p.bnw * BK * 4, &tB, &full[s], kk, 0,
+                                2 * (tile * p.wpt + j) + plane);
+            }
+            for (int kt = max(KT, STAGES); kt < KT + STAGES && ok; ++kt) {
+                const int s = kt % STAGES;
+                ok = mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            for (int kt = 0; kt < KT && ok; ++kt) {
+                const int s = kt % STAGES;
+                ok = mbar_wait(&split[s], (kt / STAGES) & 1);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+                const uint32_t ah = st, al = st + A_BYTES, bh = st + 2 * A_BYTES, bl = bh + B_BYTES;
+#pragma unroll
+                for (int k8 = 0; k8 < BK / 8; ++k8) {
+                    const uint32_t acc0 = (kt > 0 || k8 > 0) ? 1u : 0u;
+                    umma_tf32(tmem, desc_k_sw128(ah + k8 * 32), desc_k_sw128(bh + k8 * 32), p.idesc, acc0);
+                    umma_tf32(tmem, desc_k_sw128(al + k8 * 32), desc_k_sw128(bh + k8 * 32), p.idesc, 1u);
+                    umma_tf32(tmem, desc_k_sw128(ah + k8 * 32), desc_k_sw128(bl + k8 * 32), p.idesc, 1u);
+                }
+                umma_commit(&empty[s]);
+            }
+            umma_commit(tmemFull);
+        }
+        __syncwarp();
+    } else {
+        // split the raw walker tile: hi in place, lo in the slot beside it
+        const int t = threadIdx.x - 64;
+        const int n4 = (int)(bBytes / 16);
+        for (int kt = 0; kt < KT && ok; ++kt) {
+            const int s = kt % STAGES;
+            ok = mbar_wait(&full[s], (kt / STAGES) & 1);
+            if (!ok) break;
+            float4 *bh = (float4 *)(base + s * STAGE_BYTES + 2 * A_BYTES);
+            float4 *bl = (float4 *)(base + s * STAGE_BYTES + 2 * A_BYTES + B_BYTES);
+            for (int i = t; i < n4; i += 128) {
+                const float4 x = bh[i];
+                float4 h, l;
+                h.x = tf32_round(x.x); l.x = x.x - h.x;
+                h.y = tf32_round(x.y); l.y = x.y - h.y;
+                h.z = tf32_round(x.z); l.z = x.z - h.z;
+                h.w = tf32_round(x.w); l.w = x.w - h.w;
+                bh[i] = h;
+                bl[i] = l;
+            }
+            fence_proxy_async();
+            mbar_arrive(&split[s]);
+        }
+        ok = ok && mbar_wait(tmemFull, 0);
+        tc_fence_after();
+        const int q = warp & 3;
+        const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
+        const int row = q * 32 + lane;
+        const int Ns = p.Ns;
+        const int part = row >= Ns ? 1 : 0, a = row - part * Ns;
+        const int ncols = p.wpt * p.bnw;
+        if (ok) {
+#pragma unroll 1
+            for (int c0 = 0; c0 < ncols; c0 += 32) {
+                float v[32];
+                tmem_ld32(trow + c0, v);
+                if (row < 2 * Ns) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int col = c0 + j;
+                        const int wj = col / p.bnw, c = col - wj * p.bnw;
+                        const int w = tile * p.wpt + wj;
+                        if (col < ncols && c < Ns && w < p.W)
+                            p.S[2 * ((size_t)w * p.sStride + p.sOff + a + (size_t)Ns * c) + part] = (double)v[j];
+                    }
+                }
+            }
+        }
+    }
+    if (!ok && p.err) atomicExch(p.err, 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, BN);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool done = false;
+    if (!done) {
+        cudaDriverEntryPointQueryResult q;
+        void *f = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)f;
+        done = true;
+    }
+    return fn;
+}
+
+int map_f32(CUtensorMap *map, const float *ptr, int rank, const cuuint64_t *dims, const cuuint64_t *pitch,
+            const cuuint32_t *box)
+{
+    auto enc = encoder();
+    if (!enc) return (int)cudaErrorNotSupported;
+    if ((uintptr_t)ptr & 15) return (int)cudaErrorMisalignedAddress;
+    for (int i = 0; i + 1 < rank; ++i)
+        if (pitch[i] & 15) return (int)cudaErrorMisalignedAddress;
+    cuuint32_t es[3] = {1u, 1u, 1u};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<float *>(ptr), dims, pitch, box,
+                     es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? 0 : (int)r + 10000;
+}
+
+float tf32_host(float x)
+{
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    if ((u & 0x7F800000u) != 0x7F800000u) { u += 0x1000u; u &= 0xFFFFE000u; }
+    std::memcpy(&x, &u, 4);
+    return x;
+}
+
+}  // namespace
+
+bool overlap_tc_supported(int n, int Ns) { return n % 4 == 0 && Ns >= 1 && Ns <= 64; }
+
+// O rows: a -> [Re T(:,a) | Im T(:,a)], Ns + a -> [-Im T(:,a) | Re T(:,a)], split hi/lo
+int overlap_tc_build(const zd *Thost, int n, int Ns, std::vector<float> &hi, std::vector<float> &lo)
+{
+    hi.assign((size_t)4 * Ns * n, 0.f);
+    lo.assign((size_t)4 * Ns * n, 0.f);
+    auto put = [&](size_t idx, double v) {
+        const float h = tf32_host((float)v);
+        hi[idx] = h;
+        lo[idx] = tf32_host((float)(v - (double)h));
+    };
+    for (int a = 0; a < Ns; ++a)
+        for (int i = 0; i < n; ++i) {
+            const zd t = Thost[i + (size_t)n * a];
+            const size_t r0 = (size_t)a * 2 * n, r1 = (size_t)(Ns + a) * 2 * n;
+            put(r0 + i, t.x);
+            put(r0 + n + i, t.y);
+            put(r1 + i, -t.y);
+            put(r1 + n + i, t.x);
+        }
+    return 0;
+}
+
+int overlap_tc_launch(cudaStream_t s, int n, int ncol, int Ns, int W, const float *Ohi, const float *Olo,
+                      const float *w32, double *S, long long sStride, long long sOff, int *err)
+{
+    if (!overlap_tc_supported(n, Ns)) return (int)cudaErrorInvalidValue;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(ov_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        attr = true;
+    }
+    CUtensorMap ah, al, b;
+    cuuint64_t da[2] = {(cuuint64_t)2 * n, (cuuint64_t)2 * Ns}, pa[1] = {(cuuint64_t)2 * n * 4};
+    cuuint32_t boxA[2] = {BK, BM};
+    int r = map_f32(&ah, Ohi, 2, da, pa, boxA);
+    if (!r) r = map_f32(&al, Olo, 2, da, pa, boxA);
+    const int bnw = (Ns + 15) / 16 * 16;
+    cuuint64_t db[3] = {(cuuint64_t)n, (cuuint64_t)ncol, (cuuint64_t)2 * W};
+    cuuint64_t pb[2] = {(cuuint64_t)n * 4, (cuuint64_t)n * ncol * 4};
+    cuuint32_t boxB[3] = {BK, (cuuint32_t)bnw, 1u};
+    if (!r) r = map_f32(&b, w32, 3, db, pb, boxB);
+    if (r) return r;
+    OvArgs a{};
+    a.n = n; a.Ns = Ns; a.W = W;
+    a.kbA = (n + BK - 1) / BK;
+    a.bnw = bnw;
+    a.wpt = std::max(1, BN / bnw);
+    a.idesc = idesc_tf32(BM, a.wpt * bnw);
+    a.S = S; a.sStride = sStride; a.sOff = sOff; a.err = err;
+    g_launch_count++;
+    ov_split_kernel<<<(W + a.wpt - 1) / a.wpt, 192, SMEM, s>>>(ah, al, b, a);
+    return (int)cudaGetLastError();
+}
