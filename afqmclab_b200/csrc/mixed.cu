@@ -20,6 +20,7 @@
 #include "mixed.cuh"
 #include "cp_mixed.cuh"
 #include "overlap_tc.cuh"
+#include "theta_tc.cuh"
 #include "tc_common.cuh"
 #include "tc_gemm.cuh"
 
@@ -32,6 +33,7 @@ struct MixedState {
     __nv_bfloat16 *A2r[2] = {nullptr, nullptr}, *A2i[2] = {nullptr, nullptr};
     zd *ex2 = nullptr;
     float *Ohi[2] = {nullptr, nullptr}, *Olo[2] = {nullptr, nullptr};   // overlap operators
+    float *Bh = nullptr, *Bl = nullptr;   // S^{-1} operands of the theta product
     int *err = nullptr;
     int splits = 1;
     long long ws32 = 0;  // floats per walker (2 n ncol)
@@ -539,23 +541,19 @@ int overlap32(afqmc_engine *e, const float *w32, const int *mask)
     return AFQMC_OK;
 }
 
-// theta_b = phi_b S_b^{-1} (n x Ns) -> bf16 planar Theta (+ FP64 copy when thetaZ)
+// theta_b = phi_b S_b^{-1} (n x Ns) -> bf16 planar Theta (+ FP64 copy when
+// thetaZ): compensated tcgen05 tf32 product, so that the bf16 Theta rounds
+// from a value good to about 22 bits
 int theta32(afqmc_engine *e, const float *w32, const int *mask, zd *thetaZ)
 {
     MixedState *m = e->mx;
     for (int b = 0; b < e->bl.nblk; ++b) {
-        int Ns = e->bl.Ns[b];
+        const int Ns = e->bl.Ns[b];
         if (Ns == 0) continue;
-        ZGemmArgs g;
-        g.m = e->n; g.n = Ns; g.k = Ns;
-        g.A = w32; g.lda = e->n; g.strideA = m->ws32; g.a_real = ST_C32P;
-        g.planeA = (long long)e->n * e->ncol;
-        g.B = e->Sinv + e->bl.sOff[b]; g.ldb = Ns; g.strideB = e->bl.sStride;
-        g.C = thetaZ ? thetaZ + e->bl.tOff[b] : nullptr; g.ldc = e->n; g.strideC = e->bl.tStride;
-        g.outMode = OUT_BF16P;
-        g.C2 = m->Theta + e->bl.tOff[b]; g.ldc2 = e->n; g.strideC2 = 2 * e->Ktot; g.plane2 = e->Ktot;
-        g.batch = e->W; g.mask = mask;
-        MTRY(engine_gemm(g, e->stream));
+        const int r = theta_tc_launch(e->stream, e->n, e->ncol, Ns, e->W, w32, e->Sinv, e->bl.sStride,
+                                      e->bl.sOff[b], mask, 3, m->Bh, m->Bl, m->Theta, 2 * e->Ktot,
+                                      e->Ktot, e->bl.tOff[b], thetaZ, e->bl.tStride, m->err);
+        if (r) return engine_fail(AFQMC_ERR_CUDA, "theta launch: " + std::to_string(r));
     }
     return AFQMC_OK;
 }
@@ -624,6 +622,14 @@ int mixed_create(afqmc_engine *e)
     MTRY(cuda_check(cudaStreamSynchronize(e->stream), "sync"));
     for (const zd &v : h)
         if (v.y != 0.0) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision one-body needs a real exp(-dt K)");
+    // S^{-1} operand scratch of the theta product (hi and lo parts)
+    {
+        int maxNs = 0;
+        for (int b = 0; b < e->bl.nblk; ++b) maxNs = std::max(maxNs, e->bl.Ns[b]);
+        if (!theta_tc_supported(n, maxNs)) return engine_fail(AFQMC_ERR_UNSUPPORTED, "theta block too wide for the mixed form");
+        MTRY(engine_dalloc(e, &m->Bh, theta_tc_bscratch(W, maxNs)));
+        MTRY(engine_dalloc(e, &m->Bl, theta_tc_bscratch(W, maxNs)));
+    }
     // compensated tf32 overlap operators, one per spin block
     for (int b = 0; b < e->bl.nblk; ++b) {
         const int Ns = e->bl.Ns[b];
