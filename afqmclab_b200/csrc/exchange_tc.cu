@@ -8,9 +8,12 @@
 //
 // Persistent, warp-specialised: warp 0 TMA producer, warp 1 UMMA issuer (and
 // TMEM owner, 512 columns = two accumulator pairs so the epilogue of one tile
-// overlaps the MMAs of the next), warps 2..5 epilogue.  A CTA takes a work
-// item = one A tile (kept in shared memory) x a chunk of walker tiles.  All
-// waits are bounded.
+// overlaps the MMAs of the next), warps 2..9 epilogue (two warps per TMEM lane
+// quarter, each taking half of the columns).  The epilogue keeps each thread's
+// row of a block in registers and reads the transposed entries from a
+// swizzled shared-memory copy, so tr(D D) costs one shared store and one load
+// per complex product.  A CTA takes a work item = one A tile (kept in shared
+// memory) x a chunk of walker tiles.  All waits are bounded.
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -29,15 +32,22 @@ constexpr int XS_STAGES = 3;          // B stages: one 64-wide K box, both plane
 constexpr int XS_NCHUNK = 32;         // walker tiles per work item
 constexpr int XS_TILE_BYTES = 16384;  // 128 rows x 128 B
 
+constexpr int XS_THREADS = 320;
+constexpr int XS_EPI_WARPS = 8;
+
 struct XSmem {
-    // sA: 2 planes x 2 K boxes; sB: XS_STAGES x (2 planes); transpose: 4 warps x 32x33 float2
+    // sA: 2 planes x 2 K boxes; sB: XS_STAGES x (2 planes); transpose: 8 warps x 32x32 float2
     static constexpr size_t bytes()
     {
-        return 1024 + 4 * XS_TILE_BYTES + (size_t)XS_STAGES * 2 * XS_TILE_BYTES + 4 * 32 * 33 * 8 + 256;
+        return 1024 + 4 * XS_TILE_BYTES + (size_t)XS_STAGES * 2 * XS_TILE_BYTES + XS_EPI_WARPS * 32 * 32 * 8 + 256;
     }
 };
 
-__global__ void __launch_bounds__(192, 1)
+// swizzled 32 x 32 float2 tile: element (r, c) at r * 32 + (c ^ r)
+__device__ __forceinline__ int tsw(int r, int c) { return r * 32 + (c ^ r); }
+
+template <int NS>
+__global__ void __launch_bounds__(XS_THREADS, 1)
 exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_constant__ CUtensorMap tmAi,
                    const __grid_constant__ CUtensorMap tmBr, const __grid_constant__ CUtensorMap tmBi,
                    int G, int W, int Ns, int n, const int *alive, zd *ex, int *err)
@@ -47,16 +57,17 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
     uint8_t *sA = base;                                   // [plane][kb] tiles
     uint8_t *sB = base + 4 * XS_TILE_BYTES;               // [stage][plane] tiles
     float2 *sT = (float2 *)(sB + (size_t)XS_STAGES * 2 * XS_TILE_BYTES);
-    uint64_t *bars = (uint64_t *)(sT + 4 * 32 * 33);
+    uint64_t *bars = (uint64_t *)(sT + XS_EPI_WARPS * 32 * 32);
     uint64_t *full = bars, *empty = bars + XS_STAGES;
     uint64_t *aFull = bars + 2 * XS_STAGES, *aEmpty = aFull + 1;
     uint64_t *accFull = aEmpty + 1, *accEmpty = accFull + 2;
     uint32_t *tslot = (uint32_t *)(accEmpty + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rowsTotal = G * Ns;
+    (void)Ns;
+    const int rowsTotal = G * NS;
     const int MT = (rowsTotal + 127) / 128;
-    const int WB = 128 / Ns;                      // walkers per tile
+    const int WB = 128 / NS;                      // walkers per tile
     const int NT = (W + WB - 1) / WB;             // walker tiles
     const int NCH = (NT + XS_NCHUNK - 1) / XS_NCHUNK;
     const int items = MT * NCH;
@@ -66,7 +77,7 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
         for (int s = 0; s < XS_STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         mbar_init(aFull, 1);
         mbar_init(aEmpty, 1);
-        for (int b = 0; b < 2; ++b) { mbar_init(&accFull[b], 1); mbar_init(&accEmpty[b], 4); }
+        for (int b = 0; b < 2; ++b) { mbar_init(&accFull[b], 1); mbar_init(&accEmpty[b], XS_EPI_WARPS); }
         fence_mbar_init();
         tma_prefetch_desc(&tmAr); tma_prefetch_desc(&tmAi);
         tma_prefetch_desc(&tmBr); tma_prefetch_desc(&tmBi);
@@ -146,13 +157,17 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
         }
         __syncwarp();
     } else {
-        const int q = warp & 3;
-        float2 *T = sT + q * 32 * 33;
-        const int gpw = 32 / Ns;                      // vectors g per warp quarter
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        float2 *T = sT + (warp - 2) * 32 * 32;
+        const int r = q * 32 + lane;                   // tile row = (g_local, a)
+        const int a = r % NS;
+        const int gl = r / NS;                         // g inside the tile
+        const int rb = lane - a;                       // first warp row of this thread's g
         int tileCount = 0;
         for (int it = blockIdx.x; it < items && ok; it += gridDim.x) {
             const int mt = it % MT, ch = it / MT;
             const int t0 = ch * XS_NCHUNK, t1 = min(NT, t0 + XS_NCHUNK);
+            const int gg = mt * (128 / NS) + gl;
             for (int t = t0; t < t1 && ok; ++t, ++tileCount) {
                 const int ab = tileCount & 1;
                 ok = mbar_wait(&accFull[ab], (tileCount >> 1) & 1);
@@ -160,39 +175,38 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
                 tc_fence_after();
                 const uint32_t tR = tmem + ab * 256 + ((uint32_t)(q * 32) << 16);
                 const uint32_t tI = tR + 128;
-                const int r = q * 32 + lane;                   // tile row
-                const int gl = r / Ns, a = r % Ns;
-                const int g = mt * (128 / Ns) + gl;
 #pragma unroll 1
-                for (int c0 = 0; c0 < 128; c0 += 32) {
+                for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 32) {
                     float vr[32], vi[32];
                     tmem_ld32(tR + c0, vr);
                     tmem_ld32(tI + c0, vi);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) T[lane * 33 + j] = make_float2(vr[j], vi[j]);
+                    for (int j = 0; j < 32; ++j) T[tsw(lane, j)] = make_float2(vr[j], vi[j]);
                     __syncwarp();
-                    // blocks (g_local, w_local) inside this 32-column chunk
-                    for (int wb = 0; wb < 32 / Ns; ++wb) {
-                        const int cb = wb * Ns;                 // first column of the block in the chunk
+                    // blocks (g, walker) of this 32-column chunk: D[a][b] in
+                    // registers, D[b][a] from the transposed copy
+#pragma unroll
+                    for (int wb = 0; wb < 32 / NS; ++wb) {
                         float sr = 0.f, si = 0.f;
-                        for (int b = 0; b < Ns; ++b) {
-                            const float2 x = T[lane * 33 + cb + b];                // D[a][b]
-                            const float2 y = T[(lane - a + b) * 33 + cb + a];       // D[b][a]
-                            sr += x.x * y.x - x.y * y.y;
-                            si += x.x * y.y + x.y * y.x;
+#pragma unroll
+                        for (int b = 0; b < NS; ++b) {
+                            const float xr = vr[wb * NS + b], xi = vi[wb * NS + b];
+                            const float2 y = T[tsw(rb + b, wb * NS + a)];
+                            sr += xr * y.x - xi * y.y;
+                            si += xr * y.y + xi * y.x;
                         }
-                        for (int o = Ns >> 1; o > 0; o >>= 1) {
+#pragma unroll
+                        for (int o = NS >> 1; o > 0; o >>= 1) {
                             sr += __shfl_xor_sync(0xffffffffu, sr, o);
                             si += __shfl_xor_sync(0xffffffffu, si, o);
                         }
-                        const int w = t * WB + (c0 + cb) / Ns;
-                        if (a == 0 && g < G && w < W) ex[g + (size_t)G * w] = make_double2(sr, si);
+                        const int w = t * WB + (c0 + wb * NS) / NS;
+                        if (a == 0 && gg < G && w < W) ex[gg + (size_t)G * w] = make_double2(sr, si);
                     }
                     __syncwarp();
                 }
                 tc_fence_before();
                 if (lane == 0) mbar_arrive(&accEmpty[ab]);
-                (void)gpw;
             }
         }
     }
@@ -231,6 +245,19 @@ int make_map_theta(CUtensorMap *map, const void *base, int n, int Ns, int W, lon
     return r == CUDA_SUCCESS ? 0 : (int)r + 10000;
 }
 
+template <int NS>
+void launch_ns(int grid, size_t smem, cudaStream_t s, const CUtensorMap &ar, const CUtensorMap &ai,
+               const CUtensorMap &br, const CUtensorMap &bi, int G, int W, int n, const int *alive, zd *ex,
+               int *err)
+{
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(exchange_tc_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    exchange_tc_kernel<NS><<<grid, XS_THREADS, smem, s>>>(ar, ai, br, bi, G, W, NS, n, alive, ex, err);
+}
+
 }  // namespace
 
 // A2 operand of spin block b: rows (g, a) -> r = g Ns + a, K = i; two bf16 planes
@@ -264,17 +291,20 @@ int exchange_tc_launch(cudaStream_t s, int G, int W, int Ns, int n, const __nv_b
     if (!r) r = make_map_theta(&bi, Theta + Ktot + tOff, n, Ns, W, 2 * Ktot);
     if (r) return r;
     const size_t smem = XSmem::bytes();
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(exchange_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int MT = (G * Ns + 127) / 128;
     const int NT = (W + 128 / Ns - 1) / (128 / Ns);
     const int items = MT * ((NT + XS_NCHUNK - 1) / XS_NCHUNK);
-    exchange_tc_kernel<<<std::min(items, sms), 192, smem, s>>>(ar, ai, br, bi, G, W, Ns, n, alive, ex, err);
+    const int grid = std::min(items, sms);
+    switch (Ns) {
+    case 1: launch_ns<1>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 2: launch_ns<2>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 4: launch_ns<4>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 8: launch_ns<8>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 16: launch_ns<16>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    default: launch_ns<32>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    }
     return (int)cudaGetLastError();
 }
