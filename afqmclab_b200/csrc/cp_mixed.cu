@@ -182,9 +182,13 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
                         if (col < p.cols) {
                             const size_t idx = (size_t)row + (size_t)n * col;
                             const float x = v[j] + p.rhi[idx] + p.rlo[idx];
-                            const float h = tf32_round(x);
-                            p.ohi[idx] = h;
-                            p.olo[idx] = x - h;
+                            if (p.olo) {
+                                const float h = tf32_round(x);
+                                p.ohi[idx] = h;
+                                p.olo[idx] = x - h;
+                            } else {
+                                p.ohi[idx] = x;
+                            }
                         }
                     }
                 }
@@ -288,8 +292,8 @@ int make_map_f32(CUtensorMap *map, const float *base, int rank, const long long 
 }
 
 template <int MODE>
-int launch_tc(afqmc_engine *e, dim3 grid, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &b0,
-              const CUtensorMap &b1, const CpTcArgs &args)
+int launch_tc_stream(cudaStream_t s, dim3 grid, const CUtensorMap &a0, const CUtensorMap &a1,
+                     const CUtensorMap &b0, const CUtensorMap &b1, const CpTcArgs &args)
 {
     static bool attr = false;
     if (!attr) {
@@ -297,7 +301,15 @@ int launch_tc(afqmc_engine *e, dim3 grid, const CUtensorMap &a0, const CUtensorM
         attr = true;
     }
     g_launch_count++;
-    cpm_tc_kernel<MODE><<<grid, 192, SMEM, e->stream>>>(a0, a1, b0, b1, args);
+    cpm_tc_kernel<MODE><<<grid, 192, SMEM, s>>>(a0, a1, b0, b1, args);
+    return (int)cudaGetLastError();
+}
+
+template <int MODE>
+int launch_tc(afqmc_engine *e, dim3 grid, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &b0,
+              const CUtensorMap &b1, const CpTcArgs &args)
+{
+    launch_tc_stream<MODE>(e->stream, grid, a0, a1, b0, b1, args);
     return engine_check_launch();
 }
 
@@ -539,6 +551,16 @@ __global__ void combine_kernel(int W, int n, int N, const float *hi, const float
         dst[e] = make_double2((double)(h[e] + l[e]), (double)(h[e + nN] + l[e + nN]));
 }
 
+__global__ void split_f32_kernel(long long count, const float *x, float *hi, float *lo)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+         e += (long long)gridDim.x * blockDim.x) {
+        const float v = x[e], h = tf32_round(v);
+        hi[e] = h;
+        lo[e] = v - h;
+    }
+}
+
 __global__ void gather_kernel(int W, long long ws, const int *table, float *hi, float *lo, zd *logw)
 {
     const int i = blockIdx.x;
@@ -569,6 +591,51 @@ void split_host(double v, float &h, float &l)
 }
 
 }  // namespace
+
+int tf32_split_operator(const zd *E, int n, std::vector<float> &hi, std::vector<float> &lo)
+{
+    hi.assign((size_t)n * n, 0.f);
+    lo.assign((size_t)n * n, 0.f);
+    for (int i = 0; i < n; ++i)
+        for (int k = 0; k < n; ++k) {
+            const zd v = E[i + (size_t)n * k];
+            if (v.y != 0.0) return -1;
+            split_host(v.x - (i == k ? 1.0 : 0.0), hi[(size_t)i * n + k], lo[(size_t)i * n + k]);
+        }
+    return 0;
+}
+
+int split_f32_launch(cudaStream_t s, long long count, const float *x, float *hi, float *lo)
+{
+    g_launch_count++;
+    split_f32_kernel<<<1184, 256, 0, s>>>(count, x, hi, lo);
+    return (int)cudaGetLastError();
+}
+
+int onebody_tf32_launch(cudaStream_t s, int n, int ncol, int W, const float *Ehi, const float *Elo,
+                        const float *rhi, const float *rlo, float *ohi, float *olo, int *err)
+{
+    CUtensorMap a0, a1, b0, b1;
+    long long da[2] = {n, n}, pa[1] = {(long long)n * 4};
+    int boxA[2] = {BK, BM};
+    int r = make_map_f32(&a0, Ehi, 2, da, pa, boxA);
+    if (!r) r = make_map_f32(&a1, Elo, 2, da, pa, boxA);
+    const long long cols = 2LL * ncol * W;
+    long long db[2] = {n, cols}, pb[1] = {(long long)n * 4};
+    int boxB[2] = {BK, BN};
+    if (!r) r = make_map_f32(&b0, rhi, 2, db, pb, boxB);
+    if (!r) r = make_map_f32(&b1, rlo, 2, db, pb, boxB);
+    if (r) return r;
+    CpTcArgs a{};
+    a.n = n; a.N = ncol; a.W = W;
+    a.kbA = (n + BK - 1) / BK; a.nseg = 3;
+    a.cols = cols;
+    a.idesc = idesc_tf32(BM, BN);
+    a.rhi = rhi; a.rlo = rlo; a.ohi = ohi; a.olo = olo;
+    a.err = err;
+    dim3 grid((n + BM - 1) / BM, (unsigned)((cols + BN - 1) / BN));
+    return launch_tc_stream<CPM_ONEBODY>(s, grid, a0, a1, b0, b1, a);
+}
 
 bool cp_mixed_supported(int L, int N, std::string *why)
 {

@@ -2,7 +2,12 @@
 // tcgen05 kind::tf32 contractions with compensated (hi + lo) operands,
 // FP64 LU/log-determinant, weights, re-orthonormalisation and measurement.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <string>
+#include <vector>
+
+#include "common.cuh"
 
 struct afqmc_engine;
 struct CpMixedState;
@@ -17,3 +22,14 @@ int cp_mixed_pop_weights(afqmc_engine *e);
 int cp_mixed_sync_to_fp64(afqmc_engine *e);
 int cp_mixed_sync_from_fp64(afqmc_engine *e);
 int cp_mixed_status(afqmc_engine *e);
+
+// Shared tf32 tensor-core pieces (also used by the phaseless mixed form):
+// (E - I) of a real n x n operator E (host, column-major) as tf32 high/low
+// parts, row-major; -1 when E has an imaginary part
+int tf32_split_operator(const zd *E, int n, std::vector<float> &hi, std::vector<float> &lo);
+// x -> (tf32 high part, fp32 remainder), elementwise
+int split_f32_launch(cudaStream_t s, long long count, const float *x, float *hi, float *lo);
+// phi' = phi + (E - I) phi for fp32 planar walkers (2 ncol columns of n
+// per walker) given as hi + lo; output hi/lo (olo != NULL) or fp32 into ohi
+int onebody_tf32_launch(cudaStream_t s, int n, int ncol, int W, const float *Ehi, const float *Elo,
+                        const float *rhi, const float *rlo, float *ohi, float *olo, int *err);

@@ -34,6 +34,8 @@ struct MixedState {
     zd *ex2 = nullptr;
     float *Ohi[2] = {nullptr, nullptr}, *Olo[2] = {nullptr, nullptr};   // overlap operators
     float *Bh = nullptr, *Bl = nullptr;   // S^{-1} operands of the theta product
+    float *E1h = nullptr, *E1l = nullptr; // exp(+dt/2 K) - I, tf32 high/low (measurement)
+    float *sh = nullptr, *sl = nullptr;   // walkers split into tf32 high/low parts
     int *err = nullptr;
     int splits = 1;
     long long ws32 = 0;  // floats per walker (2 n ncol)
@@ -622,6 +624,20 @@ int mixed_create(afqmc_engine *e)
     MTRY(cuda_check(cudaStreamSynchronize(e->stream), "sync"));
     for (const zd &v : h)
         if (v.y != 0.0) return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision one-body needs a real exp(-dt K)");
+    // exp(+dt/2 K) of the measurement's half step on the tensor cores
+    {
+        std::vector<zd> E1((size_t)n * n);
+        MTRY(cuda_check(cudaMemcpy(E1.data(), e->expK[1], sizeof(zd) * E1.size(), cudaMemcpyDeviceToHost), "copy"));
+        std::vector<float> eh, el;
+        if (tf32_split_operator(E1.data(), n, eh, el))
+            return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed precision one-body needs a real exp(dt/2 K)");
+        MTRY(engine_dalloc(e, &m->E1h, eh.size()));
+        MTRY(engine_dalloc(e, &m->E1l, el.size()));
+        MTRY(cuda_check(cudaMemcpy(m->E1h, eh.data(), 4 * eh.size(), cudaMemcpyHostToDevice), "upload"));
+        MTRY(cuda_check(cudaMemcpy(m->E1l, el.data(), 4 * el.size(), cudaMemcpyHostToDevice), "upload"));
+        MTRY(engine_dalloc(e, &m->sh, (size_t)W * m->ws32));
+        MTRY(engine_dalloc(e, &m->sl, (size_t)W * m->ws32));
+    }
     // S^{-1} operand scratch of the theta product (hi and lo parts)
     {
         int maxNs = 0;
@@ -800,16 +816,11 @@ int mixed_add_measurement(afqmc_engine *e)
     cudaStream_t s = e->stream;
     {
         PHASE(AFQMC_PH_MEASURE);
-        // walkerTemp = exp(dt/2 K) walker (FP64 arithmetic, fp32 result)
-        ZGemmArgs g;
-        g.m = e->n; g.n = e->ncol; g.k = e->n;
-        g.A = e->expK[1]; g.lda = e->n; g.strideA = 0;
-        g.B = m->wf32; g.ldb = e->n; g.strideB = m->ws32; g.b_real = ST_C32P;
-        g.planeB = (long long)e->n * e->ncol;
-        g.C = nullptr; g.outMode = OUT_C32P;
-        g.C3 = m->tmp32; g.ldc3 = e->n; g.strideC3 = m->ws32; g.plane3 = (long long)e->n * e->ncol;
-        g.batch = W; g.mask = e->alive;
-        MTRY(engine_gemm(g, s));
+        // walkerTemp = exp(dt/2 K) walker: compensated tf32 tensor-core
+        // product phi + (E - I) phi, fp32 result
+        int r = split_f32_launch(s, (long long)W * m->ws32, m->wf32, m->sh, m->sl);
+        if (!r) r = onebody_tf32_launch(s, e->n, e->ncol, W, m->E1h, m->E1l, m->sh, m->sl, m->tmp32, nullptr, m->err);
+        if (r) return engine_fail(AFQMC_ERR_CUDA, "measurement one-body: " + std::to_string(r));
         MTRY(overlap32(e, m->tmp32, e->alive));
         launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, engine_one_body_logw(e, 1),
                                  e->logwT, e->logov, e->alive, nullptr, nullptr, nullptr,

@@ -390,6 +390,7 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
     }
     bool singular = false;
     zd logdetSum = make_double2(0.0, 0.0);
+    const bool inv = wantInverse && Sinv;
     for (int b = 0; b < bl.nblk; ++b) {
         const int Ns = bl.Ns[b];
         if (Ns == 0) continue;
@@ -434,13 +435,28 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
             for (int j = lane; j < Ns; j += 32)
                 A[k * GJ_LD + j] = (j == k) ? pinv : zmul(A[k * GJ_LD + j], pinv);
             __syncwarp();
-            // eliminate column k from every other row (lane i owns row i)
-            if (lane < Ns && lane != k) {
+            // eliminate column k from every other row (lane i owns row i);
+            // without the inverse only the trailing block below and right of
+            // the pivot (the LU elimination) is needed
+            if (inv) {
+                if (lane < Ns && lane != k) {
+                    zd *row = A + lane * GJ_LD;
+                    const zd *prow = A + k * GJ_LD;
+                    const zd dum = row[k];
+                    row[k] = make_double2(0.0, 0.0);
+                    for (int j = 0; j < Ns; ++j) {
+                        const zd pv = prow[j];
+                        zd r = row[j];
+                        r.x -= pv.x * dum.x - pv.y * dum.y;
+                        r.y -= pv.x * dum.y + pv.y * dum.x;
+                        row[j] = r;
+                    }
+                }
+            } else if (lane > k && lane < Ns) {
                 zd *row = A + lane * GJ_LD;
                 const zd *prow = A + k * GJ_LD;
                 const zd dum = row[k];
-                row[k] = make_double2(0.0, 0.0);
-                for (int j = 0; j < Ns; ++j) {
+                for (int j = k + 1; j < Ns; ++j) {
                     const zd pv = prow[j];
                     zd r = row[j];
                     r.x -= pv.x * dum.x - pv.y * dum.y;
@@ -451,7 +467,7 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
             __syncwarp();
         }
         // undo the row interchanges as column swaps, last first
-        for (int k = Ns - 1; k >= 0; --k) {
+        for (int k = Ns - 1; k >= 0 && inv; --k) {
             const int p = __shfl_sync(0xffffffffu, myPartner, k);
             if (p != k && lane < Ns) {
                 zd t = A[lane * GJ_LD + k];
