@@ -293,22 +293,35 @@ __global__ void xbar_combine_kernel(int G, int W, const float *xbarp, int splits
 // bit for -Im(M) Im(term).  After the series converges the one-body
 // operator (exp(-dt K) - 1, real) is applied the same way and the walker is
 // written back in place.  Rows beyond n (n = 64) are padding.
+// Shared memory of the Taylor kernel: M (re, im planes; the one-body
+// operator E - I is loaded into the re plane after the series) and the bf16
+// operand (re, im planes) holding the current term, K-major with the
+// 128-byte swizzle (NC rows of n).  Two CTAs fit on an SM for n = 128, NC <= 32.
 template <int NC>
 struct TaylorSmem {
-    static constexpr size_t b_plane(int n) { return (size_t)NC * n * 2; }
-    static constexpr size_t bytes(int n)
-    {
-        return 1024 + (size_t)2 * (n / 64) * 16384 + 2 * b_plane(n) + 64;
-    }
+    static constexpr size_t m_bytes(int n) { return (size_t)2 * (n / 64) * 16384; }
+    static constexpr size_t b_plane(int n) { return (size_t)(n / 64) * NC * 128; }
+    static constexpr size_t bytes(int n) { return 1024 + m_bytes(n) + 2 * b_plane(n) + 64; }
 };
 
-__device__ __forceinline__ void store_b_bf16(uint8_t *sB, int n, int a, int i, float v)
+// element (a, i) of a K-major, 128-byte-swizzled bf16 operand of NC rows
+template <int NC>
+__device__ __forceinline__ void store_b_sw(uint8_t *sB, int a, int i, float v)
 {
-    const uint32_t off = (uint32_t)(a >> 3) * (uint32_t)(n * 16) + (uint32_t)(i >> 3) * 128u +
-                         (uint32_t)(a & 7) * 16u + (uint32_t)(i & 7) * 2u;
+    const uint32_t off = (uint32_t)(i >> 6) * (NC * 128) + (uint32_t)a * 128u +
+                         (uint32_t)((((i & 63) >> 3) ^ (a & 7)) << 4) + (uint32_t)(i & 7) * 2u;
     *(__nv_bfloat16 *)(sB + off) = __float2bfloat16_rn(v);
 }
 
+// Taylor series of exp(M) phi (M = sqrt(-dt) sum_g x_g L_g, bf16 operands,
+// fp32 accumulation) for one walker at a time, then the one-body factor:
+//   phi' = S + (E - I) S,  S = sum_k M^k phi / k!
+// Thread i keeps row i of the running sum S in registers; the product
+// accumulators are read back 16 columns at a time and each term is written
+// back as the next bf16 operand.  The
+// order stops at k >= checkFrom once max |term| <= acc (the dynamicOrder
+// rule of the reference's Taylor expansion, CholeskyRealSampleSDOperation /
+// applyToRight with taylor accuracy 1e-10) or at kmax.
 template <int NC>
 __global__ void __launch_bounds__(128, 1)
 taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmE,
@@ -321,9 +334,9 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     uint8_t *sMr = base;
     uint8_t *sMi = base + KB * 16384;
     uint8_t *sBr = base + 2 * KB * 16384;
-    uint8_t *sBi = sBr + (size_t)NC * n * 2;
-    uint64_t *bars = (uint64_t *)(sBi + (size_t)NC * n * 2);
-    uint32_t *tslot = (uint32_t *)(bars + 2);
+    uint8_t *sBi = sBr + (size_t)KB * NC * 128;
+    uint64_t *bars = (uint64_t *)(sBi + (size_t)KB * NC * 128);   // [0] M, [1] MMA, [2] E
+    uint32_t *tslot = (uint32_t *)(bars + 3);
     __shared__ float red[4];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -332,6 +345,7 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     if (tid == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
         fence_mbar_init();
         tma_prefetch_desc(&tmM);
         tma_prefetch_desc(&tmE);
@@ -341,26 +355,26 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     __syncthreads();
     tc_fence_after();
     const uint32_t tm = *tslot;
-    const uint32_t tCr = tm, tCi = tm + 64;
     const uint32_t lanebase = (uint32_t)(warp * 32) << 16;
+    const uint32_t tCr = tm, tCi = tm + 64;
     constexpr uint32_t IDESC = idesc_bf16(128, NC);
     constexpr uint32_t IDESCN = idesc_bf16(128, NC, true);
-    const uint32_t LBO = 128, SBO = (uint32_t)n * 16;
     uint32_t phL = 0, phD = 0;
     bool ok = true;
+    uint32_t phE = 0;
 
-    auto issue = [&](bool complexA) {
+    auto issue = [&](const uint8_t *Ar, const uint8_t *Ai) {
         // C_r (+)= Ar Br - Ai Bi ; C_i (+)= Ai Br + Ar Bi  (Ai absent for the real one-body)
         tc_fence_after();
         for (int kk = 0; kk < n / 16; ++kk) {
             const uint32_t kb = kk >> 2, ko = (kk & 3) * 32;
-            const uint64_t aR = desc_k_sw128(smem_u32(sMr + kb * 16384) + ko);
-            const uint64_t aI = desc_k_sw128(smem_u32(sMi + kb * 16384) + ko);
-            const uint64_t bR = desc_k_noswz(smem_u32(sBr) + kk * 256, LBO, SBO);
-            const uint64_t bI = desc_k_noswz(smem_u32(sBi) + kk * 256, LBO, SBO);
+            const uint64_t aR = desc_k_sw128(smem_u32(Ar + kb * 16384) + ko);
+            const uint64_t bR = desc_k_sw128(smem_u32(sBr + kb * NC * 128) + ko);
+            const uint64_t bI = desc_k_sw128(smem_u32(sBi + kb * NC * 128) + ko);
             umma_bf16(tCr, aR, bR, IDESC, kk > 0 ? 1u : 0u);
             umma_bf16(tCi, aR, bI, IDESC, kk > 0 ? 1u : 0u);
-            if (complexA) {
+            if (Ai) {
+                const uint64_t aI = desc_k_sw128(smem_u32(Ai + kb * 16384) + ko);
                 umma_bf16(tCr, aI, bI, IDESCN, 1u);
                 umma_bf16(tCi, aI, bR, IDESC, 1u);
             }
@@ -368,7 +382,6 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
         umma_commit(&bars[1]);
     };
 
-    float pr[NC], pi[NC];
     for (int w = blockIdx.x; w < W && ok; w += gridDim.x) {
         if (!surv[w]) continue;
         if (tid == 0) {
@@ -379,11 +392,13 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             }
         }
         float *gw = w32 + (size_t)w * 2 * n * NC;
+        // order 0: S = phi, operand = bf16(phi)
+        float pr[NC], pi[NC];
 #pragma unroll
         for (int a = 0; a < NC; ++a) {
             pr[a] = rowOK ? gw[row + (size_t)n * a] : 0.f;
             pi[a] = rowOK ? gw[(size_t)n * NC + row + (size_t)n * a] : 0.f;
-            if (rowOK) { store_b_bf16(sBr, n, a, row, pr[a]); store_b_bf16(sBi, n, a, row, pi[a]); }
+            if (rowOK) { store_b_sw<NC>(sBr, a, row, pr[a]); store_b_sw<NC>(sBi, a, row, pi[a]); }
         }
         fence_proxy_async();
         tc_fence_before();
@@ -394,7 +409,7 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
         int k = 0;
         while (true) {
             ++k;
-            if (tid == 0) issue(true);
+            if (tid == 0) issue(sMr, sMi);
             ok = __syncthreads_and(mbar_wait(&bars[1], phD)) != 0;
             phD ^= 1;
             if (!ok) break;
@@ -402,21 +417,19 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             const float inv = 1.0f / (float)k;
             float mx = 0.f;
 #pragma unroll
-            for (int c0 = 0; c0 < NC; c0 += 32) {
-                float vr[32], vi[32];
-                tmem_ld32(tCr + lanebase + c0, vr);
-                tmem_ld32(tCi + lanebase + c0, vi);
+            for (int c0 = 0; c0 < NC; c0 += 16) {
+                float vr[16], vi[16];
+                tmem_ld16(tCr + lanebase + c0, vr);
+                tmem_ld16(tCi + lanebase + c0, vi);
 #pragma unroll
-                for (int a = 0; a < 32; ++a) {
-                    if (c0 + a < NC) {
-                        const float tr = vr[a] * inv, ti = vi[a] * inv;
-                        pr[c0 + a] += tr;
-                        pi[c0 + a] += ti;
-                        if (rowOK) {
-                            mx = fmaxf(mx, tr * tr + ti * ti);
-                            store_b_bf16(sBr, n, c0 + a, row, tr);
-                            store_b_bf16(sBi, n, c0 + a, row, ti);
-                        }
+                for (int a = 0; a < 16; ++a) {
+                    const float tr = vr[a] * inv, ti = vi[a] * inv;
+                    pr[c0 + a] += tr;
+                    pi[c0 + a] += ti;
+                    if (rowOK) {
+                        mx = fmaxf(mx, tr * tr + ti * ti);
+                        store_b_sw<NC>(sBr, c0 + a, row, tr);
+                        store_b_sw<NC>(sBi, c0 + a, row, ti);
                     }
                 }
             }
@@ -435,33 +448,34 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
         }
         if (!ok) break;
         if (doOneBody) {
-            // one-body operator into the M buffer, current walker as operand
+            // E - I into the M buffer (its MMAs are complete), operand = bf16(S)
             if (tid == 0) {
-                mbar_arrive_expect_tx(&bars[0], (uint32_t)(KB * 16384));
-                for (int kb = 0; kb < KB; ++kb) tma_load_2d(sMr + kb * 16384, &tmE, &bars[0], kb * 64, 0);
+                mbar_arrive_expect_tx(&bars[2], (uint32_t)(KB * 16384));
+                for (int kb = 0; kb < KB; ++kb) tma_load_2d(sMr + kb * 16384, &tmE, &bars[2], kb * 64, 0);
             }
 #pragma unroll
             for (int a = 0; a < NC; ++a)
-                if (rowOK) { store_b_bf16(sBr, n, a, row, pr[a]); store_b_bf16(sBi, n, a, row, pi[a]); }
+                if (rowOK) { store_b_sw<NC>(sBr, a, row, pr[a]); store_b_sw<NC>(sBi, a, row, pi[a]); }
             fence_proxy_async();
             tc_fence_before();
             __syncthreads();
-            ok = __syncthreads_and(mbar_wait(&bars[0], phL)) != 0;
-            phL ^= 1;
+            ok = __syncthreads_and(mbar_wait(&bars[2], phE)) != 0;
+            phE ^= 1;
             if (!ok) break;
-            if (tid == 0) issue(false);
+            if (tid == 0) issue(sMr, nullptr);
             ok = __syncthreads_and(mbar_wait(&bars[1], phD)) != 0;
             phD ^= 1;
             if (!ok) break;
             tc_fence_after();
+        }
+        if (doOneBody) {
 #pragma unroll
-            for (int c0 = 0; c0 < NC; c0 += 32) {
-                float vr[32], vi[32];
-                tmem_ld32(tCr + lanebase + c0, vr);
-                tmem_ld32(tCi + lanebase + c0, vi);
+            for (int c0 = 0; c0 < NC; c0 += 16) {
+                float vr[16], vi[16];
+                tmem_ld16(tCr + lanebase + c0, vr);
+                tmem_ld16(tCi + lanebase + c0, vi);
 #pragma unroll
-                for (int a = 0; a < 32; ++a)
-                    if (c0 + a < NC) { pr[c0 + a] += vr[a]; pi[c0 + a] += vi[a]; }
+                for (int a = 0; a < 16; ++a) { pr[c0 + a] += vr[a]; pi[c0 + a] += vi[a]; }
             }
         }
         if (rowOK) {
@@ -495,7 +509,8 @@ int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE,
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int grid = std::min(e->W, 2 * sms);
+    const int perSm = TaylorSmem<NC>::bytes(e->n) <= 112 * 1024 ? 2 : 1;
+    int grid = std::min(e->W, perSm * sms);
     taylor_onebody_kernel<NC><<<grid, 128, smem, e->stream>>>(
         mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, 30, 1e-10f, 4, doOneBody, e->status,
         e->mx->err);
