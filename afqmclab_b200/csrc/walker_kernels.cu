@@ -189,31 +189,75 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
 // ---------------------------------------------------------------------------
 // Same contract as lu_kernel for blocks of 33..GJ_CTA_MAX_NS columns, one CTA
 // per walker, the block resident in shared memory (column-major, as in S).
+// Warp w owns the columns c = w (mod warps); lane l holds rows l, l+32, ...
 // With the inverse requested: Gauss-Jordan elimination in place (zgetf2 pivot
 // choice, row interchanges undone as column swaps at the end).  Without it:
-// the LU elimination of the trailing block only.  In both cases the pivots
-// are the U diagonal of zgetrf, so the log-determinant follows
-// logDeterminant (tensor_2d_common_fun.cpp:75-105).  Three barriers per
-// column: pivot search, interchange + row scaling, elimination.
+// the LU elimination of the trailing block only.  Per column j, two barriers:
+//   A  every warp interchanges rows j and p and scales row j in its columns;
+//      the owner of column j gathers that column (and rewrites it);
+//   B  every warp applies the rank-1 update to its columns; the owner of
+//      column j+1 updates it first and finds the next pivot and its
+//      reciprocal, so the search overlaps the other warps' updates.
+// The pivots are the U diagonal of zgetrf; the log-determinant is summed from
+// them at the end with the interchange signs, as logDeterminant does
+// (tensor_2d_common_fun.cpp:75-105).
 // ---------------------------------------------------------------------------
 constexpr int GJ_CTA_MAX_NS = 120;
 
+// column buffer: ns complex values during the elimination, then the pivot
+// list, the column permutation and the log-determinant partial sums
+__host__ __device__ constexpr size_t gj_cta_col_bytes(int ns)
+{
+    return (((size_t)16 * ns > (size_t)8 * ns + 400 ? (size_t)16 * ns : (size_t)8 * ns + 400) + 15) / 16 * 16;
+}
 __host__ __device__ constexpr size_t gj_cta_smem(int ns)
 {
-    return (size_t)ns * ns * sizeof(zd) + (size_t)ns * sizeof(zd) + 4 * sizeof(int);
+    return (size_t)ns * ns * sizeof(zd) + gj_cta_col_bytes(ns) + 3 * sizeof(zd);
 }
 
-template <int NT>
+// pivot of column j (rows >= j) by one warp whose lanes hold rows lane + 32 r;
+// lane 0 publishes (1/pivot, (row, zero flag), pivot)
+template <int RPL>
+__device__ __forceinline__ void gj_cta_pivot(const zd *A, int Ns, int j, int lane, zd *sc)
+{
+    double best = -1.0;
+    int bi = Ns;
+#pragma unroll
+    for (int r = 0; r < RPL; ++r) {
+        const int i = lane + 32 * r;
+        if (i >= j && i < Ns) {
+            const double v = zcabs1(A[i + (size_t)Ns * j]);
+            if (v > best) { best = v; bi = i; }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+    }
+    if (lane == 0) {
+        const zd d = A[bi + (size_t)Ns * j];
+        const bool z = zeq0(d);
+        sc[0] = z ? make_double2(0.0, 0.0) : zdiv(make_double2(1.0, 0.0), d);
+        sc[1] = make_double2((double)bi, z ? 1.0 : 0.0);
+        sc[2] = d;
+    }
+}
+
+template <int NT, int RPL>
 __global__ void __launch_bounds__(NT)
 gj_cta_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const zd *logw,
               zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut, double *weight,
               int *status, int mode, int wantInverse, int maxNs)
 {
+    constexpr int NW = NT / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     zd *A = (zd *)smem_raw;
     zd *col = A + (size_t)maxNs * maxNs;
-    int *sc = (int *)(col + maxNs);   // [0] pivot row of the current column
-    const int w = blockIdx.x, tid = threadIdx.x;
+    // [0] 1 / pivot, [1] (pivot row, zero pivot flag), [2] pivot
+    zd *sc = (zd *)((unsigned char *)col + gj_cta_col_bytes(maxNs));
+    const int w = blockIdx.x, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const bool act = (active == nullptr) || active[w] != 0;
     if (!act) {
         if (tid == 0) {
@@ -233,78 +277,92 @@ gj_cta_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const 
         __syncthreads();
         for (int e = tid; e < Ns * Ns; e += NT) A[e] = Sg[e];
         __syncthreads();
-        double lognorm = 0.0;
-        zd phase = make_double2(1.0, 0.0);
-        int myPiv = tid;   // thread k keeps the pivot row of column k
+        if (warp == 0) gj_cta_pivot<RPL>(A, Ns, 0, lane, sc);
+        __syncthreads();
+        int myPiv = tid;   // thread k keeps the pivot row and value of column k
+        zd myD = make_double2(1.0, 0.0);
         bool sing = false;
         for (int j = 0; j < Ns; ++j) {
-            if (tid < 32) {
-                double best = -1.0;
-                int bi = Ns;
-                for (int i = j + tid; i < Ns; i += 32) {
-                    const double v = zcabs1(A[i + (size_t)Ns * j]);
-                    if (v > best) { best = v; bi = i; }
-                }
-                for (int o = 16; o > 0; o >>= 1) {
-                    const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-                }
-                if (tid == 0) sc[0] = bi;
-            }
-            __syncthreads();
-            const int p = sc[0];
-            if (tid == j) myPiv = p;
-            const zd d = A[p + (size_t)Ns * j];
-            const bool zero = zeq0(d);
-            const zd dinv = zero ? make_double2(0.0, 0.0) : zdiv(make_double2(1.0, 0.0), d);
-            if (zero) {
-                sing = true;
-            } else if (tid == 0) {
-                const double a = zabs(d);
-                lognorm += log(a);
-                const zd f = (p != j) ? zneg(d) : d;
-                phase = zmul(phase, make_double2(f.x / a, f.y / a));
-            }
-            // interchange rows j and p, scale the new row j, gather column j
-            // of the other rows (col[p] is the old A[j][j])
-            for (int c = tid; c < Ns; c += NT) {
+            const int p = (int)sc[1].x;
+            if (sc[1].y != 0.0) sing = true;
+            const zd dinv = sc[0];
+            if (tid == j) { myPiv = p; myD = sc[2]; }
+            // A: interchange + row scaling in this warp's columns (one lane per column)
+            for (int c = warp + NW * lane; c < Ns; c += NW * 32) {
                 const zd a = A[j + (size_t)Ns * c], bq = A[p + (size_t)Ns * c];
-                A[j + (size_t)Ns * c] = (inv && c == j) ? dinv : zmul(bq, dinv);
                 if (p != j) A[p + (size_t)Ns * c] = a;
-                if (c == j && p != j) col[p] = a;
+                A[j + (size_t)Ns * c] = (c == j) ? bq : zmul(bq, dinv);
             }
-            for (int i = tid; i < Ns; i += NT)
-                if (i != j && i != p) col[i] = A[i + (size_t)Ns * j];
-            __syncthreads();
-            if (inv) {
-                for (int e = tid; e < Ns * Ns; e += NT) {
-                    const int i = e % Ns, c = e / Ns;
-                    if (i == j) continue;
-                    const zd f = col[i];
-                    if (c == j) {
-                        A[e] = zneg(zmul(f, dinv));
-                    } else {
-                        const zd u = A[j + (size_t)Ns * c];
-                        zd v = A[e];
-                        v.x -= f.x * u.x - f.y * u.y;
-                        v.y -= f.x * u.y + f.y * u.x;
-                        A[e] = v;
+            if (warp == j % NW) {
+                __syncwarp();
+                // column j after the interchange: gather, then its final values
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) {
+                    const int i = lane + 32 * r;
+                    if (i < Ns && i != j) {
+                        const zd f = A[i + (size_t)Ns * j];
+                        col[i] = f;
+                        if (inv) A[i + (size_t)Ns * j] = zneg(zmul(f, dinv));
                     }
                 }
-            } else {
-                const int r = Ns - j - 1;
-                for (int e = tid; e < r * r; e += NT) {
-                    const int i = j + 1 + e % r, c = j + 1 + e / r;
-                    const zd f = col[i], u = A[j + (size_t)Ns * c];
-                    zd v = A[i + (size_t)Ns * c];
-                    v.x -= f.x * u.x - f.y * u.y;
-                    v.y -= f.x * u.y + f.y * u.x;
-                    A[i + (size_t)Ns * c] = v;
-                }
+                if (inv && lane == 0) A[j + (size_t)Ns * j] = dinv;
             }
             __syncthreads();
+            // B: rank-1 update of this warp's columns; column j+1 first
+            zd f[RPL];
+            bool mine[RPL];
+#pragma unroll
+            for (int r = 0; r < RPL; ++r) {
+                const int i = lane + 32 * r;
+                mine[r] = i < Ns && i != j && (inv || i > j);
+                f[r] = mine[r] ? col[i] : make_double2(0.0, 0.0);
+            }
+            const int cn = j + 1;
+            const bool ownNext = cn < Ns && (cn % NW) == warp;
+            auto update = [&](int c) {
+                const zd u = A[j + (size_t)Ns * c];
+#pragma unroll
+                for (int r = 0; r < RPL; ++r) {
+                    if (mine[r]) {
+                        zd *ap = A + lane + 32 * r + (size_t)Ns * c;
+                        zd v = *ap;
+                        v.x -= f[r].x * u.x - f[r].y * u.y;
+                        v.y -= f[r].x * u.y + f[r].y * u.x;
+                        *ap = v;
+                    }
+                }
+            };
+            if (ownNext) {
+                update(cn);
+                __syncwarp();
+                gj_cta_pivot<RPL>(A, Ns, cn, lane, sc);
+            }
+            int c0 = warp;
+            if (!inv && c0 <= j) c0 += ((j + 1 - c0 + NW - 1) / NW) * NW;   // first column > j
+            for (int c = c0; c < Ns; c += NW)
+                if (c != j && c != cn) update(c);
+            __syncthreads();
         }
+        // log-determinant from the pivots, sign flip per interchange
+        unsigned char *cb = (unsigned char *)col;
+        double *redL = (double *)(cb + ((8 * Ns + 15) & ~15));
+        zd *redP = (zd *)(cb + ((8 * Ns + 15) & ~15) + ((8 * NW + 15) & ~15));
+        double ln = 0.0;
+        zd ph = make_double2(1.0, 0.0);
+        if (!sing && tid < Ns) {
+            const double ad = zabs(myD);
+            ln = log(ad);
+            ph = make_double2(myD.x / ad, myD.y / ad);
+            if (myPiv != tid) ph = zneg(ph);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            ln += __shfl_xor_sync(0xffffffffu, ln, o);
+            zd q;
+            q.x = __shfl_xor_sync(0xffffffffu, ph.x, o);
+            q.y = __shfl_xor_sync(0xffffffffu, ph.y, o);
+            ph = zmul(ph, q);
+        }
+        if (lane == 0) { redL[warp] = ln; redP[warp] = ph; }
         if (inv) {
             // column permutation that undoes the row interchanges, last first
             int *pv = (int *)col, *idx = pv + Ns;
@@ -323,10 +381,14 @@ gj_cta_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const 
                 Xg[e] = A[i + (size_t)Ns * idx[k]];
             }
         }
+        __syncthreads();
         if (sing) {
             singular = true;
         } else if (tid == 0) {
-            const zd ld = zadd(make_double2(lognorm, 0.0), zlog(phase));
+            double lnT = 0.0;
+            zd phT = make_double2(1.0, 0.0);
+            for (int k = 0; k < NW; ++k) { lnT += redL[k]; phT = zmul(phT, redP[k]); }
+            const zd ld = zadd(make_double2(lnT, 0.0), zlog(phT));
             if (logdetSum.x > -1e299) logdetSum = zadd(logdetSum, ld);
         }
     }
@@ -1180,20 +1242,20 @@ void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const in
         const size_t smem = gj_cta_smem(maxNs);
         static bool cattr = false;
         if (!cattr) {
-            cudaFuncSetAttribute(gj_cta_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)gj_cta_smem(GJ_CTA_MAX_NS));
-            cudaFuncSetAttribute(gj_cta_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(gj_cta_kernel<256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)gj_cta_smem(64));
+            cudaFuncSetAttribute(gj_cta_kernel<512, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)gj_cta_smem(GJ_CTA_MAX_NS));
             cattr = true;
         }
         if (maxNs <= 64)
-            gj_cta_kernel<256><<<W, 256, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
-                                                     alive, surv, logwOut, weight, status, mode,
-                                                     wantInverse ? 1 : 0, maxNs);
+            gj_cta_kernel<256, 2><<<W, 256, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
+                                                        alive, surv, logwOut, weight, status, mode,
+                                                        wantInverse ? 1 : 0, maxNs);
         else
-            gj_cta_kernel<512><<<W, 512, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
-                                                     alive, surv, logwOut, weight, status, mode,
-                                                     wantInverse ? 1 : 0, maxNs);
+            gj_cta_kernel<512, 4><<<W, 512, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
+                                                        alive, surv, logwOut, weight, status, mode,
+                                                        wantInverse ? 1 : 0, maxNs);
         return;
     }
     if (maxNs <= LU_SMEM_MAX_NS) {
