@@ -988,6 +988,131 @@ __global__ void pop_comb_kernel(int W, const double *weight, const double *unifo
     if (bad && status) status[0] |= 16;
 }
 
+// Same table as pop_comb_kernel, with the serial parts reduced to the two
+// FP64 summation chains whose order the reference fixes (the weight sum and
+// the running probability sum of popConfiguration,
+// populationControlConfiguration.cpp:24-101); everything else is parallel:
+//  - sample i lands on the first parent k whose running sum P_k >= (i+u_i)/W
+//    (capped at W-1): a binary search, since (i+u_i)/W increases with i and
+//    the serial pointer only moves forward;
+//  - the k-th empty slot (in index order) receives the k-th surplus copy,
+//    parents enumerated in index order, each giving number-1 copies: ranks
+//    from block scans and a binary search over the surplus prefix.
+// One CTA of 1024 threads; weights, uniforms, sums and counts in shared memory.
+constexpr int POP_PAR_THREADS = 1024;
+
+__device__ int block_excl_scan_1024(int v, int *scratch)
+{
+    // scratch: 32 ints
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) scratch[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        int t = scratch[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        scratch[lane] = t;
+    }
+    __syncthreads();
+    const int base = warp > 0 ? scratch[warp - 1] : 0;
+    const int r = base + x - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(POP_PAR_THREADS)
+pop_comb_par_kernel(int W, const double *weight, const double *uniforms, uint64_t seed,
+                    unsigned long long *counter, int *table, int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sw = (double *)smem_raw;     // weights, then running sums P
+    double *su = sw + W;                 // uniforms, then two int arrays
+    int *sn = (int *)(su + W);           // copies per parent
+    __shared__ int scan[32];
+    __shared__ double ssum;
+    const int tid = threadIdx.x;
+    const unsigned long long c0 = counter ? *counter : 0ULL;
+    for (int i = tid; i < W; i += POP_PAR_THREADS) {
+        sw[i] = weight[i];
+        su[i] = uniforms ? uniforms[i] : rng_uniform(seed, c0 + (unsigned long long)i);
+        sn[i] = 0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        double sum = 0.0;
+        for (int i = 0; i < W; ++i) sum += sw[i];
+        ssum = sum;
+    }
+    __syncthreads();
+    const double sum = ssum;
+    for (int i = tid; i < W; i += POP_PAR_THREADS) sw[i] = sw[i] / sum;
+    __syncthreads();
+    if (tid == 0) {
+        double acc = sw[0];
+        for (int i = 1; i < W; ++i) {
+            acc += sw[i];
+            sw[i] = acc;
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < W; i += POP_PAR_THREADS) {
+        const double t = (i + su[i]) / (W * 1.0);
+        int lo = 0, hi = W - 1;   // first k with P_k >= t, else W - 1
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (t > sw[mid]) lo = mid + 1;
+            else hi = mid;
+        }
+        atomicAdd(&sn[lo], 1);
+    }
+    __syncthreads();
+    if (tid == 0 && counter) *counter = c0 + (unsigned long long)W;
+    // ranks of the empty slots and prefix of surplus copies (contiguous chunks per thread)
+    int *rankE = (int *)su, *endX = rankE + W;
+    const int chunk = (W + POP_PAR_THREADS - 1) / POP_PAR_THREADS;
+    const int b0 = min(W, tid * chunk), b1 = min(W, b0 + chunk);
+    int ce = 0, cx = 0;
+    for (int i = b0; i < b1; ++i) {
+        ce += sn[i] == 0 ? 1 : 0;
+        cx += sn[i] > 1 ? sn[i] - 1 : 0;
+    }
+    int e0 = block_excl_scan_1024(ce, scan);
+    int x0 = block_excl_scan_1024(cx, scan);
+    for (int i = b0; i < b1; ++i) {
+        rankE[i] = e0;
+        e0 += sn[i] == 0 ? 1 : 0;
+        x0 += sn[i] > 1 ? sn[i] - 1 : 0;
+        endX[i] = x0;
+    }
+    __syncthreads();
+    int bad = 0;
+    for (int i = tid; i < W; i += POP_PAR_THREADS) {
+        if (sn[i] != 0) {
+            table[i] = i;
+        } else {
+            const int k = rankE[i];
+            int lo = 0, hi = W - 1;   // first parent whose surplus prefix exceeds k
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (endX[mid] > k) hi = mid;
+                else lo = mid + 1;
+            }
+            if (endX[lo] > k) table[i] = lo;
+            else { table[i] = -1; bad = 1; }
+        }
+    }
+    if (bad && status) atomicOr(status, 16);
+}
+
 // populationControl<T> serial branch (populationControl.h:110-117): parents
 // keep their own slot, so the copies can run in parallel in place.
 __global__ void pop_gather_kernel(int W, long long wsize, const int *table, zd *wf, zd *logw)
@@ -1343,6 +1468,15 @@ void launch_pop_comb(int W, const double *weight, const double *uniforms, uint64
 {
     g_launch_count++;
     const size_t smem = (size_t)W * (2 * sizeof(double) + sizeof(int));
+    if (smem <= 200 * 1024) {
+        static bool pattr = false;
+        if (!pattr) {
+            cudaFuncSetAttribute(pop_comb_par_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            pattr = true;
+        }
+        pop_comb_par_kernel<<<1, POP_PAR_THREADS, smem, s>>>(W, weight, uniforms, seed, counter, table, status);
+        return;
+    }
     const int useSmem = smem <= 160 * 1024 ? 1 : 0;
     static bool attr = false;
     if (!attr) {

@@ -57,19 +57,29 @@ class ClockSampler:
         self.lines = []
 
     def start(self):
+        """Start sampling and wait (at most 3 s) for the first sample, so that
+        the sampler is running when the timed region begins."""
+        self.t0 = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-i", str(self.gpu), "-lms", "100"], stdout=subprocess.PIPE,
+                 "-i", str(self.gpu), "-lms", "50"], stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            deadline = time.time() + 3.0
+            while not self.lines and time.time() < deadline:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
 
+    def begin(self):
+        """Mark the start of the timed region; earlier samples are dropped."""
+        self.t0 = time.time()
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
 
     def stop(self):
         if self.proc is None:
@@ -81,7 +91,9 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ts, ln in self.lines:
+            if self.t0 is not None and ts < self.t0:
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -223,6 +235,7 @@ def bench_uneven(args, capi, inputs, torch, rank, world):
         clocks = ClockSampler(torch.cuda.current_device())
         torch.cuda.synchronize()
         clocks.start()
+        clocks.begin()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -321,7 +334,7 @@ def cpu_measure(name, steps, measure_skip, max_procs=None, walkers_per_proc=None
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="molecule128")
@@ -408,6 +421,7 @@ def main():
     barrier()
     torch.cuda.synchronize()
     clocks.start()
+    clocks.begin()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
