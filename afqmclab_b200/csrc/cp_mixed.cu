@@ -53,7 +53,7 @@ namespace {
 constexpr int BM = 128;
 constexpr int BK = 32;                    // fp32 elements per 128-byte swizzle row
 constexpr int BN = 256;
-constexpr int STAGES = 4;
+constexpr int STAGES = 2;   // two CTAs per SM: one epilogue overlaps the other's K loop
 constexpr int A_BYTES = BM * BK * 4;
 constexpr int B_BYTES = BN * BK * 4;
 constexpr size_t SMEM = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256;
@@ -172,16 +172,24 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
         if (ok && MODE == CPM_ONEBODY) {
             const long long n = p.n;
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 32) {
-                float v[32];
-                tmem_ld32(trow + c0, v);
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                // residuals first (independent loads in flight), then the accumulator
+                float res[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const long long col = (long long)tile * BN + c0 + j;
+                    const size_t idx = (size_t)row + (size_t)n * col;
+                    res[j] = (row < p.n && col < p.cols) ? p.rhi[idx] + p.rlo[idx] : 0.f;
+                }
+                float v[16];
+                tmem_ld16(trow + c0, v);
                 if (row < p.n) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
+                    for (int j = 0; j < 16; ++j) {
                         const long long col = (long long)tile * BN + c0 + j;
                         if (col < p.cols) {
                             const size_t idx = (size_t)row + (size_t)n * col;
-                            const float x = v[j] + p.rhi[idx] + p.rlo[idx];
+                            const float x = v[j] + res[j];
                             if (p.olo) {
                                 const float h = tf32_round(x);
                                 p.ohi[idx] = h;
