@@ -126,6 +126,14 @@ def phase_flops(c, m, taylor_avg):
     return f
 
 
+# DRAM bytes (read + write) per phase occurrence of the dominant kernel, from
+# one ncu capture of the same workload (dram__bytes_read.sum +
+# dram__bytes_write.sum, summed over the phase's launches).
+NCU_TRAFFIC = {
+    ("molecule128", "mixed", "exchange"): (2 * (44.08e6 + 3.07e6), "2 exchange_tc_kernel launches (one per spin)"),
+}
+
+
 def cp_phase_model(m, W, precision):
     """Algorithmic work of one launch of each timed phase of the constrained-path
     step: ("bytes", B) for the mixed form (HBM-bound: fp32 hi/lo walker planes
@@ -485,6 +493,10 @@ def main():
         roof = {"bound": bound, "kernel": top, "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                 "flops_per_launch": fl[top], "launch_ms": t_launch * 1e3, "peak_source": psrc}
+        tr = NCU_TRAFFIC.get((args.workload, precision, top))
+        if tr:
+            roof["traffic"] = tr[0]
+            roof["traffic_note"] = "bytes per phase occurrence, " + tr[1] + ", from ncu"
     else:
         model = cp_phase_model(m, W, precision)
         cand = {k: v for k, v in prof.items() if k in model and v[1] > 0}
