@@ -43,8 +43,10 @@ struct XSmem {
     }
 };
 
-// swizzled 32 x 32 float2 tile: element (r, c) at r * 32 + (c ^ r)
-__device__ __forceinline__ int tsw(int r, int c) { return r * 32 + (c ^ r); }
+// swizzled 32 x 32 float2 tile, swizzled in 16-byte pairs: element (r, c)
+// at r * 32 + 2 * ((c / 2) ^ (r % 16)) + c % 2, so a row is written with
+// 16-byte stores and a column is read without bank conflicts
+__device__ __forceinline__ int tsw(int r, int c) { return r * 32 + ((((c >> 1) ^ (r & 15)) << 1) | (c & 1)); }
 
 template <int NS>
 __global__ void __launch_bounds__(XS_THREADS, 1)
@@ -181,7 +183,8 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
                     tmem_ld32(tR + c0, vr);
                     tmem_ld32(tI + c0, vi);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) T[tsw(lane, j)] = make_float2(vr[j], vi[j]);
+                    for (int j = 0; j < 32; j += 2)
+                        *(float4 *)(T + tsw(lane, j)) = make_float4(vr[j], vi[j], vr[j + 1], vi[j + 1]);
                     __syncwarp();
                     // blocks (g, walker) of this 32-column chunk: D[a][b] in
                     // registers, D[b][a] from the transposed copy
