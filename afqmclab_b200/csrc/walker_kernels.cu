@@ -500,30 +500,27 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
             // eliminate column k from every other row (lane i owns row i);
             // without the inverse only the trailing block below and right of
             // the pivot (the LU elimination) is needed
-            if (inv) {
-                if (lane < Ns && lane != k) {
-                    zd *row = A + lane * GJ_LD;
-                    const zd *prow = A + k * GJ_LD;
-                    const zd dum = row[k];
-                    row[k] = make_double2(0.0, 0.0);
-                    for (int j = 0; j < Ns; ++j) {
-                        const zd pv = prow[j];
-                        zd r = row[j];
-                        r.x -= pv.x * dum.x - pv.y * dum.y;
-                        r.y -= pv.x * dum.y + pv.y * dum.x;
-                        row[j] = r;
-                    }
-                }
-            } else if (lane > k && lane < Ns) {
+            // (columns in chunks of 8: the chunk's loads are issued before its
+            // stores, which the compiler cannot reorder across the shared tile)
+            const bool elim = inv ? (lane < Ns && lane != k) : (lane > k && lane < Ns);
+            if (elim) {
                 zd *row = A + lane * GJ_LD;
                 const zd *prow = A + k * GJ_LD;
                 const zd dum = row[k];
-                for (int j = k + 1; j < Ns; ++j) {
-                    const zd pv = prow[j];
-                    zd r = row[j];
-                    r.x -= pv.x * dum.x - pv.y * dum.y;
-                    r.y -= pv.x * dum.y + pv.y * dum.x;
-                    row[j] = r;
+                if (inv) row[k] = make_double2(0.0, 0.0);
+                const int j1 = inv ? 0 : k + 1;
+                for (int j0 = j1; j0 < Ns; j0 += 8) {
+                    zd pv[8], r[8];
+#pragma unroll
+                    for (int t = 0; t < 8; ++t)
+                        if (j0 + t < Ns) { pv[t] = prow[j0 + t]; r[t] = row[j0 + t]; }
+#pragma unroll
+                    for (int t = 0; t < 8; ++t)
+                        if (j0 + t < Ns) {
+                            r[t].x -= pv[t].x * dum.x - pv[t].y * dum.y;
+                            r[t].y -= pv[t].x * dum.y + pv[t].y * dum.x;
+                            row[j0 + t] = r[t];
+                        }
                 }
             }
             __syncwarp();
