@@ -295,6 +295,50 @@ def bench_uneven(args, capi, inputs, torch, rank, world):
     return 0
 
 
+def bench_adjoint(args, capi, inputs, torch, rank, world):
+    """Adjoint throughput: afqmc_pl_adjoint (mixed local energy, mean
+    log-overlap and their gradients with respect to t, the Cholesky vectors and
+    the trial orbitals, FP64, per-walker recomputation) on the population of a
+    phaseless workload after a few projection steps."""
+    name = args.adjoint_workload
+    m, c = inputs.make_config(name)
+    W = c["W"]
+    eng = capi.pl_engine(m, W, 77 + rank, c["mgs"], c["pop"], precision=capi.AFQMC_FP64)
+    eng.set_walkers(*inputs.initial_walkers(m.phiTUp, W))
+    eng.modify_gm()
+    eng.pop_control()
+    eng.step(3)
+    eng.synchronize()
+    reps = max(1, args.steps // 50)
+    eng.adjoint()           # warm-up (allocations, first launches)
+    eng.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    clocks.begin()
+    t0 = time.perf_counter()
+    out = None
+    for _ in range(reps):
+        out = eng.adjoint()
+    eng.synchronize()
+    dt = time.perf_counter() - t0
+    clk = clocks.stop()
+    n, G, N = m.n, m.G, m.nup + m.ndn
+    line = {"metric": "walker adjoint evaluations/s (E, dE/dt, dE/dL_g, dE/dconj(phiT)), FP64",
+            "value": W * reps / dt, "unit": "walker-evaluations/s", "n_gpus": world, "steps": reps,
+            "warmup": 1, "ms_per_step": dt / reps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "adjoint", "model": name, "n_orbitals": n, "electrons": [m.nup, m.ndn],
+                       "cholesky": G, "walkers": W, "timing": "host wall clock around synchronous calls"},
+            "energy": [float(out["E"].real), float(out["E"].imag)],
+            "gradient_norms": {"dE_dt": float(np.abs(out["dE_dt"]).max()),
+                               "dE_dchol": float(np.abs(out["dE_dchol"]).max())},
+            "clocks": clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
 # ---------------------------------------------------------------- CPU arm
 def _cpu_worker(args):
     name, nwalk, steps, seed, measure_skip = args
@@ -353,6 +397,7 @@ def main():
     ap.add_argument("--no-fp64-side", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--energy-steps", type=int, default=60)
+    ap.add_argument("--adjoint-workload", default="molecule256")
     args = ap.parse_args()
     rank, world, local = dist_info()
 
@@ -383,6 +428,12 @@ def main():
     else:
         torch.cuda.set_device(0)
     dev = torch.cuda.current_device()
+
+    if args.workload == "adjoint":
+        r = bench_adjoint(args, capi, inputs, torch, rank, world)
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return r
 
     if args.workload == "uneven":
         r = bench_uneven(args, capi, inputs, torch, rank, world)
