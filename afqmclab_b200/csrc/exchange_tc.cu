@@ -180,8 +180,14 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
 #pragma unroll 1
                 for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 32) {
                     float vr[32], vi[32];
-                    tmem_ld32(tR + c0, vr);
-                    tmem_ld32(tI + c0, vi);
+                    {
+                        uint32_t ur[32], ui[32];
+                        tmem_ld32_nw(tR + c0, ur);
+                        tmem_ld32_nw(tI + c0, ui);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) { vr[j] = __uint_as_float(ur[j]); vi[j] = __uint_as_float(ui[j]); }
+                    }
 #pragma unroll
                     for (int j = 0; j < 32; j += 2)
                         *(float4 *)(T + tsw(lane, j)) = make_float4(vr[j], vi[j], vr[j + 1], vi[j + 1]);

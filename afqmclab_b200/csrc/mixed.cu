@@ -382,8 +382,17 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
         umma_commit(&bars[1]);
     };
 
-    for (int w = blockIdx.x; w < W && ok; w += gridDim.x) {
-        if (!surv[w]) continue;
+    // Walkers of this CTA: blockIdx.x, +gridDim.x, ... skipping the dead ones.
+    auto next_walker = [&](int w) {
+        while (w < W && !surv[w]) w += gridDim.x;
+        return w;
+    };
+    // M of the first walker; later walkers' M planes are prefetched while the
+    // previous walker finishes (imaginary plane once the series has converged,
+    // real plane once the one-body product is done).
+    int w = next_walker(blockIdx.x);
+    bool mPending = false;
+    if (w < W) {
         if (tid == 0) {
             mbar_arrive_expect_tx(&bars[0], (uint32_t)(2 * KB * 16384));
             for (int kb = 0; kb < KB; ++kb) {
@@ -391,20 +400,28 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
                 tma_load_2d(sMi + kb * 16384, &tmM, &bars[0], kb * 64, (2 * w + 1) * n);
             }
         }
+        mPending = true;
+    }
+    while (w < W) {
+        const int wn = next_walker(w + gridDim.x);
         float *gw = w32 + (size_t)w * 2 * n * NC;
-        // order 0: S = phi, operand = bf16(phi)
+        // order 0: S = phi, operand = bf16(phi); all loads issue before the stores
         float pr[NC], pi[NC];
 #pragma unroll
         for (int a = 0; a < NC; ++a) {
             pr[a] = rowOK ? gw[row + (size_t)n * a] : 0.f;
             pi[a] = rowOK ? gw[(size_t)n * NC + row + (size_t)n * a] : 0.f;
-            if (rowOK) { store_b_sw<NC>(sBr, a, row, pr[a]); store_b_sw<NC>(sBi, a, row, pi[a]); }
+        }
+        if (rowOK) {
+#pragma unroll
+            for (int a = 0; a < NC; ++a) { store_b_sw<NC>(sBr, a, row, pr[a]); store_b_sw<NC>(sBi, a, row, pi[a]); }
         }
         fence_proxy_async();
         tc_fence_before();
         __syncthreads();
         ok = __syncthreads_and(mbar_wait(&bars[0], phL)) != 0;
         phL ^= 1;
+        mPending = false;
         if (!ok) break;
         int k = 0;
         while (true) {
@@ -416,20 +433,31 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             tc_fence_after();
             const float inv = 1.0f / (float)k;
             float mx = 0.f;
+            // Accumulator columns come out of TMEM in chunks of up to 32: all
+            // loads of a chunk are issued before the one completion wait.
+            constexpr int CH = (NC % 32 == 0) ? 32 : 16;
 #pragma unroll
-            for (int c0 = 0; c0 < NC; c0 += 16) {
-                float vr[16], vi[16];
-                tmem_ld16(tCr + lanebase + c0, vr);
-                tmem_ld16(tCi + lanebase + c0, vi);
+            for (int cb = 0; cb < NC; cb += CH) {
+                uint32_t cr[CH], ci[CH];
 #pragma unroll
-                for (int a = 0; a < 16; ++a) {
-                    const float tr = vr[a] * inv, ti = vi[a] * inv;
-                    pr[c0 + a] += tr;
-                    pi[c0 + a] += ti;
-                    if (rowOK) {
-                        mx = fmaxf(mx, tr * tr + ti * ti);
-                        store_b_sw<NC>(sBr, c0 + a, row, tr);
-                        store_b_sw<NC>(sBi, c0 + a, row, ti);
+                for (int c1 = 0; c1 < CH; c1 += 16) {
+                    tmem_ld16_nw(tCr + lanebase + cb + c1, cr + c1);
+                    tmem_ld16_nw(tCi + lanebase + cb + c1, ci + c1);
+                }
+                tmem_wait_ld();
+#pragma unroll
+                for (int c1 = 0; c1 < CH; c1 += 16) {
+                    const int c0 = cb + c1;
+#pragma unroll
+                    for (int a = 0; a < 16; ++a) {
+                        const float tr = __uint_as_float(cr[c1 + a]) * inv, ti = __uint_as_float(ci[c1 + a]) * inv;
+                        pr[c0 + a] += tr;
+                        pi[c0 + a] += ti;
+                        if (rowOK) {
+                            mx = fmaxf(mx, tr * tr + ti * ti);
+                            store_b_sw<NC>(sBr, c0 + a, row, tr);
+                            store_b_sw<NC>(sBi, c0 + a, row, ti);
+                        }
                     }
                 }
             }
@@ -447,15 +475,28 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             __syncthreads();  // red[] is rewritten by the next order
         }
         if (!ok) break;
+        // Every MMA of the series has completed: the M planes are free.
+        if (wn < W) {
+            if (tid == 0) {
+                mbar_arrive_expect_tx(&bars[0], (uint32_t)(2 * KB * 16384));
+                for (int kb = 0; kb < KB; ++kb)
+                    tma_load_2d(sMi + kb * 16384, &tmM, &bars[0], kb * 64, (2 * wn + 1) * n);
+                if (!doOneBody)
+                    for (int kb = 0; kb < KB; ++kb)
+                        tma_load_2d(sMr + kb * 16384, &tmM, &bars[0], kb * 64, (2 * wn) * n);
+            }
+            mPending = true;
+        }
         if (doOneBody) {
-            // E - I into the M buffer (its MMAs are complete), operand = bf16(S)
+            // E - I into the real M plane, operand = bf16(S)
             if (tid == 0) {
                 mbar_arrive_expect_tx(&bars[2], (uint32_t)(KB * 16384));
                 for (int kb = 0; kb < KB; ++kb) tma_load_2d(sMr + kb * 16384, &tmE, &bars[2], kb * 64, 0);
             }
+            if (rowOK) {
 #pragma unroll
-            for (int a = 0; a < NC; ++a)
-                if (rowOK) { store_b_sw<NC>(sBr, a, row, pr[a]); store_b_sw<NC>(sBi, a, row, pi[a]); }
+                for (int a = 0; a < NC; ++a) { store_b_sw<NC>(sBr, a, row, pr[a]); store_b_sw<NC>(sBi, a, row, pi[a]); }
+            }
             fence_proxy_async();
             tc_fence_before();
             __syncthreads();
@@ -467,15 +508,18 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             phD ^= 1;
             if (!ok) break;
             tc_fence_after();
-        }
-        if (doOneBody) {
+            // the one-body product has read E: the real plane of the next M may land
+            if (wn < W && tid == 0)
+                for (int kb = 0; kb < KB; ++kb)
+                    tma_load_2d(sMr + kb * 16384, &tmM, &bars[0], kb * 64, (2 * wn) * n);
 #pragma unroll
             for (int c0 = 0; c0 < NC; c0 += 16) {
-                float vr[16], vi[16];
-                tmem_ld16(tCr + lanebase + c0, vr);
-                tmem_ld16(tCi + lanebase + c0, vi);
+                uint32_t vr[16], vi[16];
+                tmem_ld16_nw(tCr + lanebase + c0, vr);
+                tmem_ld16_nw(tCi + lanebase + c0, vi);
+                tmem_wait_ld();
 #pragma unroll
-                for (int a = 0; a < 16; ++a) { pr[c0 + a] += vr[a]; pi[c0 + a] += vi[a]; }
+                for (int a = 0; a < 16; ++a) { pr[c0 + a] += __uint_as_float(vr[a]); pi[c0 + a] += __uint_as_float(vi[a]); }
             }
         }
         if (rowOK) {
@@ -488,7 +532,11 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
         if (tid == 0) order[w] = k;
         tc_fence_before();
         __syncthreads();
+        w = wn;
     }
+    // An abandoned prefetch still lands in this CTA's shared memory: wait
+    // (bounded) for it before the CTA exits.
+    if (!ok && mPending) (void)mbar_wait(&bars[0], phL);
     if (!ok && err) atomicExch(err, 2);
     tc_fence_before();
     __syncthreads();
