@@ -577,6 +577,181 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
 }
 
 // ---------------------------------------------------------------------------
+// Same contract as gj_warp_kernel for one or two blocks of 17..32 columns, one
+// warp per (walker, block) and the matrix in registers: lane i holds row i
+// (padded to 32 x 32 with the identity, which adds no interchange and a unit
+// pivot).  The column loop is not unrolled; instead every lane's row rotates
+// by one slot per step, so the current column is always register slot 0 and
+// every register index is static.
+//   - pivot: zgetf2's choice, first position >= k of maximal |re|+|im| in the
+//     column; rows are not moved, each lane keeps the position its row has in
+//     the interchanged matrix (ties go to the lower position, as in izamax);
+//   - the chosen lane writes its row to shared memory (a broadcast source for
+//     the warp); every other row i takes a_ij -= (a_ik / piv) a_pj and
+//     a_ik = -a_ik / piv (in-place Gauss-Jordan, which leaves the inverse of the
+//     interchanged matrix); the pivot row is not rescaled but keeps a row scale
+//     1/piv, applied once at the end.
+// The pivots are the U diagonal of the LU factorisation: log|det| is the sum of
+// their logs and the phase their product with one sign flip per interchange
+// (logDeterminant, tensor_2d_common_fun.cpp:75-105).
+// ---------------------------------------------------------------------------
+constexpr int GR_WARPS = 4;
+
+__global__ void __launch_bounds__(GR_WARPS * 32, 3)
+gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const zd *logw,
+              zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut, double *weight,
+              int *status, int mode, int wantInverse)
+{
+    __shared__ __align__(16) zd prow[GR_WARPS][2][32];
+    __shared__ int pvS[GR_WARPS][32];
+    __shared__ int ixS[GR_WARPS][32];
+    __shared__ zd pivS[GR_WARPS][32];
+    __shared__ zd ldS[GR_WARPS];
+    __shared__ int sgS[GR_WARPS];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nb = bl.nblk;   // 1 or 2, so a walker's warps share this CTA
+    const int mIdx = blockIdx.x * GR_WARPS + warp;
+    const int w = mIdx / nb, b = mIdx - w * nb;
+    const bool inW = w < W;
+    const bool act = inW && ((active == nullptr) || active[w] != 0);
+    const int Ns = b == 0 ? bl.Ns[0] : bl.Ns[1];
+    const long long sOff = b == 0 ? bl.sOff[0] : bl.sOff[1];
+    const bool inv = wantInverse && Sinv;
+    bool sing = false;
+    zd ld = make_double2(0.0, 0.0);
+    if (act && Ns > 0) {
+        const zd *Sg = S + (size_t)w * bl.sStride + sOff;
+        zd a[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            a[j] = (lane < Ns && j < Ns) ? Sg[lane + (size_t)Ns * j] : make_double2(lane == j ? 1.0 : 0.0, 0.0);
+        // A row chosen at step k keeps position k for good, so a lane's final
+        // position names the step whose pivot it supplied (and its row scale).
+        int pos = lane;
+#pragma unroll 1
+        for (int k = 0; k < 32; ++k) {
+            double v = pos >= k ? zcabs1(a[0]) : -1.0;
+            if (!(v == v)) v = INFINITY;   // a NaN row wins, so every lane agrees on p
+            int key = pos;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+                const int ok = __shfl_xor_sync(0xffffffffu, key, o);
+                if (ov > v || (ov == v && ok < key)) { v = ov; key = ok; }
+            }
+            const int p = key;
+            const bool isP = (pos == p);
+            zd *pr = prow[warp][k & 1];
+            if (isP) {
+#pragma unroll
+                for (int s = 0; s < 32; ++s) pr[s] = a[s];
+            }
+            if (lane == 0) pvS[warp][k] = p;
+            __syncwarp();
+            const zd piv = pr[0];
+            if (lane == 0) pivS[warp][k] = piv;
+            if (pos == k) pos = p;
+            if (isP) pos = k;
+            const bool z = zeq0(piv);
+            sing = sing || z;
+            const zd q = z ? make_double2(0.0, 0.0) : zdiv(make_double2(1.0, 0.0), piv);
+            const zd f = isP ? make_double2(0.0, 0.0) : zmul(a[0], q);
+            const zd nk = isP ? make_double2(1.0, 0.0) : zneg(f);
+#pragma unroll
+            for (int s = 1; s < 32; ++s) {
+                const zd pv = pr[s];
+                a[s - 1].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[s].x));
+                a[s - 1].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[s].y));
+            }
+            a[31] = nk;
+        }
+        // log-determinant: every lane supplied exactly one pivot
+        __syncwarp();
+        const zd myD = pivS[warp][pos];
+        double ln = 0.0;
+        zd ph = make_double2(1.0, 0.0);
+        if (!sing) {
+            const double ad = zabs(myD);
+            ln = log(ad);
+            ph = make_double2(myD.x / ad, myD.y / ad);
+            if (pvS[warp][pos] != pos) ph = zneg(ph);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ln += __shfl_xor_sync(0xffffffffu, ln, o);
+            zd t;
+            t.x = __shfl_xor_sync(0xffffffffu, ph.x, o);
+            t.y = __shfl_xor_sync(0xffffffffu, ph.y, o);
+            ph = zmul(ph, t);
+        }
+        if (!sing) ld = zadd(make_double2(ln, 0.0), zlog(ph));
+        if (inv) {
+            // columns of the inverse: undo the interchanges as column swaps,
+            // last first; row slot j of this lane lands in column ixS^-1[j]
+            if (lane == 0) {
+                int *ix = ixS[warp], *pv = pvS[warp];
+                for (int c = 0; c < Ns; ++c) ix[c] = c;
+                for (int k = Ns - 1; k >= 0; --k) {
+                    const int q2 = pv[k];
+                    if (q2 < 0 || q2 >= Ns) continue;   // only a non-finite matrix
+                    const int t = ix[k]; ix[k] = ix[q2]; ix[q2] = t;
+                }
+                for (int c = 0; c < Ns; ++c) pv[ix[c]] = c;
+            }
+            __syncwarp();
+            zd *Xg = Sinv + (size_t)w * bl.sStride + sOff;
+            const zd sc = sing ? make_double2(0.0, 0.0) : zdiv(make_double2(1.0, 0.0), myD);
+            if (pos < Ns) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int c = pvS[warp][j];
+                    if (j < Ns && c >= 0 && c < Ns) Xg[pos + (size_t)Ns * c] = zmul(sc, a[j]);
+                }
+            }
+        }
+    }
+    if (lane == 0) { ldS[warp] = ld; sgS[warp] = sing ? 1 : 0; }
+    __syncthreads();
+    if (lane != 0 || b != 0 || !inW) return;
+    if (!act) {
+        if (mode == LU_PROJECT) surv[w] = 0;
+        if (mode == LU_POPWEIGHT) { weight[w] = 0.0; alive[w] = 1; }
+        return;
+    }
+    bool singular = false;
+    zd logdetSum = make_double2(0.0, 0.0);
+    for (int t = 0; t < nb; ++t) {
+        singular = singular || sgS[warp + t] != 0;
+        logdetSum = zadd(logdetSum, ldS[warp + t]);
+    }
+    if (singular) logdetSum = make_double2(-1e300, 0.0);
+    const zd lwR = zadd(logwAdd, logw[w]);
+    const zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
+    logov[w] = lo;
+    if (singular && status) atomicOr(status + w, (int)ST_SINGULAR);
+    if (!(isfinite(lo.x) && isfinite(lo.y)) && status && !singular) atomicOr(status + w, (int)ST_NONFINITE);
+    if (mode == LU_PROJECT) {
+        const double ph = lo.y;
+        const double c = cos(ph);
+        if (c <= 0.0) {
+            alive[w] = 0; surv[w] = 0;
+        } else {
+            logwOut[w] = zadd(logw[w], make_double2(log(c), -ph));
+            surv[w] = 1;
+        }
+    } else if (mode == LU_POPWEIGHT) {
+        const zd e = zexp(lo);
+        if (e.x <= 0.0) {
+            weight[w] = 0.0;
+        } else {
+            weight[w] = e.x;
+            logwOut[w] = zsub(logw[w], lo);
+        }
+        alive[w] = 1;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Exclusive scan of survivors x draws -> per-walker offset into the random
 // stream; reproduces the reference's sequential walker-major draw order
 // (afqmcPhaselessProjection.cpp:80-101, NiupNidn.cpp:66-84).
@@ -1348,6 +1523,13 @@ void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const in
     g_launch_count++;
     int maxNs = 0;
     for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
+    if (maxNs > 16 && maxNs <= 32 && (bl.nblk == 1 || bl.nblk == 2)) {
+        const long long mats = (long long)W * bl.nblk;
+        gj_reg_kernel<<<(unsigned)((mats + GR_WARPS - 1) / GR_WARPS), GR_WARPS * 32, 0, s>>>(
+            W, bl, S, Sinv, active, logw, logwAdd, logwT, logov, alive, surv, logwOut, weight, status,
+            mode, wantInverse ? 1 : 0);
+        return;
+    }
     if (maxNs <= 32) {
         const size_t smem = (size_t)GJ_WARPS * 32 * GJ_LD * sizeof(zd);
         static bool gattr = false;
