@@ -33,6 +33,7 @@ struct MixedState {
     __nv_bfloat16 *A2r[2] = {nullptr, nullptr}, *A2i[2] = {nullptr, nullptr};
     zd *ex2 = nullptr;
     float *Ohi[2] = {nullptr, nullptr}, *Olo[2] = {nullptr, nullptr};   // overlap operators
+    bool ovStacked = false;   // Ohi[0]/Olo[0] hold both blocks' operators
     float *Bh = nullptr, *Bl = nullptr;   // S^{-1} operands of the theta product
     float *E1h = nullptr, *E1l = nullptr; // exp(+dt/2 K) - I, tf32 high/low (measurement)
     float *sh = nullptr, *sl = nullptr;   // walkers split into tf32 high/low parts
@@ -596,11 +597,20 @@ int overlap32(afqmc_engine *e, const float *w32, const int *mask)
 {
     (void)mask;
     MixedState *m = e->mx;
-    for (int b = 0; b < e->bl.nblk; ++b) {
-        const int Ns = e->bl.Ns[b];
-        if (Ns == 0) continue;
-        const int r = overlap_tc_launch(e->stream, e->n, e->ncol, Ns, e->W, m->Ohi[b], m->Olo[b], w32,
-                                        (double *)e->S, e->bl.sStride, e->bl.sOff[b], m->err);
+    int nb = 0, Ns[2];
+    long long sOff[2];
+    for (int b = 0; b < e->bl.nblk; ++b)
+        if (e->bl.Ns[b] > 0) { Ns[nb] = e->bl.Ns[b]; sOff[nb] = e->bl.sOff[b]; ++nb; }
+    if (nb == 0) return AFQMC_OK;
+    if (m->ovStacked) {
+        const int r = overlap_tc_launch(e->stream, e->n, e->ncol, nb, Ns, e->W, m->Ohi[0], m->Olo[0], w32, e->S,
+                                        e->bl.sStride, sOff, m->err);
+        if (r) return engine_fail(AFQMC_ERR_CUDA, "overlap launch: " + std::to_string(r));
+        return AFQMC_OK;
+    }
+    for (int b = 0; b < nb; ++b) {
+        const int r = overlap_tc_launch(e->stream, e->n, e->ncol, 1, Ns + b, e->W, m->Ohi[b], m->Olo[b], w32,
+                                        e->S, e->bl.sStride, sOff + b, m->err);
         if (r) return engine_fail(AFQMC_ERR_CUDA, "overlap launch: " + std::to_string(r));
     }
     return AFQMC_OK;
@@ -709,19 +719,35 @@ int mixed_create(afqmc_engine *e)
         MTRY(engine_dalloc(e, &m->Bh, theta_tc_bscratch(W, maxNs)));
         MTRY(engine_dalloc(e, &m->Bl, theta_tc_bscratch(W, maxNs)));
     }
-    // compensated tf32 overlap operators, one per spin block
-    for (int b = 0; b < e->bl.nblk; ++b) {
-        const int Ns = e->bl.Ns[b];
-        if (Ns == 0) continue;
-        if (!overlap_tc_supported(n, Ns)) return engine_fail(AFQMC_ERR_UNSUPPORTED, "overlap block too wide for the mixed form");
-        std::vector<zd> T((size_t)n * Ns);
-        MTRY(cuda_check(cudaMemcpy(T.data(), e->phiT[b], sizeof(zd) * T.size(), cudaMemcpyDeviceToHost), "copy"));
-        std::vector<float> oh, ol;
-        overlap_tc_build(T.data(), n, Ns, oh, ol);
-        MTRY(engine_dalloc(e, &m->Ohi[b], oh.size()));
-        MTRY(engine_dalloc(e, &m->Olo[b], ol.size()));
-        MTRY(cuda_check(cudaMemcpy(m->Ohi[b], oh.data(), 4 * oh.size(), cudaMemcpyHostToDevice), "upload"));
-        MTRY(cuda_check(cudaMemcpy(m->Olo[b], ol.data(), 4 * ol.size(), cudaMemcpyHostToDevice), "upload"));
+    // compensated tf32 overlap operator of the spin blocks, stacked
+    {
+        int nb = 0, Ns[2];
+        std::vector<zd> T[2];
+        const zd *Tp[2];
+        for (int b = 0; b < e->bl.nblk; ++b) {
+            if (e->bl.Ns[b] == 0) continue;
+            Ns[nb] = e->bl.Ns[b];
+            T[nb].resize((size_t)n * Ns[nb]);
+            MTRY(cuda_check(cudaMemcpy(T[nb].data(), e->phiT[b], sizeof(zd) * T[nb].size(), cudaMemcpyDeviceToHost),
+                            "copy"));
+            Tp[nb] = T[nb].data();
+            ++nb;
+        }
+        // one operator for both blocks when it fits the 128 rows of a tile,
+        // else one per block
+        m->ovStacked = nb > 0 && overlap_tc_supported(n, nb, Ns);
+        const int nop = m->ovStacked ? 1 : nb;
+        for (int o = 0; o < nop; ++o) {
+            const int nbo = m->ovStacked ? nb : 1;
+            if (!overlap_tc_supported(n, nbo, Ns + o))
+                return engine_fail(AFQMC_ERR_UNSUPPORTED, "overlap block too wide for the mixed form");
+            std::vector<float> oh, ol;
+            overlap_tc_build(nbo, Tp + o, n, Ns + o, oh, ol);
+            MTRY(engine_dalloc(e, &m->Ohi[o], oh.size()));
+            MTRY(engine_dalloc(e, &m->Olo[o], ol.size()));
+            MTRY(cuda_check(cudaMemcpy(m->Ohi[o], oh.data(), 4 * oh.size(), cudaMemcpyHostToDevice), "upload"));
+            MTRY(cuda_check(cudaMemcpy(m->Olo[o], ol.data(), 4 * ol.size(), cudaMemcpyHostToDevice), "upload"));
+        }
     }
     m->ready = true;
     return AFQMC_OK;

@@ -9,10 +9,19 @@
 // (SDSDOperation.cpp:154-164, SD2sSD2isOperation.cpp:84-94) in the
 // mixed-precision form.
 //
-//   warp 0 lane 0 : TMA producer (O_hi, O_lo tiles; raw fp32 walker tiles)
-//   warp 1        : TMEM owner; lane 0 issues the UMMAs
-//   warps 2..5    : split each walker tile in place (hi) and beside it (lo),
-//                   then the epilogue (TMEM lane quarter = warp % 4)
+// The spin blocks share the walker (SD2is: both use its leading columns), so
+// their operators are stacked into one A operand of at most 128 rows and a
+// walker tile is read once for both: block b occupies rows from 2 sum_{b'<b}
+// Ns_b', row 2a = [Re T(:,a) | Im T(:,a)], row 2a+1 = [-Im T(:,a) | Re T(:,a)],
+// so the real and imaginary parts of S(a, c) land in neighbouring TMEM lanes.
+//
+// Persistent CTAs over tiles of BN walker columns (whole walkers), K = 2n in
+// chunks of 32:
+//   warp 0 lane 0 : TMA producer (O_hi, O_lo chunks; raw fp32 walker chunks)
+//   warp 1        : TMEM owner; lane 0 issues the UMMAs (double-buffered TMEM)
+//   warps 2..5    : split each walker chunk in place (hi) and beside it (lo)
+//   warps 6..9    : epilogue (TMEM lane quarter = warp % 4), one complex
+//                   double per lane and column pair after a lane-pair exchange
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -29,21 +38,23 @@ extern std::atomic<long long> g_launch_count;
 
 namespace {
 
-constexpr int BM = 128, BK = 32, BN = 256, STAGES = 2;
+constexpr int BM = 128, BK = 32, BN = 128, STAGES = 3, NT = 320;
 constexpr int A_BYTES = BM * BK * 4;
 constexpr int B_BYTES = BN * BK * 4;
 constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
 constexpr size_t SMEM = 1024 + (size_t)STAGES * STAGE_BYTES + 256;
 
 struct OvArgs {
-    int n, Ns, W, kbA, bnw, wpt;
+    int n, W, kbA, bnw, wpt, tiles, rows;
+    int nb, Ns[2], rowBase[2];
+    long long sOff[2];
     uint32_t idesc;
-    double *S;
-    long long sStride, sOff;
+    double2 *S;
+    long long sStride;
     int *err;
 };
 
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(NT, 1)
 ov_split_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
                 const __grid_constant__ CUtensorMap tB, OvArgs p)
 {
@@ -52,13 +63,15 @@ ov_split_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__
     uint64_t *full = (uint64_t *)(base + STAGES * STAGE_BYTES);
     uint64_t *split = full + STAGES;
     uint64_t *empty = split + STAGES;
-    uint64_t *tmemFull = empty + STAGES;
-    uint32_t *tmemSlot = (uint32_t *)(tmemFull + 1);
+    uint64_t *tfull = empty + STAGES;   // 2
+    uint64_t *tempty = tfull + 2;       // 2
+    uint32_t *tmemSlot = (uint32_t *)(tempty + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int tile = blockIdx.x;
     const int KT = 2 * p.kbA;
-    const uint32_t bBytes = (uint32_t)(p.wpt * p.bnw * BK * 4);
+    const int ncols = p.wpt * p.bnw;
+    const uint32_t bBytes = (uint32_t)(ncols * BK * 4);
+    const int myTiles = (p.tiles - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -66,12 +79,13 @@ ov_split_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__
             mbar_init(&split[s], 128);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(tmemFull, 1);
+        for (int b = 0; b < 2; ++b) { mbar_init(&tfull[b], 1); mbar_init(&tempty[b], 128); }
         fence_mbar_init();
         tma_prefetch_desc(&tAh);
+        tma_prefetch_desc(&tAl);
         tma_prefetch_desc(&tB);
     }
-    if (warp == 1) { tmem_alloc(tmemSlot, BN); tmem_relinquish(); }
+    if (warp == 1) { tmem_alloc(tmemSlot, 2 * BN); tmem_relinquish(); }
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -80,52 +94,62 @@ ov_split_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__
 
     if (warp == 0) {
         if (lane == 0) {
-            for (int kt = 0; kt < KT && ok; ++kt) {
-                const int s = kt % STAGES;
-                if (kt >= STAGES) ok = mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1);
-                if (!ok) break;
-                const int plane = kt / p.kbA, kk = (kt % p.kbA) * BK;
-                uint8_t *st = base + s * STAGE_BYTES;
-                mbar_arrive_expect_tx(&full[s], 2 * A_BYTES + bBytes);
-                tma_load_2d(st, &tAh, &full[s], plane * p.n + kk, 0);
-                tma_load_2d(st + A_BYTES, &tAl, &full[s], plane * p.n + kk, 0);
-                for (int j = 0; j < p.wpt; ++j)
-                    tma_load_3d(st + 2 * A_BYTES + j * p.bnw * BK * 4, &tB, &full[s], kk, 0,
-                                2 * (tile * p.wpt + j) + plane);
-            }
-            for (int kt = max(KT, STAGES); kt < KT + STAGES && ok; ++kt) {
-                const int s = kt % STAGES;
-                ok = mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1);
+            int it = 0;
+            for (int ti = 0; ti < myTiles && ok; ++ti) {
+                const int t = (int)blockIdx.x + ti * (int)gridDim.x;
+                for (int kt = 0; kt < KT && ok; ++kt, ++it) {
+                    const int s = it % STAGES;
+                    if (it >= STAGES) ok = mbar_wait(&empty[s], ((it / STAGES) - 1) & 1);
+                    if (!ok) break;
+                    const int plane = kt / p.kbA, kk = (kt % p.kbA) * BK;
+                    uint8_t *st = base + s * STAGE_BYTES;
+                    // walkers past W are not loaded (their columns are never written)
+                    const int nv = min(p.wpt, p.W - t * p.wpt);
+                    mbar_arrive_expect_tx(&full[s], 2 * A_BYTES + (uint32_t)(nv * p.bnw * BK * 4));
+                    tma_load_2d(st, &tAh, &full[s], plane * p.n + kk, 0);
+                    tma_load_2d(st + A_BYTES, &tAl, &full[s], plane * p.n + kk, 0);
+                    for (int j = 0; j < nv; ++j)
+                        tma_load_3d(st + 2 * A_BYTES + j * p.bnw * BK * 4, &tB, &full[s], kk, 0,
+                                    2 * (t * p.wpt + j) + plane);
+                }
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            for (int kt = 0; kt < KT && ok; ++kt) {
-                const int s = kt % STAGES;
-                ok = mbar_wait(&split[s], (kt / STAGES) & 1);
+            int it = 0;
+            for (int ti = 0; ti < myTiles && ok; ++ti) {
+                const int buf = ti & 1;
+                if (ti >= 2) ok = mbar_wait(&tempty[buf], ((ti >> 1) - 1) & 1);
                 if (!ok) break;
-                tc_fence_after();
-                const uint32_t st = smem_u32(base + s * STAGE_BYTES);
-                const uint32_t ah = st, al = st + A_BYTES, bh = st + 2 * A_BYTES, bl = bh + B_BYTES;
+                const uint32_t d = tmem + (uint32_t)(buf * BN);
+                for (int kt = 0; kt < KT && ok; ++kt, ++it) {
+                    const int s = it % STAGES;
+                    ok = mbar_wait(&split[s], (it / STAGES) & 1);
+                    if (!ok) break;
+                    tc_fence_after();
+                    const uint32_t st = smem_u32(base + s * STAGE_BYTES);
+                    const uint32_t ah = st, al = st + A_BYTES, bh = st + 2 * A_BYTES, bl = bh + B_BYTES;
 #pragma unroll
-                for (int k8 = 0; k8 < BK / 8; ++k8) {
-                    const uint32_t acc0 = (kt > 0 || k8 > 0) ? 1u : 0u;
-                    umma_tf32(tmem, desc_k_sw128(ah + k8 * 32), desc_k_sw128(bh + k8 * 32), p.idesc, acc0);
-                    umma_tf32(tmem, desc_k_sw128(al + k8 * 32), desc_k_sw128(bh + k8 * 32), p.idesc, 1u);
-                    umma_tf32(tmem, desc_k_sw128(ah + k8 * 32), desc_k_sw128(bl + k8 * 32), p.idesc, 1u);
+                    for (int k8 = 0; k8 < BK / 8; ++k8) {
+                        const uint32_t acc0 = (kt > 0 || k8 > 0) ? 1u : 0u;
+                        umma_tf32(d, desc_k_sw128(ah + k8 * 32), desc_k_sw128(bh + k8 * 32), p.idesc, acc0);
+                        umma_tf32(d, desc_k_sw128(al + k8 * 32), desc_k_sw128(bh + k8 * 32), p.idesc, 1u);
+                        umma_tf32(d, desc_k_sw128(ah + k8 * 32), desc_k_sw128(bl + k8 * 32), p.idesc, 1u);
+                    }
+                    umma_commit(&empty[s]);
                 }
-                umma_commit(&empty[s]);
+                if (ok) umma_commit(&tfull[buf]);
             }
-            umma_commit(tmemFull);
         }
         __syncwarp();
-    } else {
-        // split the raw walker tile: hi in place, lo in the slot beside it
+    } else if (warp < 6) {
+        // split the raw walker chunk: hi in place, lo in the slot beside it
         const int t = threadIdx.x - 64;
         const int n4 = (int)(bBytes / 16);
-        for (int kt = 0; kt < KT && ok; ++kt) {
-            const int s = kt % STAGES;
-            ok = mbar_wait(&full[s], (kt / STAGES) & 1);
+        const int items = myTiles * KT;
+        for (int it = 0; it < items && ok; ++it) {
+            const int s = it % STAGES;
+            ok = mbar_wait(&full[s], (it / STAGES) & 1);
             if (!ok) break;
             float4 *bh = (float4 *)(base + s * STAGE_BYTES + 2 * A_BYTES);
             float4 *bl = (float4 *)(base + s * STAGE_BYTES + 2 * A_BYTES + B_BYTES);
@@ -142,37 +166,49 @@ ov_split_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__
             fence_proxy_async();
             mbar_arrive(&split[s]);
         }
-        ok = ok && mbar_wait(tmemFull, 0);
-        tc_fence_after();
+    } else {
         const int q = warp & 3;
-        const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
         const int row = q * 32 + lane;
-        const int Ns = p.Ns;
-        const int part = row >= Ns ? 1 : 0, a = row - part * Ns;
-        const int ncols = p.wpt * p.bnw;
-        if (ok) {
+        const int b = (p.nb > 1 && row >= p.rowBase[1]) ? 1 : 0;
+        const int rr = row - (b ? p.rowBase[1] : 0);
+        const int a = rr >> 1;
+        const int Ns = b ? p.Ns[1] : p.Ns[0];
+        const long long sOff = b ? p.sOff[1] : p.sOff[0];
+        const bool rowOK = row < p.rows;
+        const int odd = lane & 1;
+        for (int ti = 0; ti < myTiles && ok; ++ti) {
+            const int buf = ti & 1;
+            ok = mbar_wait(&tfull[buf], (ti >> 1) & 1);
+            if (!ok) break;
+            tc_fence_after();
+            const int t = (int)blockIdx.x + ti * (int)gridDim.x;
+            const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN);
 #pragma unroll 1
             for (int c0 = 0; c0 < ncols; c0 += 32) {
                 float v[32];
-                tmem_ld32(trow + c0, v);
-                if (row < 2 * Ns) {
+                tmem_ld32(trow + (uint32_t)c0, v);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int col = c0 + j;
-                        const int wj = col / p.bnw, c = col - wj * p.bnw;
-                        const int w = tile * p.wpt + wj;
-                        if (col < ncols && c < Ns && w < p.W)
-                            p.S[2 * ((size_t)w * p.sStride + p.sOff + a + (size_t)Ns * c) + part] = (double)v[j];
-                    }
+                for (int j = 0; j < 32; j += 2) {
+                    // even lane: Re S(a, col j) and Re S(a, col j+1); odd lane: the Im parts
+                    const float send = odd ? v[j] : v[j + 1];
+                    const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+                    const int col = c0 + j + odd;
+                    const int wj = col / p.bnw, c = col - wj * p.bnw;
+                    const int w = t * p.wpt + wj;
+                    if (rowOK && a < Ns && c < Ns && w < p.W)
+                        p.S[(size_t)w * p.sStride + sOff + a + (size_t)Ns * c] =
+                            odd ? make_double2((double)recv, (double)v[j + 1]) : make_double2((double)v[j], (double)recv);
                 }
             }
+            tc_fence_before();
+            mbar_arrive(&tempty[buf]);
         }
     }
     if (!ok && p.err) atomicExch(p.err, 1);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 1) tmem_dealloc(tmem, BN);
+    if (warp == 1) tmem_dealloc(tmem, 2 * BN);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encoder()
@@ -216,58 +252,89 @@ float tf32_host(float x)
 
 }  // namespace
 
-bool overlap_tc_supported(int n, int Ns) { return n % 4 == 0 && Ns >= 1 && Ns <= 64; }
-
-// O rows: a -> [Re T(:,a) | Im T(:,a)], Ns + a -> [-Im T(:,a) | Re T(:,a)], split hi/lo
-int overlap_tc_build(const zd *Thost, int n, int Ns, std::vector<float> &hi, std::vector<float> &lo)
+bool overlap_tc_supported(int n, int nb, const int *Ns)
 {
-    hi.assign((size_t)4 * Ns * n, 0.f);
-    lo.assign((size_t)4 * Ns * n, 0.f);
+    if (n % 4 != 0 || nb < 1 || nb > 2) return false;
+    int rows = 0;
+    for (int b = 0; b < nb; ++b) {
+        if (Ns[b] < 0 || Ns[b] > 64) return false;
+        rows += 2 * Ns[b];
+    }
+    return rows >= 2 && rows <= BM;
+}
+
+// rows of block b from 2 sum_{b' < b} Ns_b': 2a -> [Re T(:,a) | Im T(:,a)],
+// 2a + 1 -> [-Im T(:,a) | Re T(:,a)]; tf32 high parts and the tf32 remainders
+int overlap_tc_build(int nb, const zd *const *Thost, int n, const int *Ns, std::vector<float> &hi,
+                     std::vector<float> &lo)
+{
+    int rows = 0;
+    for (int b = 0; b < nb; ++b) rows += 2 * Ns[b];
+    hi.assign((size_t)rows * 2 * n, 0.f);
+    lo.assign((size_t)rows * 2 * n, 0.f);
     auto put = [&](size_t idx, double v) {
         const float h = tf32_host((float)v);
         hi[idx] = h;
         lo[idx] = tf32_host((float)(v - (double)h));
     };
-    for (int a = 0; a < Ns; ++a)
-        for (int i = 0; i < n; ++i) {
-            const zd t = Thost[i + (size_t)n * a];
-            const size_t r0 = (size_t)a * 2 * n, r1 = (size_t)(Ns + a) * 2 * n;
-            put(r0 + i, t.x);
-            put(r0 + n + i, t.y);
-            put(r1 + i, -t.y);
-            put(r1 + n + i, t.x);
-        }
+    int r0 = 0;
+    for (int b = 0; b < nb; ++b) {
+        for (int a = 0; a < Ns[b]; ++a)
+            for (int i = 0; i < n; ++i) {
+                const zd t = Thost[b][i + (size_t)n * a];
+                const size_t re = (size_t)(r0 + 2 * a) * 2 * n, im = re + 2 * n;
+                put(re + i, t.x);
+                put(re + n + i, t.y);
+                put(im + i, -t.y);
+                put(im + n + i, t.x);
+            }
+        r0 += 2 * Ns[b];
+    }
     return 0;
 }
 
-int overlap_tc_launch(cudaStream_t s, int n, int ncol, int Ns, int W, const float *Ohi, const float *Olo,
-                      const float *w32, double *S, long long sStride, long long sOff, int *err)
+int overlap_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, int W, const float *Ohi,
+                      const float *Olo, const float *w32, zd *S, long long sStride, const long long *sOff,
+                      int *err)
 {
-    if (!overlap_tc_supported(n, Ns)) return (int)cudaErrorInvalidValue;
+    if (!overlap_tc_supported(n, nb, Ns)) return (int)cudaErrorInvalidValue;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(ov_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
         attr = true;
     }
+    OvArgs a{};
+    a.n = n; a.W = W; a.nb = nb;
+    int rows = 0, maxNs = 0;
+    for (int b = 0; b < 2; ++b) {
+        a.Ns[b] = b < nb ? Ns[b] : 0;
+        a.sOff[b] = b < nb ? sOff[b] : 0;
+        a.rowBase[b] = rows;
+        rows += 2 * a.Ns[b];
+        maxNs = std::max(maxNs, a.Ns[b]);
+    }
+    a.rows = rows;
     CUtensorMap ah, al, b;
-    cuuint64_t da[2] = {(cuuint64_t)2 * n, (cuuint64_t)2 * Ns}, pa[1] = {(cuuint64_t)2 * n * 4};
+    cuuint64_t da[2] = {(cuuint64_t)2 * n, (cuuint64_t)rows}, pa[1] = {(cuuint64_t)2 * n * 4};
     cuuint32_t boxA[2] = {BK, BM};
     int r = map_f32(&ah, Ohi, 2, da, pa, boxA);
     if (!r) r = map_f32(&al, Olo, 2, da, pa, boxA);
-    const int bnw = (Ns + 15) / 16 * 16;
+    const int bnw = (maxNs + 15) / 16 * 16;
     cuuint64_t db[3] = {(cuuint64_t)n, (cuuint64_t)ncol, (cuuint64_t)2 * W};
     cuuint64_t pb[2] = {(cuuint64_t)n * 4, (cuuint64_t)n * ncol * 4};
     cuuint32_t boxB[3] = {BK, (cuuint32_t)bnw, 1u};
     if (!r) r = map_f32(&b, w32, 3, db, pb, boxB);
     if (r) return r;
-    OvArgs a{};
-    a.n = n; a.Ns = Ns; a.W = W;
     a.kbA = (n + BK - 1) / BK;
     a.bnw = bnw;
     a.wpt = std::max(1, BN / bnw);
+    a.tiles = (W + a.wpt - 1) / a.wpt;
     a.idesc = idesc_tf32(BM, a.wpt * bnw);
-    a.S = S; a.sStride = sStride; a.sOff = sOff; a.err = err;
+    a.S = S; a.sStride = sStride; a.err = err;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     g_launch_count++;
-    ov_split_kernel<<<(W + a.wpt - 1) / a.wpt, 192, SMEM, s>>>(ah, al, b, a);
+    ov_split_kernel<<<std::min(a.tiles, sms), NT, SMEM, s>>>(ah, al, b, a);
     return (int)cudaGetLastError();
 }

@@ -7,9 +7,14 @@
 
 #include "common.cuh"
 
-bool overlap_tc_supported(int n, int Ns);
-// host: the 2 Ns x 2 n operator rows (tf32 high / low parts) of the trial block T (n x Ns)
-int overlap_tc_build(const zd *Thost, int n, int Ns, std::vector<float> &hi, std::vector<float> &lo);
-// S[w * sStride + sOff + a + Ns * c] for every walker w of the fp32 population w32
-int overlap_tc_launch(cudaStream_t s, int n, int ncol, int Ns, int W, const float *Ohi, const float *Olo,
-                      const float *w32, double *S, long long sStride, long long sOff, int *err);
+// nb (1 or 2) spin blocks sharing the walker's leading columns, 2 sum Ns <= 128
+bool overlap_tc_supported(int n, int nb, const int *Ns);
+// host: the stacked 2 sum Ns x 2 n operator rows (tf32 high / low parts) of the
+// trial blocks T_b (n x Ns_b)
+int overlap_tc_build(int nb, const zd *const *Thost, int n, const int *Ns, std::vector<float> &hi,
+                     std::vector<float> &lo);
+// S[w * sStride + sOff[b] + a + Ns[b] * c] of every block for every walker w of
+// the fp32 population w32
+int overlap_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, int W, const float *Ohi,
+                      const float *Olo, const float *w32, zd *S, long long sStride, const long long *sOff,
+                      int *err);
