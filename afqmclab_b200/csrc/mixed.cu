@@ -34,7 +34,7 @@ struct MixedState {
     zd *ex2 = nullptr;
     float *Ohi[2] = {nullptr, nullptr}, *Olo[2] = {nullptr, nullptr};   // overlap operators
     bool ovStacked = false;   // Ohi[0]/Olo[0] hold both blocks' operators
-    float *Bh = nullptr, *Bl = nullptr;   // S^{-1} operands of the theta product
+    float *Sinv32 = nullptr;   // S^{-1} as fp32 planes [re | im] per block slot
     float *E1h = nullptr, *E1l = nullptr; // exp(+dt/2 K) - I, tf32 high/low (measurement)
     float *sh = nullptr, *sl = nullptr;   // walkers split into tf32 high/low parts
     int *err = nullptr;
@@ -622,12 +622,19 @@ int overlap32(afqmc_engine *e, const float *w32, const int *mask)
 int theta32(afqmc_engine *e, const float *w32, const int *mask, zd *thetaZ)
 {
     MixedState *m = e->mx;
-    for (int b = 0; b < e->bl.nblk; ++b) {
-        const int Ns = e->bl.Ns[b];
-        if (Ns == 0) continue;
-        const int r = theta_tc_launch(e->stream, e->n, e->ncol, Ns, e->W, w32, e->Sinv, e->bl.sStride,
-                                      e->bl.sOff[b], mask, 3, m->Bh, m->Bl, m->Theta, 2 * e->Ktot,
-                                      e->Ktot, e->bl.tOff[b], thetaZ, e->bl.tStride, m->err);
+    int nb = 0, Ns[2];
+    long long sOff[2], tOff[2];
+    for (int b = 0; b < e->bl.nblk; ++b)
+        if (e->bl.Ns[b] > 0) { Ns[nb] = e->bl.Ns[b]; sOff[nb] = e->bl.sOff[b]; tOff[nb] = e->bl.tOff[b]; ++nb; }
+    if (nb == 0) return AFQMC_OK;
+    const long long s32 = sinv32_stride(e->bl);
+    // both blocks in one pass when they fit, else one pass per block
+    const int groups = theta_tc_supported(e->n, nb, Ns, s32) ? 1 : nb;
+    for (int gi = 0; gi < groups; ++gi) {
+        const int nbg = groups == 1 ? nb : 1;
+        const int r = theta_tc_launch(e->stream, e->n, e->ncol, nbg, Ns + gi, e->W, w32, m->Sinv32, s32,
+                                      sOff + gi, mask, m->Theta, 2 * e->Ktot, e->Ktot, tOff + gi, thetaZ,
+                                      e->bl.tStride, m->err);
         if (r) return engine_fail(AFQMC_ERR_CUDA, "theta launch: " + std::to_string(r));
     }
     return AFQMC_OK;
@@ -711,14 +718,11 @@ int mixed_create(afqmc_engine *e)
         MTRY(engine_dalloc(e, &m->sh, (size_t)W * m->ws32));
         MTRY(engine_dalloc(e, &m->sl, (size_t)W * m->ws32));
     }
-    // S^{-1} operand scratch of the theta product (hi and lo parts)
-    {
-        int maxNs = 0;
-        for (int b = 0; b < e->bl.nblk; ++b) maxNs = std::max(maxNs, e->bl.Ns[b]);
-        if (!theta_tc_supported(n, maxNs)) return engine_fail(AFQMC_ERR_UNSUPPORTED, "theta block too wide for the mixed form");
-        MTRY(engine_dalloc(e, &m->Bh, theta_tc_bscratch(W, maxNs)));
-        MTRY(engine_dalloc(e, &m->Bl, theta_tc_bscratch(W, maxNs)));
-    }
+    // S^{-1} of the theta product, fp32 planes written by the LU
+    MTRY(engine_dalloc(e, &m->Sinv32, (size_t)W * sinv32_stride(e->bl)));
+    for (int b = 0; b < e->bl.nblk; ++b)
+        if (e->bl.Ns[b] > 0 && !theta_tc_supported(n, 1, &e->bl.Ns[b], sinv32_stride(e->bl)))
+            return engine_fail(AFQMC_ERR_UNSUPPORTED, "theta block too wide for the mixed form");
     // compensated tf32 overlap operator of the spin blocks, stacked
     {
         int nb = 0, Ns[2];
@@ -799,9 +803,9 @@ int mixed_project_dtk_dtv(afqmc_engine *e)
     { PHASE(AFQMC_PH_OVERLAP); MTRY(overlap32(e, m->wf32, e->alive)); }
     {
         PHASE(AFQMC_PH_LU);
-        launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, make_double2(0, 0),
-                                 e->logwT, e->logov, e->alive, e->surv, e->logw, nullptr, e->status,
-                                 LU_PROJECT, needTheta, s);
+        launch_lu_logdet_inverse32(W, e->bl, e->S, e->Sinv, m->Sinv32, e->alive, e->logw, make_double2(0, 0),
+                                   e->logwT, e->logov, e->alive, e->surv, e->logw, nullptr, e->status,
+                                   LU_PROJECT, needTheta, s);
         MTRY(engine_check_launch());
     }
     if (needTheta) {
@@ -911,9 +915,9 @@ int mixed_add_measurement(afqmc_engine *e)
         if (!r) r = onebody_tf32_launch(s, e->n, e->ncol, W, m->E1h, m->E1l, m->sh, m->sl, m->tmp32, nullptr, m->err);
         if (r) return engine_fail(AFQMC_ERR_CUDA, "measurement one-body: " + std::to_string(r));
         MTRY(overlap32(e, m->tmp32, e->alive));
-        launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, engine_one_body_logw(e, 1),
-                                 e->logwT, e->logov, e->alive, nullptr, nullptr, nullptr,
-                                 e->status, LU_PLAIN, true, s);
+        launch_lu_logdet_inverse32(W, e->bl, e->S, e->Sinv, m->Sinv32, e->alive, e->logw,
+                                   engine_one_body_logw(e, 1), e->logwT, e->logov, e->alive, nullptr, nullptr,
+                                   nullptr, e->status, LU_PLAIN, true, s);
         MTRY(engine_check_launch());
         MTRY(theta32(e, m->tmp32, e->alive, e->thetaT));
         MTRY(force_tc(e));

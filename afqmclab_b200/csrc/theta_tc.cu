@@ -1,22 +1,28 @@
-// theta_b = phi_b S_b^{-1} (n x Ns per walker and spin block) on the tcgen05
+// theta_b = phi S_b^{-1} (n x Ns_b per walker and spin block) on the tcgen05
 // tensor cores (kind::tf32, fp32 accumulation), from the fp32 planar walkers
-// and the FP64 inverse overlaps.  The walker tile arrives by TMA with the
-// sites contiguous and is rewritten in shared memory as a K-major operand
-// (128-byte swizzle); S^{-1} is the K-major B operand:
+// and the inverse overlaps (fp32 planes written by the LU).  The spin blocks
+// share the walker (SD2is: both use its leading columns), so one walker
+// operand serves both: the walker tile arrives by TMA with the sites
+// contiguous and is rewritten in shared memory as a K-major operand P
+// (row = site, 128-byte swizzle), and the operand X stacks the blocks'
+// S^{-1} rows (block, column a, re/im):
 //   theta_re = phi_re S_re - phi_im S_im,  theta_im = phi_re S_im + phi_im S_re
-// as one real product over K = (re part, im part) x electrons, N = (re, im)
-// output columns.  The walker values are rounded to tf32 when they are
-// rewritten; with `comp` = 3 both operands are split into tf32 high and low
-// parts (A in shared memory, B when it is built) and
-// A_hi B_hi + A_lo B_hi + A_hi B_lo is accumulated (about 22 significant
-// bits), for the measurement; the force uses a single product.
-// Replaces the zgetrs('T') solve of SDSDOperation.cpp:166-173 /
+// as one real product X P^T over K = (re part, im part) x electrons.  Both
+// operands are split into tf32 high and low parts and
+// X_hi P_hi + X_lo P_hi + X_hi P_lo is accumulated (about 22 significant
+// bits).  Replaces the zgetrs('T') solve of SDSDOperation.cpp:166-173 /
 // SD2sSD2isOperation.cpp:187-198 in the mixed-precision form.
 //
-// Persistent CTAs, one walker at a time, two pipeline items per walker (the
-// re and im halves of K):
-//   warp 0 lane 0 : TMA producer        warp 1     : TMEM owner, UMMA issuer
-//   warps 2..5    : rewrite of A (K-major, hi/lo)   warps 6..9 : epilogue (double-buffered TMEM)
+// Persistent CTAs, one walker at a time, two items per walker (the re and im
+// halves of K).  Three rings keep the loads ahead of the work: raw walker
+// chunks (TMA, per item), the walker's inverse slot (bulk copy, per walker)
+// and the split operands (per item).
+//   warp 0 lane 0 : producer (TMA walker chunks, bulk copy of the inverses)
+//   warp 1        : TMEM owner, UMMA issuer
+//   warps 2..5    : rewrite of P (K-major, hi/lo) and build of X (hi/lo)
+//   warps 6..9    : epilogue (double-buffered TMEM): TMEM lane = output
+//                   column, so each thread writes its column over the sites
+//                   with 16-byte stores
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -31,47 +37,89 @@ extern std::atomic<long long> g_launch_count;
 
 namespace {
 
-constexpr int BK = 32;
 constexpr int NT = 320;
+constexpr int MAX_RS = 4, MAX_XS = 2, MAX_OS = 2;
+constexpr size_t SMEM_CAP = 227 * 1024;
 
 struct ThArgs {
-    int n, Ns, Nsp, W, nchunk, nkb, comp, stages;
-    uint32_t rawBytes, aBytes, bBytes, stageBytes, idesc;
-    __nv_bfloat16 *Theta;  // + w * thetaStride + tOff, planes Ktot apart
-    long long thetaStride, plane, tOff;
-    zd *thetaZ;            // optional FP64 copy, + w * zStride + tOff
+    int n, Nsp, W, nchunk, nkb, nb;
+    int RS, XS, OS;
+    int Ns[2];
+    long long sOff[2], tOff[2];
+    uint32_t rawBytes, xBytes, opBytes, idesc;
+    const float *Sinv32;   // fp32 planes [re | im] of S_b^{-1} at + w s32 + 2 sOff[b]
+    long long s32;
+    const int *mask;
+    __nv_bfloat16 *Theta;  // + w * thetaStride + tOff[b], planes `plane` apart
+    long long thetaStride, plane;
+    zd *thetaZ;            // optional FP64 copy, + w * zStride + tOff[b]
     long long zStride;
     int *err;
 };
 
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// element (row, k) of a K-major, 128-byte-swizzled fp32 operand of 128 rows
+__device__ __forceinline__ uint32_t sw_off(int row, int k)
+{
+    return (uint32_t)((k >> 5) * 128 * 128 + row * 128 + ((((k & 31) >> 2) ^ (row & 7)) << 4) + (k & 3) * 4);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+    return *(const uint32_t *)&h;
+}
+
+// four fp32 values as tf32 high parts and tf32-rounded remainders (16-byte stores)
+__device__ __forceinline__ void store_split(uint8_t *hi, uint8_t *lo, uint32_t off, const float *v)
+{
+    float4 h, l;
+    h.x = tf32_round(v[0]); l.x = tf32_round(v[0] - h.x);
+    h.y = tf32_round(v[1]); l.y = tf32_round(v[1] - h.y);
+    h.z = tf32_round(v[2]); l.z = tf32_round(v[2] - h.z);
+    h.w = tf32_round(v[3]); l.w = tf32_round(v[3] - h.w);
+    *(float4 *)(hi + off) = h;
+    *(float4 *)(lo + off) = l;
+}
+
 __global__ void __launch_bounds__(NT, 1)
-theta_tc_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tBh,
-                const __grid_constant__ CUtensorMap tBl, ThArgs p)
+theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    // stage: [raw A | A hi | A lo | B hi | B lo]
-    uint64_t *full = (uint64_t *)(base + (size_t)p.stages * p.stageBytes);
-    uint64_t *split = full + p.stages;
-    uint64_t *empty = split + p.stages;
-    uint64_t *tfull = empty + p.stages;   // 2
+    // [OS operand stages: P hi | P lo | X hi | X lo][RS raw chunks][XS inverse slots][barriers]
+    uint8_t *ops = base;
+    uint8_t *raws = ops + (size_t)p.OS * p.opBytes;
+    uint8_t *xsl = raws + (size_t)p.RS * p.rawBytes;
+    uint64_t *rawFull = (uint64_t *)(xsl + (size_t)p.XS * p.xBytes);
+    uint64_t *rawEmpty = rawFull + MAX_RS;
+    uint64_t *xFull = rawEmpty + MAX_RS;
+    uint64_t *xEmpty = xFull + MAX_XS;
+    uint64_t *opFull = xEmpty + MAX_XS;
+    uint64_t *opEmpty = opFull + MAX_OS;
+    uint64_t *tfull = opEmpty + MAX_OS;   // 2
     uint64_t *tempty = tfull + 2;         // 2
     uint32_t *tmemSlot = (uint32_t *)(tempty + 2);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int nw = (p.W - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x;   // walkers of this CTA
     const int items = 2 * nw;
+    const uint32_t pBytes = (uint32_t)p.nkb * 128 * 128;   // one of P hi, P lo, X hi, X lo
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < p.stages; ++s) {
-            mbar_init(&full[s], 1);
-            mbar_init(&split[s], 128);
-            mbar_init(&empty[s], 1);
-        }
+        for (int s = 0; s < p.RS; ++s) { mbar_init(&rawFull[s], 1); mbar_init(&rawEmpty[s], 128); }
+        for (int s = 0; s < p.XS; ++s) { mbar_init(&xFull[s], 1); mbar_init(&xEmpty[s], 128); }
+        for (int s = 0; s < p.OS; ++s) { mbar_init(&opFull[s], 128); mbar_init(&opEmpty[s], 1); }
         for (int b = 0; b < 2; ++b) { mbar_init(&tfull[b], 1); mbar_init(&tempty[b], 128); }
         fence_mbar_init();
         tma_prefetch_desc(&tA);
-        tma_prefetch_desc(&tBh);
     }
     if (warp == 1) { tmem_alloc(tmemSlot, 256); tmem_relinquish(); }
     tc_fence_before();
@@ -82,94 +130,126 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
 
     if (warp == 0) {
         if (lane == 0) {
-            for (int it = 0; it < items && ok; ++it) {
-                const int s = it % p.stages;
-                if (it >= p.stages) ok = mbar_wait(&empty[s], ((it / p.stages) - 1) & 1);
+            for (int lw = 0; lw < nw && ok; ++lw) {
+                const int w = (int)blockIdx.x + lw * (int)gridDim.x;
+                const int xs = lw % p.XS;
+                if (lw >= p.XS) ok = mbar_wait(&xEmpty[xs], ((lw / p.XS) - 1) & 1);
                 if (!ok) break;
-                const int w = (int)blockIdx.x + (it >> 1) * (int)gridDim.x, part = it & 1;
-                uint8_t *st = base + (size_t)s * p.stageBytes;
-                mbar_arrive_expect_tx(&full[s], p.rawBytes + (p.comp == 3 ? 2u : 1u) * p.bBytes);
-                for (int c = 0; c < p.nchunk; ++c)
-                    tma_load_3d(st + c * p.Nsp * 128, &tA, &full[s], c * 32, 0, 2 * w + part);
-                uint8_t *bh = st + p.rawBytes + 2 * p.aBytes;
-                for (int kb = 0; kb < p.nkb; ++kb) {
-                    tma_load_2d(bh + kb * 2 * p.Nsp * 128, &tBh, &full[s], part * p.Nsp + kb * BK, w * 2 * p.Nsp);
-                    if (p.comp == 3)
-                        tma_load_2d(bh + p.bBytes + kb * 2 * p.Nsp * 128, &tBl, &full[s], part * p.Nsp + kb * BK,
-                                    w * 2 * p.Nsp);
+                mbar_arrive_expect_tx(&xFull[xs], p.xBytes);
+                bulk_load(xsl + (size_t)xs * p.xBytes, p.Sinv32 + (size_t)w * p.s32, p.xBytes, &xFull[xs]);
+                for (int part = 0; part < 2 && ok; ++part) {
+                    const int it = 2 * lw + part, rs = it % p.RS;
+                    if (it >= p.RS) ok = mbar_wait(&rawEmpty[rs], ((it / p.RS) - 1) & 1);
+                    if (!ok) break;
+                    uint8_t *dst = raws + (size_t)rs * p.rawBytes;
+                    mbar_arrive_expect_tx(&rawFull[rs], p.rawBytes);
+                    for (int c = 0; c < p.nchunk; ++c)
+                        tma_load_3d(dst + c * p.Nsp * 128, &tA, &rawFull[rs], c * 32, 0, 2 * w + part);
                 }
-            }
-            for (int it = max(items, p.stages); it < items + p.stages && ok; ++it) {
-                const int s = it % p.stages;
-                ok = mbar_wait(&empty[s], ((it / p.stages) - 1) & 1);
             }
         }
     } else if (warp == 1) {
         if (lane == 0) {
             for (int it = 0; it < items && ok; ++it) {
-                const int s = it % p.stages, lw = it >> 1, part = it & 1, buf = lw & 1;
+                const int os = it % p.OS, lw = it >> 1, part = it & 1, buf = lw & 1;
                 if (part == 0 && lw >= 2) {
                     ok = mbar_wait(&tempty[buf], ((lw >> 1) - 1) & 1);
                     if (!ok) break;
                 }
-                ok = mbar_wait(&split[s], (it / p.stages) & 1);
+                ok = mbar_wait(&opFull[os], (it / p.OS) & 1);
                 if (!ok) break;
                 tc_fence_after();
-                const uint32_t st = smem_u32(base + (size_t)s * p.stageBytes);
-                const uint32_t ah = st + p.rawBytes, al = ah + p.aBytes, bh = al + p.aBytes, bl = bh + p.bBytes;
+                const uint32_t st = smem_u32(ops + (size_t)os * p.opBytes);
+                const uint32_t ph = st, pl = st + pBytes, xh = st + 2 * pBytes, xl = st + 3 * pBytes;
                 const uint32_t d = tmem + (uint32_t)(buf * 128);
                 for (int kk = 0; kk < p.Nsp / 8; ++kk) {
-                    const uint32_t aoff = (uint32_t)((kk >> 2) * 128 * 128 + (kk & 3) * 32);
-                    const uint32_t boff = (uint32_t)((kk >> 2) * 2 * p.Nsp * 128 + (kk & 3) * 32);
+                    // D (rows = block, column, re/im; columns = sites) = X P^T
+                    const uint32_t off = (uint32_t)((kk >> 2) * 128 * 128 + (kk & 3) * 32);
                     const uint32_t acc0 = (part > 0 || kk > 0) ? 1u : 0u;
-                    umma_tf32(d, desc_k_sw128(ah + aoff), desc_k_sw128(bh + boff), p.idesc, acc0);
-                    if (p.comp == 3) {
-                        umma_tf32(d, desc_k_sw128(al + aoff), desc_k_sw128(bh + boff), p.idesc, 1u);
-                        umma_tf32(d, desc_k_sw128(ah + aoff), desc_k_sw128(bl + boff), p.idesc, 1u);
-                    }
+                    umma_tf32(d, desc_k_sw128(xh + off), desc_k_sw128(ph + off), p.idesc, acc0);
+                    umma_tf32(d, desc_k_sw128(xl + off), desc_k_sw128(ph + off), p.idesc, 1u);
+                    umma_tf32(d, desc_k_sw128(xh + off), desc_k_sw128(pl + off), p.idesc, 1u);
                 }
-                umma_commit(&empty[s]);
+                umma_commit(&opEmpty[os]);
                 if (part == 1) umma_commit(&tfull[buf]);
             }
         }
         __syncwarp();
     } else if (warp < 6) {
-        // rewrite the raw tile (Nsp rows of 32 sites per 32-site chunk) as a
-        // K-major, 128-byte-swizzled operand: row = site, 16-byte chunk
-        // (k % 32) / 4 stored at chunk ^ (site % 8) of the 128-byte row
         const int t = threadIdx.x - 64;
-        const int units = 128 * (p.Nsp / 4);
+        const int Nsp = p.Nsp, G4 = Nsp / 4;
+        const int units = 128 * G4;
+        const int tasks = p.nb * Nsp * G4;   // (block, column a, group of 4 electrons c)
         for (int it = 0; it < items && ok; ++it) {
-            const int s = it % p.stages;
-            ok = mbar_wait(&full[s], (it / p.stages) & 1);
+            const int lw = it >> 1, part = it & 1;
+            const int w = (int)blockIdx.x + lw * (int)gridDim.x;
+            const int rs = it % p.RS, os = it % p.OS, xs = lw % p.XS;
+            const bool on = p.mask == nullptr || p.mask[w] != 0;
+            ok = mbar_wait(&rawFull[rs], (it / p.RS) & 1);
+            if (ok && it >= p.OS) ok = mbar_wait(&opEmpty[os], ((it / p.OS) - 1) & 1);
+            if (ok) ok = mbar_wait(&xFull[xs], (lw / p.XS) & 1);
             if (!ok) break;
-            const uint8_t *raw = base + (size_t)s * p.stageBytes;
-            uint8_t *ah = base + (size_t)s * p.stageBytes + p.rawBytes;
-            uint8_t *al = ah + p.aBytes;
+            const uint8_t *raw = raws + (size_t)rs * p.rawBytes;
+            const float *xsrc = (const float *)(xsl + (size_t)xs * p.xBytes);
+            uint8_t *ph = ops + (size_t)os * p.opBytes;
+            uint8_t *pl = ph + pBytes, *xh = ph + 2 * pBytes, *xl = ph + 3 * pBytes;
+            // P: the raw chunks (Nsp rows of 32 sites each) as K-major rows
+            // (row = site), split into hi and lo
             for (int u = t; u < units; u += 128) {
                 const int i = u & 127, k4 = u >> 7;
                 float x[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
-                    x[j] = i < p.n ? *(const float *)(raw + (i >> 5) * p.Nsp * 128 + (4 * k4 + j) * 128 + (i & 31) * 4)
+                    x[j] = i < p.n ? *(const float *)(raw + (i >> 5) * Nsp * 128 + (4 * k4 + j) * 128 + (i & 31) * 4)
                                    : 0.f;
                 float4 h, l;
                 h.x = tf32_round(x[0]); l.x = x[0] - h.x;
                 h.y = tf32_round(x[1]); l.y = x[1] - h.y;
                 h.z = tf32_round(x[2]); l.z = x[2] - h.z;
                 h.w = tf32_round(x[3]); l.w = x[3] - h.w;
-                const int kb = k4 >> 3, c16 = (k4 & 7) ^ (i & 7);
-                const size_t off = (size_t)kb * 128 * 128 + (size_t)i * 128 + c16 * 16;
-                *(float4 *)(ah + off) = h;
-                if (p.comp == 3) *(float4 *)(al + off) = l;
+                const uint32_t off = sw_off(i, 4 * k4);
+                *(float4 *)(ph + off) = h;
+                *(float4 *)(pl + off) = l;
             }
+            mbar_arrive(&rawEmpty[rs]);
+            // X: rows 2 Nsp b + 2 a (theta_re) and 2 Nsp b + 2 a + 1 (theta_im);
+            // K = electron c of this item's part:
+            //   re part: [S_re(c, a) ; S_im(c, a)],  im part: [-S_im(c, a) ; S_re(c, a)]
+            for (int q = t; q < tasks; q += 128) {
+                const int g = q % G4, a = (q / G4) % Nsp, b = q / (G4 * Nsp);
+                const int Ns = b ? p.Ns[1] : p.Ns[0];
+                const long long so = 2 * (b ? p.sOff[1] : p.sOff[0]);
+                float xr[4] = {0.f, 0.f, 0.f, 0.f}, xi[4] = {0.f, 0.f, 0.f, 0.f};
+                if (on && a < Ns) {
+                    const float *Xr = xsrc + so + (size_t)Ns * a, *Xi = Xr + (size_t)Ns * Ns;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (4 * g + j < Ns) { xr[j] = Xr[4 * g + j]; xi[j] = Xi[4 * g + j]; }
+                }
+                float vre[4], vim[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    vre[j] = part ? -xi[j] : xr[j];
+                    vim[j] = part ? xr[j] : xi[j];
+                }
+                const int rRe = 2 * Nsp * b + 2 * a;
+                store_split(xh, xl, sw_off(rRe, 4 * g), vre);
+                store_split(xh, xl, sw_off(rRe + 1, 4 * g), vim);
+            }
+            if (part == 1) mbar_arrive(&xEmpty[xs]);
             fence_proxy_async();
-            mbar_arrive(&split[s]);
+            mbar_arrive(&opFull[os]);
         }
     } else {
+        // lane r of the accumulator = (block b, column a, re/im): theta_b(:, a)
+        // of one part over the sites, contiguous in Theta and thetaZ
         const int q = warp & 3;
-        const int row = q * 32 + lane;
-        const int Ns = p.Ns, Nsp = p.Nsp, n = p.n;
+        const int r = q * 32 + lane;
+        const int Nsp = p.Nsp, n = p.n;
+        const int b = r / (2 * Nsp), rr = r - b * 2 * Nsp, a = rr >> 1, im = rr & 1;
+        const int Ns = b == 0 ? p.Ns[0] : (b == 1 ? p.Ns[1] : 0);
+        const bool valid = b < p.nb && a < Ns;
+        const long long tOff = b ? p.tOff[1] : p.tOff[0];
         for (int lw = 0; lw < nw && ok; ++lw) {
             const int buf = lw & 1;
             ok = mbar_wait(&tfull[buf], (lw >> 1) & 1);
@@ -177,22 +257,31 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
             tc_fence_after();
             const int w = (int)blockIdx.x + lw * (int)gridDim.x;
             const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 128);
-            __nv_bfloat16 *th = p.Theta + (size_t)w * p.thetaStride + p.tOff;
-            zd *tz = p.thetaZ ? p.thetaZ + (size_t)w * p.zStride + p.tOff : nullptr;
-            double *tzd = (double *)tz;
-            for (int c0 = 0; c0 < 2 * Nsp; c0 += 32) {
+            __nv_bfloat16 *th = p.Theta + (size_t)w * p.thetaStride + tOff + (size_t)im * p.plane + (size_t)n * a;
+            double2 *tz = p.thetaZ ? (double2 *)(p.thetaZ + (size_t)w * p.zStride + tOff + (size_t)n * a) : nullptr;
+            for (int c0 = 0; c0 < n; c0 += 32) {
                 float v[32];
                 tmem_ld32(trow + (uint32_t)c0, v);
-                if (row < n) {
+                if (valid) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int col = c0 + j;
-                        const int im = col >= Nsp ? 1 : 0;
-                        const int a = col - im * Nsp;
-                        if (a < Ns) {
-                            const size_t o = (size_t)row + (size_t)n * a;
-                            th[o + im * p.plane] = __float2bfloat16_rn(v[j]);
-                            if (tzd) tzd[2 * o + im] = (double)v[j];
+                    for (int j = 0; j < 32; j += 8) {
+                        uint4 pk;
+                        pk.x = pack_bf16x2(v[j], v[j + 1]);
+                        pk.y = pack_bf16x2(v[j + 2], v[j + 3]);
+                        pk.z = pack_bf16x2(v[j + 4], v[j + 5]);
+                        pk.w = pack_bf16x2(v[j + 6], v[j + 7]);
+                        *(uint4 *)(th + c0 + j) = pk;
+                    }
+                }
+                if (tz) {
+                    // the re lane keeps sites c0..c0+15, the im lane c0+16..c0+31
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) {
+                        const float send = im ? v[j] : v[16 + j];
+                        const float recv = __shfl_xor_sync(0xffffffffu, send, 1);
+                        if (valid) {
+                            if (im) tz[c0 + 16 + j] = make_double2((double)recv, (double)v[16 + j]);
+                            else tz[c0 + j] = make_double2((double)v[j], (double)recv);
                         }
                     }
                 }
@@ -206,34 +295,6 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ 
     __syncthreads();
     tc_fence_after();
     if (warp == 1) tmem_dealloc(tmem, 256);
-}
-
-// B rows of walker w (K-major, 2 Nsp values each): row a (< Nsp): [Re S(b, a) | -Im S(b, a)],
-// row Nsp + a: [Im S(b, a) | Re S(b, a)], b over Nsp (zero beyond Ns); hi and
-// (with comp = 3) lo tf32 parts.  Walkers outside `mask` get zeros.
-__global__ void build_b_kernel(int W, int Ns, int Nsp, const zd *Sinv, long long sStride, long long sOff,
-                               const int *mask, int comp, float *Bh, float *Bl)
-{
-    const int w = blockIdx.x;
-    const bool on = mask == nullptr || mask[w] != 0;
-    const int K2 = 2 * Nsp;
-    float *bh = Bh + (size_t)w * K2 * K2;
-    float *bl = comp == 3 ? Bl + (size_t)w * K2 * K2 : nullptr;
-    const zd *S = Sinv + (size_t)w * sStride + sOff;
-    for (int e = threadIdx.x; e < Nsp * Nsp; e += blockDim.x) {
-        const int b = e % Nsp, a = e / Nsp;
-        zd v = make_double2(0.0, 0.0);
-        if (on && a < Ns && b < Ns) v = S[b + (size_t)Ns * a];
-        const double vals[4] = {v.x, -v.y, v.y, v.x};
-        const size_t idx[4] = {(size_t)a * K2 + b, (size_t)a * K2 + Nsp + b, (size_t)(Nsp + a) * K2 + b,
-                               (size_t)(Nsp + a) * K2 + Nsp + b};
-#pragma unroll
-        for (int t = 0; t < 4; ++t) {
-            const float h = tf32_round((float)vals[t]);
-            bh[idx[t]] = h;
-            if (bl) bl[idx[t]] = tf32_round((float)(vals[t] - (double)h));
-        }
-    }
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encoder()
@@ -252,7 +313,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder()
 }
 
 int map_f32(CUtensorMap *map, const float *ptr, int rank, const cuuint64_t *dims, const cuuint64_t *pitch,
-            const cuuint32_t *box, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B)
+            const cuuint32_t *box, CUtensorMapSwizzle swz)
 {
     auto enc = encoder();
     if (!enc) return (int)cudaErrorNotSupported;
@@ -266,57 +327,79 @@ int map_f32(CUtensorMap *map, const float *ptr, int rank, const cuuint64_t *dims
     return r == CUDA_SUCCESS ? 0 : (int)r + 10000;
 }
 
-}  // namespace
+struct Plan {
+    int Nsp, nkb, nchunk, RS, XS, OS;
+    uint32_t rawBytes, xBytes, opBytes;
+    size_t smem;
+};
 
-bool theta_tc_supported(int n, int Ns) { return (n == 64 || n == 128) && Ns >= 1 && Ns <= 64; }
-
-size_t theta_tc_bscratch(int W, int Ns)
+// ring depths: the deepest (operand stages, raw chunks, inverse slots) that fits
+bool make_plan(int n, int nb, const int *Ns, long long s32, Plan &pl)
 {
-    const int Nsp = (Ns + 15) / 16 * 16;
-    return (size_t)W * 4 * Nsp * Nsp;
+    if ((n != 64 && n != 128) || nb < 1 || nb > 2 || s32 <= 0 || (s32 & 3)) return false;
+    int maxNs = 0;
+    for (int b = 0; b < nb; ++b) {
+        if (Ns[b] < 1 || Ns[b] > 64) return false;
+        maxNs = std::max(maxNs, Ns[b]);
+    }
+    pl.Nsp = (maxNs + 15) / 16 * 16;
+    if (2 * nb * pl.Nsp > 128) return false;
+    pl.nkb = (pl.Nsp + 31) / 32;
+    pl.nchunk = n / 32;
+    pl.rawBytes = (uint32_t)(pl.nchunk * pl.Nsp * 128);
+    pl.xBytes = (uint32_t)(s32 * 4);
+    pl.opBytes = (uint32_t)(4 * pl.nkb * 128 * 128);
+    const int tries[][3] = {{2, 4, 2}, {2, 3, 2}, {2, 2, 2}, {2, 2, 1}, {1, 4, 2}, {1, 2, 2}, {1, 2, 1}, {1, 1, 1}};
+    for (const auto &t : tries) {
+        const size_t smem = 1024 + (size_t)t[0] * pl.opBytes + (size_t)t[1] * pl.rawBytes + (size_t)t[2] * pl.xBytes + 256;
+        if (smem <= SMEM_CAP) {
+            pl.OS = t[0]; pl.RS = t[1]; pl.XS = t[2]; pl.smem = smem;
+            return true;
+        }
+    }
+    return false;
 }
 
-int theta_tc_launch(cudaStream_t s, int n, int ncol, int Ns, int W, const float *w32, const zd *Sinv,
-                    long long sStride, long long sOff, const int *mask, int comp, float *Bh, float *Bl,
-                    __nv_bfloat16 *Theta, long long thetaStride, long long plane, long long tOff, zd *thetaZ,
-                    long long zStride, int *err)
-{
-    if (!theta_tc_supported(n, Ns) || (comp != 1 && comp != 3)) return (int)cudaErrorInvalidValue;
-    const int Nsp = (Ns + 15) / 16 * 16;
-    g_launch_count++;
-    build_b_kernel<<<W, 256, 0, s>>>(W, Ns, Nsp, Sinv, sStride, sOff, mask, comp, Bh, Bl);
-    cudaError_t ce = cudaGetLastError();
-    if (ce != cudaSuccess) return (int)ce;
+}  // namespace
 
+bool theta_tc_supported(int n, int nb, const int *Ns, long long s32)
+{
+    Plan pl;
+    return make_plan(n, nb, Ns, s32, pl);
+}
+
+int theta_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, int W, const float *w32,
+                    const float *Sinv32, long long s32, const long long *sOff, const int *mask,
+                    __nv_bfloat16 *Theta, long long thetaStride, long long plane, const long long *tOff,
+                    zd *thetaZ, long long zStride, int *err)
+{
+    Plan pl;
+    if (!make_plan(n, nb, Ns, s32, pl)) return (int)cudaErrorInvalidValue;
+    if ((uintptr_t)Sinv32 & 15) return (int)cudaErrorMisalignedAddress;
     ThArgs a{};
-    a.n = n; a.Ns = Ns; a.Nsp = Nsp; a.W = W; a.comp = comp;
-    a.nchunk = n / 32;
-    a.nkb = (Nsp + BK - 1) / BK;
-    a.rawBytes = (uint32_t)(a.nchunk * Nsp * 128);
-    a.aBytes = (uint32_t)(a.nkb * 128 * 128);
-    a.bBytes = (uint32_t)(a.nkb * 2 * Nsp * 128);
-    a.stageBytes = a.rawBytes + 2 * a.aBytes + 2 * a.bBytes;
-    const size_t budget = 200 * 1024;
-    a.stages = (int)std::max<size_t>(1, std::min<size_t>(4, budget / a.stageBytes));
-    a.idesc = idesc_tf32(128, 2 * Nsp);
-    a.Theta = Theta; a.thetaStride = thetaStride; a.plane = plane; a.tOff = tOff;
+    a.n = n; a.Nsp = pl.Nsp; a.W = W; a.nb = nb;
+    a.nchunk = pl.nchunk; a.nkb = pl.nkb;
+    a.RS = pl.RS; a.XS = pl.XS; a.OS = pl.OS;
+    for (int b = 0; b < 2; ++b) {
+        a.Ns[b] = b < nb ? Ns[b] : 0;
+        a.sOff[b] = b < nb ? sOff[b] : 0;
+        a.tOff[b] = b < nb ? tOff[b] : 0;
+    }
+    a.rawBytes = pl.rawBytes; a.xBytes = pl.xBytes; a.opBytes = pl.opBytes;
+    a.idesc = idesc_tf32(128, 128);
+    a.Sinv32 = Sinv32; a.s32 = s32; a.mask = mask;
+    a.Theta = Theta; a.thetaStride = thetaStride; a.plane = plane;
     a.thetaZ = thetaZ; a.zStride = zStride; a.err = err;
 
-    CUtensorMap mA, mBh, mBl;
+    CUtensorMap mA;
     cuuint64_t dA[3] = {(cuuint64_t)n, (cuuint64_t)ncol, (cuuint64_t)2 * W};
     cuuint64_t pA[2] = {(cuuint64_t)n * 4, (cuuint64_t)n * ncol * 4};
-    cuuint32_t bA[3] = {32u, (cuuint32_t)Nsp, 1u};
+    cuuint32_t bA[3] = {32u, (cuuint32_t)pl.Nsp, 1u};
     int r = map_f32(&mA, w32, 3, dA, pA, bA, CU_TENSOR_MAP_SWIZZLE_NONE);
-    cuuint64_t dB[2] = {(cuuint64_t)2 * Nsp, (cuuint64_t)2 * Nsp * W};
-    cuuint64_t pB[1] = {(cuuint64_t)2 * Nsp * 4};
-    cuuint32_t bB[2] = {(cuuint32_t)BK, (cuuint32_t)(2 * Nsp)};
-    if (!r) r = map_f32(&mBh, Bh, 2, dB, pB, bB);
-    if (!r) r = map_f32(&mBl, comp == 3 ? Bl : Bh, 2, dB, pB, bB);
     if (r) return r;
-    const size_t smem = 1024 + (size_t)a.stages * a.stageBytes + 256;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(theta_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        cudaFuncSetAttribute(theta_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
         attr = true;
     }
     int dev = 0, sms = 148;
@@ -324,6 +407,6 @@ int theta_tc_launch(cudaStream_t s, int n, int ncol, int Ns, int W, const float 
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = std::min(W, sms);
     g_launch_count++;
-    theta_tc_kernel<<<grid, NT, smem, s>>>(mA, mBh, mBl, a);
+    theta_tc_kernel<<<grid, NT, pl.smem, s>>>(mA, a);
     return (int)cudaGetLastError();
 }

@@ -597,10 +597,21 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
 // ---------------------------------------------------------------------------
 constexpr int GR_WARPS = 4;
 
+// 1 / b by Smith's scaling (one ratio, one reciprocal)
+__device__ __forceinline__ zd zrcp(zd b)
+{
+    if (fabs(b.y) <= fabs(b.x)) {
+        const double r = b.y / b.x, d = 1.0 / (b.x + b.y * r);
+        return make_double2(d, -r * d);
+    }
+    const double r = b.x / b.y, d = 1.0 / (b.y + b.x * r);
+    return make_double2(r * d, -d);
+}
+
 __global__ void __launch_bounds__(GR_WARPS * 32, 3)
-gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const zd *logw,
-              zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut, double *weight,
-              int *status, int mode, int wantInverse)
+gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
+              const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
+              double *weight, int *status, int mode, int wantInverse)
 {
     __shared__ __align__(16) zd prow[GR_WARPS][2][32];
     __shared__ int pvS[GR_WARPS][32];
@@ -616,7 +627,7 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const 
     const bool act = inW && ((active == nullptr) || active[w] != 0);
     const int Ns = b == 0 ? bl.Ns[0] : bl.Ns[1];
     const long long sOff = b == 0 ? bl.sOff[0] : bl.sOff[1];
-    const bool inv = wantInverse && Sinv;
+    const bool inv = wantInverse && (Sinv || Sinv32);
     bool sing = false;
     zd ld = make_double2(0.0, 0.0);
     if (act && Ns > 0) {
@@ -654,7 +665,7 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const 
             if (isP) pos = k;
             const bool z = zeq0(piv);
             sing = sing || z;
-            const zd q = z ? make_double2(0.0, 0.0) : zdiv(make_double2(1.0, 0.0), piv);
+            const zd q = z ? make_double2(0.0, 0.0) : zrcp(piv);
             const zd f = isP ? make_double2(0.0, 0.0) : zmul(a[0], q);
             const zd nk = isP ? make_double2(1.0, 0.0) : zneg(f);
 #pragma unroll
@@ -699,9 +710,21 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const 
                 for (int c = 0; c < Ns; ++c) pv[ix[c]] = c;
             }
             __syncwarp();
-            zd *Xg = Sinv + (size_t)w * bl.sStride + sOff;
-            const zd sc = sing ? make_double2(0.0, 0.0) : zdiv(make_double2(1.0, 0.0), myD);
-            if (pos < Ns) {
+            const zd sc = sing ? make_double2(0.0, 0.0) : zrcp(myD);
+            if (pos < Ns && Sinv32) {
+                // fp32 planes [re | im], each Ns x Ns column-major
+                float *Xr = Sinv32 + (size_t)w * s32 + 2 * sOff, *Xi = Xr + (size_t)Ns * Ns;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int c = pvS[warp][j];
+                    if (j < Ns && c >= 0 && c < Ns) {
+                        const zd v = zmul(sc, a[j]);
+                        Xr[pos + (size_t)Ns * c] = (float)v.x;
+                        Xi[pos + (size_t)Ns * c] = (float)v.y;
+                    }
+                }
+            } else if (pos < Ns) {
+                zd *Xg = Sinv + (size_t)w * bl.sStride + sOff;
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int c = pvS[warp][j];
@@ -1512,24 +1535,71 @@ measure_reduce_kernel(int W, const int *alive, const zd *eloc, const zd *den, co
     }
 }
 
+// FP64 inverses -> fp32 planes [re | im] (each Ns x Ns column-major), for the
+// LU kernels that write FP64 only
+__global__ void sinv_to_f32_kernel(int W, Blocks bl, const zd *Sinv, float *Sinv32, long long s32)
+{
+    const int w = blockIdx.x;
+    for (int b = 0; b < bl.nblk; ++b) {
+        const int Ns = b == 0 ? bl.Ns[0] : bl.Ns[1];
+        const long long sOff = b == 0 ? bl.sOff[0] : bl.sOff[1];
+        const zd *X = Sinv + (size_t)w * bl.sStride + sOff;
+        float *Xr = Sinv32 + (size_t)w * s32 + 2 * sOff, *Xi = Xr + (size_t)Ns * Ns;
+        for (int e = threadIdx.x; e < Ns * Ns; e += blockDim.x) {
+            const zd v = X[e];
+            Xr[e] = (float)v.x;
+            Xi[e] = (float)v.y;
+        }
+    }
+}
+
 }  // namespace
 
 // ============================================================== launchers
+static void launch_lu_fp64(int W, const Blocks &bl, zd *S, zd *Sinv, const int *active, const zd *logw,
+                           zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
+                           double *weight, int *status, int mode, bool wantInverse, cudaStream_t s);
+
 void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const int *active,
                               const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive,
                               int *surv, zd *logwOut, double *weight, int *status, int mode,
                               bool wantInverse, cudaStream_t s)
 {
+    launch_lu_logdet_inverse32(W, bl, S, Sinv, nullptr, active, logw, logwAdd, logwT, logov, alive, surv,
+                               logwOut, weight, status, mode, wantInverse, s);
+}
+
+void launch_lu_logdet_inverse32(int W, const Blocks &bl, zd *S, zd *Sinv, float *Sinv32, const int *active,
+                                const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv,
+                                zd *logwOut, double *weight, int *status, int mode, bool wantInverse,
+                                cudaStream_t s)
+{
+    int maxNs = 0;
+    for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
+    const long long s32 = sinv32_stride(bl);
+    if (maxNs > 16 && maxNs <= 32 && (bl.nblk == 1 || bl.nblk == 2)) {
+        g_launch_count++;
+        const long long mats = (long long)W * bl.nblk;
+        gj_reg_kernel<<<(unsigned)((mats + GR_WARPS - 1) / GR_WARPS), GR_WARPS * 32, 0, s>>>(
+            W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov, alive, surv,
+            logwOut, weight, status, mode, wantInverse ? 1 : 0);
+        return;
+    }
+    launch_lu_fp64(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov, alive, surv, logwOut, weight, status,
+                   mode, wantInverse, s);
+    if (Sinv32 && wantInverse && Sinv) {
+        g_launch_count++;
+        sinv_to_f32_kernel<<<W, 256, 0, s>>>(W, bl, Sinv, Sinv32, s32);
+    }
+}
+
+static void launch_lu_fp64(int W, const Blocks &bl, zd *S, zd *Sinv, const int *active, const zd *logw,
+                           zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
+                           double *weight, int *status, int mode, bool wantInverse, cudaStream_t s)
+{
     g_launch_count++;
     int maxNs = 0;
     for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
-    if (maxNs > 16 && maxNs <= 32 && (bl.nblk == 1 || bl.nblk == 2)) {
-        const long long mats = (long long)W * bl.nblk;
-        gj_reg_kernel<<<(unsigned)((mats + GR_WARPS - 1) / GR_WARPS), GR_WARPS * 32, 0, s>>>(
-            W, bl, S, Sinv, active, logw, logwAdd, logwT, logov, alive, surv, logwOut, weight, status,
-            mode, wantInverse ? 1 : 0);
-        return;
-    }
     if (maxNs <= 32) {
         const size_t smem = (size_t)GJ_WARPS * 32 * GJ_LD * sizeof(zd);
         static bool gattr = false;

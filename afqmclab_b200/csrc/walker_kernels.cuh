@@ -20,6 +20,17 @@ void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const in
                               const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive,
                               int *surv, zd *logwOut, double *weight, int *status, int mode,
                               bool wantInverse, cudaStream_t s);
+// Floats per walker of the fp32 inverse slots: 2 sStride rounded up to a
+// multiple of 4, so every walker's slot starts on a 16-byte boundary.
+inline long long sinv32_stride(const Blocks &bl) { return (2 * bl.sStride + 3) & ~3LL; }
+// Same as launch_lu_logdet_inverse, with the inverses (when wanted) written as
+// fp32 planes [re | im] (each Ns x Ns column-major) at
+// Sinv32 + w * sinv32_stride(bl) + 2 sOff[b]; Sinv is FP64 scratch for the
+// kernels that produce FP64 first.
+void launch_lu_logdet_inverse32(int W, const Blocks &bl, zd *S, zd *Sinv, float *Sinv32, const int *active,
+                                const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv,
+                                zd *logwOut, double *weight, int *status, int mode, bool wantInverse,
+                                cudaStream_t s);
 
 void launch_rng_scan(int W, const int *surv, int draws, unsigned long long *counter,
                      unsigned long long *offs, cudaStream_t s);
