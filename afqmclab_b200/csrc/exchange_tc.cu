@@ -1,7 +1,9 @@
 // Exchange term of the phaseless mixed estimator on the tcgen05 tensor cores
 // (RealMaterialMoleculeMeasureFixedSD2sSD2is::calculateCholeskyEx, :258-284):
 //   D_{g,w} = A_g theta_w  (Ns x Ns, complex),  ex[g, w] += sum_ab D_ab D_ba
-// for one spin block per launch.  As a GEMM: rows (g, a) of A (K = orbital
+// for one spin block per launch.  When every A_g is real (real trial and real
+// Cholesky vectors, the molecular case) the imaginary-A products are skipped:
+// D = A_re theta_re + i A_re theta_im, half the tensor work.  As a GEMM: rows (g, a) of A (K = orbital
 // i), columns (w, b) of theta (K = i), both bf16 K-major; the 128 x 128 output
 // tile holds 128/Ns vectors g times 128/Ns walkers w, and the epilogue reduces
 // each Ns x Ns block to its trace tr(D D) without writing D.
@@ -48,7 +50,7 @@ struct XSmem {
 // 16-byte stores and a column is read without bank conflicts
 __device__ __forceinline__ int tsw(int r, int c) { return r * 32 + ((((c >> 1) ^ (r & 15)) << 1) | (c & 1)); }
 
-template <int NS>
+template <int NS, bool REALA>
 __global__ void __launch_bounds__(XS_THREADS, 1)
 exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_constant__ CUtensorMap tmAi,
                    const __grid_constant__ CUtensorMap tmBr, const __grid_constant__ CUtensorMap tmBi,
@@ -98,10 +100,10 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
                 const int mt = it % MT, ch = it / MT;
                 if (itemCount > 0) ok = mbar_wait(aEmpty, (itemCount - 1) & 1);
                 if (!ok) break;
-                mbar_arrive_expect_tx(aFull, 2 * KB * XS_TILE_BYTES);
+                mbar_arrive_expect_tx(aFull, (REALA ? 1 : 2) * KB * XS_TILE_BYTES);
                 for (int kb = 0; kb < KB; ++kb) {
                     tma_load_2d(sA + (0 * 2 + kb) * XS_TILE_BYTES, &tmAr, aFull, kb * 64, mt * 128);
-                    tma_load_2d(sA + (1 * 2 + kb) * XS_TILE_BYTES, &tmAi, aFull, kb * 64, mt * 128);
+                    if (!REALA) tma_load_2d(sA + (1 * 2 + kb) * XS_TILE_BYTES, &tmAi, aFull, kb * 64, mt * 128);
                 }
                 const int t0 = ch * XS_NCHUNK, t1 = min(NT, t0 + XS_NCHUNK);
                 for (int t = t0; t < t1 && ok; ++t) {
@@ -146,8 +148,10 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
                             const uint64_t dbr = desc_k_sw128(br + kk * 32), dbi = desc_k_sw128(bi + kk * 32);
                             umma_bf16(dR, dar, dbr, ID, acc);
                             umma_bf16(dI, dar, dbi, ID, acc);
-                            umma_bf16(dR, dai, dbi, IDN, 1u);
-                            umma_bf16(dI, dai, dbr, ID, 1u);
+                            if (!REALA) {
+                                umma_bf16(dR, dai, dbi, IDN, 1u);
+                                umma_bf16(dI, dai, dbr, ID, 1u);
+                            }
                         }
                         umma_commit(&empty[stage]);
                         if (++stage == XS_STAGES) { stage = 0; sphase ^= 1; }
@@ -254,17 +258,26 @@ int make_map_theta(CUtensorMap *map, const void *base, int n, int Ns, int W, lon
     return r == CUDA_SUCCESS ? 0 : (int)r + 10000;
 }
 
-template <int NS>
-void launch_ns(int grid, size_t smem, cudaStream_t s, const CUtensorMap &ar, const CUtensorMap &ai,
-               const CUtensorMap &br, const CUtensorMap &bi, int G, int W, int n, const int *alive, zd *ex,
-               int *err)
+template <int NS, bool REALA>
+void launch_ns_a(int grid, size_t smem, cudaStream_t s, const CUtensorMap &ar, const CUtensorMap &ai,
+                 const CUtensorMap &br, const CUtensorMap &bi, int G, int W, int n, const int *alive, zd *ex,
+                 int *err)
 {
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(exchange_tc_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(exchange_tc_kernel<NS, REALA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    exchange_tc_kernel<NS><<<grid, XS_THREADS, smem, s>>>(ar, ai, br, bi, G, W, NS, n, alive, ex, err);
+    exchange_tc_kernel<NS, REALA><<<grid, XS_THREADS, smem, s>>>(ar, ai, br, bi, G, W, NS, n, alive, ex, err);
+}
+
+template <int NS>
+void launch_ns(bool realA, int grid, size_t smem, cudaStream_t s, const CUtensorMap &ar, const CUtensorMap &ai,
+               const CUtensorMap &br, const CUtensorMap &bi, int G, int W, int n, const int *alive, zd *ex,
+               int *err)
+{
+    if (realA) launch_ns_a<NS, true>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err);
+    else launch_ns_a<NS, false>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err);
 }
 
 }  // namespace
@@ -290,7 +303,7 @@ int exchange_tc_supported(int n, int Ns) { return (n == 64 || n == 128) && Ns > 
 // ex (G x W, complex) = exchange of one spin block (every (g, w) written once)
 int exchange_tc_launch(cudaStream_t s, int G, int W, int Ns, int n, const __nv_bfloat16 *A2r,
                        const __nv_bfloat16 *A2i, const __nv_bfloat16 *Theta, long long tOff,
-                       long long Ktot, const int *alive, zd *ex, int *err)
+                       long long Ktot, const int *alive, zd *ex, int *err, bool realA)
 {
     g_launch_count++;
     CUtensorMap ar, ai, br, bi;
@@ -308,12 +321,12 @@ int exchange_tc_launch(cudaStream_t s, int G, int W, int Ns, int n, const __nv_b
     const int items = MT * ((NT + XS_NCHUNK - 1) / XS_NCHUNK);
     const int grid = std::min(items, sms);
     switch (Ns) {
-    case 1: launch_ns<1>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
-    case 2: launch_ns<2>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
-    case 4: launch_ns<4>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
-    case 8: launch_ns<8>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
-    case 16: launch_ns<16>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
-    default: launch_ns<32>(grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 1: launch_ns<1>(realA, grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 2: launch_ns<2>(realA, grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 4: launch_ns<4>(realA, grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 8: launch_ns<8>(realA, grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    case 16: launch_ns<16>(realA, grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
+    default: launch_ns<32>(realA, grid, smem, s, ar, ai, br, bi, G, W, n, alive, ex, err); break;
     }
     return (int)cudaGetLastError();
 }

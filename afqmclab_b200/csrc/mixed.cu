@@ -31,6 +31,7 @@ struct MixedState {
     float *xbarp = nullptr;
     zd *wfDaggerTm = nullptr;
     __nv_bfloat16 *A2r[2] = {nullptr, nullptr}, *A2i[2] = {nullptr, nullptr};
+    bool realA = false;   // every A_g has a zero imaginary part (real trial, real Cholesky vectors)
     zd *ex2 = nullptr;
     float *Ohi[2] = {nullptr, nullptr}, *Olo[2] = {nullptr, nullptr};   // overlap operators
     bool ovStacked = false;   // Ohi[0]/Olo[0] hold both blocks' operators
@@ -660,6 +661,15 @@ int check_err(afqmc_engine *e)
 
 }  // namespace
 
+// flag = 1 when any element of A has a nonzero imaginary part
+__global__ void any_imag_kernel(long long count, const zd *A, int *flag)
+{
+    bool any = false;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count; e += (long long)gridDim.x * blockDim.x)
+        any = any || A[e].y != 0.0;
+    if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
 int mixed_create(afqmc_engine *e)
 {
     if (e->kind == KIND_CP) return cp_mixed_create(e);
@@ -692,6 +702,16 @@ int mixed_create(afqmc_engine *e)
         MTRY(engine_dalloc(e, (unsigned short **)&m->A2i[b], (size_t)G * Ns * n));
         build_a2_kernel<<<1184, 256, 0, e->stream>>>(G, Ns, n, Ktot, e->bl.tOff[b], e->Aall, m->A2r[b],
                                                      m->A2i[b]);
+    }
+    {
+        // exact test on the FP64 half-rotated vectors
+        MTRY(cuda_check(cudaMemsetAsync(m->err, 0, sizeof(int), e->stream), "memset"));
+        any_imag_kernel<<<592, 256, 0, e->stream>>>((long long)G * Ktot, e->Aall, m->err);
+        int h = 1;
+        MTRY(cuda_check(cudaMemcpyAsync(&h, m->err, sizeof(int), cudaMemcpyDeviceToHost, e->stream), "copy"));
+        MTRY(cuda_check(cudaStreamSynchronize(e->stream), "sync"));
+        MTRY(cuda_check(cudaMemsetAsync(m->err, 0, sizeof(int), e->stream), "memset"));
+        m->realA = (h == 0);
     }
     build_abig_kernel<<<1184, 256, 0, e->stream>>>(G, Ktot, n, e->bl, e->Aall, m->Abig);
     build_lt_kernel<<<1184, 256, 0, e->stream>>>((long long)n * n, G, e->chol, m->Lt);
@@ -894,7 +914,7 @@ int mixed_exchange(afqmc_engine *e)
         if (e->bl.Ns[b] == 0) continue;
         zd *out = nb == 0 ? e->ex : m->ex2;
         int r = exchange_tc_launch(e->stream, e->G, e->W, e->bl.Ns[b], e->n, m->A2r[b], m->A2i[b],
-                                   m->Theta, e->bl.tOff[b], e->Ktot, e->alive, out, m->err);
+                                   m->Theta, e->bl.tOff[b], e->Ktot, e->alive, out, m->err, m->realA);
         if (r) return engine_fail(AFQMC_ERR_CUDA, "exchange launch: " + std::to_string(r));
         ++nb;
     }

@@ -26,6 +26,6 @@ int mixed_exchange(afqmc_engine *e);
 int exchange_tc_supported(int n, int Ns);
 int exchange_tc_launch(cudaStream_t s, int G, int W, int Ns, int n, const __nv_bfloat16 *A2r,
                        const __nv_bfloat16 *A2i, const __nv_bfloat16 *Theta, long long tOff,
-                       long long Ktot, const int *alive, zd *ex, int *err);
+                       long long Ktot, const int *alive, zd *ex, int *err, bool realA);
 __global__ void build_a2_kernel(int G, int Ns, int n, long long Ktot, long long tOff, const zd *Aall,
                                 __nv_bfloat16 *A2r, __nv_bfloat16 *A2i);

@@ -56,6 +56,31 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     return true;
 }
 
+// Same as mbar_wait, but each try may suspend the thread for up to `hint_ns`
+// (it resumes early when the phase completes), so a waiting role leaves the
+// issue slots of its scheduler to the warps that share it.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t *bar, uint32_t parity, uint32_t hint_ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t hint_ns = 20000)
+{
+    if (mbar_try_wait_hint(bar, parity, hint_ns)) return true;
+    long long t0 = clock64();
+    while (!mbar_try_wait_hint(bar, parity, hint_ns)) {
+        if (clock64() - t0 > TC_WAIT_LIMIT) return false;
+    }
+    return true;
+}
+
 // 2-D TMA tile load into shared memory, completion counted on `bar`.
 // c0 is the innermost coordinate (elements); it must be 16-byte aligned.
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0,

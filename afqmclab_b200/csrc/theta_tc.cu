@@ -19,8 +19,8 @@
 // and the split operands (per item).
 //   warp 0 lane 0 : producer (TMA walker chunks, bulk copy of the inverses)
 //   warp 1        : TMEM owner, UMMA issuer
-//   warps 2..5    : rewrite of P (K-major, hi/lo) and build of X (hi/lo)
-//   warps 6..9    : epilogue (double-buffered TMEM): TMEM lane = output
+//   warps 2..9    : rewrite of P (K-major, hi/lo) and build of X (hi/lo)
+//   warps 10..13  : epilogue (double-buffered TMEM): TMEM lane = output
 //                   column, so each thread writes its column over the sites
 //                   with 16-byte stores
 #include <cudaTypedefs.h>
@@ -37,7 +37,8 @@ extern std::atomic<long long> g_launch_count;
 
 namespace {
 
-constexpr int NT = 320;
+constexpr int NCONV = 256;                 // converter threads (warps 2..9)
+constexpr int NT = 64 + NCONV + 128;       // + producer, MMA warps and 4 epilogue warps
 constexpr int MAX_RS = 4, MAX_XS = 2, MAX_OS = 2;
 constexpr size_t SMEM_CAP = 227 * 1024;
 
@@ -89,6 +90,7 @@ __device__ __forceinline__ void store_split(uint8_t *hi, uint8_t *lo, uint32_t o
     *(float4 *)(lo + off) = l;
 }
 
+template <int NSP>
 __global__ void __launch_bounds__(NT, 1)
 theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
 {
@@ -114,9 +116,9 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
     const uint32_t pBytes = (uint32_t)p.nkb * 128 * 128;   // one of P hi, P lo, X hi, X lo
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < p.RS; ++s) { mbar_init(&rawFull[s], 1); mbar_init(&rawEmpty[s], 128); }
-        for (int s = 0; s < p.XS; ++s) { mbar_init(&xFull[s], 1); mbar_init(&xEmpty[s], 128); }
-        for (int s = 0; s < p.OS; ++s) { mbar_init(&opFull[s], 128); mbar_init(&opEmpty[s], 1); }
+        for (int s = 0; s < p.RS; ++s) { mbar_init(&rawFull[s], 1); mbar_init(&rawEmpty[s], NCONV); }
+        for (int s = 0; s < p.XS; ++s) { mbar_init(&xFull[s], 1); mbar_init(&xEmpty[s], NCONV); }
+        for (int s = 0; s < p.OS; ++s) { mbar_init(&opFull[s], NCONV); mbar_init(&opEmpty[s], 1); }
         for (int b = 0; b < 2; ++b) { mbar_init(&tfull[b], 1); mbar_init(&tempty[b], 128); }
         fence_mbar_init();
         tma_prefetch_desc(&tA);
@@ -133,13 +135,13 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
             for (int lw = 0; lw < nw && ok; ++lw) {
                 const int w = (int)blockIdx.x + lw * (int)gridDim.x;
                 const int xs = lw % p.XS;
-                if (lw >= p.XS) ok = mbar_wait(&xEmpty[xs], ((lw / p.XS) - 1) & 1);
+                if (lw >= p.XS) ok = mbar_wait_sleep(&xEmpty[xs], ((lw / p.XS) - 1) & 1);
                 if (!ok) break;
                 mbar_arrive_expect_tx(&xFull[xs], p.xBytes);
                 bulk_load(xsl + (size_t)xs * p.xBytes, p.Sinv32 + (size_t)w * p.s32, p.xBytes, &xFull[xs]);
                 for (int part = 0; part < 2 && ok; ++part) {
                     const int it = 2 * lw + part, rs = it % p.RS;
-                    if (it >= p.RS) ok = mbar_wait(&rawEmpty[rs], ((it / p.RS) - 1) & 1);
+                    if (it >= p.RS) ok = mbar_wait_sleep(&rawEmpty[rs], ((it / p.RS) - 1) & 1);
                     if (!ok) break;
                     uint8_t *dst = raws + (size_t)rs * p.rawBytes;
                     mbar_arrive_expect_tx(&rawFull[rs], p.rawBytes);
@@ -153,16 +155,17 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
             for (int it = 0; it < items && ok; ++it) {
                 const int os = it % p.OS, lw = it >> 1, part = it & 1, buf = lw & 1;
                 if (part == 0 && lw >= 2) {
-                    ok = mbar_wait(&tempty[buf], ((lw >> 1) - 1) & 1);
+                    ok = mbar_wait_sleep(&tempty[buf], ((lw >> 1) - 1) & 1);
                     if (!ok) break;
                 }
-                ok = mbar_wait(&opFull[os], (it / p.OS) & 1);
+                ok = mbar_wait_sleep(&opFull[os], (it / p.OS) & 1);
                 if (!ok) break;
                 tc_fence_after();
                 const uint32_t st = smem_u32(ops + (size_t)os * p.opBytes);
                 const uint32_t ph = st, pl = st + pBytes, xh = st + 2 * pBytes, xl = st + 3 * pBytes;
                 const uint32_t d = tmem + (uint32_t)(buf * 128);
-                for (int kk = 0; kk < p.Nsp / 8; ++kk) {
+#pragma unroll
+                for (int kk = 0; kk < NSP / 8; ++kk) {
                     // D (rows = block, column, re/im; columns = sites) = X P^T
                     const uint32_t off = (uint32_t)((kk >> 2) * 128 * 128 + (kk & 3) * 32);
                     const uint32_t acc0 = (part > 0 || kk > 0) ? 1u : 0u;
@@ -175,19 +178,19 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
             }
         }
         __syncwarp();
-    } else if (warp < 6) {
+    } else if (warp < 2 + NCONV / 32) {
         const int t = threadIdx.x - 64;
-        const int Nsp = p.Nsp, G4 = Nsp / 4;
-        const int units = 128 * G4;
+        constexpr int Nsp = NSP, G4 = NSP / 4;
+        constexpr int units = 128 * G4;
         const int tasks = p.nb * Nsp * G4;   // (block, column a, group of 4 electrons c)
         for (int it = 0; it < items && ok; ++it) {
             const int lw = it >> 1, part = it & 1;
             const int w = (int)blockIdx.x + lw * (int)gridDim.x;
             const int rs = it % p.RS, os = it % p.OS, xs = lw % p.XS;
             const bool on = p.mask == nullptr || p.mask[w] != 0;
-            ok = mbar_wait(&rawFull[rs], (it / p.RS) & 1);
-            if (ok && it >= p.OS) ok = mbar_wait(&opEmpty[os], ((it / p.OS) - 1) & 1);
-            if (ok) ok = mbar_wait(&xFull[xs], (lw / p.XS) & 1);
+            ok = mbar_wait_sleep(&rawFull[rs], (it / p.RS) & 1);
+            if (ok && it >= p.OS) ok = mbar_wait_sleep(&opEmpty[os], ((it / p.OS) - 1) & 1);
+            if (ok) ok = mbar_wait_sleep(&xFull[xs], (lw / p.XS) & 1);
             if (!ok) break;
             const uint8_t *raw = raws + (size_t)rs * p.rawBytes;
             const float *xsrc = (const float *)(xsl + (size_t)xs * p.xBytes);
@@ -195,7 +198,8 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
             uint8_t *pl = ph + pBytes, *xh = ph + 2 * pBytes, *xl = ph + 3 * pBytes;
             // P: the raw chunks (Nsp rows of 32 sites each) as K-major rows
             // (row = site), split into hi and lo
-            for (int u = t; u < units; u += 128) {
+#pragma unroll
+            for (int u = t; u < units; u += NCONV) {
                 const int i = u & 127, k4 = u >> 7;
                 float x[4];
 #pragma unroll
@@ -215,7 +219,8 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
             // X: rows 2 Nsp b + 2 a (theta_re) and 2 Nsp b + 2 a + 1 (theta_im);
             // K = electron c of this item's part:
             //   re part: [S_re(c, a) ; S_im(c, a)],  im part: [-S_im(c, a) ; S_re(c, a)]
-            for (int q = t; q < tasks; q += 128) {
+#pragma unroll 2
+            for (int q = t; q < tasks; q += NCONV) {
                 const int g = q % G4, a = (q / G4) % Nsp, b = q / (G4 * Nsp);
                 const int Ns = b ? p.Ns[1] : p.Ns[0];
                 const long long so = 2 * (b ? p.sOff[1] : p.sOff[0]);
@@ -245,14 +250,15 @@ theta_tc_kernel(const __grid_constant__ CUtensorMap tA, ThArgs p)
         // of one part over the sites, contiguous in Theta and thetaZ
         const int q = warp & 3;
         const int r = q * 32 + lane;
-        const int Nsp = p.Nsp, n = p.n;
+        constexpr int Nsp = NSP;
+        const int n = p.n;
         const int b = r / (2 * Nsp), rr = r - b * 2 * Nsp, a = rr >> 1, im = rr & 1;
         const int Ns = b == 0 ? p.Ns[0] : (b == 1 ? p.Ns[1] : 0);
         const bool valid = b < p.nb && a < Ns;
         const long long tOff = b ? p.tOff[1] : p.tOff[0];
         for (int lw = 0; lw < nw && ok; ++lw) {
             const int buf = lw & 1;
-            ok = mbar_wait(&tfull[buf], (lw >> 1) & 1);
+            ok = mbar_wait_sleep(&tfull[buf], (lw >> 1) & 1);
             if (!ok) break;
             tc_fence_after();
             const int w = (int)blockIdx.x + lw * (int)gridDim.x;
@@ -399,7 +405,10 @@ int theta_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, int 
     if (r) return r;
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(theta_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
+        cudaFuncSetAttribute(theta_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
+        cudaFuncSetAttribute(theta_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
+        cudaFuncSetAttribute(theta_tc_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
+        cudaFuncSetAttribute(theta_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
         attr = true;
     }
     int dev = 0, sms = 148;
@@ -407,6 +416,11 @@ int theta_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, int 
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = std::min(W, sms);
     g_launch_count++;
-    theta_tc_kernel<<<grid, NT, pl.smem, s>>>(mA, a);
+    switch (pl.Nsp) {
+    case 16: theta_tc_kernel<16><<<grid, NT, pl.smem, s>>>(mA, a); break;
+    case 32: theta_tc_kernel<32><<<grid, NT, pl.smem, s>>>(mA, a); break;
+    case 48: theta_tc_kernel<48><<<grid, NT, pl.smem, s>>>(mA, a); break;
+    default: theta_tc_kernel<64><<<grid, NT, pl.smem, s>>>(mA, a); break;
+    }
     return (int)cudaGetLastError();
 }

@@ -115,11 +115,15 @@ def phase_flops(c, m, taylor_avg):
     real x complex MAC = 4), for the phaseless workload."""
     n, nup, ndn, G, W = m.n, m.nup, m.ndn, m.G, c["W"]
     K = (nup + ndn) * n
+    # A_g = phiT^H L_g is real for a real trial (the Cholesky vectors are
+    # real): the exchange product D = A_g theta is then real x complex
+    real_a = not (np.any(np.asarray(m.phiTUp).imag) or np.any(np.asarray(m.phiTDn).imag))
+    fa = 4.0 if real_a else 8.0
     f = {
         "mbuild": 4.0 * n * n * G * W,
         "force": 8.0 * G * K * W,
         "taylor": 8.0 * n * n * max(nup, ndn) * W * taylor_avg,
-        "exchange": 8.0 * (nup * nup + ndn * ndn) * n * G * W + 8.0 * (nup * nup + ndn * ndn) * G * W,
+        "exchange": fa * (nup * nup + ndn * ndn) * n * G * W + 8.0 * (nup * nup + ndn * ndn) * G * W,
         "overlap": 8.0 * (nup * nup + ndn * ndn) * n * W,
         "onebody": 8.0 * n * n * max(nup, ndn) * W,
     }
