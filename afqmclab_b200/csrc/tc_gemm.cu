@@ -6,6 +6,7 @@
 // error code, skips the remaining work and still releases its TMEM.
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 
@@ -133,6 +134,173 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     if (warp == 1) tmem_dealloc(tmem, BN);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form for large outputs: the product is formed transposed,
+// D[n][m] = sum_k B[n, k] A[m, k], so a TMEM lane holds one output column
+// (128 consecutive m of it per epilogue thread) and writes it with 16-byte
+// stores.  Tiles of 128 n x 256 m, double-buffered TMEM (2 x 256 columns) so
+// the epilogue of one tile overlaps the MMAs of the next.
+//   warp 0 lane 0 : TMA producer      warp 1 : TMEM owner, UMMA issuer
+//   warps 2..9    : epilogue (lane quarter = warp % 4, column half = (warp - 2) / 4)
+// ---------------------------------------------------------------------------
+constexpr int TT_BN = 128, TT_BM = 256, TT_STAGES = 4, TT_THREADS = 320;
+constexpr int TT_A_BYTES = TT_BM * TC_BK * 2, TT_B_BYTES = TT_BN * TC_BK * 2;
+constexpr size_t TT_SMEM = 1024 + (size_t)TT_STAGES * (TT_A_BYTES + TT_B_BYTES) + 256;
+
+template <int OUT>
+__global__ void __launch_bounds__(TT_THREADS, 1)
+tc_gemm_t_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M,
+                 int N, int K, int kSplit, int splits, void *C, long long ldc, long long splitStride,
+                 float alpha, int *err)
+{
+    constexpr uint32_t IDESC = idesc_bf16(TT_BN, TT_BM);
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t *sA = base;
+    uint8_t *sB = base + TT_STAGES * TT_A_BYTES;
+    uint64_t *full = (uint64_t *)(sB + TT_STAGES * TT_B_BYTES);
+    uint64_t *empty = full + TT_STAGES;
+    uint64_t *tfull = empty + TT_STAGES;   // 2
+    uint64_t *tempty = tfull + 2;          // 2
+    uint32_t *tmemSlot = (uint32_t *)(tempty + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int MT = (M + TT_BM - 1) / TT_BM, NTn = (N + TT_BN - 1) / TT_BN;
+    const int tiles = MT * NTn * splits;
+    auto tile_kt = [&](int t, int &m0, int &n0, int &k0) {
+        const int z = t / (MT * NTn), r = t - z * (MT * NTn);
+        m0 = (r % MT) * TT_BM;
+        n0 = (r / MT) * TT_BN;
+        k0 = z * kSplit;
+        const int kEnd = min(K, k0 + kSplit);
+        return kEnd > k0 ? (kEnd - k0 + TC_BK - 1) / TC_BK : 0;
+    };
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TT_STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+        for (int b = 0; b < 2; ++b) { mbar_init(&tfull[b], 1); mbar_init(&tempty[b], 256); }
+        fence_mbar_init();
+        tma_prefetch_desc(&tmA);
+        tma_prefetch_desc(&tmB);
+    }
+    if (warp == 1) { tmem_alloc(tmemSlot, 512); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmemSlot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int it = 0;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+                int m0, n0, k0;
+                const int KT = tile_kt(t, m0, n0, k0);
+                for (int kt = 0; kt < KT && ok; ++kt, ++it) {
+                    const int s = it % TT_STAGES;
+                    if (it >= TT_STAGES) ok = mbar_wait_sleep(&empty[s], ((it / TT_STAGES) - 1) & 1);
+                    if (!ok) break;
+                    mbar_arrive_expect_tx(&full[s], TT_A_BYTES + TT_B_BYTES);
+                    tma_load_2d(sA + s * TT_A_BYTES, &tmA, &full[s], k0 + kt * TC_BK, m0);
+                    tma_load_2d(sB + s * TT_B_BYTES, &tmB, &full[s], k0 + kt * TC_BK, n0);
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int it = 0, tc = 0;
+            for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++tc) {
+                int m0, n0, k0;
+                const int KT = tile_kt(t, m0, n0, k0);
+                const int buf = tc & 1;
+                if (tc >= 2) ok = mbar_wait_sleep(&tempty[buf], ((tc >> 1) - 1) & 1);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(buf * TT_BM);
+                for (int kt = 0; kt < KT && ok; ++kt, ++it) {
+                    const int s = it % TT_STAGES;
+                    ok = mbar_wait_sleep(&full[s], (it / TT_STAGES) & 1);
+                    if (!ok) break;
+                    tc_fence_after();
+                    const uint32_t a0 = smem_u32(sA + s * TT_A_BYTES);
+                    const uint32_t b0 = smem_u32(sB + s * TT_B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < TC_BK / 16; ++kk)
+                        umma_bf16(d, desc_k_sw128(b0 + kk * 32), desc_k_sw128(a0 + kk * 32), IDESC,
+                                  (kt > 0 || kk > 0) ? 1u : 0u);
+                    umma_commit(&empty[s]);
+                }
+                umma_commit(&tfull[buf]);
+            }
+        }
+        __syncwarp();
+    } else {
+        const int q = warp & 3, half = (warp - 2) >> 2;
+        int tc = 0;
+        for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++tc) {
+            int m0, n0, k0;
+            const int KT = tile_kt(t, m0, n0, k0);
+            const int buf = tc & 1;
+            ok = mbar_wait_sleep(&tfull[buf], (tc >> 1) & 1);
+            if (!ok) break;
+            tc_fence_after();
+            const int n = n0 + q * 32 + lane;
+            const size_t colOff = (size_t)(t / (MT * NTn)) * splitStride + (size_t)n * ldc;
+            const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * TT_BM);
+#pragma unroll 1
+            for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
+                float v[32];
+                tmem_ld32(trow + (uint32_t)c0, v);
+                if (KT == 0) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] = 0.f;
+                }
+                const int mb = m0 + c0;
+                if (n < N) {
+                    if (OUT == TC_OUT_BF16) {
+                        __nv_bfloat16 *dst = (__nv_bfloat16 *)C + colOff + mb;
+#pragma unroll
+                        for (int j = 0; j < 32; j += 8) {
+                            if (mb + j + 8 <= M) {
+                                uint4 pk;
+                                __nv_bfloat162 h0 = __floats2bfloat162_rn(alpha * v[j], alpha * v[j + 1]);
+                                __nv_bfloat162 h1 = __floats2bfloat162_rn(alpha * v[j + 2], alpha * v[j + 3]);
+                                __nv_bfloat162 h2 = __floats2bfloat162_rn(alpha * v[j + 4], alpha * v[j + 5]);
+                                __nv_bfloat162 h3 = __floats2bfloat162_rn(alpha * v[j + 6], alpha * v[j + 7]);
+                                pk.x = *(uint32_t *)&h0; pk.y = *(uint32_t *)&h1;
+                                pk.z = *(uint32_t *)&h2; pk.w = *(uint32_t *)&h3;
+                                *(uint4 *)(dst + j) = pk;
+                            } else {
+                                for (int u = 0; u < 8; ++u)
+                                    if (mb + j + u < M) dst[j + u] = __float2bfloat16_rn(alpha * v[j + u]);
+                            }
+                        }
+                    } else {
+                        float *dst = (float *)C + colOff + mb;
+#pragma unroll
+                        for (int j = 0; j < 32; j += 4) {
+                            if (mb + j + 4 <= M) {
+                                *(float4 *)(dst + j) =
+                                    make_float4(alpha * v[j], alpha * v[j + 1], alpha * v[j + 2], alpha * v[j + 3]);
+                            } else {
+                                for (int u = 0; u < 4; ++u)
+                                    if (mb + j + u < M) dst[j + u] = alpha * v[j + u];
+                            }
+                        }
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[buf]);
+        }
+    }
+    if (!ok && err) atomicExch(err, 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, 512);
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 get_encode()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -169,6 +337,32 @@ int launch_bn(const TcGemmArgs &a, cudaStream_t s)
     return (int)cudaGetLastError();
 }
 
+template <int OUT>
+int launch_t(const TcGemmArgs &a, cudaStream_t s)
+{
+    CUtensorMap ma, mb;
+    int r = tc_make_map_bf16(&ma, a.A, a.K, a.M, a.lda, TT_BM);
+    if (r) return r;
+    r = tc_make_map_bf16(&mb, a.B, a.K, a.N, a.ldb, TT_BN);
+    if (r) return r;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(tc_gemm_t_kernel<OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT_SMEM);
+        attr = true;
+    }
+    const int splits = a.splits > 1 ? a.splits : 1;
+    int kSplit = a.K;
+    if (splits > 1) kSplit = ((a.K + splits - 1) / splits + TC_BK - 1) / TC_BK * TC_BK;
+    const long long tiles = (long long)((a.M + TT_BM - 1) / TT_BM) * ((a.N + TT_BN - 1) / TT_BN) * splits;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (int)std::min<long long>(tiles, sms);
+    tc_gemm_t_kernel<OUT><<<grid, TT_THREADS, TT_SMEM, s>>>(ma, mb, a.M, a.N, a.K, kSplit, splits, a.C, a.ldc,
+                                                            a.splitStride, a.alpha, a.err);
+    return (int)cudaGetLastError();
+}
+
 }  // namespace
 
 int tc_make_map_bf16(void *map, const void *base, long long inner, long long rows, long long pitch,
@@ -191,6 +385,18 @@ int tc_gemm_bf16(const TcGemmArgs &a, cudaStream_t s)
 {
     g_launch_count++;
     if (a.M <= 0 || a.N <= 0 || a.K <= 0) return 0;
+    // large outputs: the persistent transposed form, when its 16-byte column
+    // stores are aligned
+    {
+        const int es = a.outType == TC_OUT_F32 ? 4 : 2;
+        const bool aligned = ((uintptr_t)a.C % 16 == 0) && ((a.ldc * es) % 16 == 0) &&
+                             (a.splits <= 1 || (a.splitStride * es) % 16 == 0);
+        const long long tiles = (long long)((a.M + TT_BM - 1) / TT_BM) * ((a.N + TT_BN - 1) / TT_BN);
+        if (aligned && a.M >= TT_BM && a.N >= TT_BN && tiles * (a.splits > 1 ? a.splits : 1) >= 148) {
+            if (a.outType == TC_OUT_F32) return launch_t<TC_OUT_F32>(a, s);
+            return launch_t<TC_OUT_BF16>(a, s);
+        }
+    }
     if (a.N >= 192) {
         if (a.outType == TC_OUT_F32) return launch_bn<256, TC_OUT_F32>(a, s);
         return launch_bn<256, TC_OUT_BF16>(a, s);

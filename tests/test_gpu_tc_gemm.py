@@ -46,3 +46,20 @@ def test_tc_gemm_bf16_output_and_alpha():
     got, ref = run(256, 512, 640, out_bf16=True, alpha=0.25)
     err = (got - ref).abs().max().item() / ref.abs().max().item()
     assert err < 1e-2, err
+
+
+# Large outputs take the persistent transposed kernel (at least one tile per
+# SM): full tiles, ragged M / N / K edges, split K and bf16 output.
+@pytest.mark.parametrize("M,N,K,splits", [(4096, 2048, 640, 1), (4100, 2000, 130, 1),
+                                          (1280, 2048, 4096, 4), (16384, 256, 64, 1)])
+def test_tc_gemm_persistent_matches_fp32(M, N, K, splits):
+    lda = (K + 7) // 8 * 8
+    got, ref = run(M, N, K, lda=lda, ldb=lda, splits=splits)
+    err = (got - ref).abs().max().item() / ref.abs().max().item()
+    assert err < TOL, err
+
+
+def test_tc_gemm_persistent_bf16_output():
+    got, ref = run(4096, 1024, 640, out_bf16=True, alpha=0.5)
+    err = (got - ref).abs().max().item() / ref.abs().max().item()
+    assert err < 1e-2, err
