@@ -645,10 +645,21 @@ int force_tc(afqmc_engine *e)
 {
     MixedState *m = e->mx;
     TcGemmArgs a;
-    a.M = 2 * e->G; a.N = e->W; a.K = (int)(2 * e->Ktot);
-    a.A = m->Abig; a.lda = 2 * e->Ktot;
-    a.B = m->Theta; a.ldb = 2 * e->Ktot;
-    a.C = m->xbarp; a.ldc = 2 * e->G; a.outType = TC_OUT_F32;
+    if (m->realA) {
+        // real A_g: xbar_re = A theta_re, xbar_im = A theta_im as one real
+        // product over the theta planes (column 2w + p = plane p of walker w),
+        // which lands in the same layout as the complex form
+        a.M = e->G; a.N = 2 * e->W; a.K = (int)e->Ktot;
+        a.A = m->Abig; a.lda = 2 * e->Ktot;
+        a.B = m->Theta; a.ldb = e->Ktot;
+        a.C = m->xbarp; a.ldc = e->G;
+    } else {
+        a.M = 2 * e->G; a.N = e->W; a.K = (int)(2 * e->Ktot);
+        a.A = m->Abig; a.lda = 2 * e->Ktot;
+        a.B = m->Theta; a.ldb = 2 * e->Ktot;
+        a.C = m->xbarp; a.ldc = 2 * e->G;
+    }
+    a.outType = TC_OUT_F32;
     a.splits = m->splits; a.splitStride = (long long)2 * e->G * e->W;
     return tc(e, a);
 }

@@ -121,7 +121,7 @@ def phase_flops(c, m, taylor_avg):
     fa = 4.0 if real_a else 8.0
     f = {
         "mbuild": 4.0 * n * n * G * W,
-        "force": 8.0 * G * K * W,
+        "force": fa * G * K * W,
         "taylor": 8.0 * n * n * max(nup, ndn) * W * taylor_avg,
         "exchange": fa * (nup * nup + ndn * ndn) * n * G * W + 8.0 * (nup * nup + ndn * ndn) * G * W,
         "overlap": 8.0 * (nup * nup + ndn * ndn) * n * W,
