@@ -21,6 +21,7 @@ FORCE = {"dynamicForce": 0, "constForce": 1}
 SYMBOLS = [
     "afqmc_last_error", "afqmc_version", "afqmc_cp_create", "afqmc_pl_create", "afqmc_destroy",
     "afqmc_set_stream", "afqmc_synchronize", "afqmc_set_walkers", "afqmc_get_walkers",
+    "afqmc_set_walkers_async", "afqmc_upload_wait",
     "afqmc_set_rng", "afqmc_get_rng", "afqmc_set_ET", "afqmc_set_cadence",
     "afqmc_project_one_step", "afqmc_project_half", "afqmc_modify_gm", "afqmc_pop_control",
     "afqmc_reset_measurement", "afqmc_add_mixed_measurement", "afqmc_get_measurement",
@@ -73,6 +74,8 @@ def _declare(L):
     L.afqmc_set_stream.argtypes = [P, P]
     L.afqmc_set_walkers.argtypes = [P, P, P, P]
     L.afqmc_get_walkers.argtypes = [P, P, P, P]
+    L.afqmc_set_walkers_async.argtypes = [P, P, P, P]
+    L.afqmc_upload_wait.argtypes = [P]
     L.afqmc_set_rng.argtypes = [P, U64, U64]
     L.afqmc_get_rng.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64)]
     L.afqmc_set_ET.argtypes = [P, D]
@@ -160,6 +163,15 @@ class Engine:
         lw = np.ascontiguousarray(logw, dtype=np.complex128)
         al = np.ascontiguousarray(alive, dtype=np.int32)
         _check(lib().afqmc_set_walkers(self.h, _p(wf), _p(lw), _p(al)))
+
+    def set_walkers_async(self, wf_ptr, logw_ptr, alive_ptr):
+        """Pipelined upload from pinned host buffers given by address (they
+        must stay unchanged until upload_wait() or a synchronizing call)."""
+        _check(lib().afqmc_set_walkers_async(self.h, ctypes.c_void_p(wf_ptr), ctypes.c_void_p(logw_ptr),
+                                             ctypes.c_void_p(alive_ptr)))
+
+    def upload_wait(self):
+        _check(lib().afqmc_upload_wait(self.h))
 
     def get_walkers(self):
         wf = np.zeros((self.n, self.ncol, self.W), np.complex128, order="F")

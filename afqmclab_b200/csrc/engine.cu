@@ -523,6 +523,12 @@ void free_engine(afqmc_engine *e)
     if (e->mx || e->cpm) mixed_destroy(e);
     prof_resolve(e);
     for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
+    if (e->upStream) cudaStreamSynchronize(e->upStream);
+    for (int k = 0; k < 2; ++k) {
+        if (e->upReady[k]) cudaEventDestroy(e->upReady[k]);
+        if (e->upFree[k]) cudaEventDestroy(e->upFree[k]);
+    }
+    if (e->upStream) cudaStreamDestroy(e->upStream);
     for (void *p : e->allocs) cudaFree(p);
     if (e->own) cudaStreamDestroy(e->own);
     delete e;
@@ -768,6 +774,45 @@ int afqmc_set_walkers(afqmc_engine *e, const double *wf, const double *logw, con
     CUDA_TRY(cudaMemcpyAsync(e->alive, alive, sizeof(int) * e->W, cudaMemcpyHostToDevice, e->stream));
     if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_set_walkers_async(afqmc_engine *e, const double *wf, const double *logw, const int *alive)
+{
+    if (!e || !wf || !logw || !alive) return fail(AFQMC_ERR_ARG, "null argument");
+    if (!e->upStream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&e->upStream, cudaStreamNonBlocking));
+        for (int k = 0; k < 2; ++k) {
+            CUDA_TRY(cudaEventCreateWithFlags(&e->upReady[k], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&e->upFree[k], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventRecord(e->upFree[k], e->stream));
+            TRY(dalloc(e, &e->stgWf[k], (size_t)e->wsize * e->W));
+            TRY(dalloc(e, &e->stgLw[k], (size_t)e->W));
+            TRY(dalloc(e, &e->stgAl[k], (size_t)e->W));
+        }
+    }
+    const int k = e->upNext;
+    e->upNext ^= 1;
+    // the slot's previous contents must have been installed first
+    CUDA_TRY(cudaStreamWaitEvent(e->upStream, e->upFree[k], 0));
+    CUDA_TRY(cudaMemcpyAsync(e->stgWf[k], wf, sizeof(zd) * e->wsize * e->W, cudaMemcpyHostToDevice, e->upStream));
+    CUDA_TRY(cudaMemcpyAsync(e->stgLw[k], logw, sizeof(zd) * e->W, cudaMemcpyHostToDevice, e->upStream));
+    CUDA_TRY(cudaMemcpyAsync(e->stgAl[k], alive, sizeof(int) * e->W, cudaMemcpyHostToDevice, e->upStream));
+    CUDA_TRY(cudaEventRecord(e->upReady[k], e->upStream));
+    // installed on the work stream after everything enqueued before this call
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->upReady[k], 0));
+    CUDA_TRY(cudaMemcpyAsync(e->wf, e->stgWf[k], sizeof(zd) * e->wsize * e->W, cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->logw, e->stgLw[k], sizeof(zd) * e->W, cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->alive, e->stgAl[k], sizeof(int) * e->W, cudaMemcpyDeviceToDevice, e->stream));
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
+    CUDA_TRY(cudaEventRecord(e->upFree[k], e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_upload_wait(afqmc_engine *e)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    if (e->upStream) CUDA_TRY(cudaStreamSynchronize(e->upStream));
     return AFQMC_OK;
 }
 

@@ -24,6 +24,12 @@ struct afqmc_engine {
     int mgsStep = 1, popStep = 1, mgsIndex = 0, popIndex = 0;
     uint64_t seed = 0;
     cudaStream_t own = nullptr, stream = nullptr;
+    // asynchronous population upload: copy stream, two device staging slots
+    cudaStream_t upStream = nullptr;
+    cudaEvent_t upReady[2] = {nullptr, nullptr}, upFree[2] = {nullptr, nullptr};
+    zd *stgWf[2] = {nullptr, nullptr}, *stgLw[2] = {nullptr, nullptr};
+    int *stgAl[2] = {nullptr, nullptr};
+    int upNext = 0;
     Blocks bl{};
     long long wsize = 0;
     zd logwT{0, 0};

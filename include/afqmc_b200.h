@@ -113,6 +113,16 @@ int afqmc_synchronize(afqmc_engine *e);
  * alive: the driver's walkerIsAlive vector. */
 int afqmc_set_walkers(afqmc_engine *e, const double *wf, const double *logw, const int *alive);
 int afqmc_get_walkers(afqmc_engine *e, double *wf, double *logw, int *alive);
+/* Pipelined form of afqmc_set_walkers (same layout; no counterpart in the
+ * reference, whose walkers stay in host memory): the host-to-device copy runs
+ * on an internal copy stream while earlier work on the engine's stream is still
+ * running, and the population is installed on the engine's stream after all
+ * work enqueued before the call; returns without waiting.  Host buffers should
+ * be pinned and must stay unchanged until the copy has finished
+ * (afqmc_upload_wait, or any call that synchronizes the engine's stream after
+ * the install).  The first call allocates two device staging slots. */
+int afqmc_set_walkers_async(afqmc_engine *e, const double *wf, const double *logw, const int *alive);
+int afqmc_upload_wait(afqmc_engine *e);
 
 /* Counter-based random stream: replaces randomHaoInit/randomHaoSave/Read
  * (common/randomHao/source/random_hao.cpp:10-71).  The stream is the
