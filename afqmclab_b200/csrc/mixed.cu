@@ -328,7 +328,7 @@ template <int NC>
 __global__ void __launch_bounds__(128, 1)
 taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmE,
                       int W, int n, float *w32, const int *surv, int *order, int kmax, float acc,
-                      int checkFrom, int doOneBody, int *status, int *err)
+                      float relTol, int checkFrom, int doOneBody, int *status, int *err)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -339,7 +339,7 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     uint8_t *sBi = sBr + (size_t)KB * NC * 128;
     uint64_t *bars = (uint64_t *)(sBi + (size_t)KB * NC * 128);   // [0] M, [1] MMA, [2] E
     uint32_t *tslot = (uint32_t *)(bars + 3);
-    __shared__ float red[4];
+    __shared__ float red[4], red0[4];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int row = tid;
@@ -414,13 +414,23 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             pr[a] = rowOK ? gw[row + (size_t)n * a] : 0.f;
             pi[a] = rowOK ? gw[(size_t)n * NC + row + (size_t)n * a] : 0.f;
         }
+        float s2 = 0.f;
         if (rowOK) {
 #pragma unroll
-            for (int a = 0; a < NC; ++a) { store_b_sw<NC>(sBr, a, row, pr[a]); store_b_sw<NC>(sBi, a, row, pi[a]); }
+            for (int a = 0; a < NC; ++a) {
+                store_b_sw<NC>(sBr, a, row, pr[a]);
+                store_b_sw<NC>(sBi, a, row, pi[a]);
+                s2 = fmaxf(s2, pr[a] * pr[a] + pi[a] * pi[a]);
+            }
         }
+        for (int o = 16; o > 0; o >>= 1) s2 = fmaxf(s2, __shfl_xor_sync(0xffffffffu, s2, o));
+        if (lane == 0) red0[warp] = s2;
         fence_proxy_async();
         tc_fence_before();
         __syncthreads();
+        // terms below fp32 resolution of the walker's largest entry cannot
+        // change the fp32 sum: the series stops there (or at acc)
+        const float tol = fmaxf(acc, relTol * sqrtf(fmaxf(fmaxf(red0[0], red0[1]), fmaxf(red0[2], red0[3]))));
         ok = __syncthreads_and(mbar_wait(&bars[0], phL)) != 0;
         phL ^= 1;
         mPending = false;
@@ -469,7 +479,7 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             tc_fence_before();
             __syncthreads();
             const float m4 = fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]));
-            const bool conv = (k >= checkFrom) && (sqrtf(m4) <= acc);
+            const bool conv = (k >= checkFrom) && (sqrtf(m4) <= tol);
             if (conv || k >= kmax) {
                 if (!conv && tid == 0 && status) atomicOr(status + w, (int)ST_TAYLOR_CAP);
                 break;
@@ -562,7 +572,7 @@ int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE,
     const int perSm = TaylorSmem<NC>::bytes(e->n) <= 112 * 1024 ? 2 : 1;
     int grid = std::min(e->W, perSm * sms);
     taylor_onebody_kernel<NC><<<grid, 128, smem, e->stream>>>(
-        mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, 30, 1e-10f, 4, doOneBody, e->status,
+        mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, 30, 1e-10f, 5.9604645e-8f, 4, doOneBody, e->status,
         e->mx->err);
     return engine_check_launch();
 }
