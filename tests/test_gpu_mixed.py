@@ -96,3 +96,22 @@ def test_mixed_rejects_unsupported_shapes():
     m = inputs.molecule_inputs(16, 4, 3, 24, dt=0.01, decay=6.0)
     with pytest.raises(capi.AfqmcError):
         capi.pl_engine(m, 8, 1, precision=capi.AFQMC_MIXED)
+
+
+@pytest.mark.parametrize("n,nup,ndn,G", [(64, 16, 16, 64), (128, 32, 32, 64), (64, 16, 8, 64)])
+def test_mixed_stabilisation_matches_fp64(n, nup, ndn, G):
+    """The mixed form's FP64 Cholesky QR of the fp32 walkers gives the same
+    orthonormal columns (R with positive real diagonal, so the same gauge)
+    and log-weight shift as the FP64 form's Gram-Schmidt, to fp32 accuracy."""
+    m = molecule(n, nup, ndn, G)
+    W = 40
+    f, x = pair(m, W, 31, noise=0.2)
+    f.modify_gm()
+    x.modify_gm()
+    wf_f, lw_f, _ = f.get_walkers()
+    wf_x, lw_x, _ = x.get_walkers()
+    assert np.abs(lw_x - lw_f).max() < 1e-5
+    assert np.abs(wf_x - wf_f).max() < 1e-5
+    q = wf_x[:, :, 0]
+    assert np.abs(q.conj().T @ q - np.eye(q.shape[1])).max() < 1e-5
+    assert x.status() == 0
