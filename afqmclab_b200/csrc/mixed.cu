@@ -952,8 +952,13 @@ int mixed_add_measurement(afqmc_engine *e)
         PHASE(AFQMC_PH_MEASURE);
         // walkerTemp = exp(dt/2 K) walker: compensated tf32 tensor-core
         // product phi + (E - I) phi, fp32 result
-        int r = split_f32_launch(s, (long long)W * m->ws32, m->wf32, m->sh, m->sl);
-        if (!r) r = onebody_tf32_launch(s, e->n, e->ncol, W, m->E1h, m->E1l, m->sh, m->sl, m->tmp32, nullptr, m->err);
+        int r = 0;
+        if (onebody_split_supported(e->n)) {
+            r = onebody_split_launch(s, e->n, e->ncol, W, m->E1h, m->E1l, m->wf32, m->tmp32, m->err);
+        } else {
+            r = split_f32_launch(s, (long long)W * m->ws32, m->wf32, m->sh, m->sl);
+            if (!r) r = onebody_tf32_launch(s, e->n, e->ncol, W, m->E1h, m->E1l, m->sh, m->sl, m->tmp32, nullptr, m->err);
+        }
         if (r) return engine_fail(AFQMC_ERR_CUDA, "measurement one-body: " + std::to_string(r));
         MTRY(overlap32(e, m->tmp32, e->alive));
         launch_lu_logdet_inverse32(W, e->bl, e->S, e->Sinv, m->Sinv32, e->alive, e->logw,

@@ -211,6 +211,183 @@ ov_split_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__
     if (warp == 1) tmem_dealloc(tmem, 2 * BN);
 }
 
+// ---------------------------------------------------------------------------
+// One-body product of the measurement's half step on the tensor cores:
+//   out = phi + (E - I) phi   for every column of the fp32 population
+// (columns (walker, plane, orbital), n sites each), compensated tf32:
+// (E - I) is held resident in shared memory as tf32 high and low parts, each
+// raw walker chunk is split in place into high part and remainder, and
+//   phi_hi (E-I)_hi + phi_lo (E-I)_hi + phi_hi (E-I)_lo
+// is accumulated in fp32.  The product is formed transposed (TMEM lane =
+// population column, TMEM column = site), so each epilogue thread adds its
+// column's fp32 residual and writes the column with 16-byte stores.
+// Replaces Hop2isSD2isOperation::applyToRight (hop2isSD2isOperation.cpp:14-19)
+// for the half step of the mixed estimator.
+//   warp 0 lane 0 : TMA producer (the operator once, then walker chunks)
+//   warp 1        : TMEM owner, UMMA issuer (double-buffered accumulators)
+//   warps 2..5    : in-place split of each walker chunk
+//   warps 6..9    : epilogue
+// ---------------------------------------------------------------------------
+constexpr int OB_STAGES = 3, OB_TILE = 128, OB_KC = 32;
+constexpr int OB_CHUNK_BYTES = OB_TILE * OB_KC * 4;   // 16 KB: 128 columns x 32 sites
+
+struct ObArgs {
+    int n, nkc;
+    long long cols, tiles;
+    uint32_t idesc;
+    const float *res;    // the walkers (residual)
+    float *out;
+    int *err;
+};
+
+__global__ void __launch_bounds__(320, 1)
+ob_split_kernel(const __grid_constant__ CUtensorMap tEh, const __grid_constant__ CUtensorMap tEl,
+                const __grid_constant__ CUtensorMap tP, ObArgs p)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const uint32_t eBytes = (uint32_t)p.n * 128;          // one k chunk of (E - I): n rows x 32 sites
+    uint8_t *sEh = base;                                   // nkc chunks
+    uint8_t *sEl = sEh + (size_t)p.nkc * eBytes;
+    uint8_t *stg = sEl + (size_t)p.nkc * eBytes;           // OB_STAGES x (raw->hi | lo)
+    uint64_t *full = (uint64_t *)(stg + (size_t)OB_STAGES * 2 * OB_CHUNK_BYTES);
+    uint64_t *split = full + OB_STAGES;
+    uint64_t *empty = split + OB_STAGES;
+    uint64_t *eFull = empty + OB_STAGES;
+    uint64_t *tfull = eFull + 1;    // 2
+    uint64_t *tempty = tfull + 2;   // 2
+    uint32_t *tmemSlot = (uint32_t *)(tempty + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long myTiles = (p.tiles - (long long)blockIdx.x + gridDim.x - 1) / gridDim.x;
+    const int KT = p.nkc;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < OB_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&split[s], 128);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(eFull, 1);
+        for (int b = 0; b < 2; ++b) { mbar_init(&tfull[b], 1); mbar_init(&tempty[b], 128); }
+        fence_mbar_init();
+        tma_prefetch_desc(&tEh);
+        tma_prefetch_desc(&tEl);
+        tma_prefetch_desc(&tP);
+    }
+    if (warp == 1) { tmem_alloc(tmemSlot, 256); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmemSlot;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            mbar_arrive_expect_tx(eFull, 2 * KT * eBytes);
+            for (int kc = 0; kc < KT; ++kc) {
+                tma_load_2d(sEh + kc * eBytes, &tEh, eFull, kc * OB_KC, 0);
+                tma_load_2d(sEl + kc * eBytes, &tEl, eFull, kc * OB_KC, 0);
+            }
+            long long it = 0;
+            for (long long ti = 0; ti < myTiles && ok; ++ti) {
+                const long long t = blockIdx.x + ti * gridDim.x;
+                for (int kc = 0; kc < KT && ok; ++kc, ++it) {
+                    const int s = (int)(it % OB_STAGES);
+                    if (it >= OB_STAGES) ok = mbar_wait_sleep(&empty[s], (uint32_t)(((it / OB_STAGES) - 1) & 1));
+                    if (!ok) break;
+                    mbar_arrive_expect_tx(&full[s], OB_CHUNK_BYTES);
+                    tma_load_2d(stg + (size_t)s * 2 * OB_CHUNK_BYTES, &tP, &full[s], kc * OB_KC, (int)(t * OB_TILE));
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            ok = mbar_wait_sleep(eFull, 0);
+            long long it = 0;
+            for (long long ti = 0; ti < myTiles && ok; ++ti) {
+                const int buf = (int)(ti & 1);
+                if (ti >= 2) ok = mbar_wait_sleep(&tempty[buf], (uint32_t)(((ti >> 1) - 1) & 1));
+                if (!ok) break;
+                const uint32_t d = tmem + (uint32_t)(buf * 128);
+                for (int kc = 0; kc < KT && ok; ++kc, ++it) {
+                    const int s = (int)(it % OB_STAGES);
+                    ok = mbar_wait_sleep(&split[s], (uint32_t)((it / OB_STAGES) & 1));
+                    if (!ok) break;
+                    tc_fence_after();
+                    const uint32_t ph = smem_u32(stg + (size_t)s * 2 * OB_CHUNK_BYTES), pl = ph + OB_CHUNK_BYTES;
+                    const uint32_t eh = smem_u32(sEh + kc * eBytes), el = smem_u32(sEl + kc * eBytes);
+#pragma unroll
+                    for (int k8 = 0; k8 < OB_KC / 8; ++k8) {
+                        const uint32_t acc0 = (kc > 0 || k8 > 0) ? 1u : 0u;
+                        umma_tf32(d, desc_k_sw128(ph + k8 * 32), desc_k_sw128(eh + k8 * 32), p.idesc, acc0);
+                        umma_tf32(d, desc_k_sw128(pl + k8 * 32), desc_k_sw128(eh + k8 * 32), p.idesc, 1u);
+                        umma_tf32(d, desc_k_sw128(ph + k8 * 32), desc_k_sw128(el + k8 * 32), p.idesc, 1u);
+                    }
+                    umma_commit(&empty[s]);
+                }
+                if (ok) umma_commit(&tfull[buf]);
+            }
+        }
+        __syncwarp();
+    } else if (warp < 6) {
+        const int t = threadIdx.x - 64;
+        const long long items = myTiles * KT;
+        for (long long it = 0; it < items && ok; ++it) {
+            const int s = (int)(it % OB_STAGES);
+            ok = mbar_wait_sleep(&full[s], (uint32_t)((it / OB_STAGES) & 1));
+            if (!ok) break;
+            float4 *bh = (float4 *)(stg + (size_t)s * 2 * OB_CHUNK_BYTES);
+            float4 *bl = (float4 *)(stg + (size_t)s * 2 * OB_CHUNK_BYTES + OB_CHUNK_BYTES);
+#pragma unroll 4
+            for (int i = t; i < OB_CHUNK_BYTES / 16; i += 128) {
+                const float4 x = bh[i];
+                float4 h, l;
+                h.x = tf32_round(x.x); l.x = x.x - h.x;
+                h.y = tf32_round(x.y); l.y = x.y - h.y;
+                h.z = tf32_round(x.z); l.z = x.z - h.z;
+                h.w = tf32_round(x.w); l.w = x.w - h.w;
+                bh[i] = h;
+                bl[i] = l;
+            }
+            fence_proxy_async();
+            mbar_arrive(&split[s]);
+        }
+    } else {
+        const int q = warp & 3;
+        const int r = q * 32 + lane;
+        for (long long ti = 0; ti < myTiles && ok; ++ti) {
+            const int buf = (int)(ti & 1);
+            ok = mbar_wait_sleep(&tfull[buf], (uint32_t)((ti >> 1) & 1));
+            if (!ok) break;
+            tc_fence_after();
+            const long long t = blockIdx.x + ti * gridDim.x;
+            const long long col = t * OB_TILE + r;
+            const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 128);
+            const float *rc = p.res + col * p.n;
+            float *oc = p.out + col * p.n;
+            for (int c0 = 0; c0 < p.n; c0 += 32) {
+                float v[32];
+                tmem_ld32(trow + (uint32_t)c0, v);
+                if (col < p.cols) {
+#pragma unroll
+                    for (int j = 0; j < 32; j += 4) {
+                        const float4 x = *(const float4 *)(rc + c0 + j);
+                        *(float4 *)(oc + c0 + j) = make_float4(x.x + v[j], x.y + v[j + 1], x.z + v[j + 2], x.w + v[j + 3]);
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(&tempty[buf]);
+        }
+    }
+    if (!ok && p.err) atomicExch(p.err, 1);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmem, 256);
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -336,5 +513,41 @@ int overlap_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, in
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     g_launch_count++;
     ov_split_kernel<<<std::min(a.tiles, sms), NT, SMEM, s>>>(ah, al, b, a);
+    return (int)cudaGetLastError();
+}
+
+bool onebody_split_supported(int n) { return n == 64 || n == 128; }
+
+int onebody_split_launch(cudaStream_t s, int n, int ncol, int W, const float *Ehi, const float *Elo,
+                         const float *w32, float *out, int *err)
+{
+    if (!onebody_split_supported(n)) return (int)cudaErrorInvalidValue;
+    const int nkc = n / OB_KC;
+    const size_t smem = 1024 + (size_t)2 * nkc * n * 128 + (size_t)OB_STAGES * 2 * OB_CHUNK_BYTES + 256;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(ob_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        attr = true;
+    }
+    CUtensorMap eh, el, pm;
+    cuuint64_t de[2] = {(cuuint64_t)n, (cuuint64_t)n}, pe[1] = {(cuuint64_t)n * 4};
+    cuuint32_t be[2] = {(cuuint32_t)OB_KC, (cuuint32_t)n};
+    int r = map_f32(&eh, Ehi, 2, de, pe, be);
+    if (!r) r = map_f32(&el, Elo, 2, de, pe, be);
+    const long long cols = 2LL * ncol * W;
+    cuuint64_t dp[2] = {(cuuint64_t)n, (cuuint64_t)cols}, pp[1] = {(cuuint64_t)n * 4};
+    cuuint32_t bp[2] = {(cuuint32_t)OB_KC, (cuuint32_t)OB_TILE};
+    if (!r) r = map_f32(&pm, w32, 2, dp, pp, bp);
+    if (r) return r;
+    ObArgs a{};
+    a.n = n; a.nkc = nkc; a.cols = cols;
+    a.tiles = (cols + OB_TILE - 1) / OB_TILE;
+    a.idesc = idesc_tf32(OB_TILE, n);
+    a.res = w32; a.out = out; a.err = err;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    g_launch_count++;
+    ob_split_kernel<<<(unsigned)std::min<long long>(a.tiles, sms), 320, smem, s>>>(eh, el, pm, a);
     return (int)cudaGetLastError();
 }

@@ -18,3 +18,10 @@ int overlap_tc_build(int nb, const zd *const *Thost, int n, const int *Ns, std::
 int overlap_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, int W, const float *Ohi,
                       const float *Olo, const float *w32, zd *S, long long sStride, const long long *sOff,
                       int *err);
+
+// Half-step one-body of the mixed estimator: out = phi + (E - I) phi for every
+// column of the fp32 population w32 (W walkers, 2 ncol columns of n sites
+// each), (E - I) given as tf32 high / low parts (n x n row-major); n in {64, 128}
+bool onebody_split_supported(int n);
+int onebody_split_launch(cudaStream_t s, int n, int ncol, int W, const float *Ehi, const float *Elo,
+                         const float *w32, float *out, int *err);
