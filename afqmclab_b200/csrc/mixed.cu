@@ -208,18 +208,21 @@ mgs32_kernel(int W, int n, int ncol, int nup, int ndn, float *w32, zd *logw, con
 
 // Phaseless force from the tensor-core xbar partials, aux sampling, sample
 // log-weight and second cos projection (same arithmetic as the FP64 form),
-// writing y = sqrt(-dt) x as the bf16 operand of the two-body GEMM.
-__global__ void __launch_bounds__(256)
-mixed_sample_kernel(int W, CholDev c, const float *xbarp, int splits, long long splitStride,
-                    int *surv, int *alive, const unsigned long long *offs, uint64_t seed,
-                    __nv_bfloat16 *Y, zd *logw, double dtET, zd hopLogw)
+// writing y = sqrt(-dt) x as the bf16 operand of the two-body GEMM.  One warp
+// per walker (four walkers per block): a walker's sums need no block barrier
+// and more walkers are in flight per SM.
+__global__ void __launch_bounds__(128)
+mixed_sample_warp_kernel(int W, CholDev c, const float *xbarp, int splits, long long splitStride,
+                         int *surv, int *alive, const unsigned long long *offs, uint64_t seed,
+                         __nv_bfloat16 *Y, zd *logw, double dtET, zd hopLogw)
 {
-    __shared__ double red[32];
-    const int w = blockIdx.x;
-    if (!surv[w]) return;
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (w >= W || !surv[w]) return;
     const int G = c.G;
+    const unsigned long long off = offs[w];
     zd f2 = make_double2(0, 0), xf = make_double2(0, 0), xb = make_double2(0, 0);
-    for (int g = threadIdx.x; g < G; g += blockDim.x) {
+    for (int g = lane; g < G; g += 32) {
         zd f;
         if (c.constForce) {
             f = c.constForce[g];
@@ -234,7 +237,7 @@ mixed_sample_kernel(int W, CholDev c, const float *xbarp, int splits, long long 
             double af = zabs(f);
             if (af > c.forceCap) f = make_double2(f.x * c.forceCap / af, f.y * c.forceCap / af);
         }
-        double gs = rng_gaussian(seed, offs[w] + 2ULL * g);
+        double gs = rng_gaussian(seed, off + 2ULL * g);
         zd x = make_double2(gs + f.x, f.y);
         Y[(size_t)(2 * w) * G + g] = __double2bfloat16(-c.sqrtDt * x.y);
         Y[(size_t)(2 * w + 1) * G + g] = __double2bfloat16(c.sqrtDt * x.x);
@@ -242,10 +245,10 @@ mixed_sample_kernel(int W, CholDev c, const float *xbarp, int splits, long long 
         zfma(xf, x, f);
         zfma(xb, x, make_double2(c.bg[g], 0.0));
     }
-    f2 = block_zsum(f2, red);
-    xf = block_zsum(xf, red);
-    xb = block_zsum(xb, red);
-    if (threadIdx.x == 0) {
+    f2.x = warp_sum(f2.x); f2.y = warp_sum(f2.y);
+    xf.x = warp_sum(xf.x); xf.y = warp_sum(xf.y);
+    xb.x = warp_sum(xb.x); xb.y = warp_sum(xb.y);
+    if (lane == 0) {
         double phase = xf.y;
         double cs = cos(phase);
         if (cs <= 0.0) {
@@ -856,10 +859,10 @@ int mixed_project_dtk_dtv(afqmc_engine *e)
     {
         PHASE(AFQMC_PH_SAMPLE);
         launch_rng_scan(W, e->surv, 2 * e->G, e->counter, e->offs, s);
-        mixed_sample_kernel<<<W, 256, 0, s>>>(W, e->cdv, m->xbarp, m->splits,
-                                             (long long)2 * e->G * W, e->surv, e->alive, e->offs,
-                                             e->seed, m->Y, e->logw, e->dt * e->ET,
-                                             engine_one_body_logw(e, 0));
+        mixed_sample_warp_kernel<<<(W + 3) / 4, 128, 0, s>>>(W, e->cdv, m->xbarp, m->splits,
+                                                            (long long)2 * e->G * W, e->surv, e->alive,
+                                                            e->offs, e->seed, m->Y, e->logw, e->dt * e->ET,
+                                                            engine_one_body_logw(e, 0));
         MTRY(engine_check_launch());
     }
     {
