@@ -150,7 +150,9 @@ __global__ void gather32_kernel(int W, long long ws32, const int *table, float *
     if (threadIdx.x == 0) logw[i] = logw[j];
 }
 
-// Gram-Schmidt (SD2is::stabilize, SD2is.cpp:48-76) in FP64 on an fp32 walker
+// Gram-Schmidt (SD2is::stabilize, SD2is.cpp:48-76) on an fp32 walker: norms,
+// projections and updates in FP64, the columns kept in fp32 between updates
+// (the walker's own precision), which halves the shared memory per walker
 __global__ void __launch_bounds__(256)
 mgs32_kernel(int W, int n, int ncol, int nup, int ndn, float *w32, zd *logw, const int *alive,
              int *status)
@@ -159,23 +161,29 @@ mgs32_kernel(int W, int n, int ncol, int nup, int ndn, float *w32, zd *logw, con
     __shared__ double red[32];
     const int w = blockIdx.x;
     if (alive && !alive[w]) return;
-    zd *A = (zd *)smem_raw;
+    float2 *A = (float2 *)smem_raw;   // the walker, fp32 (columns stored between FP64 updates)
     float *g = w32 + (size_t)w * 2 * n * ncol;
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
     const long long ws = (long long)n * ncol;
-    for (long long e = tid; e < ws; e += nt) A[e] = make_double2(g[e], g[ws + e]);
+    for (long long e = tid; e < ws; e += nt) A[e] = make_float2(g[e], g[ws + e]);
     __syncthreads();
     const int nmin = nup < ndn ? nup : ndn;
     double logR = 0.0, logRmin = 0.0;
     int bad = 0;
     for (int j = 0; j < ncol; ++j) {
         double s = 0.0;
-        for (int i = tid; i < n; i += nt) { zd v = A[i + (size_t)n * j]; s += v.x * v.x + v.y * v.y; }
+        for (int i = tid; i < n; i += nt) {
+            const float2 v = A[i + (size_t)n * j];
+            s += (double)v.x * v.x + (double)v.y * v.y;
+        }
         s = block_sum(s, red);
         double r = sqrt(s);
         if (r == 0.0) bad = 1;
         double inv = r > 0.0 ? 1.0 / r : 0.0;
-        for (int i = tid; i < n; i += nt) A[i + (size_t)n * j] = zscale(A[i + (size_t)n * j], inv);
+        for (int i = tid; i < n; i += nt) {
+            const float2 v = A[i + (size_t)n * j];
+            A[i + (size_t)n * j] = make_float2((float)(v.x * inv), (float)(v.y * inv));
+        }
         if (tid == 0) {
             double lr = log(r);
             logR += lr;
@@ -184,19 +192,22 @@ mgs32_kernel(int W, int n, int ncol, int nup, int ndn, float *w32, zd *logw, con
         __syncthreads();
         for (int c = j + 1 + wid; c < ncol; c += nw) {
             zd d = make_double2(0.0, 0.0);
-            for (int i = lane; i < n; i += 32) zfma(d, zconj(A[i + (size_t)n * j]), A[i + (size_t)n * c]);
+            for (int i = lane; i < n; i += 32) {
+                const float2 q = A[i + (size_t)n * j], v = A[i + (size_t)n * c];
+                zfma(d, make_double2(q.x, -q.y), make_double2(v.x, v.y));
+            }
             d.x = warp_sum(d.x);
             d.y = warp_sum(d.y);
             for (int i = lane; i < n; i += 32) {
-                zd q = A[i + (size_t)n * j], v = A[i + (size_t)n * c];
-                v.x -= d.x * q.x - d.y * q.y;
-                v.y -= d.x * q.y + d.y * q.x;
-                A[i + (size_t)n * c] = v;
+                const float2 q = A[i + (size_t)n * j], v = A[i + (size_t)n * c];
+                const double vx = v.x - (d.x * q.x - d.y * q.y);
+                const double vy = v.y - (d.x * q.y + d.y * q.x);
+                A[i + (size_t)n * c] = make_float2((float)vx, (float)vy);
             }
         }
         __syncthreads();
     }
-    for (long long e = tid; e < ws; e += nt) { g[e] = (float)A[e].x; g[ws + e] = (float)A[e].y; }
+    for (long long e = tid; e < ws; e += nt) { g[e] = A[e].x; g[ws + e] = A[e].y; }
     if (tid == 0) {
         zd lw = logw[w];
         if (nup == ndn) lw.x += 2.0 * logR;
@@ -885,7 +896,7 @@ int mixed_project_dtk_dtv(afqmc_engine *e)
 int mixed_modify_gm(afqmc_engine *e)
 {
     if (e->kind == KIND_CP) return cp_mixed_modify_gm(e);
-    const size_t bytes = (size_t)e->n * e->ncol * sizeof(zd);
+    const size_t bytes = (size_t)e->n * e->ncol * sizeof(float2);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(mgs32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
