@@ -801,10 +801,15 @@ int afqmc_set_walkers_async(afqmc_engine *e, const double *wf, const double *log
     CUDA_TRY(cudaEventRecord(e->upReady[k], e->upStream));
     // installed on the work stream after everything enqueued before this call
     CUDA_TRY(cudaStreamWaitEvent(e->stream, e->upReady[k], 0));
-    CUDA_TRY(cudaMemcpyAsync(e->wf, e->stgWf[k], sizeof(zd) * e->wsize * e->W, cudaMemcpyDeviceToDevice, e->stream));
     CUDA_TRY(cudaMemcpyAsync(e->logw, e->stgLw[k], sizeof(zd) * e->W, cudaMemcpyDeviceToDevice, e->stream));
     CUDA_TRY(cudaMemcpyAsync(e->alive, e->stgAl[k], sizeof(int) * e->W, cudaMemcpyDeviceToDevice, e->stream));
-    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
+    if (e->precision == AFQMC_MIXED && mixed_can_load_direct(e)) {
+        TRY(mixed_load_direct(e, e->stgWf[k]));
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(e->wf, e->stgWf[k], sizeof(zd) * e->wsize * e->W, cudaMemcpyDeviceToDevice,
+                                 e->stream));
+        if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
+    }
     CUDA_TRY(cudaEventRecord(e->upFree[k], e->stream));
     return AFQMC_OK;
 }

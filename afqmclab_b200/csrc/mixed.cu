@@ -840,6 +840,14 @@ int mixed_sync_from_fp64(afqmc_engine *e)
     return engine_check_launch();
 }
 
+bool mixed_can_load_direct(const afqmc_engine *e) { return e->kind != KIND_CP; }
+
+int mixed_load_direct(afqmc_engine *e, const zd *src)
+{
+    wf_to_f32p_kernel<<<e->W, 256, 0, e->stream>>>(e->W, e->wsize, src, e->mx->wf32, nullptr);
+    return engine_check_launch();
+}
+
 int mixed_status(afqmc_engine *e)
 {
     if (e->kind == KIND_CP) return cp_mixed_status(e);

@@ -13,6 +13,11 @@ int mixed_update_operators(afqmc_engine *e);
 // keep the FP64 walker copy and the reduced-precision working copy in step
 int mixed_sync_to_fp64(afqmc_engine *e);
 int mixed_sync_from_fp64(afqmc_engine *e);
+// The phaseless mixed form can take a population (FP64, reference layout) into
+// its fp32 walkers directly from another device buffer; the FP64 copy is
+// refreshed from the fp32 walkers before any FP64 use.
+bool mixed_can_load_direct(const afqmc_engine *e);
+int mixed_load_direct(afqmc_engine *e, const zd *src);
 int mixed_status(afqmc_engine *e);
 int mixed_pop_control(afqmc_engine *e);
 // overlaps, population-control weights and the log-weight shift, as the
