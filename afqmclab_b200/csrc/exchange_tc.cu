@@ -13,11 +13,9 @@
 // overlaps the MMAs of the next), warps 2..9 epilogue (two warps per TMEM lane
 // quarter, each taking half of the columns).  The epilogue keeps each thread's
 // row of a block in registers and reads the transposed entries from a
-// swizzled shared-memory copy (fp16 pairs when the chunk fits fp16's range,
-// else fp32), so tr(D D) costs one shared store and one load per complex
-// product.  A CTA takes a work item = one A tile (kept in shared
+// swizzled shared-memory copy (bf16 pairs), so tr(D D) costs one shared
+// store and one load per complex product.  A CTA takes a work item = one A tile (kept in shared
 // memory) x a chunk of walker tiles.  All waits are bounded.
-#include <cuda_fp16.h>
 #include <cudaTypedefs.h>
 
 #include <algorithm>
@@ -51,12 +49,13 @@ struct XSmem {
 // at r * 32 + 2 * ((c / 2) ^ (r % 16)) + c % 2, so a row is written with
 // 16-byte stores and a column is read without bank conflicts
 __device__ __forceinline__ int tsw(int r, int c) { return r * 32 + ((((c >> 1) ^ (r & 15)) << 1) | (c & 1)); }
-// the same tile as fp16 pairs (128-byte rows): element (r, c) at
+// the same tile as 4-byte pairs (128-byte rows): element (r, c) at
 // r * 32 + 4 * ((c / 4) ^ (r % 8)) + c % 4
 __device__ __forceinline__ int tsw16(int r, int c) { return r * 32 + ((((c >> 2) ^ (r & 7)) << 2) | (c & 3)); }
-__device__ __forceinline__ uint32_t h2bits(float re, float im)
+// (re, im) as a bf16 pair: re in the low half, im in the high half
+__device__ __forceinline__ uint32_t bf2bits(float re, float im)
 {
-    const __half2 h = __floats2half2_rn(re, im);
+    const __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
     return *(const uint32_t *)&h;
 }
 
@@ -202,24 +201,19 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
 #pragma unroll
                         for (int j = 0; j < 32; ++j) { vr[j] = __uint_as_float(ur[j]); vi[j] = __uint_as_float(ui[j]); }
                     }
-                    // The transposed factor goes through shared memory as fp16
-                    // pairs (half the bytes) when the warp's chunk is inside
-                    // fp16's range, else as fp32 pairs; the register factor
-                    // stays fp32.
-                    float mx = 0.f;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) mx = fmaxf(mx, fmaxf(fabsf(vr[j]), fabsf(vi[j])));
-                    const bool h16 = __all_sync(0xffffffffu, mx < 32768.f);
+                    // The transposed factor goes through shared memory as bf16
+                    // pairs (half the bytes of fp32, fp32's range); the register
+                    // factor and the accumulation stay fp32.
                     float2 acc[32 / NS];
-                    if (h16) {
-                        __half2 *T16 = (__half2 *)T;
+                    {
+                        uint32_t *T16 = (uint32_t *)T;
 #pragma unroll
                         for (int j = 0; j < 32; j += 4) {
                             uint4 pk;
-                            pk.x = h2bits(vr[j], vi[j]);
-                            pk.y = h2bits(vr[j + 1], vi[j + 1]);
-                            pk.z = h2bits(vr[j + 2], vi[j + 2]);
-                            pk.w = h2bits(vr[j + 3], vi[j + 3]);
+                            pk.x = bf2bits(vr[j], vi[j]);
+                            pk.y = bf2bits(vr[j + 1], vi[j + 1]);
+                            pk.z = bf2bits(vr[j + 2], vi[j + 2]);
+                            pk.w = bf2bits(vr[j + 3], vi[j + 3]);
                             *(uint4 *)(T16 + tsw16(lane, j)) = pk;
                         }
                         __syncwarp();
@@ -229,26 +223,10 @@ exchange_tc_kernel(const __grid_constant__ CUtensorMap tmAr, const __grid_consta
 #pragma unroll
                             for (int b = 0; b < NS; ++b) {
                                 const float xr = vr[wb * NS + b], xi = vi[wb * NS + b];
-                                const float2 y = __half22float2(T16[tsw16(rb + b, wb * NS + a)]);
-                                if (b & 1) { sr1 += xr * y.x - xi * y.y; si1 += xr * y.y + xi * y.x; }
-                                else { sr0 += xr * y.x - xi * y.y; si0 += xr * y.y + xi * y.x; }
-                            }
-                            acc[wb] = make_float2(sr0 + sr1, si0 + si1);
-                        }
-                    } else {
-#pragma unroll
-                        for (int j = 0; j < 32; j += 2)
-                            *(float4 *)(T + tsw(lane, j)) = make_float4(vr[j], vi[j], vr[j + 1], vi[j + 1]);
-                        __syncwarp();
-#pragma unroll
-                        for (int wb = 0; wb < 32 / NS; ++wb) {
-                            float sr0 = 0.f, si0 = 0.f, sr1 = 0.f, si1 = 0.f;
-#pragma unroll
-                            for (int b = 0; b < NS; ++b) {
-                                const float xr = vr[wb * NS + b], xi = vi[wb * NS + b];
-                                const float2 y = T[tsw(rb + b, wb * NS + a)];
-                                if (b & 1) { sr1 += xr * y.x - xi * y.y; si1 += xr * y.y + xi * y.x; }
-                                else { sr0 += xr * y.x - xi * y.y; si0 += xr * y.y + xi * y.x; }
+                                const uint32_t u = T16[tsw16(rb + b, wb * NS + a)];
+                                const float yx = __uint_as_float(u << 16), yy = __uint_as_float(u & 0xffff0000u);
+                                if (b & 1) { sr1 += xr * yx - xi * yy; si1 += xr * yy + xi * yx; }
+                                else { sr0 += xr * yx - xi * yy; si0 += xr * yy + xi * yx; }
                             }
                             acc[wb] = make_float2(sr0 + sr1, si0 + si1);
                         }
