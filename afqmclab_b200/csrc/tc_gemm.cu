@@ -1,4 +1,9 @@
-// tcgen05 BF16 GEMM: one 128 x BN output tile per CTA, warp-specialised.
+// tcgen05 BF16 GEMM in two forms, both warp-specialised:
+//   - tc_gemm_t_kernel (large outputs, at least one tile per SM): persistent,
+//     the product formed transposed so a TMEM lane holds an output column,
+//     double-buffered accumulators, 16-byte column stores;
+//   - tc_gemm_kernel (small outputs): one 128 x BN output tile per CTA.
+// In the second form:
 //   warp 0 lane 0 : TMA producer (A 128x64, B BNx64 per stage, 128B swizzle)
 //   warp 1        : TMEM allocation; lane 0 issues the UMMAs and commits
 //   warps 2..5    : epilogue, TMEM -> registers -> global (coalesced along m)
