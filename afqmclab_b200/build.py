@@ -7,7 +7,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libafqmc_b200.so")
-SOURCES = ["engine.cu", "zgemm.cu", "walker_kernels.cu", "mixed.cu", "tc_gemm.cu", "exchange_tc.cu", "noalloc.cu", "adjoint.cu", "cp_mixed.cu", "overlap_tc.cu", "theta_tc.cu"]
+SOURCES = ["engine.cu", "zgemm.cu", "walker_kernels.cu", "mixed.cu", "tc_gemm.cu", "exchange_tc.cu", "noalloc.cu", "adjoint.cu", "cp_mixed.cu", "overlap_tc.cu", "theta_tc.cu", "exchange_gemm.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

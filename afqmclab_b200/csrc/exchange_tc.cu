@@ -45,12 +45,9 @@ struct XSmem {
     }
 };
 
-// swizzled 32 x 32 float2 tile, swizzled in 16-byte pairs: element (r, c)
-// at r * 32 + 2 * ((c / 2) ^ (r % 16)) + c % 2, so a row is written with
+// swizzled 32 x 32 tile of 4-byte pairs (128-byte rows): element (r, c) at
+// r * 32 + 4 * ((c / 4) ^ (r % 8)) + c % 4, so a row is written with
 // 16-byte stores and a column is read without bank conflicts
-__device__ __forceinline__ int tsw(int r, int c) { return r * 32 + ((((c >> 1) ^ (r & 15)) << 1) | (c & 1)); }
-// the same tile as 4-byte pairs (128-byte rows): element (r, c) at
-// r * 32 + 4 * ((c / 4) ^ (r % 8)) + c % 4
 __device__ __forceinline__ int tsw16(int r, int c) { return r * 32 + ((((c >> 2) ^ (r & 7)) << 2) | (c & 3)); }
 // (re, im) as a bf16 pair: re in the low half, im in the high half
 __device__ __forceinline__ uint32_t bf2bits(float re, float im)

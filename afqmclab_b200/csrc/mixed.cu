@@ -19,6 +19,7 @@
 #include "engine_internal.cuh"
 #include "mixed.cuh"
 #include "cp_mixed.cuh"
+#include "exchange_gemm.cuh"
 #include "overlap_tc.cuh"
 #include "theta_tc.cuh"
 #include "tc_common.cuh"
@@ -33,6 +34,11 @@ struct MixedState {
     __nv_bfloat16 *A2r[2] = {nullptr, nullptr}, *A2i[2] = {nullptr, nullptr};
     bool realA = false;   // every A_g has a zero imaginary part (real trial, real Cholesky vectors)
     zd *ex2 = nullptr;
+    // exchange as GEMMs (real A): per-block V, scratch, per-walker sum over g
+    bool exGemm = false;
+    ExGemmBlock exg[2];
+    ExGemmScratch exs;
+    zd *exTot = nullptr;
     float *Ohi[2] = {nullptr, nullptr}, *Olo[2] = {nullptr, nullptr};   // overlap operators
     bool ovStacked = false;   // Ohi[0]/Olo[0] hold both blocks' operators
     float *Sinv32 = nullptr;   // S^{-1} as fp32 planes [re | im] per block slot
@@ -732,7 +738,7 @@ int mixed_create(afqmc_engine *e)
     MTRY(engine_dalloc(e, &m->ex2, (size_t)G * W));
     for (int b = 0; b < e->bl.nblk; ++b) {
         const int Ns = e->bl.Ns[b];
-        if (Ns == 0 || !exchange_tc_supported(n, Ns)) continue;
+        if (Ns == 0 || !(exchange_tc_supported(n, Ns) || exchange_gemm_supported(n, Ns, W, G))) continue;
         MTRY(engine_dalloc(e, (unsigned short **)&m->A2r[b], (size_t)G * Ns * n));
         MTRY(engine_dalloc(e, (unsigned short **)&m->A2i[b], (size_t)G * Ns * n));
         build_a2_kernel<<<1184, 256, 0, e->stream>>>(G, Ns, n, Ktot, e->bl.tOff[b], e->Aall, m->A2r[b],
@@ -747,6 +753,23 @@ int mixed_create(afqmc_engine *e)
         MTRY(cuda_check(cudaStreamSynchronize(e->stream), "sync"));
         MTRY(cuda_check(cudaMemsetAsync(m->err, 0, sizeof(int), e->stream), "memset"));
         m->realA = (h == 0);
+    }
+    // with real A the exchange runs as dense GEMMs over K = Ns n
+    if (m->realA) {
+        bool ok = true;
+        long long Kmax = 0;
+        for (int b = 0; b < e->bl.nblk; ++b) {
+            if (e->bl.Ns[b] == 0) continue;
+            ok = ok && exchange_gemm_supported(n, e->bl.Ns[b], W, G);
+            Kmax = std::max(Kmax, (long long)n * e->bl.Ns[b]);
+        }
+        if (ok && Kmax > 0) {
+            for (int b = 0; b < e->bl.nblk; ++b)
+                if (e->bl.Ns[b] > 0) MTRY(exchange_gemm_build(e, b, m->exg[b]));
+            MTRY(exchange_gemm_alloc(e, Kmax, m->exs));
+            MTRY(engine_dalloc(e, &m->exTot, (size_t)W));
+            m->exGemm = true;
+        }
     }
     build_abig_kernel<<<1184, 256, 0, e->stream>>>(G, Ktot, n, e->bl, e->Aall, m->Abig);
     build_lt_kernel<<<1184, 256, 0, e->stream>>>((long long)n * n, G, e->chol, m->Lt);
@@ -937,12 +960,25 @@ int mixed_pop_control(afqmc_engine *e)
     return engine_check_launch();
 }
 
-// Exchange term of the mixed estimator: tcgen05 kernel per spin block
-// (bf16 operands: A2 planes, Theta), FP64 CUDA-core kernel for block widths
-// that do not divide 32.
+// Exchange term of the mixed estimator.  Real A: quadratic forms as dense
+// GEMMs (exchange_gemm.cu; per-walker sum over g and the den-weighted
+// per-vector sums, both written here).  Complex A: tcgen05 kernel per spin
+// block (bf16 operands: A2 planes, Theta) writing ex[g, w], FP64 CUDA-core
+// kernel for block widths that do not divide 32.
 int mixed_exchange(afqmc_engine *e)
 {
     MixedState *m = e->mx;
+    if (m->exGemm) {
+        // exTot[w] = sum over blocks and g of ex; exNum[g] += sum_w den_w ex[g, w]
+        bool first = true;
+        for (int b = 0; b < e->bl.nblk; ++b) {
+            if (e->bl.Ns[b] == 0) continue;
+            MTRY(exchange_gemm_run(e, m->exg[b], m->A2r[b], m->Theta, m->exs, !first, m->exTot, e->exNum,
+                                   m->err));
+            first = false;
+        }
+        return AFQMC_OK;
+    }
     bool allTc = true;
     for (int b = 0; b < e->bl.nblk; ++b)
         if (e->bl.Ns[b] > 0 && !exchange_tc_supported(e->n, e->bl.Ns[b])) allTc = false;
@@ -999,9 +1035,9 @@ int mixed_add_measurement(afqmc_engine *e)
     {
         PHASE(AFQMC_PH_MEASURE);
         launch_pl_energy(W, e->G, e->Ktot, m->wfDaggerTm, e->thetaT, e->xbar, e->ex, e->alive,
-                         e->logov, e->eloc, e->den, e->parts, s);
+                         e->logov, e->eloc, e->den, e->parts, s, m->exGemm ? m->exTot : nullptr);
         launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 1, e->acc, e->G, e->xbar,
-                              e->ex, e->bgNum, e->exNum, s);
+                              m->exGemm ? nullptr : e->ex, e->bgNum, e->exNum, s);
     }
     return engine_check_launch();
 }

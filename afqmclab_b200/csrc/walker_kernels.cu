@@ -1458,8 +1458,8 @@ pl_exchange_kernel(int W, int n, int G, Blocks bl, const zd *Aall, long long Kto
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256)
 pl_energy_kernel(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
-                 const zd *xbar, const zd *ex, const int *alive, const zd *logov, zd *eloc, zd *den,
-                 zd *tloc)
+                 const zd *xbar, const zd *ex, const zd *exTot, const int *alive, const zd *logov,
+                 zd *eloc, zd *den, zd *tloc)
 {
     __shared__ double red[32];
     const int w = blockIdx.x;
@@ -1470,11 +1470,12 @@ pl_energy_kernel(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *th
     for (int g = threadIdx.x; g < G; g += blockDim.x) {
         zd x = xbar[g + (size_t)G * w];
         zd t = zmul(x, x);
-        H = zadd(H, zsub(t, ex[g + (size_t)G * w]));
+        H = zadd(H, exTot ? t : zsub(t, ex[g + (size_t)G * w]));
     }
     T = block_zsum(T, red);
     H = block_zsum(H, red);
     if (threadIdx.x == 0) {
+        if (exTot) H = zsub(H, exTot[w]);
         zd e = zadd(zscale(H, 0.5), T);
         eloc[w] = e;
         den[w] = zexp(logov[w]);
@@ -1525,13 +1526,13 @@ measure_reduce_kernel(int W, const int *alive, const zd *eloc, const zd *den, co
         if (!alive[w]) continue;
         zd d = den[w];
         sb = zadd(sb, zmul(xbar[g + (size_t)G * w], d));
-        se = zadd(se, zmul(ex[g + (size_t)G * w], d));
+        if (ex) se = zadd(se, zmul(ex[g + (size_t)G * w], d));
     }
     sb = block_zsum_fixed(sb, red);
     se = block_zsum_fixed(se, red);
     if (tid == 0) {
         bgNum[g] = zadd(bgNum[g], sb);
-        exNum[g] = zadd(exNum[g], se);
+        if (ex) exNum[g] = zadd(exNum[g], se);
     }
 }
 
@@ -1786,11 +1787,11 @@ int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, lo
 
 void launch_pl_energy(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
                       const zd *xbar, const zd *ex, const int *alive, const zd *logov, zd *eloc,
-                      zd *den, zd *tloc, cudaStream_t s)
+                      zd *den, zd *tloc, cudaStream_t s, const zd *exTot)
 {
     g_launch_count++;
-    pl_energy_kernel<<<W, 256, 0, s>>>(W, G, Ktot, wfDaggerT, thetaT, xbar, ex, alive, logov, eloc,
-                                        den, tloc);
+    pl_energy_kernel<<<W, 256, 0, s>>>(W, G, Ktot, wfDaggerT, thetaT, xbar, ex, exTot, alive, logov,
+                                        eloc, den, tloc);
 }
 
 void launch_measure_reduce(int W, const int *alive, const zd *eloc, const zd *den, const zd *parts,

@@ -93,10 +93,12 @@ int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, lo
                        int thetaLayout = 0);
 void launch_pl_energy(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
                       const zd *xbar, const zd *ex, const int *alive, const zd *logov, zd *eloc,
-                      zd *den, zd *tloc, cudaStream_t s);
+                      zd *den, zd *tloc, cudaStream_t s, const zd *exTot = nullptr);
+// (exTot: the per-walker sum over g of ex, used instead of ex when given)
 // Sums over alive walkers into device accumulators:
 // acc[0] += sum den, acc[1] += sum eloc*den, acc[2+k] += sum parts[w*nparts+k]*den;
-// with xbar/ex (phaseless): bgNum[g] += sum xbar*den, exNum[g] += sum ex*den.
+// with xbar/ex (phaseless): bgNum[g] += sum xbar*den, exNum[g] += sum ex*den
+// (exNum untouched when ex is null).
 void launch_measure_reduce(int W, const int *alive, const zd *eloc, const zd *den, const zd *parts,
                            int nparts, zd *acc, int G, const zd *xbar, const zd *ex, zd *bgNum,
                            zd *exNum, cudaStream_t s);
