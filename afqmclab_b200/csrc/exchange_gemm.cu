@@ -112,26 +112,6 @@ ex_transpose_kernel(int W, long long K, long long Ktot, long long tOff, const __
     }
 }
 
-// Rt(p K + j + n b, i + n a) = M_p(i + n b, j + n a) for M_p column-major
-// (element (q1, q2) at q1 + K q2); runs of n along i are moved whole.
-__global__ void ex_permute_kernel(int n, int Ns, const __nv_bfloat16 *Mr, const __nv_bfloat16 *Mi,
-                                  __nv_bfloat16 *Rt)
-{
-    const long long K = (long long)n * Ns;
-    const long long runs = 2 * K * Ns;   // (p, b, j, a)
-    for (long long rid = blockIdx.x; rid < runs; rid += gridDim.x) {
-        const int a = (int)(rid % Ns);
-        long long t = rid / Ns;
-        const int j = (int)(t % n);
-        t /= n;
-        const int b = (int)(t % Ns);
-        const int p = (int)(t / Ns);
-        const __nv_bfloat16 *src = (p ? Mi : Mr) + (size_t)(n * b) + (size_t)K * (j + (long long)n * a);
-        __nv_bfloat16 *dst = Rt + (size_t)(p * K + j + (long long)n * b) * K + (size_t)n * a;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
-    }
-}
-
 // exNum[g] += exp(shift) sum_q x_g(q) (Y_g(q) + i Y_g(K + q)), Y_g = row g (2K)
 __global__ void __launch_bounds__(256)
 ex_rowdot_kernel(long long K, const __nv_bfloat16 *X, const float *Y, const double *shift, zd *exNum)
@@ -182,10 +162,11 @@ ex_dot_kernel(int W, long long K, long long Ktot, long long tOff, const __nv_bfl
 
 bool exchange_gemm_supported(int n, int Ns, int W, int G)
 {
-    // operand pitches (K, 2W, Ktot) and offsets must be 16-byte multiples for
-    // the TMA maps; K x K scratch bounded to 2^28 elements
+    // operand pitches (K, 2W, Ktot) and offsets 16-byte multiples for the TMA
+    // maps; the exchanged store of M wants whole 32-orbital runs and K a
+    // multiple of the 256-row tile; K x K scratch bounded to 2^28 elements
     const long long K = (long long)n * Ns;
-    return Ns > 0 && n % 8 == 0 && W % 4 == 0 && G > 0 && K * K <= (1LL << 28);
+    return Ns > 0 && n % 32 == 0 && K % 256 == 0 && W % 4 == 0 && G > 0 && K * K <= (1LL << 28);
 }
 
 int exchange_gemm_build(afqmc_engine *e, int b, ExGemmBlock &blk)
@@ -220,10 +201,7 @@ int exchange_gemm_alloc(afqmc_engine *e, long long Kmax, ExGemmScratch &s)
 {
     const long long W2 = 2LL * e->W;
     int r = engine_dalloc(e, (unsigned short **)&s.Bt, (size_t)(Kmax * W2));
-    if (!r) r = engine_dalloc(e, (unsigned short **)&s.Ar, (size_t)(Kmax * W2));
-    if (!r) r = engine_dalloc(e, (unsigned short **)&s.Ai, (size_t)(Kmax * W2));
-    if (!r) r = engine_dalloc(e, (unsigned short **)&s.Mr, (size_t)(Kmax * Kmax));
-    if (!r) r = engine_dalloc(e, (unsigned short **)&s.Mi, (size_t)(Kmax * Kmax));
+    if (!r) r = engine_dalloc(e, (unsigned short **)&s.Av, (size_t)(2 * Kmax * W2));
     if (!r) r = engine_dalloc(e, (unsigned short **)&s.Rt, (size_t)(2 * Kmax * Kmax));
     if (!r) r = engine_dalloc(e, &s.Y, (size_t)(e->G * 2 * Kmax));
     if (!r) r = engine_dalloc(e, &s.Z, (size_t)(Kmax * W2));
@@ -236,7 +214,7 @@ int exchange_gemm_run(afqmc_engine *e, const ExGemmBlock &blk, const __nv_bfloat
                       zd *exNum, int *err)
 {
     cudaStream_t st = e->stream;
-    const int W = e->W, G = e->G, n = e->n, Ns = blk.Ns;
+    const int W = e->W, G = e->G, n = e->n;
     const long long K = blk.K, W2 = 2LL * W;
     // energy: Z = V U^T (column 2w + p = plane p of walker w), exTot_w (+)= u_w^T Z_w
     {
@@ -253,22 +231,24 @@ int exchange_gemm_run(afqmc_engine *e, const ExGemmBlock &blk, const __nv_bfloat
     // per vector: M = sum_w den_w u_w u_w^T, Rt = M with b and a exchanged,
     // Y_g = Rt x_g, exNum_g += x_g^T Y_g
     {
-        g_launch_count += 2;
-        ex_shift_kernel<<<1, 256, 0, st>>>(W, e->logov, e->alive, s.shift);
+        // the shift depends only on the walkers: once per measurement
+        if (!accumulate) {
+            g_launch_count++;
+            ex_shift_kernel<<<1, 256, 0, st>>>(W, e->logov, e->alive, s.shift);
+        }
+        g_launch_count++;
         dim3 tg((unsigned)((K + 31) / 32), (unsigned)((W + 31) / 32));
         ex_transpose_kernel<<<tg, 256, 0, st>>>(W, K, e->Ktot, blk.tOff, Theta, e->logov, e->alive, s.shift,
-                                                s.Bt, s.Ar, s.Ai);
+                                                s.Bt, s.Av, s.Av + K * W2);
+        // [M_re; M_im] = [Ar; Ai] Bt^T, stored exchanged as Rt
         TcGemmArgs a;
-        a.M = (int)K; a.N = (int)K; a.K = (int)W2;
-        a.A = s.Ar; a.lda = W2;
+        a.M = (int)(2 * K); a.N = (int)K; a.K = (int)W2;
+        a.A = s.Av; a.lda = W2;
         a.B = s.Bt; a.ldb = W2;
-        a.C = s.Mr; a.ldc = K; a.outType = TC_OUT_BF16; a.err = err;
+        a.C = s.Rt; a.outType = TC_OUT_BF16; a.err = err;
+        a.permN = n; a.permK = K;
         int r = tc_gemm_bf16(a, st);
-        a.A = s.Ai; a.C = s.Mi;
-        if (!r) r = tc_gemm_bf16(a, st);
         if (r) return engine_fail(AFQMC_ERR_CUDA, "exchange M gemm: " + std::to_string(r));
-        g_launch_count++;
-        ex_permute_kernel<<<4736, 128, 0, st>>>(n, Ns, s.Mr, s.Mi, s.Rt);
         TcGemmArgs y;
         y.M = (int)(2 * K); y.N = G; y.K = (int)K;
         y.A = s.Rt; y.lda = K;

@@ -15,9 +15,9 @@ struct ExGemmBlock {
 };
 
 struct ExGemmScratch {
-    __nv_bfloat16 *Bt = nullptr, *Ar = nullptr, *Ai = nullptr;   // K x 2W each
-    __nv_bfloat16 *Mr = nullptr, *Mi = nullptr;                  // K x K each
-    __nv_bfloat16 *Rt = nullptr;                                 // 2K x K
+    __nv_bfloat16 *Bt = nullptr;   // K x 2W
+    __nv_bfloat16 *Av = nullptr;   // [Ar; Ai], 2K x 2W
+    __nv_bfloat16 *Rt = nullptr;   // 2K x K
     float *Y = nullptr;                                          // 2K per vector
     float *Z = nullptr;                                          // K x 2W
     double *shift = nullptr;   // max Re logov of the alive walkers

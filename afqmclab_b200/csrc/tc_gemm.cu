@@ -156,7 +156,7 @@ template <int OUT>
 __global__ void __launch_bounds__(TT_THREADS, 1)
 tc_gemm_t_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, int M,
                  int N, int K, int kSplit, int splits, void *C, long long ldc, long long splitStride,
-                 float alpha, int *err)
+                 float alpha, int *err, int permN, long long permK)
 {
     constexpr uint32_t IDESC = idesc_bf16(TT_BN, TT_BM);
     extern __shared__ uint8_t smem_raw[];
@@ -264,6 +264,15 @@ tc_gemm_t_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
                 if (n < N) {
                     if (OUT == TC_OUT_BF16) {
                         __nv_bfloat16 *dst = (__nv_bfloat16 *)C + colOff + mb;
+                        if (permN > 0) {
+                            // exchanged store: (p K + i + n b, j + n a) -> row p K + j + n b,
+                            // column i + n a of a K-pitched output (32 rows never cross b or p)
+                            const int p = mb >= permK ? 1 : 0;
+                            const long long r = mb - p * permK;
+                            const long long i0 = r % permN, b = r / permN;
+                            const long long j = n % permN, a = n / permN;
+                            dst = (__nv_bfloat16 *)C + ((p * permK + j + permN * b) * permK + permN * a + i0);
+                        }
 #pragma unroll
                         for (int j = 0; j < 32; j += 8) {
                             if (mb + j + 8 <= M) {
@@ -364,7 +373,7 @@ int launch_t(const TcGemmArgs &a, cudaStream_t s)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = (int)std::min<long long>(tiles, sms);
     tc_gemm_t_kernel<OUT><<<grid, TT_THREADS, TT_SMEM, s>>>(ma, mb, a.M, a.N, a.K, kSplit, splits, a.C, a.ldc,
-                                                            a.splitStride, a.alpha, a.err);
+                                                            a.splitStride, a.alpha, a.err, a.permN, a.permK);
     return (int)cudaGetLastError();
 }
 
@@ -390,6 +399,14 @@ int tc_gemm_bf16(const TcGemmArgs &a, cudaStream_t s)
 {
     g_launch_count++;
     if (a.M <= 0 || a.N <= 0 || a.K <= 0) return 0;
+    if (a.permN > 0) {
+        // exchanged bf16 store of the persistent form: M = 2 permK, N = permK,
+        // 32-row runs inside one orbital run, 16-byte aligned destinations
+        if (a.outType != TC_OUT_BF16 || a.splits > 1 || a.permN % 32 != 0 || a.permK % TT_BM != 0 ||
+            a.permK % a.permN != 0 || a.M != 2 * a.permK || a.N != a.permK || ((uintptr_t)a.C % 16) != 0)
+            return (int)cudaErrorInvalidValue;
+        return launch_t<TC_OUT_BF16>(a, s);
+    }
     // large outputs: the persistent transposed form, when its 16-byte column
     // stores are aligned
     {

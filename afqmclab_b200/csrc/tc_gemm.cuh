@@ -18,6 +18,10 @@ struct TcGemmArgs {
     int splits = 1; long long splitStride = 0;
     float alpha = 1.0f;
     int *err = nullptr;        // set to a non-zero code when a wait times out
+    // exchanged store (bf16, persistent form only): with permN = n > 0 and
+    // M = 2 permK, N = permK, element (p permK + i + n b, j + n a) goes to
+    // C[(p permK + j + n b) permK + i + n a] (ldc unused)
+    int permN = 0; long long permK = 0;
 };
 
 // Returns 0 on success, a cudaError_t / CUresult value otherwise.
