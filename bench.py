@@ -127,15 +127,19 @@ def phase_flops(c, m, taylor_avg):
         "overlap": 8.0 * (nup * nup + ndn * ndn) * n * W,
         "onebody": 8.0 * n * n * max(nup, ndn) * W,
     }
+    # with real A the exchange runs as three GEMMs per spin block of
+    # Kb = Ns n: Z = V U^T (2 Kb^2 2W), [M_re; M_im] = [Ar; Ai] Bt^T
+    # (2 2Kb Kb 2W) and Y = Rt X^T (2 2Kb G Kb); the flops counted are those
+    # executed, fewer than the blockwise tr(DD) count above
+    if real_a and n % 32 == 0 and W % 4 == 0 and all((ns * n) % 256 == 0 for ns in (nup, ndn) if ns):
+        f["exchange"] = sum((ns * n) ** 2 * (12.0 * W + 4.0 * G) for ns in (nup, ndn) if ns)
     return f
 
 
 # DRAM bytes (read + write) per phase occurrence of the dominant kernel, from
 # one ncu capture of the same workload (dram__bytes_read.sum +
 # dram__bytes_write.sum, summed over the phase's launches).
-NCU_TRAFFIC = {
-    ("molecule128", "mixed", "exchange"): (2 * (38.83e6 + 2.76e6), "2 exchange_tc_kernel launches (one per spin)"),
-}
+NCU_TRAFFIC = {}
 
 
 def cp_phase_model(m, W, precision):
