@@ -112,9 +112,10 @@ ex_transpose_kernel(int W, long long K, long long Ktot, long long tOff, const __
     }
 }
 
-// exNum[g] += exp(shift) sum_q x_g(q) (Y_g(q) + i Y_g(K + q)), Y_g = row g (2K)
+// exNum[g] += mult exp(shift) sum_q x_g(q) (Y_g(q) + i Y_g(K + q)), Y_g = row g (2K)
 __global__ void __launch_bounds__(256)
-ex_rowdot_kernel(long long K, const __nv_bfloat16 *X, const float *Y, const double *shift, zd *exNum)
+ex_rowdot_kernel(long long K, const __nv_bfloat16 *X, const float *Y, const double *shift, double mult,
+                 zd *exNum)
 {
     __shared__ double red[32];
     const int g = blockIdx.x;
@@ -129,15 +130,15 @@ ex_rowdot_kernel(long long K, const __nv_bfloat16 *X, const float *Y, const doub
     sr = block_sum(sr, red);
     si = block_sum(si, red);
     if (threadIdx.x == 0) {
-        const double f = exp(shift[0]);
+        const double f = mult * exp(shift[0]);
         exNum[g] = zadd(exNum[g], make_double2(f * sr, f * si));
     }
 }
 
-// exTot[w] (+)= sum_q u_w(q) (Z_w,re(q) + i Z_w,im(q)), Z column-major (ld K)
+// exTot[w] (+)= mult sum_q u_w(q) (Z_w,re(q) + i Z_w,im(q)), Z column-major (ld K)
 __global__ void __launch_bounds__(256)
 ex_dot_kernel(int W, long long K, long long Ktot, long long tOff, const __nv_bfloat16 *Theta, const float *Z,
-              int accumulate, zd *exTot)
+              int accumulate, double mult, zd *exTot)
 {
     __shared__ double red[32];
     const int w = blockIdx.x;
@@ -153,7 +154,7 @@ ex_dot_kernel(int W, long long K, long long Ktot, long long tOff, const __nv_bfl
     sr = block_sum(sr, red);
     si = block_sum(si, red);
     if (threadIdx.x == 0) {
-        const zd v = make_double2(sr, si);
+        const zd v = make_double2(mult * sr, mult * si);
         exTot[w] = accumulate ? zadd(exTot[w], v) : v;
     }
 }
@@ -210,8 +211,8 @@ int exchange_gemm_alloc(afqmc_engine *e, long long Kmax, ExGemmScratch &s)
 }
 
 int exchange_gemm_run(afqmc_engine *e, const ExGemmBlock &blk, const __nv_bfloat16 *A2r,
-                      const __nv_bfloat16 *Theta, const ExGemmScratch &s, bool accumulate, zd *exTot,
-                      zd *exNum, int *err)
+                      const __nv_bfloat16 *Theta, const ExGemmScratch &s, bool accumulate, int mult,
+                      zd *exTot, zd *exNum, int *err)
 {
     cudaStream_t st = e->stream;
     const int W = e->W, G = e->G, n = e->n;
@@ -226,7 +227,8 @@ int exchange_gemm_run(afqmc_engine *e, const ExGemmBlock &blk, const __nv_bfloat
         int r = tc_gemm_bf16(a, st);
         if (r) return engine_fail(AFQMC_ERR_CUDA, "exchange Z gemm: " + std::to_string(r));
         g_launch_count++;
-        ex_dot_kernel<<<W, 256, 0, st>>>(W, K, e->Ktot, blk.tOff, Theta, s.Z, accumulate ? 1 : 0, exTot);
+        ex_dot_kernel<<<W, 256, 0, st>>>(W, K, e->Ktot, blk.tOff, Theta, s.Z, accumulate ? 1 : 0, (double)mult,
+                                         exTot);
     }
     // per vector: M = sum_w den_w u_w u_w^T, Rt = M with b and a exchanged,
     // Y_g = Rt x_g, exNum_g += x_g^T Y_g
@@ -257,7 +259,7 @@ int exchange_gemm_run(afqmc_engine *e, const ExGemmBlock &blk, const __nv_bfloat
         r = tc_gemm_bf16(y, st);
         if (r) return engine_fail(AFQMC_ERR_CUDA, "exchange Y gemm: " + std::to_string(r));
         g_launch_count++;
-        ex_rowdot_kernel<<<G, 256, 0, st>>>(K, A2r, s.Y, s.shift, exNum);
+        ex_rowdot_kernel<<<G, 256, 0, st>>>(K, A2r, s.Y, s.shift, (double)mult, exNum);
     }
     return engine_check_launch();
 }

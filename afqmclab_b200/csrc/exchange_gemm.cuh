@@ -29,8 +29,9 @@ int exchange_gemm_build(afqmc_engine *e, int b, ExGemmBlock &blk);
 int exchange_gemm_alloc(afqmc_engine *e, long long Kmax, ExGemmScratch &s);
 // exTot[w] (= or +=) sum_g ex[g, w] of this block; exNum[g] += sum_w den_w ex[g, w]
 // (den_w = exp(logov_w) of the alive walkers); A2r = the block's real A rows
-// (g, a) x i, Theta = the bf16 theta planes of the population.  Launches on
-// the engine's stream.
+// (g, a) x i, Theta = the bf16 theta planes of the population; both sums
+// are counted `mult` times (a block standing for two identical spin blocks).
+// Launches on the engine's stream.
 int exchange_gemm_run(afqmc_engine *e, const ExGemmBlock &blk, const __nv_bfloat16 *A2r,
-                      const __nv_bfloat16 *Theta, const ExGemmScratch &s, bool accumulate, zd *exTot,
-                      zd *exNum, int *err);
+                      const __nv_bfloat16 *Theta, const ExGemmScratch &s, bool accumulate, int mult,
+                      zd *exTot, zd *exNum, int *err);

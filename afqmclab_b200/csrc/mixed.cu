@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "engine_internal.cuh"
@@ -39,6 +40,12 @@ struct MixedState {
     ExGemmBlock exg[2];
     ExGemmScratch exs;
     zd *exTot = nullptr;
+    // spin-restricted: the two spin blocks have the same trial and (nup = ndn)
+    // the same walker columns, so every per-spin quantity of block 1 equals
+    // block 0's; bl1 lists block 0 alone with log-det multiplicity 2 and the
+    // force, exchange and kinetic sums of block 0 are doubled
+    bool restricted = false;
+    Blocks bl1{};
     float *Ohi[2] = {nullptr, nullptr}, *Olo[2] = {nullptr, nullptr};   // overlap operators
     bool ovStacked = false;   // Ohi[0]/Olo[0] hold both blocks' operators
     float *Sinv32 = nullptr;   // S^{-1} as fp32 planes [re | im] per block slot
@@ -622,16 +629,20 @@ int tc(afqmc_engine *e, TcGemmArgs a)
     return AFQMC_OK;
 }
 
+// the spin blocks the mixed form computes (block 0 alone when restricted)
+const Blocks &mbl(const afqmc_engine *e) { return e->mx->restricted ? e->mx->bl1 : e->bl; }
+
 // S_b = phiT_b^H phi_b from the fp32 walkers (compensated tf32 tensor-core
 // product, FP64 result); every walker's slot is written
 int overlap32(afqmc_engine *e, const float *w32, const int *mask)
 {
     (void)mask;
     MixedState *m = e->mx;
+    const Blocks &bl = mbl(e);
     int nb = 0, Ns[2];
     long long sOff[2];
-    for (int b = 0; b < e->bl.nblk; ++b)
-        if (e->bl.Ns[b] > 0) { Ns[nb] = e->bl.Ns[b]; sOff[nb] = e->bl.sOff[b]; ++nb; }
+    for (int b = 0; b < bl.nblk; ++b)
+        if (bl.Ns[b] > 0) { Ns[nb] = bl.Ns[b]; sOff[nb] = bl.sOff[b]; ++nb; }
     if (nb == 0) return AFQMC_OK;
     if (m->ovStacked) {
         const int r = overlap_tc_launch(e->stream, e->n, e->ncol, nb, Ns, e->W, m->Ohi[0], m->Olo[0], w32, e->S,
@@ -653,12 +664,13 @@ int overlap32(afqmc_engine *e, const float *w32, const int *mask)
 int theta32(afqmc_engine *e, const float *w32, const int *mask, zd *thetaZ)
 {
     MixedState *m = e->mx;
+    const Blocks &bl = mbl(e);
     int nb = 0, Ns[2];
     long long sOff[2], tOff[2];
-    for (int b = 0; b < e->bl.nblk; ++b)
-        if (e->bl.Ns[b] > 0) { Ns[nb] = e->bl.Ns[b]; sOff[nb] = e->bl.sOff[b]; tOff[nb] = e->bl.tOff[b]; ++nb; }
+    for (int b = 0; b < bl.nblk; ++b)
+        if (bl.Ns[b] > 0) { Ns[nb] = bl.Ns[b]; sOff[nb] = bl.sOff[b]; tOff[nb] = bl.tOff[b]; ++nb; }
     if (nb == 0) return AFQMC_OK;
-    const long long s32 = sinv32_stride(e->bl);
+    const long long s32 = sinv32_stride(bl);
     // both blocks in one pass when they fit, else one pass per block
     const int groups = theta_tc_supported(e->n, nb, Ns, s32) ? 1 : nb;
     for (int gi = 0; gi < groups; ++gi) {
@@ -679,10 +691,12 @@ int force_tc(afqmc_engine *e)
         // real A_g: xbar_re = A theta_re, xbar_im = A theta_im as one real
         // product over the theta planes (column 2w + p = plane p of walker w),
         // which lands in the same layout as the complex form
-        a.M = e->G; a.N = 2 * e->W; a.K = (int)e->Ktot;
+        // (restricted: block 0's columns only, doubled exactly by alpha)
+        a.M = e->G; a.N = 2 * e->W; a.K = (int)(m->restricted ? e->bl.tOff[1] : e->Ktot);
         a.A = m->Abig; a.lda = 2 * e->Ktot;
         a.B = m->Theta; a.ldb = e->Ktot;
         a.C = m->xbarp; a.ldc = e->G;
+        a.alpha = m->restricted ? 2.0f : 1.0f;
     } else {
         a.M = 2 * e->G; a.N = e->W; a.K = (int)(2 * e->Ktot);
         a.A = m->Abig; a.lda = 2 * e->Ktot;
@@ -764,7 +778,22 @@ int mixed_create(afqmc_engine *e)
             Kmax = std::max(Kmax, (long long)n * e->bl.Ns[b]);
         }
         if (ok && Kmax > 0) {
-            for (int b = 0; b < e->bl.nblk; ++b)
+            // spin-restricted when both blocks carry the same trial bit for bit
+            if (e->bl.nblk == 2 && e->nup == e->ndn && e->nup > 0) {
+                std::vector<zd> t0((size_t)n * e->nup), t1((size_t)n * e->ndn);
+                MTRY(cuda_check(cudaMemcpy(t0.data(), e->phiT[0], sizeof(zd) * t0.size(), cudaMemcpyDeviceToHost),
+                                "copy"));
+                MTRY(cuda_check(cudaMemcpy(t1.data(), e->phiT[1], sizeof(zd) * t1.size(), cudaMemcpyDeviceToHost),
+                                "copy"));
+                if (std::memcmp(t0.data(), t1.data(), sizeof(zd) * t0.size()) == 0) {
+                    m->restricted = true;
+                    m->bl1 = e->bl;
+                    m->bl1.nblk = 1;
+                    m->bl1.Ns[1] = 0;
+                    m->bl1.mult = 2;
+                }
+            }
+            for (int b = 0; b < (m->restricted ? 1 : e->bl.nblk); ++b)
                 if (e->bl.Ns[b] > 0) MTRY(exchange_gemm_build(e, b, m->exg[b]));
             MTRY(exchange_gemm_alloc(e, Kmax, m->exs));
             MTRY(engine_dalloc(e, &m->exTot, (size_t)W));
@@ -806,9 +835,10 @@ int mixed_create(afqmc_engine *e)
         int nb = 0, Ns[2];
         std::vector<zd> T[2];
         const zd *Tp[2];
-        for (int b = 0; b < e->bl.nblk; ++b) {
-            if (e->bl.Ns[b] == 0) continue;
-            Ns[nb] = e->bl.Ns[b];
+        const Blocks &bl = mbl(e);
+        for (int b = 0; b < bl.nblk; ++b) {
+            if (bl.Ns[b] == 0) continue;
+            Ns[nb] = bl.Ns[b];
             T[nb].resize((size_t)n * Ns[nb]);
             MTRY(cuda_check(cudaMemcpy(T[nb].data(), e->phiT[b], sizeof(zd) * T[nb].size(), cudaMemcpyDeviceToHost),
                             "copy"));
@@ -889,7 +919,7 @@ int mixed_project_dtk_dtv(afqmc_engine *e)
     { PHASE(AFQMC_PH_OVERLAP); MTRY(overlap32(e, m->wf32, e->alive)); }
     {
         PHASE(AFQMC_PH_LU);
-        launch_lu_logdet_inverse32(W, e->bl, e->S, e->Sinv, m->Sinv32, e->alive, e->logw, make_double2(0, 0),
+        launch_lu_logdet_inverse32(W, mbl(e), e->S, e->Sinv, m->Sinv32, e->alive, e->logw, make_double2(0, 0),
                                    e->logwT, e->logov, e->alive, e->surv, e->logw, nullptr, e->status,
                                    LU_PROJECT, needTheta, s);
         MTRY(engine_check_launch());
@@ -943,7 +973,7 @@ int mixed_pop_weights(afqmc_engine *e)
 {
     if (e->kind == KIND_CP) return cp_mixed_pop_weights(e);
     MTRY(overlap32(e, e->mx->wf32, e->alive));
-    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
+    launch_lu_logdet_inverse(e->W, mbl(e), e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
                              e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
                              LU_POPWEIGHT, false, e->stream);
     return engine_check_launch();
@@ -970,11 +1000,13 @@ int mixed_exchange(afqmc_engine *e)
     MixedState *m = e->mx;
     if (m->exGemm) {
         // exTot[w] = sum over blocks and g of ex; exNum[g] += sum_w den_w ex[g, w]
+        // (restricted: block 0 counted twice)
+        const Blocks &bl = mbl(e);
         bool first = true;
-        for (int b = 0; b < e->bl.nblk; ++b) {
-            if (e->bl.Ns[b] == 0) continue;
-            MTRY(exchange_gemm_run(e, m->exg[b], m->A2r[b], m->Theta, m->exs, !first, m->exTot, e->exNum,
-                                   m->err));
+        for (int b = 0; b < bl.nblk; ++b) {
+            if (bl.Ns[b] == 0) continue;
+            MTRY(exchange_gemm_run(e, m->exg[b], m->A2r[b], m->Theta, m->exs, !first, bl.mult, m->exTot,
+                                   e->exNum, m->err));
             first = false;
         }
         return AFQMC_OK;
@@ -1019,7 +1051,7 @@ int mixed_add_measurement(afqmc_engine *e)
         }
         if (r) return engine_fail(AFQMC_ERR_CUDA, "measurement one-body: " + std::to_string(r));
         MTRY(overlap32(e, m->tmp32, e->alive));
-        launch_lu_logdet_inverse32(W, e->bl, e->S, e->Sinv, m->Sinv32, e->alive, e->logw,
+        launch_lu_logdet_inverse32(W, mbl(e), e->S, e->Sinv, m->Sinv32, e->alive, e->logw,
                                    engine_one_body_logw(e, 1), e->logwT, e->logov, e->alive, nullptr, nullptr,
                                    nullptr, e->status, LU_PLAIN, true, s);
         MTRY(engine_check_launch());
@@ -1035,7 +1067,8 @@ int mixed_add_measurement(afqmc_engine *e)
     {
         PHASE(AFQMC_PH_MEASURE);
         launch_pl_energy(W, e->G, e->Ktot, m->wfDaggerTm, e->thetaT, e->xbar, e->ex, e->alive,
-                         e->logov, e->eloc, e->den, e->parts, s, m->exGemm ? m->exTot : nullptr);
+                         e->logov, e->eloc, e->den, e->parts, s, m->exGemm ? m->exTot : nullptr,
+                         m->restricted ? e->bl.tOff[1] : e->Ktot, mbl(e).mult);
         launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 1, e->acc, e->G, e->xbar,
                               m->exGemm ? nullptr : e->ex, e->bgNum, e->exNum, s);
     }

@@ -157,6 +157,7 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
 
     if (tid == 0) {
         zd lwR = zadd(logwAdd, logw[w]);
+        if (bl.mult == 2) logdetSum = zadd(logdetSum, logdetSum);
         zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
         logov[w] = lo;
         if (sFlag && status) atomicOr(status + w, (int)ST_SINGULAR);
@@ -395,6 +396,7 @@ gj_cta_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const 
     if (singular) logdetSum = make_double2(-1e300, 0.0);
     if (tid == 0) {
         const zd lwR = zadd(logwAdd, logw[w]);
+        if (bl.mult == 2) logdetSum = zadd(logdetSum, logdetSum);
         const zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
         logov[w] = lo;
         if (singular && status) atomicOr(status + w, (int)ST_SINGULAR);
@@ -550,6 +552,7 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
     if (singular) logdetSum = make_double2(-1e300, 0.0);
     if (lane == 0) {
         zd lwR = zadd(logwAdd, logw[w]);
+        if (bl.mult == 2) logdetSum = zadd(logdetSum, logdetSum);
         zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
         logov[w] = lo;
         if (singular && status) atomicOr(status + w, (int)ST_SINGULAR);
@@ -749,6 +752,7 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long 
     }
     if (singular) logdetSum = make_double2(-1e300, 0.0);
     const zd lwR = zadd(logwAdd, logw[w]);
+    if (bl.mult == 2) logdetSum = zadd(logdetSum, logdetSum);
     const zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
     logov[w] = lo;
     if (singular && status) atomicOr(status + w, (int)ST_SINGULAR);
@@ -1459,14 +1463,14 @@ pl_exchange_kernel(int W, int n, int G, Blocks bl, const zd *Aall, long long Kto
 __global__ void __launch_bounds__(256)
 pl_energy_kernel(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
                  const zd *xbar, const zd *ex, const zd *exTot, const int *alive, const zd *logov,
-                 zd *eloc, zd *den, zd *tloc)
+                 zd *eloc, zd *den, zd *tloc, long long tLen, int tMult)
 {
     __shared__ double red[32];
     const int w = blockIdx.x;
     if (!alive[w]) return;
     const zd *th = thetaT + (size_t)w * Ktot;
     zd T = make_double2(0, 0), H = make_double2(0, 0);
-    for (long long e = threadIdx.x; e < Ktot; e += blockDim.x) zfma(T, wfDaggerT[e], th[e]);
+    for (long long e = threadIdx.x; e < tLen; e += blockDim.x) zfma(T, wfDaggerT[e], th[e]);
     for (int g = threadIdx.x; g < G; g += blockDim.x) {
         zd x = xbar[g + (size_t)G * w];
         zd t = zmul(x, x);
@@ -1475,6 +1479,7 @@ pl_energy_kernel(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *th
     T = block_zsum(T, red);
     H = block_zsum(H, red);
     if (threadIdx.x == 0) {
+        if (tMult == 2) T = zadd(T, T);
         if (exTot) H = zsub(H, exTot[w]);
         zd e = zadd(zscale(H, 0.5), T);
         eloc[w] = e;
@@ -1787,11 +1792,11 @@ int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, lo
 
 void launch_pl_energy(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
                       const zd *xbar, const zd *ex, const int *alive, const zd *logov, zd *eloc,
-                      zd *den, zd *tloc, cudaStream_t s, const zd *exTot)
+                      zd *den, zd *tloc, cudaStream_t s, const zd *exTot, long long tLen, int tMult)
 {
     g_launch_count++;
     pl_energy_kernel<<<W, 256, 0, s>>>(W, G, Ktot, wfDaggerT, thetaT, xbar, ex, exTot, alive, logov,
-                                        eloc, den, tloc);
+                                        eloc, den, tloc, tLen < 0 ? Ktot : tLen, tMult);
 }
 
 void launch_measure_reduce(int W, const int *alive, const zd *eloc, const zd *den, const zd *parts,

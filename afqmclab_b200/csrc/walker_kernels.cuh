@@ -12,6 +12,9 @@ struct Blocks {
     long long tOff[2];   // offset of block b inside a walker's thetaT slot
     long long sStride;   // per-walker S slot size (elements)
     long long tStride;   // per-walker thetaT slot size (elements)
+    // log-det multiplicity of the listed blocks: 2 when one listed block
+    // stands for two identical spin blocks (same trial, same walker columns)
+    int mult = 1;
 };
 
 enum { LU_PLAIN = 0, LU_PROJECT = 1, LU_POPWEIGHT = 2 };
@@ -93,8 +96,11 @@ int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, lo
                        int thetaLayout = 0);
 void launch_pl_energy(int W, int G, long long Ktot, const zd *wfDaggerT, const zd *thetaT,
                       const zd *xbar, const zd *ex, const int *alive, const zd *logov, zd *eloc,
-                      zd *den, zd *tloc, cudaStream_t s, const zd *exTot = nullptr);
-// (exTot: the per-walker sum over g of ex, used instead of ex when given)
+                      zd *den, zd *tloc, cudaStream_t s, const zd *exTot = nullptr, long long tLen = -1,
+                      int tMult = 1);
+// (exTot: the per-walker sum over g of ex, used instead of ex when given;
+// the kinetic sum runs over the first tLen entries of a walker's thetaT
+// slot, default all Ktot, counted tMult times)
 // Sums over alive walkers into device accumulators:
 // acc[0] += sum den, acc[1] += sum eloc*den, acc[2+k] += sum parts[w*nparts+k]*den;
 // with xbar/ex (phaseless): bgNum[g] += sum xbar*den, exNum[g] += sum ex*den

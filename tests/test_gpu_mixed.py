@@ -115,3 +115,34 @@ def test_mixed_stabilisation_matches_fp64(n, nup, ndn, G):
     q = wf_x[:, :, 0]
     assert np.abs(q.conj().T @ q - np.eye(q.shape[1])).max() < 1e-5
     assert x.status() == 0
+
+
+def test_mixed_restricted_matches_two_block_form():
+    """With the same trial for both spins (nup = ndn) the mixed form computes
+    one spin block and doubles it; a trial whose down block differs from the
+    up block in one last bit takes the two-block path.  Both agree on the
+    log-overlaps, the energy and the per-vector sums to mixed-precision
+    accuracy after a few steps with a measurement."""
+    m = molecule(128, 32, 32, 128)
+    assert np.array_equal(m.phiTUp, m.phiTDn)
+    m2 = molecule(128, 32, 32, 128)
+    d = m2.phiTDn.copy()
+    d[0, 0] = np.nextafter(d[0, 0].real, np.inf) + 1j * d[0, 0].imag
+    m2.phiTDn = np.asfortranarray(d)
+    W = 64
+    out = []
+    for mm in (m, m2):
+        x = capi.pl_engine(mm, W, 41, 1000, 1000, precision=capi.AFQMC_MIXED)
+        wf, lw, al = inputs.initial_walkers(mm.phiTUp, W, seed=42, noise=0.05)
+        x.set_walkers(wf, lw, al)
+        x.step(3)
+        x.reset_measurement()
+        x.add_mixed_measurement()
+        mm_ = x.measurement()
+        out.append((x.log_overlaps(), mm_[1] / mm_[0], x.cholesky_nums(), x.status()))
+    (l1, e1, (b1, x1), s1), (l2, e2, (b2, x2), s2) = out
+    assert s1 == 0 and s2 == 0
+    assert np.abs(l1 - l2).max() < 1e-4
+    assert abs(e1 - e2) < 2e-6 * abs(e1)
+    assert np.abs(b1 - b2).max() < 1e-4 * np.abs(b1).max()
+    assert np.abs(x1 - x2).max() < 1e-4 * np.abs(x1).max()
