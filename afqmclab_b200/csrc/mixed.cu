@@ -354,8 +354,8 @@ __device__ __forceinline__ void store_b_sw(uint8_t *sB, int a, int i, float v)
 template <int NC>
 __global__ void __launch_bounds__(128, 1)
 taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmE,
-                      int W, int n, float *w32, const int *surv, int *order, int kmax, float acc,
-                      float relTol, int checkFrom, int doOneBody, int *status, int *err)
+                      int W, int n, float *w32, const int *surv, int *order, long long *stats, int kmax,
+                      float acc, float relTol, int checkFrom, int doOneBody, int *status, int *err)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -568,7 +568,17 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
                 gw[(size_t)n * NC + row + (size_t)n * a] = pi[a];
             }
         }
-        if (tid == 0) order[w] = k;
+        if (tid == 0) {
+            order[w] = k;
+            // order statistics: calls, total order, min, max (integer
+            // atomics, so the result does not depend on the walker order)
+            if (stats) {
+                atomicAdd((unsigned long long *)&stats[0], 1ULL);
+                atomicAdd((unsigned long long *)&stats[1], (unsigned long long)k);
+                atomicMin(&stats[2], (long long)k);
+                atomicMax(&stats[3], (long long)k);
+            }
+        }
         tc_fence_before();
         __syncthreads();
         w = wn;
@@ -599,8 +609,8 @@ int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE,
     const int perSm = TaylorSmem<NC>::bytes(e->n) <= 112 * 1024 ? 2 : 1;
     int grid = std::min(e->W, perSm * sms);
     taylor_onebody_kernel<NC><<<grid, 128, smem, e->stream>>>(
-        mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, 30, 1e-10f, 5.9604645e-8f, 4, doOneBody, e->status,
-        e->mx->err);
+        mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, e->tstats, 30, 1e-10f, 5.9604645e-8f, 4, doOneBody,
+        e->status, e->mx->err);
     return engine_check_launch();
 }
 
@@ -949,7 +959,6 @@ int mixed_project_dtk_dtv(afqmc_engine *e)
     {
         PHASE(AFQMC_PH_TAYLOR);
         MTRY(run_taylor(e));
-        launch_taylor_stats(W, e->surv, e->order, e->tstats, s);
     }
     return check_err(e);
 }
