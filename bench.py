@@ -139,7 +139,9 @@ def phase_flops(c, m, taylor_avg):
 # DRAM bytes (read + write) per phase occurrence of the dominant kernel, from
 # one ncu capture of the same workload (dram__bytes_read.sum +
 # dram__bytes_write.sum, summed over the phase's launches).
-NCU_TRAFFIC = {}
+NCU_TRAFFIC = {
+    ("molecule128", "mixed", "taylor"): (201.43e6 + 35.21e6, "1 taylor_onebody_kernel<32> launch"),
+}
 
 
 def cp_phase_model(m, W, precision):
