@@ -63,52 +63,106 @@ __global__ void __launch_bounds__(256) ex_shift_kernel(int W, const zd *logov, c
 // Operands of M over the walkers (K-major in the walker index, 2W per row):
 //   Bt(q) = [u_re(q, .) | u_im(q, .)],  Ar(q) = [v_re | -v_im],  Ai(q) = [v_im | v_re],
 // v_w = exp(logov_w - shift) u_w for alive walkers and 0 otherwise.
-// 32 x 32 tiles (q, w) through shared memory.
+// 64 x 64 tiles (q, w) through shared memory; theta rows are read and the
+// operand rows written 8 bf16 (16 bytes) at a time.
+constexpr int EXT = 64;
+
+__device__ __forceinline__ uint32_t bf2pack(float a, float b)
+{
+    const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *(const uint32_t *)&h;
+}
+
 __global__ void __launch_bounds__(256)
 ex_transpose_kernel(int W, long long K, long long Ktot, long long tOff, const __nv_bfloat16 *Theta,
                     const zd *logov, const int *alive, const double *shift, __nv_bfloat16 *Bt,
                     __nv_bfloat16 *Ar, __nv_bfloat16 *Ai)
 {
-    __shared__ float tr[32][33], ti[32][33];
-    __shared__ double dr[32], di[32];
-    const long long q0 = (long long)blockIdx.x * 32;
-    const int w0 = blockIdx.y * 32;
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 8 rows of 32
-    if (threadIdx.x < 32) {
-        const int w = w0 + threadIdx.x;
+    __shared__ float tr[EXT][EXT + 1], ti[EXT][EXT + 1];   // [walker][q]
+    __shared__ double dr[EXT], di[EXT];
+    const long long q0 = (long long)blockIdx.x * EXT;
+    const int w0 = blockIdx.y * EXT;
+    const int tid = threadIdx.x;
+    if (tid < EXT) {
+        const int w = w0 + tid;
         double r = 0.0, im = 0.0;
         if (w < W && alive[w]) {
             const zd d = zexp(make_double2(logov[w].x - shift[0], logov[w].y));
             r = d.x; im = d.y;
         }
-        dr[threadIdx.x] = r; di[threadIdx.x] = im;
+        dr[tid] = r; di[tid] = im;
     }
-    for (int r = ty; r < 32; r += 8) {
+    // 64 walkers x 8 runs of 8 q per plane
+    for (int idx = tid; idx < EXT * 8; idx += 256) {
+        const int r = idx >> 3, c8 = (idx & 7) * 8;
         const int w = w0 + r;
-        const long long q = q0 + tx;
-        float vr = 0.f, vi = 0.f;
-        if (w < W && q < K) {
+        const long long q = q0 + c8;
+        float vr[8], vi[8];
+        if (w < W && q + 8 <= K) {
             const __nv_bfloat16 *t = Theta + (size_t)w * 2 * Ktot + tOff + q;
-            vr = __bfloat162float(t[0]);
-            vi = __bfloat162float(t[Ktot]);
+            const uint4 a = *(const uint4 *)t, b = *(const uint4 *)(t + Ktot);
+            const uint32_t av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float2 fa = __bfloat1622float2(*(const __nv_bfloat162 *)&av[j]);
+                const float2 fb = __bfloat1622float2(*(const __nv_bfloat162 *)&bv[j]);
+                vr[2 * j] = fa.x; vr[2 * j + 1] = fa.y;
+                vi[2 * j] = fb.x; vi[2 * j + 1] = fb.y;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const bool in = w < W && q + j < K;
+                const __nv_bfloat16 *t = Theta + (size_t)(in ? w : 0) * 2 * Ktot + tOff + (in ? q + j : 0);
+                vr[j] = in ? __bfloat162float(t[0]) : 0.f;
+                vi[j] = in ? __bfloat162float(t[Ktot]) : 0.f;
+            }
         }
-        tr[r][tx] = vr;
-        ti[r][tx] = vi;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) { tr[r][c8 + j] = vr[j]; ti[r][c8 + j] = vi[j]; }
     }
     __syncthreads();
     const long long W2 = 2LL * W;
-    for (int r = ty; r < 32; r += 8) {
-        const long long q = q0 + r;
-        const int w = w0 + tx;
-        if (q >= K || w >= W) continue;
-        const float ur = tr[tx][r], ui = ti[tx][r];
-        const double vr = dr[tx] * ur - di[tx] * ui, vi = dr[tx] * ui + di[tx] * ur;
-        Bt[q * W2 + w] = __float2bfloat16(ur);
-        Bt[q * W2 + W + w] = __float2bfloat16(ui);
-        Ar[q * W2 + w] = __double2bfloat16(vr);
-        Ar[q * W2 + W + w] = __double2bfloat16(-vi);
-        Ai[q * W2 + w] = __double2bfloat16(vi);
-        Ai[q * W2 + W + w] = __double2bfloat16(vr);
+    // 64 q rows x 8 runs of 8 walkers; each run goes to six 16-byte pieces
+    for (int idx = tid; idx < EXT * 8; idx += 256) {
+        const int qr = idx >> 3, c8 = (idx & 7) * 8;
+        const long long q = q0 + qr;
+        const int wb = w0 + c8;
+        if (q >= K || wb >= W) continue;
+        float ur[8], ui[8], xr[8], xi[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            ur[j] = tr[c8 + j][qr];
+            ui[j] = ti[c8 + j][qr];
+            xr[j] = (float)(dr[c8 + j] * ur[j] - di[c8 + j] * ui[j]);
+            xi[j] = (float)(dr[c8 + j] * ui[j] + di[c8 + j] * ur[j]);
+        }
+        const size_t row = (size_t)q * W2;
+        if ((W & 7) == 0 && wb + 8 <= W) {
+            uint4 a, b, c, d;
+            a.x = bf2pack(ur[0], ur[1]); a.y = bf2pack(ur[2], ur[3]); a.z = bf2pack(ur[4], ur[5]); a.w = bf2pack(ur[6], ur[7]);
+            b.x = bf2pack(ui[0], ui[1]); b.y = bf2pack(ui[2], ui[3]); b.z = bf2pack(ui[4], ui[5]); b.w = bf2pack(ui[6], ui[7]);
+            c.x = bf2pack(xr[0], xr[1]); c.y = bf2pack(xr[2], xr[3]); c.z = bf2pack(xr[4], xr[5]); c.w = bf2pack(xr[6], xr[7]);
+            d.x = bf2pack(xi[0], xi[1]); d.y = bf2pack(xi[2], xi[3]); d.z = bf2pack(xi[4], xi[5]); d.w = bf2pack(xi[6], xi[7]);
+            uint4 nd;   // -v_im
+            nd.x = d.x ^ 0x80008000u; nd.y = d.y ^ 0x80008000u; nd.z = d.z ^ 0x80008000u; nd.w = d.w ^ 0x80008000u;
+            *(uint4 *)(Bt + row + wb) = a;
+            *(uint4 *)(Bt + row + W + wb) = b;
+            *(uint4 *)(Ar + row + wb) = c;
+            *(uint4 *)(Ar + row + W + wb) = nd;
+            *(uint4 *)(Ai + row + wb) = d;
+            *(uint4 *)(Ai + row + W + wb) = c;
+        } else {
+            for (int j = 0; j < 8 && wb + j < W; ++j) {
+                const int w = wb + j;
+                Bt[row + w] = __float2bfloat16(ur[j]);
+                Bt[row + W + w] = __float2bfloat16(ui[j]);
+                Ar[row + w] = __float2bfloat16(xr[j]);
+                Ar[row + W + w] = __float2bfloat16(-xi[j]);
+                Ai[row + w] = __float2bfloat16(xi[j]);
+                Ai[row + W + w] = __float2bfloat16(xr[j]);
+            }
+        }
     }
 }
 
@@ -239,7 +293,7 @@ int exchange_gemm_run(afqmc_engine *e, const ExGemmBlock &blk, const __nv_bfloat
             ex_shift_kernel<<<1, 256, 0, st>>>(W, e->logov, e->alive, s.shift);
         }
         g_launch_count++;
-        dim3 tg((unsigned)((K + 31) / 32), (unsigned)((W + 31) / 32));
+        dim3 tg((unsigned)((K + EXT - 1) / EXT), (unsigned)((W + EXT - 1) / EXT));
         ex_transpose_kernel<<<tg, 256, 0, st>>>(W, K, e->Ktot, blk.tOff, Theta, e->logov, e->alive, s.shift,
                                                 s.Bt, s.Av, s.Av + K * W2);
         // [M_re; M_im] = [Ar; Ai] Bt^T, stored exchanged as Rt
