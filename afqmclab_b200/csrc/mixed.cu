@@ -434,6 +434,9 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     while (w < W) {
         const int wn = next_walker(w + gridDim.x);
         float *gw = w32 + (size_t)w * 2 * n * NC;
+        // the next walker's fp32 planes (2 n NC floats, contiguous) are
+        // pulled into L2 while this walker's series runs
+        if (tid == 0 && wn < W) bulk_prefetch_l2(w32 + (size_t)wn * 2 * n * NC, (uint32_t)(2 * n * NC * sizeof(float)));
         // order 0: S = phi, operand = bf16(phi); all loads issue before the stores
         float pr[NC], pi[NC];
 #pragma unroll
@@ -511,7 +514,8 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
                 if (!conv && tid == 0 && status) atomicOr(status + w, (int)ST_TAYLOR_CAP);
                 break;
             }
-            __syncthreads();  // red[] is rewritten by the next order
+            // red[] is next written after the following order's
+            // __syncthreads_and, which every thread reaches after reading it
         }
         if (!ok) break;
         // Every MMA of the series has completed: the M planes are free.

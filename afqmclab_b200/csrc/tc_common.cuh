@@ -96,6 +96,13 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map)
 {
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
+// Bulk prefetch of a global range into L2 (a hint: nothing waits on it and
+// results do not depend on it).  Address and size are multiples of 16 bytes.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)), "r"(bytes)
+                 : "memory");
+}
 
 // ---- tcgen05 ----
 __device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t ncols)
