@@ -358,23 +358,37 @@ ob_split_kernel(const __grid_constant__ CUtensorMap tEh, const __grid_constant__
         const int r = q * 32 + lane;
         for (long long ti = 0; ti < myTiles && ok; ++ti) {
             const int buf = (int)(ti & 1);
+            const long long t = blockIdx.x + ti * gridDim.x;
+            const long long col = t * OB_TILE + r;
+            const float *rc = p.res + col * p.n;
+            float *oc = p.out + col * p.n;
+            // the first 32 sites of this column's residual are loaded while
+            // the tile's products are still running
+            float4 x0[8];
+            if (col < p.cols) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) x0[j] = *(const float4 *)(rc + 4 * j);
+            }
             ok = mbar_wait_sleep(&tfull[buf], (uint32_t)((ti >> 1) & 1));
             if (!ok) break;
             tc_fence_after();
-            const long long t = blockIdx.x + ti * gridDim.x;
-            const long long col = t * OB_TILE + r;
             const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * 128);
-            const float *rc = p.res + col * p.n;
-            float *oc = p.out + col * p.n;
             for (int c0 = 0; c0 < p.n; c0 += 32) {
                 float v[32];
                 tmem_ld32(trow + (uint32_t)c0, v);
                 if (col < p.cols) {
+                    // the next 32 sites' residual loads issue before this chunk's stores
+                    float4 x1[8];
+                    const bool more = c0 + 32 < p.n;
 #pragma unroll
-                    for (int j = 0; j < 32; j += 4) {
-                        const float4 x = *(const float4 *)(rc + c0 + j);
-                        *(float4 *)(oc + c0 + j) = make_float4(x.x + v[j], x.y + v[j + 1], x.z + v[j + 2], x.w + v[j + 3]);
-                    }
+                    for (int j = 0; j < 8; ++j)
+                        if (more) x1[j] = *(const float4 *)(rc + c0 + 32 + 4 * j);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                        *(float4 *)(oc + c0 + 4 * j) = make_float4(x0[j].x + v[4 * j], x0[j].y + v[4 * j + 1],
+                                                                   x0[j].z + v[4 * j + 2], x0[j].w + v[4 * j + 3]);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) x0[j] = x1[j];
                 }
             }
             tc_fence_before();
