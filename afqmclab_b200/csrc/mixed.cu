@@ -234,8 +234,10 @@ mgs32_kernel(int W, int n, int ncol, int nup, int ndn, float *w32, zd *logw, con
 // log-weight and second cos projection (same arithmetic as the FP64 form),
 // writing y = sqrt(-dt) x as the bf16 operand of the two-body GEMM.  One warp
 // per walker (four walkers per block): a walker's sums need no block barrier
-// and more walkers are in flight per SM.
-__global__ void __launch_bounds__(128)
+// and more walkers are in flight per SM.  Each lane takes its fields two at a
+// time (g and g + 32): both fields' loads and Gaussians are issued before the
+// first field's stores, and the sums still run in field order.
+__global__ void __launch_bounds__(128, 4)
 mixed_sample_warp_kernel(int W, CholDev c, const float *xbarp, int splits, long long splitStride,
                          int *surv, int *alive, const unsigned long long *offs, uint64_t seed,
                          __nv_bfloat16 *Y, zd *logw, double dtET, zd hopLogw)
@@ -246,28 +248,49 @@ mixed_sample_warp_kernel(int W, CholDev c, const float *xbarp, int splits, long 
     const int G = c.G;
     const unsigned long long off = offs[w];
     zd f2 = make_double2(0, 0), xf = make_double2(0, 0), xb = make_double2(0, 0);
-    for (int g = lane; g < G; g += 32) {
-        zd f;
-        if (c.constForce) {
-            f = c.constForce[g];
-        } else {
-            double xr = 0.0, xi = 0.0;
-            for (int s = 0; s < splits; ++s) {
-                xr += xbarp[s * splitStride + g + (size_t)2 * G * w];
-                xi += xbarp[s * splitStride + G + g + (size_t)2 * G * w];
+    for (int g0 = lane; g0 < G; g0 += 64) {
+        const int nf = g0 + 32 < G ? 2 : 1;
+        double xr[2] = {0.0, 0.0}, xi[2] = {0.0, 0.0}, bgv[2] = {0.0, 0.0}, gs[2] = {0.0, 0.0};
+        zd cf[2] = {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (u < nf) {
+                const int g = g0 + 32 * u;
+                bgv[u] = c.bg[g];
+                if (c.constForce) {
+                    cf[u] = c.constForce[g];
+                } else {
+                    for (int s = 0; s < splits; ++s) {
+                        xr[u] += xbarp[s * splitStride + g + (size_t)2 * G * w];
+                        xi[u] += xbarp[s * splitStride + G + g + (size_t)2 * G * w];
+                    }
+                }
             }
-            double a = xr - c.bg[g], b = xi;
-            f = make_double2(-b * c.sqrtDt, a * c.sqrtDt);
-            double af = zabs(f);
-            if (af > c.forceCap) f = make_double2(f.x * c.forceCap / af, f.y * c.forceCap / af);
         }
-        double gs = rng_gaussian(seed, off + 2ULL * g);
-        zd x = make_double2(gs + f.x, f.y);
-        Y[(size_t)(2 * w) * G + g] = __double2bfloat16(-c.sqrtDt * x.y);
-        Y[(size_t)(2 * w + 1) * G + g] = __double2bfloat16(c.sqrtDt * x.x);
-        zfma(f2, f, f);
-        zfma(xf, x, f);
-        zfma(xb, x, make_double2(c.bg[g], 0.0));
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+            if (u < nf) gs[u] = rng_gaussian(seed, off + 2ULL * (g0 + 32 * u));
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            if (u < nf) {
+                const int g = g0 + 32 * u;
+                zd f;
+                if (c.constForce) {
+                    f = cf[u];
+                } else {
+                    double a = xr[u] - bgv[u], b = xi[u];
+                    f = make_double2(-b * c.sqrtDt, a * c.sqrtDt);
+                    double af = zabs(f);
+                    if (af > c.forceCap) f = make_double2(f.x * c.forceCap / af, f.y * c.forceCap / af);
+                }
+                zd x = make_double2(gs[u] + f.x, f.y);
+                Y[(size_t)(2 * w) * G + g] = __double2bfloat16(-c.sqrtDt * x.y);
+                Y[(size_t)(2 * w + 1) * G + g] = __double2bfloat16(c.sqrtDt * x.x);
+                zfma(f2, f, f);
+                zfma(xf, x, f);
+                zfma(xb, x, make_double2(bgv[u], 0.0));
+            }
+        }
     }
     f2.x = warp_sum(f2.x); f2.y = warp_sum(f2.y);
     xf.x = warp_sum(xf.x); xf.y = warp_sum(xf.y);
