@@ -165,8 +165,9 @@ __global__ void gather32_kernel(int W, long long ws32, const int *table, float *
 
 // Gram-Schmidt (SD2is::stabilize, SD2is.cpp:48-76) on an fp32 walker: norms,
 // projections and updates in FP64, the columns kept in fp32 between updates
-// (the walker's own precision), which halves the shared memory per walker
-__global__ void __launch_bounds__(256)
+// (the walker's own precision), which halves the shared memory per walker.
+// n <= 128 (the mixed form runs n = 64 or 128).
+__global__ void __launch_bounds__(256, 5)
 mgs32_kernel(int W, int n, int ncol, int nup, int ndn, float *w32, zd *logw, const int *alive,
              int *status)
 {
@@ -203,19 +204,37 @@ mgs32_kernel(int W, int n, int ncol, int nup, int ndn, float *w32, zd *logw, con
             if (j < nmin) logRmin += lr;
         }
         __syncthreads();
+        // This lane's rows i = lane + 32 r of column j (n <= 128: at most four),
+        // converted to FP64 once per column; each column c's rows are converted
+        // once and kept for both the projection and the update (the fp32 <->
+        // FP64 conversions, not the FMAs, bound this loop).
+        zd qv[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const int i = lane + 32 * r;
+            const float2 q = i < n ? A[i + (size_t)n * j] : make_float2(0.f, 0.f);
+            qv[r] = make_double2(q.x, q.y);
+        }
         for (int c = j + 1 + wid; c < ncol; c += nw) {
             zd d = make_double2(0.0, 0.0);
-            for (int i = lane; i < n; i += 32) {
-                const float2 q = A[i + (size_t)n * j], v = A[i + (size_t)n * c];
-                zfma(d, make_double2(q.x, -q.y), make_double2(v.x, v.y));
+            zd vv[4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int i = lane + 32 * r;
+                const float2 v = i < n ? A[i + (size_t)n * c] : make_float2(0.f, 0.f);
+                vv[r] = make_double2(v.x, v.y);
+                if (i < n) zfma(d, make_double2(qv[r].x, -qv[r].y), vv[r]);
             }
             d.x = warp_sum(d.x);
             d.y = warp_sum(d.y);
-            for (int i = lane; i < n; i += 32) {
-                const float2 q = A[i + (size_t)n * j], v = A[i + (size_t)n * c];
-                const double vx = v.x - (d.x * q.x - d.y * q.y);
-                const double vy = v.y - (d.x * q.y + d.y * q.x);
-                A[i + (size_t)n * c] = make_float2((float)vx, (float)vy);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int i = lane + 32 * r;
+                if (i < n) {
+                    const double vx = vv[r].x - (d.x * qv[r].x - d.y * qv[r].y);
+                    const double vy = vv[r].y - (d.x * qv[r].y + d.y * qv[r].x);
+                    A[i + (size_t)n * c] = make_float2((float)vx, (float)vy);
+                }
             }
         }
         __syncthreads();
