@@ -33,7 +33,7 @@ SYMBOLS = [
     "afqmc_copy_walker_out", "afqmc_copy_walker_in", "afqmc_apply_table",
     "afqmc_batch_create", "afqmc_batch_step", "afqmc_batch_synchronize", "afqmc_batch_destroy",
     "afqmc_batch_set_stream",
-    "afqmc_set_autotune",
+    "afqmc_set_autotune", "afqmc_bounded_wait_check",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -111,6 +111,7 @@ def _declare(L):
     L.afqmc_batch_destroy.argtypes = [P]
     L.afqmc_batch_set_stream.argtypes = [P, P]
     L.afqmc_set_autotune.argtypes = [I]
+    L.afqmc_bounded_wait_check.argtypes = [ctypes.c_longlong, ctypes.POINTER(I), P]
     LL = ctypes.c_longlong
     L.afqmc_gemm_bf16_dev.argtypes = [I, I, I, P, LL, P, LL, P, LL, I, I, LL, ctypes.c_float, P]
     for name in SYMBOLS[2:]:
@@ -369,6 +370,13 @@ def pop_configuration_host(weights, uniforms, size=1):
     table = np.zeros(len(w), np.int32)
     _check(lib().afqmc_pop_configuration_host(len(w), size, _p(w), _p(u), _p(table)))
     return table
+
+
+def bounded_wait_check(limit_cycles, stream=None):
+    """Error bits of the bounded-wait self-check (see afqmc_bounded_wait_check)."""
+    w = ctypes.c_int(-1)
+    _check(lib().afqmc_bounded_wait_check(int(limit_cycles), ctypes.byref(w), stream))
+    return w.value
 
 
 def set_autotune(enable=True):

@@ -30,6 +30,7 @@
 #include "cp_mixed.cuh"
 #include "engine_internal.cuh"
 #include "tc_common.cuh"
+#include "once.cuh"
 
 extern std::atomic<long long> g_launch_count;
 
@@ -303,10 +304,9 @@ template <int MODE>
 int launch_tc_stream(cudaStream_t s, dim3 grid, const CUtensorMap &a0, const CUtensorMap &a1,
                      const CUtensorMap &b0, const CUtensorMap &b1, const CpTcArgs &args)
 {
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(cpm_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-        attr = true;
     }
     g_launch_count++;
     cpm_tc_kernel<MODE><<<grid, 192, SMEM, s>>>(a0, a1, b0, b1, args);

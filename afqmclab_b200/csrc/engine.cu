@@ -27,6 +27,7 @@
 #include "zgemm.cuh"
 
 #include <atomic>
+#include <mutex>
 extern std::atomic<long long> g_launch_count;
 
 namespace {
@@ -59,48 +60,62 @@ constexpr double TAYLOR_ACC = 1e-10;    // accuracy default
 typedef std::complex<double> cd;
 
 // ------------------------------------------------ NiupNidn constants (host)
-// solveCoshxEqExpy / solveCosxEqExpy / exp2by2Matrix (common/mathHao/source/simple_fun.cpp:7-91)
+// The Hubbard-Stratonovich coupling gamma solves cosh(gamma) = e^y
+// (solveCoshxEqExpy) or cos(gamma) = e^y (solveCosxEqExpy), and the
+// field-dependent on-site factor is the exponential of a Hermitian 2x2 matrix
+// (exp2by2Matrix), common/mathHao/source/simple_fun.cpp:7-91.  The root is
+// either purely real or purely imaginary; the reference's choice of branch
+// (negative root for the cosh form, e^y > 1; negative imaginary root
+// otherwise) fixes the sign convention of the sampled fields, so it is kept.
 cd solve_cosh_eq_exp(double y)
 {
-    cd ey(std::exp(y), 0.0);
-    cd g = std::log(ey - std::sqrt(ey * ey - 1.0));
-    if (std::abs(g.real()) < std::abs(g.imag())) g = cd(0, g.imag());
-    else g = cd(g.real(), 0);
-    return g;
+    const double ey = std::exp(y);
+    if (ey >= 1.0) return cd(-std::acosh(ey), 0.0);   // cosh(-a) = e^y, a >= 0
+    return cd(0.0, -std::acos(ey));                    // cosh(-i b) = cos(b) = e^y
 }
 cd solve_cos_eq_exp(double y)
 {
-    cd ey(std::exp(y), 0.0);
-    cd g = std::acos(ey);
-    if (std::abs(g.real()) < std::abs(g.imag())) g = cd(0, g.imag());
-    else g = cd(g.real(), 0);
-    return g;
+    const double ey = std::exp(y);
+    if (ey <= 1.0) return cd(std::acos(ey), 0.0);      // cos(a) = e^y, a in [0, pi/2]
+    return cd(0.0, -std::acosh(ey));                   // cos(-i b) = cosh(b) = e^y
 }
+// exp(H) for H = [[a, conj(c)], [c, b]] (a, b real): with m = (a+b)/2 and
+// r = sqrt(((a-b)/2)^2 + |c|^2), (H - m I)^2 = r^2 I, so
+//   exp(H) = e^m [cosh(r) I + sinh(r)/r (H - m I)].
+// On return a, b hold the diagonal and c the lower off-diagonal entry.
 void exp2by2(double &a, double &b, cd &c)
 {
-    if (std::abs(c) < 1e-60) { a = std::exp(a); b = std::exp(b); c = 0.0; return; }
-    double abs_c = std::abs(c), arg_c = std::arg(c);
-    double d0, d1; cd v00, v01, v10, v11; cd im(0.0, 1.0);
-    if (std::abs(a - b) < 1e-60) {
-        double norm = 1.0 / std::sqrt(2.0);
-        d0 = std::exp(-abs_c + a); d1 = std::exp(abs_c + b);
-        v00 = -norm; v10 = norm * std::exp(im * arg_c); v01 = norm; v11 = norm * std::exp(im * arg_c);
-    } else {
-        double xi = 0.5 * std::atan(2.0 * abs_c / (a - b));
-        d0 = std::exp(0.5 * std::cos(2.0 * xi) * (a - b) + std::sin(2.0 * xi) * abs_c + (a + b) * 0.5);
-        d1 = std::exp(-0.5 * std::cos(2.0 * xi) * (a - b) - std::sin(2.0 * xi) * abs_c + (a + b) * 0.5);
-        v00 = std::exp(-im * arg_c * 0.5) * std::cos(xi);
-        v10 = std::exp(im * arg_c * 0.5) * std::sin(xi);
-        v01 = -std::exp(-im * arg_c * 0.5) * std::sin(xi);
-        v11 = std::exp(im * arg_c * 0.5) * std::cos(xi);
-    }
-    double na = (d0 * v00 * std::conj(v00) + d1 * v01 * std::conj(v01)).real();
-    double nb = (d0 * v10 * std::conj(v10) + d1 * v11 * std::conj(v11)).real();
-    c = d0 * v10 * std::conj(v00) + d1 * v11 * std::conj(v01);
-    a = na; b = nb;
+    const double m = 0.5 * (a + b), h = 0.5 * (a - b);
+    const double r = std::sqrt(h * h + std::norm(c));
+    const double em = std::exp(m);
+    // sinh(r)/r, by its series where r is small enough for the series to be exact in FP64
+    const double shr = (r < 1e-4) ? 1.0 + r * r / 6.0 : std::sinh(r) / r;
+    const double ch = std::cosh(r);
+    a = em * (ch + shr * h);
+    b = em * (ch - shr * h);
+    c = em * shr * c;
 }
 
 zd tozd(cd z) { return make_double2(z.real(), z.imag()); }
+
+// One device int per device for the error word of the stand-alone
+// tensor-core entry points (allocated the first time each device needs it).
+int device_error_word(int **out)
+{
+    static int *words[64] = {};
+    static std::mutex mu;
+    int dev = 0;
+    cudaError_t r = cudaGetDevice(&dev);
+    if (r != cudaSuccess) return fail(AFQMC_ERR_CUDA, cudaGetErrorString(r));
+    if (dev < 0 || dev >= 64) return fail(AFQMC_ERR_UNSUPPORTED, "device index above 63");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!words[dev]) {
+        r = cudaMalloc(&words[dev], sizeof(int));
+        if (r != cudaSuccess) { words[dev] = nullptr; return fail(AFQMC_ERR_CUDA, cudaGetErrorString(r)); }
+    }
+    *out = words[dev];
+    return AFQMC_OK;
+}
 
 }  // namespace
 
@@ -957,6 +972,11 @@ int afqmc_pl_update_background(afqmc_engine *e, const double *bg, const double *
 {
     if (!e || e->kind != KIND_PL || !bg) return fail(AFQMC_ERR_ARG, "phaseless engine and bg required");
     const size_t n2 = (size_t)e->n * e->n;
+    // In the Taylor (LogHop2is) form the half-step slots hold log-form
+    // matrices; switching to dense operators has to replace all three.
+    if (e->useLog && expMinusDtK && (!expHalfDtK || !expMinusHalfDtK))
+        return fail(AFQMC_ERR_ARG, "switching from the Taylor one-body form to dense operators needs "
+                                   "expMinusDtK, expHalfDtK and expMinusHalfDtK");
     drop_graphs(e);
     CUDA_TRY(cudaMemcpyAsync(e->bg, bg, sizeof(double) * e->G, cudaMemcpyHostToDevice, e->stream));
     if (expMinusDtK) {
@@ -1090,8 +1110,8 @@ int afqmc_gemm_bf16_dev(int M, int N, int K, const void *A, long long lda, const
 {
     if (M < 0 || N < 0 || K <= 0 || !A || !B || !C || splits < 1) return fail(AFQMC_ERR_ARG, "bad argument");
     if (splits > 1 && (K % (64 * splits)) != 0) return fail(AFQMC_ERR_ARG, "K must split into multiples of 64");
-    static int *derr = nullptr;
-    if (!derr) CUDA_TRY(cudaMalloc(&derr, sizeof(int)));
+    int *derr = nullptr;
+    TRY(device_error_word(&derr));
     cudaStream_t s = (cudaStream_t)stream;
     CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(int), s));
     TcGemmArgs a;
@@ -1106,6 +1126,22 @@ int afqmc_gemm_bf16_dev(int M, int N, int K, const void *A, long long lda, const
     CUDA_TRY(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     if (h) return fail(AFQMC_ERR_CUDA, "tcgen05 gemm: barrier wait timed out");
+    return AFQMC_OK;
+}
+
+int afqmc_bounded_wait_check(long long limit_cycles, int *error_word, void *stream)
+{
+    if (!error_word) return fail(AFQMC_ERR_ARG, "null argument");
+    if (limit_cycles < 1000) limit_cycles = 1000;
+    if (limit_cycles > TC_WAIT_LIMIT_CYCLES) limit_cycles = TC_WAIT_LIMIT_CYCLES;
+    int *derr = nullptr;
+    TRY(device_error_word(&derr));
+    cudaStream_t s = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(int), s));
+    int r = tc_bounded_wait_check(limit_cycles, derr, s);
+    if (r) return fail(AFQMC_ERR_CUDA, "bounded-wait check launch failed: " + std::to_string(r));
+    CUDA_TRY(cudaMemcpyAsync(error_word, derr, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
     return AFQMC_OK;
 }
 

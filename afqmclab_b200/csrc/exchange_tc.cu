@@ -25,6 +25,7 @@
 #include "mixed.cuh"
 #include "tc_common.cuh"
 #include "tc_gemm.cuh"
+#include "once.cuh"
 
 extern std::atomic<long long> g_launch_count;
 
@@ -288,10 +289,9 @@ void launch_ns_a(int grid, size_t smem, cudaStream_t s, const CUtensorMap &ar, c
                  const CUtensorMap &br, const CUtensorMap &bi, int G, int W, int n, const int *alive, zd *ex,
                  int *err)
 {
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(exchange_tc_kernel<NS, REALA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
     }
     exchange_tc_kernel<NS, REALA><<<grid, XS_THREADS, smem, s>>>(ar, ai, br, bi, G, W, NS, n, alive, ex, err);
 }

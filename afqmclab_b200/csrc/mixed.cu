@@ -25,6 +25,7 @@
 #include "theta_tc.cuh"
 #include "tc_common.cuh"
 #include "tc_gemm.cuh"
+#include "once.cuh"
 
 struct MixedState {
     float *wf32 = nullptr, *tmp32 = nullptr;
@@ -643,11 +644,10 @@ template <int NC>
 int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE, int doOneBody)
 {
     const size_t smem = TaylorSmem<NC>::bytes(e->n);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(taylor_onebody_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TaylorSmem<NC>::bytes(128));
-        attr = true;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -1013,10 +1013,9 @@ int mixed_modify_gm(afqmc_engine *e)
 {
     if (e->kind == KIND_CP) return cp_mixed_modify_gm(e);
     const size_t bytes = (size_t)e->n * e->ncol * sizeof(float2);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(mgs32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-        attr = true;
     }
     if (bytes > 160 * 1024) return engine_fail(AFQMC_ERR_UNSUPPORTED, "walker too large for the fp32 stabiliser");
     mgs32_kernel<<<e->W, 256, bytes, e->stream>>>(e->W, e->n, e->ncol, e->nup, e->ndn, e->mx->wf32,

@@ -33,6 +33,7 @@
 #include "engine_internal.cuh"
 #include "overlap_tc.cuh"
 #include "tc_common.cuh"
+#include "once.cuh"
 
 extern std::atomic<long long> g_launch_count;
 
@@ -489,10 +490,9 @@ int overlap_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, in
                       int *err)
 {
     if (!overlap_tc_supported(n, nb, Ns)) return (int)cudaErrorInvalidValue;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(ov_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
-        attr = true;
     }
     OvArgs a{};
     a.n = n; a.W = W; a.nb = nb;
@@ -538,10 +538,9 @@ int onebody_split_launch(cudaStream_t s, int n, int ncol, int W, const float *Eh
     if (!onebody_split_supported(n)) return (int)cudaErrorInvalidValue;
     const int nkc = n / OB_KC;
     const size_t smem = 1024 + (size_t)2 * nkc * n * 128 + (size_t)OB_STAGES * 2 * OB_CHUNK_BYTES + 256;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(ob_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-        attr = true;
     }
     CUtensorMap eh, el, pm;
     cuuint64_t de[2] = {(cuuint64_t)n, (cuuint64_t)n}, pe[1] = {(cuuint64_t)n * 4};

@@ -45,13 +45,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
         : "memory");
     return ok != 0;
 }
-// Wait until the phase with the given parity has completed; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// Wait until the phase with the given parity has completed; false once
+// `limit` SM cycles have passed without it.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit = TC_WAIT_LIMIT)
 {
     if (mbar_try_wait(bar, parity)) return true;
     long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > TC_WAIT_LIMIT) return false;
+        if (clock64() - t0 > limit) return false;
     }
     return true;
 }
@@ -71,12 +72,13 @@ __device__ __forceinline__ bool mbar_try_wait_hint(uint64_t *bar, uint32_t parit
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t hint_ns = 20000)
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t *bar, uint32_t parity, uint32_t hint_ns = 20000,
+                                                long long limit = TC_WAIT_LIMIT)
 {
     if (mbar_try_wait_hint(bar, parity, hint_ns)) return true;
     long long t0 = clock64();
     while (!mbar_try_wait_hint(bar, parity, hint_ns)) {
-        if (clock64() - t0 > TC_WAIT_LIMIT) return false;
+        if (clock64() - t0 > limit) return false;
     }
     return true;
 }

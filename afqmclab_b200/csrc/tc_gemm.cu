@@ -17,6 +17,7 @@
 
 #include "tc_common.cuh"
 #include "tc_gemm.cuh"
+#include "once.cuh"
 
 extern std::atomic<long long> g_launch_count;
 
@@ -338,10 +339,9 @@ int launch_bn(const TcGemmArgs &a, cudaStream_t s)
     r = tc_make_map_bf16(&mb, a.B, a.K, a.N, a.ldb, BN);
     if (r) return r;
     const size_t smem = smem_bytes<BN>();
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(tc_gemm_kernel<BN, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
     }
     int kSplit = a.K;
     if (a.splits > 1) kSplit = ((a.K + a.splits - 1) / a.splits + TC_BK - 1) / TC_BK * TC_BK;
@@ -359,10 +359,9 @@ int launch_t(const TcGemmArgs &a, cudaStream_t s)
     if (r) return r;
     r = tc_make_map_bf16(&mb, a.B, a.K, a.N, a.ldb, TT_BN);
     if (r) return r;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(tc_gemm_t_kernel<OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TT_SMEM);
-        attr = true;
     }
     const int splits = a.splits > 1 ? a.splits : 1;
     int kSplit = a.K;
@@ -425,4 +424,50 @@ int tc_gemm_bf16(const TcGemmArgs &a, cudaStream_t s)
     }
     if (a.outType == TC_OUT_F32) return launch_bn<128, TC_OUT_F32>(a, s);
     return launch_bn<128, TC_OUT_BF16>(a, s);
+}
+
+// ---------------------------------------------------------------------------
+// Self-check of the bounded waits.  One CTA holds a TMEM allocation (as the
+// tensor-core kernels do) and waits, with the same two wait helpers those
+// kernels use, on two mbarriers that nothing arrives at.  Each wait must give
+// up after `limit` SM cycles; the CTA then records which ones did (bit 0: the
+// spinning wait, bit 1: the suspending wait), completes both phases itself,
+// frees its TMEM and returns.  Nothing is in flight while it waits.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(64, 1) bounded_wait_check_kernel(long long limit, int *err)
+{
+    __shared__ uint64_t bars[2];
+    __shared__ uint32_t tmemSlot;
+    const int warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+    }
+    if (warp == 1) { tmem_alloc(&tmemSlot, 32); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x == 0) {
+        int bits = 0;
+        if (!mbar_wait(&bars[0], 0, limit)) bits |= 1;
+        if (!mbar_wait_sleep(&bars[1], 0, 1000, limit)) bits |= 2;
+        // complete both phases so that no wait is left pending
+        mbar_arrive(&bars[0]);
+        mbar_arrive(&bars[1]);
+        *err = bits;
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 1) tmem_dealloc(tmemSlot, 32);
+}
+
+static_assert(TC_WAIT_LIMIT_CYCLES == TC_WAIT_LIMIT, "one wait limit for the kernels and the check");
+
+int tc_bounded_wait_check(long long limitCycles, int *errDev, cudaStream_t s)
+{
+    g_launch_count++;
+    bounded_wait_check_kernel<<<1, 64, 0, s>>>(limitCycles, errDev);
+    return (int)cudaGetLastError();
 }

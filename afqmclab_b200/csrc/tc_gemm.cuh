@@ -27,6 +27,11 @@ struct TcGemmArgs {
 // Returns 0 on success, a cudaError_t / CUresult value otherwise.
 int tc_gemm_bf16(const TcGemmArgs &a, cudaStream_t s);
 
+// Bounded-wait self-check (one CTA, waits that nothing completes, limit in
+// SM cycles); writes the bits of the waits that gave up to *errDev.
+constexpr long long TC_WAIT_LIMIT_CYCLES = 2000000000LL;
+int tc_bounded_wait_check(long long limitCycles, int *errDev, cudaStream_t s);
+
 // Builds a 2-D bf16 tensor map (inner extent `inner`, `rows` rows, row pitch
 // `pitch` elements) with a 64 x boxRows box and 128-byte swizzle.
 int tc_make_map_bf16(void *map, const void *base, long long inner, long long rows, long long pitch,

@@ -32,6 +32,7 @@
 #include "engine_internal.cuh"
 #include "tc_common.cuh"
 #include "theta_tc.cuh"
+#include "once.cuh"
 
 extern std::atomic<long long> g_launch_count;
 
@@ -403,13 +404,12 @@ int theta_tc_launch(cudaStream_t s, int n, int ncol, int nb, const int *Ns, int 
     cuuint32_t bA[3] = {32u, (cuuint32_t)pl.Nsp, 1u};
     int r = map_f32(&mA, w32, 3, dA, pA, bA, CU_TENSOR_MAP_SWIZZLE_NONE);
     if (r) return r;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(theta_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
         cudaFuncSetAttribute(theta_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
         cudaFuncSetAttribute(theta_tc_kernel<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
         cudaFuncSetAttribute(theta_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_CAP);
-        attr = true;
     }
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);

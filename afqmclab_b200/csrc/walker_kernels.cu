@@ -7,6 +7,7 @@
 std::atomic<long long> g_launch_count{0};
 
 #include <stdio.h>
+#include "once.cuh"
 
 namespace {
 
@@ -1608,10 +1609,9 @@ static void launch_lu_fp64(int W, const Blocks &bl, zd *S, zd *Sinv, const int *
     for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
     if (maxNs <= 32) {
         const size_t smem = (size_t)GJ_WARPS * 32 * GJ_LD * sizeof(zd);
-        static bool gattr = false;
-        if (!gattr) {
+        static std::atomic<unsigned long long> gattr{0};
+        if (first_on_device(gattr)) {
             cudaFuncSetAttribute(gj_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            gattr = true;
         }
         gj_warp_kernel<<<(W + GJ_WARPS - 1) / GJ_WARPS, GJ_WARPS * 32, smem, s>>>(
             W, bl, S, Sinv, active, logw, logwAdd, logwT, logov, alive, surv, logwOut, weight, status,
@@ -1620,13 +1620,12 @@ static void launch_lu_fp64(int W, const Blocks &bl, zd *S, zd *Sinv, const int *
     }
     if (maxNs <= GJ_CTA_MAX_NS) {
         const size_t smem = gj_cta_smem(maxNs);
-        static bool cattr = false;
-        if (!cattr) {
+        static std::atomic<unsigned long long> cattr{0};
+        if (first_on_device(cattr)) {
             cudaFuncSetAttribute(gj_cta_kernel<256, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)gj_cta_smem(64));
             cudaFuncSetAttribute(gj_cta_kernel<512, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)gj_cta_smem(GJ_CTA_MAX_NS));
-            cattr = true;
         }
         if (maxNs <= 64)
             gj_cta_kernel<256, 2><<<W, 256, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
@@ -1640,10 +1639,9 @@ static void launch_lu_fp64(int W, const Blocks &bl, zd *S, zd *Sinv, const int *
     }
     if (maxNs <= LU_SMEM_MAX_NS) {
         size_t smem = (size_t)2 * maxNs * maxNs * sizeof(zd) + (size_t)(maxNs + 4) * sizeof(int);
-        static bool attr = false;
-        if (!attr) {
+        static std::atomic<unsigned long long> attr{0};
+        if (first_on_device(attr)) {
             cudaFuncSetAttribute(lu_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-            attr = true;
         }
         lu_kernel<true><<<W, 256, smem, s>>>(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov,
                                               alive, surv, logwOut, weight, status, mode,
@@ -1706,10 +1704,9 @@ void launch_mgs(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, z
     g_launch_count++;
     size_t bytes = (size_t)n * ncol * sizeof(zd);
     if (bytes <= 160 * 1024) {
-        static bool attr = false;
-        if (!attr) {
+        static std::atomic<unsigned long long> attr{0};
+        if (first_on_device(attr)) {
             cudaFuncSetAttribute(mgs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-            attr = true;
         }
         mgs_kernel<true><<<W, 256, bytes, s>>>(W, n, ncol, nup, ndn, isSD2is, wf, logw, alive, status);
     } else {
@@ -1724,19 +1721,17 @@ void launch_pop_comb(int W, const double *weight, const double *uniforms, uint64
     g_launch_count++;
     const size_t smem = (size_t)W * (2 * sizeof(double) + sizeof(int));
     if (smem <= 200 * 1024) {
-        static bool pattr = false;
-        if (!pattr) {
+        static std::atomic<unsigned long long> pattr{0};
+        if (first_on_device(pattr)) {
             cudaFuncSetAttribute(pop_comb_par_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-            pattr = true;
         }
         pop_comb_par_kernel<<<1, POP_PAR_THREADS, smem, s>>>(W, weight, uniforms, seed, counter, table, status);
         return;
     }
     const int useSmem = smem <= 160 * 1024 ? 1 : 0;
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(pop_comb_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-        attr = true;
     }
     pop_comb_kernel<<<1, 256, useSmem ? smem : 0, s>>>(W, weight, uniforms, seed, counter, number, table,
                                                        status, useSmem);
@@ -1779,10 +1774,9 @@ int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, lo
     for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
     if (maxNs > 64) return -1;
     size_t smem = ((size_t)2 * maxNs * EX_KC + (size_t)maxNs * maxNs) * sizeof(zd);
-    static bool attr = false;
-    if (!attr) {
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
         cudaFuncSetAttribute(pl_exchange_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-        attr = true;
     }
     dim3 grid(W, (G + EX_GCH - 1) / EX_GCH);
     pl_exchange_kernel<<<grid, 256, smem, s>>>(W, n, G, bl, Aall, Ktot, thetaT, alive, ex, maxNs,

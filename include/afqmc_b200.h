@@ -205,6 +205,17 @@ int afqmc_taylor_stats(afqmc_engine *e, long long *calls, long long *total, int 
  * 2 non-finite value, 4 Taylor order cap, 8 zero column norm, 16 comb) */
 int afqmc_status(afqmc_engine *e, int *status_or);
 
+/* Self-check of the bounded waits of the tensor-core kernels: one CTA that
+ * holds a TMEM allocation waits, with the same wait helpers those kernels
+ * use, on two mbarriers that nothing arrives at, gives up after limit_cycles
+ * SM cycles (clamped to [1000, about one second]), completes the phases
+ * itself, frees its TMEM and returns.  *error_word receives the bits of the
+ * waits that gave up (1: spinning wait, 2: suspending wait): 3 when the
+ * bounds work.  Nothing is in flight while it waits, and the context stays
+ * usable.  Synchronises `stream` (a cudaStream_t).  No counterpart in the
+ * reference (it has no device code). */
+int afqmc_bounded_wait_check(long long limit_cycles, int *error_word, void *stream);
+
 /* Phase profiler: CUDA events around each phase of the step on the engine's
  * stream (replaces the reference's 1-second TimerHao, common/timeHao/include/
  * time_hao.h:16-41).  Enabling resets the totals; afqmc_profile_get writes

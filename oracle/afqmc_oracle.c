@@ -25,6 +25,43 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <pthread.h>
+
+/* ------------------------------------------------------------------ */
+/* Walker-parallel loops.  Walkers are independent within each pass of  */
+/* the step and of the measurement; or_parallel_for runs body(ctx, i)   */
+/* for i = 0..n-1 on up to `threads` threads (one when threads <= 1).   */
+/* Every result that depends on the order of walkers (random-stream     */
+/* offsets, the estimator sums) is computed serially outside it, so    */
+/* the thread count does not change any output.                         */
+/* ------------------------------------------------------------------ */
+typedef void (*or_body_fn)(void *ctx, int i);
+typedef struct { or_body_fn fn; void *ctx; int n; int next; } or_pfor;
+static void *or_pfor_worker(void *p)
+{
+    or_pfor *f = (or_pfor *)p;
+    for (;;) {
+        int i = __atomic_fetch_add(&f->next, 1, __ATOMIC_RELAXED);
+        if (i >= f->n) break;
+        f->fn(f->ctx, i);
+    }
+    return NULL;
+}
+static void or_parallel_for(int n, int threads, or_body_fn fn, void *ctx)
+{
+    if (threads > n) threads = n;
+    if (threads <= 1) { for (int i = 0; i < n; ++i) fn(ctx, i); return; }
+    or_pfor f = {fn, ctx, n, 0};
+    pthread_t *tid = (pthread_t *)malloc(sizeof(pthread_t) * (size_t)(threads - 1));
+    int started = 0;
+    for (int t = 0; t < threads - 1; ++t)
+        if (pthread_create(&tid[t], NULL, or_pfor_worker, &f) == 0) started++;
+        else break;
+    or_pfor_worker(&f);
+    for (int t = 0; t < started; ++t) pthread_join(tid[t], NULL);
+    free(tid);
+}
+static pthread_mutex_t or_stats_mu = PTHREAD_MUTEX_INITIALIZER;
 
 typedef double complex zc;
 
@@ -935,44 +972,27 @@ static void or_apply_one_body(or_engine *e, const zc *mat, zc matLogw, int useLo
     *logwNew = matLogw + logw;
 }
 
-/* One projection step for every alive walker:
- *   CP: AfqmcConstraintPath::projectExpMinusDtKExpMinusDtV
- *       (afqmcConstraintPathProjection.cpp:37-74)
- *   PL: AfqmcPhaseless::projectExpMinusDtKExpMinusDtV
- *       (afqmcPhaselessProjection.cpp:75-121)
- * The walker loop is split at the first cos projection: survivors' stream
- * offsets follow the reference's walker-major draw order exactly. */
-static void or_project_dtk_dtv(or_engine *e)
+typedef struct { or_engine *e; size_t ws; zc *lo; int *surv; } or_pass1_ctx;
+static void or_pass1_body(void *c_, int w)
 {
-    int W = e->W, n = e->n, N = e->N;
-    size_t ws = or_wsize(e);
-    int draws = (e->kind == OR_CP) ? e->L : 2 * e->G;
-    uint64_t base = e->rng.counter;
-    int *surv = (int *)calloc((size_t)W, sizeof(int));
-    uint64_t *offs = (uint64_t *)calloc((size_t)W, sizeof(uint64_t));
-    zc *lo = (zc *)calloc((size_t)W, sizeof(zc));
-    /* pass 1: overlap and first cos projection (independent per walker) */
-#ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic) num_threads(e->nthreads > 0 ? e->nthreads : 1)
-#endif
-    for (int w = 0; w < W; ++w) {
-        if (!e->alive[w]) continue;
+    or_pass1_ctx *c = (or_pass1_ctx *)c_;
+    or_engine *e = c->e; size_t ws = c->ws; zc *lo = c->lo; int *surv = c->surv;
+        if (!e->alive[w]) return;
         int info;
         lo[w] = or_walker_logoverlap(e, e->wf + ws * w, e->logw[w], NULL, NULL, &info);
         double phase = cimag(lo[w]);
-        if (cos(phase) <= 0.0) { e->alive[w] = 0; continue; }
+        if (cos(phase) <= 0.0) { e->alive[w] = 0; return; }
         e->logw[w] += log(cos(phase)) - I * phase;
         surv[w] = 1;
     }
-    uint64_t acc = 0;
-    for (int w = 0; w < W; ++w) { offs[w] = base + acc; acc += surv[w] ? (uint64_t)draws : 0; }
-    e->rng.counter = base + acc;
-    /* pass 2: force, sampling, two-body and one-body propagation */
-#ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic) num_threads(e->nthreads > 0 ? e->nthreads : 1)
-#endif
-    for (int w = 0; w < W; ++w) {
-        if (!surv[w]) continue;
+
+typedef struct { or_engine *e; size_t ws; int n, N; const int *surv; const uint64_t *offs; } or_pass2_ctx;
+static void or_pass2_body(void *c_, int w)
+{
+    or_pass2_ctx *c = (or_pass2_ctx *)c_;
+    or_engine *e = c->e; size_t ws = c->ws; int n = c->n, N = c->N;
+    const int *surv = c->surv; const uint64_t *offs = c->offs;
+        if (!surv[w]) return;
         or_rng r = {e->rng.seed, offs[w]};
         zc *wf = e->wf + ws * w;
         zc *tmp = (zc *)malloc(sizeof(zc) * ws);
@@ -1025,17 +1045,16 @@ static void or_project_dtk_dtv(or_engine *e)
             if (cos(phase) <= 0.0) {
                 e->alive[w] = 0;
                 free(force); free(aux); free(tmp);
-                continue;
+                return;
             }
             e->logw[w] += log(cos(phase));
             zc *M = (zc *)malloc(sizeof(zc) * n * n);
             or_pl_build_M(e, aux, M);
             int ord;
             ord = or_loghop_apply(1, 0, 1e-10, 3, 'N', n, N, M, wf, tmp);
-#ifdef _OPENMP
-#pragma omp critical
-#endif
+pthread_mutex_lock(&or_stats_mu);
             or_taylor_stats(e, ord);
+            pthread_mutex_unlock(&or_stats_mu);
             logwTmp = sampleLogw + e->logw[w];
             free(M); free(force); free(aux);
         }
@@ -1053,21 +1072,58 @@ static void or_project_dtk_dtv(or_engine *e)
         }
         free(tmp);
     }
+
+/* One projection step for every alive walker:
+ *   CP: AfqmcConstraintPath::projectExpMinusDtKExpMinusDtV
+ *       (afqmcConstraintPathProjection.cpp:37-74)
+ *   PL: AfqmcPhaseless::projectExpMinusDtKExpMinusDtV
+ *       (afqmcPhaselessProjection.cpp:75-121)
+ * The walker loop is split at the first cos projection: survivors' stream
+ * offsets follow the reference's walker-major draw order exactly. */
+static void or_project_dtk_dtv(or_engine *e)
+{
+    int W = e->W, n = e->n, N = e->N;
+    size_t ws = or_wsize(e);
+    int draws = (e->kind == OR_CP) ? e->L : 2 * e->G;
+    uint64_t base = e->rng.counter;
+    int *surv = (int *)calloc((size_t)W, sizeof(int));
+    uint64_t *offs = (uint64_t *)calloc((size_t)W, sizeof(uint64_t));
+    zc *lo = (zc *)calloc((size_t)W, sizeof(zc));
+    /* pass 1: overlap and first cos projection (independent per walker) */
+{
+        or_pass1_ctx c1 = {e, ws, lo, surv};
+        or_parallel_for(W, e->nthreads, or_pass1_body, &c1);
+    }
+
+    uint64_t acc = 0;
+    for (int w = 0; w < W; ++w) { offs[w] = base + acc; acc += surv[w] ? (uint64_t)draws : 0; }
+    e->rng.counter = base + acc;
+    /* pass 2: force, sampling, two-body and one-body propagation */
+{
+        or_pass2_ctx c2 = {e, ws, n, N, surv, offs};
+        or_parallel_for(W, e->nthreads, or_pass2_body, &c2);
+    }
+
     free(surv); free(offs); free(lo);
 }
+
+typedef struct { or_engine *e; size_t ws; } or_gm_ctx;
+static void or_gm_body(void *c_, int w)
+{
+    or_gm_ctx *c = (or_gm_ctx *)c_;
+    or_engine *e = c->e; size_t ws = c->ws;
+        if (!e->alive[w]) return;
+        if (e->kind == OR_CP) or_sd_stabilize(e->n, e->N, e->wf + ws * w, &e->logw[w]);
+        else or_sd2is_stabilize(e->n, e->Nup, e->Ndn, e->wf + ws * w, &e->logw[w]);
+    }
 
 /* modifyGM (afqmcConstraintPathProjection.cpp:95-101; afqmcPhaselessProjection.cpp:142-148) */
 void or_modify_gm(or_engine *e)
 {
     size_t ws = or_wsize(e);
-#ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic) num_threads(e->nthreads > 0 ? e->nthreads : 1)
-#endif
-    for (int w = 0; w < e->W; ++w) {
-        if (!e->alive[w]) continue;
-        if (e->kind == OR_CP) or_sd_stabilize(e->n, e->N, e->wf + ws * w, &e->logw[w]);
-        else or_sd2is_stabilize(e->n, e->Nup, e->Ndn, e->wf + ws * w, &e->logw[w]);
-    }
+or_gm_ctx c = {e, ws};
+    or_parallel_for(e->W, e->nthreads, or_gm_body, &c);
+
 }
 
 /* popControl (afqmcConstraintPathProjection.cpp:103-156) in the serial
@@ -1142,7 +1198,8 @@ void or_reset_measurement(or_engine *e)
 }
 
 /* per-walker local energy of a propagated walker, accumulated with weight den */
-static void or_cp_add_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut, zc *denOut)
+static void or_cp_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut, zc *denOut,
+                                zc *KVR)
 {
     int n = e->n, N = e->N, L = e->L;
     zc *th = (zc *)malloc(sizeof(zc) * N * n), *gd = (zc *)malloc(sizeof(zc) * n),
@@ -1161,16 +1218,17 @@ static void or_cp_add_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut, z
         R += (e->hx[i] * 0.5 - I * e->hy[i] * 0.5) * god[i];
         R += (e->hx[i] * 0.5 + I * e->hy[i] * 0.5) * god[i + L];
     }
-    e->den += den;
-    e->KNum += K * den; e->VNum += V * den; e->RNum += R * den;
-    e->HNum += (K + V + R) * den;
-    if (elocOut) *elocOut = K + V + R;
-    if (denOut) *denOut = den;
+    KVR[0] = K; KVR[1] = V; KVR[2] = R;
+    *elocOut = K + V + R;
+    *denOut = den;
     free(th); free(gd); free(god);
 }
 
-/* RealMaterialMoleculeMeasureFixedSD2sSD2is::addEnergy (:197-220) */
-static void or_pl_add_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut, zc *denOut)
+/* RealMaterialMoleculeMeasureFixedSD2sSD2is::addEnergy (:197-220).  The
+ * walker's terms are written to xbOut/exOut (G each) and *Tout, *denOut,
+ * *elocOut; or_add_mixed_measurement adds them to the sums in walker order. */
+static void or_pl_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut, zc *denOut,
+                                zc *Tout, zc *xbOut, zc *exOut)
 {
     int n = e->n, G = e->G, Nu = e->Nup, Nd = e->Ndn;
     zc *thu = (zc *)malloc(sizeof(zc) * Nu * n), *thd = (zc *)malloc(sizeof(zc) * (Nd > 0 ? Nd : 1) * n);
@@ -1210,24 +1268,22 @@ static void or_pl_add_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut, z
     for (int g = 0; g < G; ++g) H += (xb[g] * xb[g] - ex[g]);
     H *= 0.5;
     H += T;
-    e->den += den;
-    e->TNum += T * den;
-    for (int g = 0; g < G; ++g) { e->bgNum[g] += xb[g] * den; e->exNum[g] += ex[g] * den; }
-    e->HNum += H * den;
-    if (elocOut) *elocOut = H;
-    if (denOut) *denOut = den;
+    *elocOut = H;
+    *denOut = den;
+    *Tout = T;
+    memcpy(xbOut, xb, sizeof(zc) * G);
+    memcpy(exOut, ex, sizeof(zc) * G);
     free(thu); free(thd); free(xb); free(ex); free(D);
 }
 
-/* addMixedMeasurement (afqmcConstraintPathMeasure.cpp:9-23,
- * afqmcPhaselessMeasure.cpp:9-28).  eloc/den per walker may be NULL. */
-void or_add_mixed_measurement(or_engine *e, double *elocOut, double *denOut)
+typedef struct { or_engine *e; size_t ws; int G; zc *el, *dn, *terms, *xb, *ex; } or_meas_ctx;
+static void or_meas_body(void *c_, int w)
 {
-    size_t ws = or_wsize(e);
-    zc *tmp = (zc *)malloc(sizeof(zc) * ws);
-    zc *el = (zc *)elocOut, *dn = (zc *)denOut;
-    for (int w = 0; w < e->W; ++w) {
-        if (!e->alive[w]) { if (el) el[w] = 0; if (dn) dn[w] = 0; continue; }
+    or_meas_ctx *c = (or_meas_ctx *)c_;
+    or_engine *e = c->e; size_t ws = c->ws; int G = c->G;
+    zc *el = c->el, *dn = c->dn, *terms = c->terms, *xb = c->xb, *ex = c->ex;
+        if (!e->alive[w]) return;
+        zc *tmp = (zc *)malloc(sizeof(zc) * ws);
         zc lwTmp;
         if (e->kind == OR_PL && e->useLogOneBody) {
             /* expHalfDtK only exists as a Taylor operator in this case */
@@ -1238,10 +1294,46 @@ void or_add_mixed_measurement(or_engine *e, double *elocOut, double *denOut)
             or_zgemm_nn(e->n, e->N, e->n, 1.0, e->expHalfDtK, e->n, e->wf + ws * w, e->n, tmp, e->n);
             lwTmp = e->logwExpHalfDtK + e->logw[w];
         }
-        if (e->kind == OR_CP) or_cp_add_energy(e, tmp, lwTmp, el ? el + w : NULL, dn ? dn + w : NULL);
-        else or_pl_add_energy(e, tmp, lwTmp, el ? el + w : NULL, dn ? dn + w : NULL);
+        if (e->kind == OR_CP) or_cp_walker_energy(e, tmp, lwTmp, el + w, dn + w, terms + 3 * w);
+        else or_pl_walker_energy(e, tmp, lwTmp, el + w, dn + w, terms + 3 * w, xb + (size_t)w * G,
+                                 ex + (size_t)w * G);
+        free(tmp);
     }
-    free(tmp);
+
+/* addMixedMeasurement (afqmcConstraintPathMeasure.cpp:9-23,
+ * afqmcPhaselessMeasure.cpp:9-28).  eloc/den per walker may be NULL.
+ * Walkers are evaluated independently (in parallel when built with OpenMP)
+ * and added to the sums serially in walker order, as the reference's loop
+ * does, so the sums do not depend on the thread count. */
+void or_add_mixed_measurement(or_engine *e, double *elocOut, double *denOut)
+{
+    size_t ws = or_wsize(e);
+    int W = e->W, G = e->kind == OR_PL ? e->G : 0;
+    zc *el = (zc *)calloc((size_t)W, sizeof(zc)), *dn = (zc *)calloc((size_t)W, sizeof(zc));
+    zc *terms = (zc *)calloc((size_t)W * 3, sizeof(zc));
+    zc *xb = G ? (zc *)calloc((size_t)W * G, sizeof(zc)) : NULL;
+    zc *ex = G ? (zc *)calloc((size_t)W * G, sizeof(zc)) : NULL;
+or_meas_ctx c = {e, ws, G, el, dn, terms, xb, ex};
+    or_parallel_for(W, e->nthreads, or_meas_body, &c);
+
+    for (int w = 0; w < W; ++w) {
+        if (!e->alive[w]) continue;
+        zc den = dn[w];
+        e->den += den;
+        if (e->kind == OR_CP) {
+            e->KNum += terms[3 * w] * den; e->VNum += terms[3 * w + 1] * den; e->RNum += terms[3 * w + 2] * den;
+        } else {
+            e->TNum += terms[3 * w] * den;
+            for (int g = 0; g < G; ++g) {
+                e->bgNum[g] += xb[(size_t)w * G + g] * den;
+                e->exNum[g] += ex[(size_t)w * G + g] * den;
+            }
+        }
+        e->HNum += el[w] * den;
+    }
+    if (elocOut) memcpy(elocOut, el, sizeof(zc) * W);
+    if (denOut) memcpy(denOut, dn, sizeof(zc) * W);
+    free(el); free(dn); free(terms); free(xb); free(ex);
 }
 
 /* measurement sums: out[0..]= den, HNum, (CP) KNum, VNum, RNum | (PL) TNum */

@@ -286,6 +286,11 @@ class Engine:
     def step(self, nsteps=1):
         lib().or_project_one_step(self.h, nsteps)
 
+    def set_threads(self, nthreads):
+        """Walker-parallel host threads for the step, modifyGM and the
+        measurement; results do not depend on the count."""
+        lib().or_set_threads(self.h, int(nthreads))
+
     def modify_gm(self):
         lib().or_modify_gm(self.h)
 
