@@ -33,7 +33,7 @@ SYMBOLS = [
     "afqmc_copy_walker_out", "afqmc_copy_walker_in", "afqmc_apply_table",
     "afqmc_batch_create", "afqmc_batch_step", "afqmc_batch_synchronize", "afqmc_batch_destroy",
     "afqmc_batch_set_stream",
-    "afqmc_set_autotune", "afqmc_bounded_wait_check",
+    "afqmc_set_autotune", "afqmc_bounded_wait_check", "afqmc_get_site_nums",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -85,6 +85,7 @@ def _declare(L):
     L.afqmc_pop_control.argtypes = [P, P, P]
     L.afqmc_get_measurement.argtypes = [P, P]
     L.afqmc_get_cholesky_nums.argtypes = [P, P, P]
+    L.afqmc_get_site_nums.argtypes = [P, P, P, P, P]
     L.afqmc_pl_update_background.argtypes = [P, P, P, D, P, D, P, D]
     L.afqmc_log_overlaps.argtypes = [P, P]
     L.afqmc_green_matrix.argtypes = [P, I, I, P]
@@ -185,9 +186,13 @@ class Engine:
         _check(lib().afqmc_set_rng(self.h, seed, counter))
 
     def rng_counter(self):
+        return self.rng_state()[1]
+
+    def rng_state(self):
+        """(seed, counter) of the engine's random stream."""
         s, c = ctypes.c_ulonglong(), ctypes.c_ulonglong()
         _check(lib().afqmc_get_rng(self.h, ctypes.byref(s), ctypes.byref(c)))
-        return c.value
+        return s.value, c.value
 
     def set_ET(self, ET):
         _check(lib().afqmc_set_ET(self.h, ET))
@@ -236,6 +241,13 @@ class Engine:
         e = np.zeros(self.G, np.complex128)
         _check(lib().afqmc_get_cholesky_nums(self.h, _p(b), _p(e)))
         return b, e
+
+    def site_nums(self):
+        """NupNum, NdnNum, SplusNum, SminusNum (L complex each), CP only."""
+        L = self.n // 2
+        out = [np.zeros(L, np.complex128) for _ in range(4)]
+        _check(lib().afqmc_get_site_nums(self.h, *[_p(a) for a in out]))
+        return out
 
     def update_background(self, m):
         """m: MoleculeInputs after set_background()."""

@@ -500,9 +500,9 @@ int add_mixed_measurement_direct(afqmc_engine *e)
     if (e->kind == KIND_CP) {
         PHASE(AFQMC_PH_MEASURE);
         launch_cp_energy(W, e->hd, e->wfDaggerK, e->thetaT, e->bl.tStride, e->U, e->mu, e->hx,
-                         e->hy, e->hz, e->alive, e->logov, e->eloc, e->den, e->parts, s);
-        launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 3, e->acc, 0, nullptr,
-                              nullptr, nullptr, nullptr, s);
+                         e->hy, e->hz, e->alive, e->logov, e->eloc, e->den, e->parts, e->sites, s);
+        launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 3, e->acc, 4 * e->L, e->sites,
+                              nullptr, e->siteNum, nullptr, s);
     } else {
         { PHASE(AFQMC_PH_MEASURE); TRY(xbar_gemm(e)); }
         {
@@ -525,6 +525,13 @@ int create_common_checks(int W, int precision)
 {
     if (W <= 0) return fail(AFQMC_ERR_ARG, "walker count must be positive");
     if (precision != AFQMC_FP64 && precision != AFQMC_MIXED) return fail(AFQMC_ERR_ARG, "unknown precision");
+    return AFQMC_OK;
+}
+
+// Runs after every argument check, so that argument errors are reported as
+// such on a machine without a GPU too.
+int create_device_check()
+{
     int dev = 0;
     cudaError_t r = cudaGetDevice(&dev);
     if (r != cudaSuccess) return fail(AFQMC_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(r));
@@ -607,6 +614,9 @@ int afqmc_cp_create(int L, int N, int W, int decomp, int force_type, double dt, 
     if (!K || !expMinusDtK || !expHalfDtK || !U || !mu || !hx || !hy || !hz || !phiT)
         return fail(AFQMC_ERR_ARG, "missing model array");
     if (mgs_step <= 0 || pop_control_step <= 0) return fail(AFQMC_ERR_ARG, "cadence must be positive");
+    if (force_type != AFQMC_DYNAMIC_FORCE && force_type != AFQMC_CONST_FORCE)
+        return fail(AFQMC_ERR_ARG, "unknown force type");
+    TRY(create_device_check());
     afqmc_engine *e = new afqmc_engine();
     e->kind = KIND_CP; e->L = L; e->n = 2 * L; e->ncol = N; e->nup = N; e->ndn = 0; e->W = W;
     e->precision = precision; e->decomp = decomp; e->forceType = force_type;
@@ -645,6 +655,8 @@ int afqmc_cp_create(int L, int N, int W, int decomp, int force_type, double dt, 
     CK(dupload(e, &e->cdiag[2], c10.data(), L)); CK(dupload(e, &e->cdiag[3], c11.data(), L));
     if (const_force) CK(dupload(e, &e->constForceCP, const_force, L));
     CK(dalloc(e, &e->forceCP, (size_t)W * L));
+    CK(dalloc(e, &e->sites, (size_t)W * 4 * L));
+    CK(dalloc(e, &e->siteNum, (size_t)4 * L));
     e->hd.L = L; e->hd.N = N; e->hd.n = n; e->hd.decomp = decomp;
     e->hd.gamma = e->gamma; e->hd.cd00 = e->cdiag[0]; e->hd.cd01 = e->cdiag[1];
     e->hd.cd10 = e->cdiag[2]; e->hd.cd11 = e->cdiag[3];
@@ -693,6 +705,9 @@ int afqmc_pl_create(int n, int Nup, int Ndn, int G, int W, int force_type, doubl
         return fail(AFQMC_ERR_ARG, "missing model array");
     if (!expMinusDtK && !logExpMinusDtK) return fail(AFQMC_ERR_ARG, "need expMinusDtK or logExpMinusDtK");
     if (mgs_step <= 0 || pop_control_step <= 0) return fail(AFQMC_ERR_ARG, "cadence must be positive");
+    if (force_type != AFQMC_DYNAMIC_FORCE && force_type != AFQMC_CONST_FORCE)
+        return fail(AFQMC_ERR_ARG, "unknown force type");
+    TRY(create_device_check());
     afqmc_engine *e = new afqmc_engine();
     e->kind = KIND_PL; e->n = n; e->nup = Nup; e->ndn = Ndn; e->ncol = std::max(Nup, Ndn);
     e->G = G; e->W = W; e->precision = precision; e->forceType = force_type;
@@ -936,6 +951,7 @@ int afqmc_reset_measurement(afqmc_engine *e)
     CUDA_TRY(cudaMemsetAsync(e->acc, 0, sizeof(zd) * 8, e->stream));
     if (e->bgNum) CUDA_TRY(cudaMemsetAsync(e->bgNum, 0, sizeof(zd) * e->G, e->stream));
     if (e->exNum) CUDA_TRY(cudaMemsetAsync(e->exNum, 0, sizeof(zd) * e->G, e->stream));
+    if (e->siteNum) CUDA_TRY(cudaMemsetAsync(e->siteNum, 0, sizeof(zd) * 4 * e->L, e->stream));
     return AFQMC_OK;
 }
 
@@ -953,6 +969,20 @@ int afqmc_get_measurement(afqmc_engine *e, double *out)
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     for (int i = 0; i < 5; ++i) { out[2 * i] = a[i].x; out[2 * i + 1] = a[i].y; }
     if (e->kind == KIND_PL) { out[6] = out[7] = out[8] = out[9] = 0.0; }
+    return AFQMC_OK;
+}
+
+int afqmc_get_site_nums(afqmc_engine *e, double *NupNum, double *NdnNum, double *SplusNum,
+                        double *SminusNum)
+{
+    if (!e || e->kind != KIND_CP) return fail(AFQMC_ERR_ARG, "constrained-path engine required");
+    const int L = e->L;
+    std::vector<zd> h((size_t)4 * L);
+    CUDA_TRY(cudaMemcpyAsync(h.data(), e->siteNum, sizeof(zd) * 4 * L, cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    double *dst[4] = {NupNum, NdnNum, SplusNum, SminusNum};
+    for (int k = 0; k < 4; ++k)
+        if (dst[k]) std::memcpy(dst[k], h.data() + (size_t)k * L, sizeof(zd) * L);
     return AFQMC_OK;
 }
 

@@ -63,6 +63,9 @@ struct afqmc_engine {
     // measurement
     zd *acc = nullptr, *bgNum = nullptr, *exNum = nullptr, *eloc = nullptr, *den = nullptr,
        *parts = nullptr;
+    // constrained path: per-walker site terms (G_ii up, G_ii down, the two
+    // spin-flip off-diagonals; W x 4L) and their den-weighted sums (4L)
+    zd *sites = nullptr, *siteNum = nullptr;
     // mixed-precision state
     MixedState *mx = nullptr;
     CpMixedState *cpm = nullptr;   // constrained-path mixed form

@@ -1348,13 +1348,15 @@ __global__ void __launch_bounds__(256)
 cp_energy_kernel(int W, HubbardDev h, const zd *wfDaggerK, const zd *thetaT, long long tStride,
                  const double *U, const double *mu, const double *hx, const double *hy,
                  const double *hz, const int *alive, const zd *logov, zd *eloc, zd *den,
-                 zd *parts)
+                 zd *parts, zd *sites)
 {
     __shared__ double red[32];
     const int w = blockIdx.x;
     if (!alive[w]) return;
     const int L = h.L, N = h.N, n = h.n;
     const zd *th = thetaT + (size_t)w * tStride;
+    // site terms of addNupNdn / addSplusSminus (HubbardSOCMeasureFixedSDSD.cpp:221-255)
+    zd *st = sites + (size_t)w * 4 * L;
     zd K = make_double2(0, 0), V = make_double2(0, 0), R = make_double2(0, 0);
     for (int e = threadIdx.x; e < N * n; e += blockDim.x) zfma(K, wfDaggerK[e], th[e]);
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
@@ -1366,6 +1368,10 @@ cp_energy_kernel(int W, HubbardDev h, const zd *wfDaggerK, const zd *thetaT, lon
             zfma(oi, pi, th[j + (size_t)N * (i + L)]);
             zfma(oL, pL, th[j + (size_t)N * i]);
         }
+        st[i] = gi;
+        st[i + L] = gL;
+        st[i + 2 * L] = oi;
+        st[i + 3 * L] = oL;
         zd t = zsub(zmul(gi, gL), zmul(oi, oL));
         V = zadd(V, zscale(t, U[i]));
         R = zadd(R, zscale(gi, -mu[i] + hz[i] * 0.5));
@@ -1759,11 +1765,11 @@ void launch_copy_masked(int W, long long wsize, const zd *src, zd *dst, const in
 void launch_cp_energy(int W, const HubbardDev &h, const zd *wfDaggerK, const zd *thetaT,
                       long long tStride, const double *U, const double *mu, const double *hx,
                       const double *hy, const double *hz, const int *alive, const zd *logov,
-                      zd *eloc, zd *den, zd *parts, cudaStream_t s)
+                      zd *eloc, zd *den, zd *parts, zd *sites, cudaStream_t s)
 {
     g_launch_count++;
     cp_energy_kernel<<<W, 256, 0, s>>>(W, h, wfDaggerK, thetaT, tStride, U, mu, hx, hy, hz, alive,
-                                        logov, eloc, den, parts);
+                                        logov, eloc, den, parts, sites);
 }
 
 int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, long long Ktot,

@@ -88,7 +88,7 @@ void launch_copy_masked(int W, long long wsize, const zd *src, zd *dst, const in
 void launch_cp_energy(int W, const HubbardDev &h, const zd *wfDaggerK, const zd *thetaT,
                       long long tStride, const double *U, const double *mu, const double *hx,
                       const double *hy, const double *hz, const int *alive, const zd *logov,
-                      zd *eloc, zd *den, zd *parts, cudaStream_t s);
+                      zd *eloc, zd *den, zd *parts, zd *sites, cudaStream_t s);
 // Aall: column g = [A_g,up (Nup x n); A_g,dn (Ndn x n)] flattened (Ktot rows);
 // returns -1 when a block is wider than 64 columns.
 int launch_pl_exchange(int W, int n, int G, const Blocks &bl, const zd *Aall, long long Ktot,

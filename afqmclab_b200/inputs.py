@@ -310,22 +310,56 @@ def write_hubbard_model_param(m: HubbardInputs, path):
                 f.write(f"{v:26.18e} \n")
 
 
+def _complex_line(z):
+    # writeFile(complex, ofstream) (common/readWriteHao/include/readWriteFstream.h):
+    # setprecision(16), scientific, two fields of width 26
+    return f"{z.real:26.16e}{z.imag:26.16e}\n"
+
+
+def _matrix_lines(wf):
+    # TensorHao::write (tensor_core.h:296-301): rank, shape, then the entries
+    # column by column, one per line
+    wf = np.asarray(wf)
+    out = [f"2\n{wf.shape[0]} {wf.shape[1]} \n"]
+    out.extend(_complex_line(z) for z in wf.ravel(order="F"))
+    return "".join(out)
+
+
+def _read_matrix(vals, k):
+    rank, r, c = int(vals[k]), int(vals[k + 1]), int(vals[k + 2])
+    if rank != 2:
+        raise ValueError(f"walker file: matrix rank {rank}, expected 2")
+    data = np.array(vals[k + 3:k + 3 + 2 * r * c], dtype=np.float64)
+    if data.size != 2 * r * c:
+        raise ValueError("walker file: truncated matrix")
+    return (data[0::2] + 1j * data[1::2]).reshape((r, c), order="F")
+
+
 def write_sd(wf, logw, path):
-    """SD::write text format (SD.cpp:85-103): logw then the matrix."""
+    """SD::write file format (SD.cpp:85-103): logw, then the matrix."""
     with open(path, "w") as f:
-        f.write(f"{np.real(logw):26.18e} {np.imag(logw):26.18e} \n")
-        f.write(f"{wf.shape[0]:26d} {wf.shape[1]:26d} \n")
-        for z in np.asarray(wf).ravel(order="F"):
-            f.write(f"{z.real:26.18e} {z.imag:26.18e} \n")
+        f.write(_complex_line(complex(logw)) + _matrix_lines(wf))
 
 
 def read_sd(path):
+    """SD::read (SD.cpp:85-93): returns (wf, logw)."""
     vals = open(path).read().split()
     logw = complex(float(vals[0]), float(vals[1]))
-    r, c = int(vals[2]), int(vals[3])
-    data = np.array(vals[4:4 + 2 * r * c], dtype=np.float64)
-    wf = (data[0::2] + 1j * data[1::2]).reshape((r, c), order="F")
-    return wf, logw
+    return _read_matrix(vals, 2), logw
+
+
+def write_sd2is(wf, logw, nup, ndn, path):
+    """SD2is::write file format (SD2is.cpp:105-127): logw, Nup, Ndn, the matrix."""
+    with open(path, "w") as f:
+        f.write(_complex_line(complex(logw)) + f"{nup:26d}\n{ndn:26d}\n" + _matrix_lines(wf))
+
+
+def read_sd2is(path):
+    """SD2is::read: returns (wf, logw, nup, ndn)."""
+    vals = open(path).read().split()
+    logw = complex(float(vals[0]), float(vals[1]))
+    nup, ndn = int(vals[2]), int(vals[3])
+    return _read_matrix(vals, 4), logw, nup, ndn
 
 
 CONFIGS = {

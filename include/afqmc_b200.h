@@ -167,6 +167,14 @@ int afqmc_pop_control(afqmc_engine *e, int *table_out, double *weight_out);
 int afqmc_reset_measurement(afqmc_engine *e);
 int afqmc_add_mixed_measurement(afqmc_engine *e);
 int afqmc_get_measurement(afqmc_engine *e, double *out);
+/* Site sums of the constrained-path mixed estimator, L complex each (NULL
+ * skips one): NupNum, NdnNum (den-weighted G diagonals of the up and down
+ * sites) and SplusNum, SminusNum (the two spin-flip off-diagonals), as
+ * HubbardSOCMeasureFixedSDSD::addNupNdn / addSplusSminus accumulate them
+ * (HubbardSOCMeasureFixedSDSD.cpp:221-255); the *TotNum totals are their sums.
+ * CP only. */
+int afqmc_get_site_nums(afqmc_engine *e, double *NupNum, double *NdnNum, double *SplusNum,
+                        double *SminusNum);
 /* choleskyBgNum / choleskyExNum (G complex each), PL only */
 int afqmc_get_cholesky_nums(afqmc_engine *e, double *bgNum, double *exNum);
 

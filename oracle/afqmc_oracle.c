@@ -644,6 +644,7 @@ typedef struct {
     /* measurement accumulators */
     zc den, HNum, KNum, VNum, RNum, TNum;
     zc *bgNum, *exNum;
+    zc *siteNum;       /* CP: NupNum, NdnNum, SplusNum, SminusNum (4 x L) */
     /* taylor statistics */
     long taylorCalls, taylorTotal; int taylorMin, taylorMax;
     int nthreads;
@@ -658,7 +659,7 @@ void or_destroy(or_engine *e)
                     e->expMinusHalfDtK, e->logExpMinusDtK, e->gamma, e->cd00, e->cd01, e->cd10,
                     e->cd11, e->constForceCP, e->U, e->mu, e->hx, e->hy, e->hz, e->wfDaggerK,
                     e->chol, e->bg, e->Aup, e->Adn, e->wfDaggerTUp, e->wfDaggerTDn,
-                    e->constForcePL, e->bgNum, e->exNum};
+                    e->constForcePL, e->bgNum, e->exNum, e->siteNum};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
     free(e);
 }
@@ -705,6 +706,7 @@ or_engine *or_cp_create(int L, int N, int W, int decomp, int forceType, double d
     e->expMinusHalfDtK = zdup(expMinusHalfDtK, (size_t)n * n);
     e->U = ddup(U, L); e->mu = ddup(mu, L); e->hx = ddup(hx, L); e->hy = ddup(hy, L); e->hz = ddup(hz, L);
     e->constForceCP = (double *)calloc((size_t)L, sizeof(double));
+    e->siteNum = (zc *)calloc((size_t)4 * L, sizeof(zc));
     if (constForce) memcpy(e->constForceCP, constForce, sizeof(double) * L);
     e->gamma = (zc *)malloc(sizeof(zc) * L);
     e->cd00 = (zc *)malloc(sizeof(zc) * L); e->cd01 = (zc *)malloc(sizeof(zc) * L);
@@ -1195,11 +1197,12 @@ void or_reset_measurement(or_engine *e)
 {
     e->den = e->HNum = e->KNum = e->VNum = e->RNum = e->TNum = 0;
     if (e->bgNum) for (int g = 0; g < e->G; ++g) e->bgNum[g] = e->exNum[g] = 0;
+    if (e->siteNum) for (int k = 0; k < 4 * e->L; ++k) e->siteNum[k] = 0;
 }
 
 /* per-walker local energy of a propagated walker, accumulated with weight den */
 static void or_cp_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut, zc *denOut,
-                                zc *KVR)
+                                zc *KVR, zc *sites)
 {
     int n = e->n, N = e->N, L = e->L;
     zc *th = (zc *)malloc(sizeof(zc) * N * n), *gd = (zc *)malloc(sizeof(zc) * n),
@@ -1219,6 +1222,13 @@ static void or_cp_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut
         R += (e->hx[i] * 0.5 + I * e->hy[i] * 0.5) * god[i + L];
     }
     KVR[0] = K; KVR[1] = V; KVR[2] = R;
+    /* addNupNdn / addSplusSminus (HubbardSOCMeasureFixedSDSD.cpp:221-255) */
+    for (int i = 0; i < L; ++i) {
+        sites[i] = gd[i];
+        sites[i + L] = gd[i + L];
+        sites[i + 2 * L] = god[i];
+        sites[i + 3 * L] = god[i + L];
+    }
     *elocOut = K + V + R;
     *denOut = den;
     free(th); free(gd); free(god);
@@ -1276,12 +1286,12 @@ static void or_pl_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut
     free(thu); free(thd); free(xb); free(ex); free(D);
 }
 
-typedef struct { or_engine *e; size_t ws; int G; zc *el, *dn, *terms, *xb, *ex; } or_meas_ctx;
+typedef struct { or_engine *e; size_t ws; int G; zc *el, *dn, *terms, *xb, *ex, *sites; } or_meas_ctx;
 static void or_meas_body(void *c_, int w)
 {
     or_meas_ctx *c = (or_meas_ctx *)c_;
     or_engine *e = c->e; size_t ws = c->ws; int G = c->G;
-    zc *el = c->el, *dn = c->dn, *terms = c->terms, *xb = c->xb, *ex = c->ex;
+    zc *el = c->el, *dn = c->dn, *terms = c->terms, *xb = c->xb, *ex = c->ex, *sites = c->sites;
         if (!e->alive[w]) return;
         zc *tmp = (zc *)malloc(sizeof(zc) * ws);
         zc lwTmp;
@@ -1294,7 +1304,8 @@ static void or_meas_body(void *c_, int w)
             or_zgemm_nn(e->n, e->N, e->n, 1.0, e->expHalfDtK, e->n, e->wf + ws * w, e->n, tmp, e->n);
             lwTmp = e->logwExpHalfDtK + e->logw[w];
         }
-        if (e->kind == OR_CP) or_cp_walker_energy(e, tmp, lwTmp, el + w, dn + w, terms + 3 * w);
+        if (e->kind == OR_CP) or_cp_walker_energy(e, tmp, lwTmp, el + w, dn + w, terms + 3 * w,
+                                                  sites + (size_t)w * 4 * e->L);
         else or_pl_walker_energy(e, tmp, lwTmp, el + w, dn + w, terms + 3 * w, xb + (size_t)w * G,
                                  ex + (size_t)w * G);
         free(tmp);
@@ -1313,7 +1324,8 @@ void or_add_mixed_measurement(or_engine *e, double *elocOut, double *denOut)
     zc *terms = (zc *)calloc((size_t)W * 3, sizeof(zc));
     zc *xb = G ? (zc *)calloc((size_t)W * G, sizeof(zc)) : NULL;
     zc *ex = G ? (zc *)calloc((size_t)W * G, sizeof(zc)) : NULL;
-or_meas_ctx c = {e, ws, G, el, dn, terms, xb, ex};
+    zc *sites = e->kind == OR_CP ? (zc *)calloc((size_t)W * 4 * e->L, sizeof(zc)) : NULL;
+    or_meas_ctx c = {e, ws, G, el, dn, terms, xb, ex, sites};
     or_parallel_for(W, e->nthreads, or_meas_body, &c);
 
     for (int w = 0; w < W; ++w) {
@@ -1322,6 +1334,7 @@ or_meas_ctx c = {e, ws, G, el, dn, terms, xb, ex};
         e->den += den;
         if (e->kind == OR_CP) {
             e->KNum += terms[3 * w] * den; e->VNum += terms[3 * w + 1] * den; e->RNum += terms[3 * w + 2] * den;
+            for (int k = 0; k < 4 * e->L; ++k) e->siteNum[k] += sites[(size_t)w * 4 * e->L + k] * den;
         } else {
             e->TNum += terms[3 * w] * den;
             for (int g = 0; g < G; ++g) {
@@ -1333,7 +1346,7 @@ or_meas_ctx c = {e, ws, G, el, dn, terms, xb, ex};
     }
     if (elocOut) memcpy(elocOut, el, sizeof(zc) * W);
     if (denOut) memcpy(denOut, dn, sizeof(zc) * W);
-    free(el); free(dn); free(terms); free(xb); free(ex);
+    free(el); free(dn); free(terms); free(xb); free(ex); free(sites);
 }
 
 /* measurement sums: out[0..]= den, HNum, (CP) KNum, VNum, RNum | (PL) TNum */
@@ -1343,6 +1356,11 @@ void or_get_measurement(const or_engine *e, double *out)
     o[0] = e->den; o[1] = e->HNum;
     if (e->kind == OR_CP) { o[2] = e->KNum; o[3] = e->VNum; o[4] = e->RNum; }
     else { o[2] = e->TNum; o[3] = 0; o[4] = 0; }
+}
+/* NupNum, NdnNum, SplusNum, SminusNum, L complex each (CP) */
+void or_get_site_nums(const or_engine *e, double *out)
+{
+    memcpy(out, e->siteNum, sizeof(zc) * 4 * e->L);
 }
 void or_get_cholesky_nums(const or_engine *e, double *bgNum, double *exNum)
 {

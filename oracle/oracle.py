@@ -114,6 +114,7 @@ def _declare(L):
     L.or_add_mixed_measurement.argtypes = [P, P, P]
     L.or_get_measurement.argtypes = [P, P]
     L.or_get_cholesky_nums.argtypes = [P, P, P]
+    L.or_get_site_nums.argtypes = [P, P]
     L.or_pl_force_single.argtypes = [P, c_int, P, P]
     L.or_cp_force_single.argtypes = [P, c_int, P]
     L.or_taylor_stats_get.argtypes = [P, P, P, P, P]
@@ -262,7 +263,11 @@ class Engine:
         return wf, lw, al
 
     def set_rng(self, seed, counter=0):
+        self.seed = seed
         lib().or_set_rng(self.h, seed, counter)
+
+    def rng_state(self):
+        return self.seed, self.rng_counter()
 
     def rng_counter(self):
         return lib().or_get_rng_counter(self.h)
@@ -317,6 +322,13 @@ class Engine:
         lib().or_get_measurement(self.h, _p(out))
         return out
 
+    def site_nums(self):
+        """NupNum, NdnNum, SplusNum, SminusNum (L complex each), CP only."""
+        L = self.n // 2
+        out = np.zeros(4 * L, np.complex128)
+        lib().or_get_site_nums(self.h, _p(out))
+        return [out[k * L:(k + 1) * L] for k in range(4)]
+
     def cholesky_nums(self):
         b = np.zeros(self.G, np.complex128)
         e = np.zeros(self.G, np.complex128)
@@ -361,7 +373,9 @@ def cp_engine(m, W, seed, mgs_step=10, pop_step=40, force_type="dynamicForce"):
                            z(m.expHalfDtK), z(m.expMinusHalfDtK), d(m.U), d(m.mu), d(m.hx),
                            d(m.hy), d(m.hz), None, z(m.phiT), float(np.real(m.logwT)),
                            float(np.imag(m.logwT)), seed)
-    return Engine(h, "cp", 2 * m.L, m.N, W)
+    eng = Engine(h, "cp", 2 * m.L, m.N, W)
+    eng.seed = seed
+    return eng
 
 
 def pl_engine(m, W, seed, mgs_step=10, pop_step=10, force_type="dynamicForce", log_one_body=False):
@@ -390,4 +404,6 @@ def pl_engine(m, W, seed, mgs_step=10, pop_step=10, force_type="dynamicForce", l
                            m.dt, m.ET, m.force_cap, mgs_step, pop_step, d(m.chol), d(m.bg), d(m.t),
                            *args, None, z(m.phiTUp), z(m.phiTDn), float(np.real(m.logwT)),
                            float(np.imag(m.logwT)), seed)
-    return Engine(h, "pl", m.n, max(m.nup, m.ndn), W, G=m.G, nup=m.nup, ndn=m.ndn)
+    eng = Engine(h, "pl", m.n, max(m.nup, m.ndn), W, G=m.G, nup=m.nup, ndn=m.ndn)
+    eng.seed = seed
+    return eng

@@ -115,6 +115,11 @@ def test_cp_measurement_parity():
     assert abs(mg[1] / mg[0] - mo[1] / mo[0]) < STEP_TOL * abs(mo[1] / mo[0])
     for k in (2, 3, 4):
         assert abs(mg[k] - mo[k]) <= STEP_TOL * max(1.0, abs(mo[1]))
+    # NupNum, NdnNum, SplusNum, SminusNum (HubbardSOCMeasureFixedSDSD.cpp:221-255)
+    sg, so = g.site_nums(), o.site_nums()
+    for a, b in zip(sg, so):
+        assert np.abs(a - b).max() <= STEP_TOL * abs(mo[0])
+    assert abs((sg[0].sum() + sg[1].sum()) / mg[0] - m.N) < 1e-9
 
 
 def test_cp_project_half_roundtrip():
