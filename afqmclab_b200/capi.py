@@ -34,6 +34,7 @@ SYMBOLS = [
     "afqmc_batch_create", "afqmc_batch_step", "afqmc_batch_synchronize", "afqmc_batch_destroy",
     "afqmc_batch_set_stream",
     "afqmc_set_autotune", "afqmc_bounded_wait_check", "afqmc_get_site_nums",
+    "afqmc_pack_walkers", "afqmc_unpack_walkers",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -106,6 +107,8 @@ def _declare(L):
     L.afqmc_copy_walker_out.argtypes = [P, I, P]
     L.afqmc_copy_walker_in.argtypes = [P, I, P]
     L.afqmc_apply_table.argtypes = [P, P]
+    L.afqmc_pack_walkers.argtypes = [P, I, P, P]
+    L.afqmc_unpack_walkers.argtypes = [P, I, P, P]
     L.afqmc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), I, PP]
     L.afqmc_batch_step.argtypes = [P, I]
     L.afqmc_batch_synchronize.argtypes = [P]
@@ -312,6 +315,14 @@ class Engine:
 
     def copy_walker_in(self, w, src_ptr):
         _check(lib().afqmc_copy_walker_in(self.h, w, src_ptr))
+
+    def pack_walkers(self, idx, dst_ptr):
+        i = np.ascontiguousarray(idx, dtype=np.int32)
+        _check(lib().afqmc_pack_walkers(self.h, len(i), _p(i), dst_ptr))
+
+    def unpack_walkers(self, slots, src_ptr):
+        i = np.ascontiguousarray(slots, dtype=np.int32)
+        _check(lib().afqmc_unpack_walkers(self.h, len(i), _p(i), src_ptr))
 
     def apply_table(self, table):
         t = np.ascontiguousarray(table, dtype=np.int32)

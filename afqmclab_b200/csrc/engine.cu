@@ -1413,6 +1413,36 @@ int afqmc_copy_walker_in(afqmc_engine *e, int w, const void *src_dev)
     return AFQMC_OK;
 }
 
+namespace {
+int walker_xfer(afqmc_engine *e, int count, const int *idx, zd *buf, bool unpack)
+{
+    if (!e || count < 0 || (count > 0 && (!idx || !buf)) || count > e->W) return fail(AFQMC_ERR_ARG, "bad argument");
+    if (count == 0) return AFQMC_OK;
+    std::vector<char> seen(e->W, 0);
+    for (int k = 0; k < count; ++k) {
+        if (idx[k] < 0 || idx[k] >= e->W) return fail(AFQMC_ERR_ARG, "walker index out of range");
+        if (unpack && seen[idx[k]]++) return fail(AFQMC_ERR_ARG, "a slot appears twice in the unpack list");
+    }
+    CUDA_TRY(cudaMemcpyAsync(e->table, idx, sizeof(int) * count, cudaMemcpyHostToDevice, e->stream));
+    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+    launch_walker_xfer(count, e->wsize, e->table, e->wf, e->logw, buf, unpack, e->stream);
+    TRY(check_launch());
+    if (unpack && e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return AFQMC_OK;
+}
+}  // namespace
+
+int afqmc_pack_walkers(afqmc_engine *e, int count, const int *idx, void *dst_dev)
+{
+    return walker_xfer(e, count, idx, (zd *)dst_dev, false);
+}
+
+int afqmc_unpack_walkers(afqmc_engine *e, int count, const int *slots, const void *src_dev)
+{
+    return walker_xfer(e, count, slots, (zd *)const_cast<void *>(src_dev), true);
+}
+
 int afqmc_apply_table(afqmc_engine *e, const int *table)
 {
     if (!e || !table) return fail(AFQMC_ERR_ARG, "null argument");

@@ -1326,6 +1326,25 @@ __global__ void pop_gather_kernel(int W, long long wsize, const int *table, zd *
     if (threadIdx.x == 0) logw[i] = logw[j];
 }
 
+// Walkers idx[k] -> transfer record k of buf (the walker's matrix, then its
+// logw), or back (unpack: record k -> slot idx[k]); one block per record.
+__global__ void walker_xfer_kernel(int count, long long wsize, const int *idx, zd *wf, zd *logw, zd *buf,
+                                   int unpack)
+{
+    const int k = blockIdx.x;
+    if (k >= count) return;
+    const int w = idx[k];
+    zd *rec = buf + (size_t)k * (wsize + 1);
+    zd *mat = wf + (size_t)w * wsize;
+    if (unpack) {
+        for (long long e = threadIdx.x; e < wsize; e += blockDim.x) mat[e] = rec[e];
+        if (threadIdx.x == 0) logw[w] = rec[wsize];
+    } else {
+        for (long long e = threadIdx.x; e < wsize; e += blockDim.x) rec[e] = mat[e];
+        if (threadIdx.x == 0) rec[wsize] = logw[w];
+    }
+}
+
 __global__ void set_int_kernel(int *p, int v, int count)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1747,6 +1766,13 @@ void launch_pop_gather(int W, long long wsize, const int *table, zd *wf, zd *log
 {
     g_launch_count++;
     pop_gather_kernel<<<W, 256, 0, s>>>(W, wsize, table, wf, logw);
+}
+
+void launch_walker_xfer(int count, long long wsize, const int *idx, zd *wf, zd *logw, zd *buf, bool unpack,
+                        cudaStream_t s)
+{
+    g_launch_count++;
+    walker_xfer_kernel<<<count, 256, 0, s>>>(count, wsize, idx, wf, logw, buf, unpack ? 1 : 0);
 }
 
 void launch_set_int(int *p, int v, int count, cudaStream_t s)

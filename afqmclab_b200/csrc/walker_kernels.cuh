@@ -78,6 +78,9 @@ void launch_mgs(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, z
 void launch_pop_comb(int W, const double *weight, const double *uniforms, uint64_t seed,
                      unsigned long long *counter, int *number, int *table, int *status,
                      cudaStream_t s);
+// Batched walker transfer records (matrix + logw each), walker idx[k] <-> record k.
+void launch_walker_xfer(int count, long long wsize, const int *idx, zd *wf, zd *logw, zd *buf, bool unpack,
+                        cudaStream_t s);
 void launch_pop_gather(int W, long long wsize, const int *table, zd *wf, zd *logw,
                        cudaStream_t s);
 void launch_set_int(int *p, int v, int count, cudaStream_t s);

@@ -1,14 +1,19 @@
-"""Population control across processes, one walker population per GPU.
+"""Population control and estimators across processes, one walker population
+per GPU.
 
 The reference runs W/P walkers per MPI rank and, at every popControlStep,
 gathers the weights on rank 0, builds the table there, scatters it and moves
-walkers with MPI_Isend/Recv (populationControl<T>, populationControl.h:20-109;
+walkers one MPI message each (populationControl<T>, populationControl.h:20-109;
 popConfiguration(size, weight), populationControlConfiguration.cpp:24-101).
+Its estimators are summed over ranks before they are used or written
+(HubbardSOCMeasureFixedSDSD::returnEnergy, HubbardSOCMeasureFixedSDSD.cpp:52-61).
 
 Here every rank all-gathers the weights, draws the comb's uniforms from one
-shared counter-based stream and builds the same table itself (no scatter);
-only the walkers whose parent lives on another rank move, point to point
-(NCCL over NVLink between GPUs, gloo between CPU processes).  popConfiguration
+shared counter-based stream and builds the same table itself (no scatter).
+Only the walkers whose parent lives on another rank move: all moves from one
+rank to another are packed into one contiguous buffer by one kernel and
+travel as one point-to-point message (NCCL over NVLink between GPUs, gloo
+between CPU processes), then one kernel unpacks them.  popConfiguration
 fills empty slots inside each rank's chunk first, so most copies stay local.
 """
 import numpy as np
@@ -47,16 +52,16 @@ class EnginePopulation:
     def weights(self):
         return self.eng.pop_weights()
 
-    def pack(self, j):
-        buf = torch.empty(self.words, dtype=torch.float64, device=self.device)
-        self.eng.copy_walker_out(j, buf.data_ptr())
+    def pack_many(self, idx):
+        buf = torch.empty(len(idx) * self.words, dtype=torch.float64, device=self.device)
+        self.eng.pack_walkers(idx, buf.data_ptr())
         return buf
 
-    def empty(self):
-        return torch.empty(self.words, dtype=torch.float64, device=self.device)
+    def empty_many(self, count):
+        return torch.empty(count * self.words, dtype=torch.float64, device=self.device)
 
-    def unpack(self, i, buf):
-        self.eng.copy_walker_in(i, buf.data_ptr())
+    def unpack_many(self, slots, buf):
+        self.eng.unpack_walkers(slots, buf.data_ptr())
 
     def apply_local(self, table):
         self.eng.apply_table(table)
@@ -73,19 +78,38 @@ class ArrayPopulation:
     def weights(self):
         return self.w
 
-    def pack(self, j):
-        return self.walkers[j].clone()
+    def pack_many(self, idx):
+        return self.walkers[list(idx)].clone().reshape(-1)
 
-    def empty(self):
-        return torch.empty_like(self.walkers[0])
+    def empty_many(self, count):
+        return torch.empty((count,) + tuple(self.walkers.shape[1:]), dtype=self.walkers.dtype).reshape(-1)
 
-    def unpack(self, i, buf):
-        self.walkers[i] = buf
+    def unpack_many(self, slots, buf):
+        self.walkers[list(slots)] = buf.reshape((len(slots),) + tuple(self.walkers.shape[1:]))
 
     def apply_local(self, table):
         for i, j in enumerate(table):
             if i != j:
                 self.walkers[i] = self.walkers[j]
+
+
+def transfer_plan(table, W, rank):
+    """For this rank: {peer: parents to send (local indices, table order)} and
+    {peer: slots to fill (local indices, same order)}, plus the local table."""
+    sends, recvs = {}, {}
+    local = np.arange(W, dtype=np.int32)
+    for i, j in enumerate(table):
+        j = int(j)
+        ri, rj = i // W, j // W
+        if ri == rj:
+            if ri == rank:
+                local[i - rank * W] = j - rank * W
+            continue
+        if rj == rank:
+            sends.setdefault(ri, []).append(j - rank * W)
+        elif ri == rank:
+            recvs.setdefault(rj, []).append(i - rank * W)
+    return sends, recvs, local
 
 
 def global_pop_control(pop, seed, counter, group=None, device="cpu"):
@@ -99,26 +123,39 @@ def global_pop_control(pop, seed, counter, group=None, device="cpu"):
     weights = torch.cat(gathered).cpu().numpy()
     L = W * world
     table = capi.pop_configuration_host(weights, stream_uniforms(seed, counter, L), size=world)
-    ops, recvd = [], []
-    for i, j in enumerate(table):
-        ri, rj = i // W, int(j) // W
-        if ri == rj:
-            continue
-        if rj == rank:
-            ops.append(dist.P2POp(dist.isend, pop.pack(int(j) - rank * W), ri, group))
-        elif ri == rank:
-            buf = pop.empty()
-            ops.append(dist.P2POp(dist.irecv, buf, rj, group))
-            recvd.append((i - rank * W, buf))
+    sends, recvs, local = transfer_plan(table, W, rank)
+    ops, incoming = [], []
+    for peer in sorted(sends):
+        ops.append(dist.P2POp(dist.isend, pop.pack_many(sends[peer]), peer, group))
+    for peer in sorted(recvs):
+        buf = pop.empty_many(len(recvs[peer]))
+        ops.append(dist.P2POp(dist.irecv, buf, peer, group))
+        incoming.append((recvs[peer], buf))
     if ops:
         for req in dist.batch_isend_irecv(ops):
             req.wait()
-    for i, buf in recvd:
-        pop.unpack(i, buf)
-    local = np.arange(W, dtype=np.int32)
-    for i in range(rank * W, (rank + 1) * W):
-        j = int(table[i])
-        if j // W == rank:
-            local[i - rank * W] = j - rank * W
+    # local copies read only this rank's own parents, which the incoming
+    # walkers never overwrite (a slot filled from another rank is not a
+    # parent here), so the order of the two steps is free
     pop.apply_local(local)
+    for slots, buf in incoming:
+        pop.unpack_many(slots, buf)
     return table, counter + L
+
+
+def global_measurement(eng, group=None, device="cpu"):
+    """Mixed-estimator sums of all ranks (MPISum of den, HNum, ...):
+    returns the summed 5-vector of afqmc_get_measurement and, for a
+    phaseless engine, the summed choleskyBgNum / choleskyExNum."""
+    m = eng.measurement()
+    parts = [m]
+    if eng.kind == "pl":
+        parts.extend(eng.cholesky_nums())
+    flat = np.concatenate(parts)
+    t = torch.from_numpy(flat.view(np.float64).copy()).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    tot = t.cpu().numpy().view(np.complex128)
+    if eng.kind == "pl":
+        G = eng.G
+        return tot[:5], tot[5:5 + G], tot[5 + G:5 + 2 * G]
+    return tot[:5], None, None

@@ -11,11 +11,14 @@ G=640 Cholesky vectors, 2048 walkers, dt=0.005.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload molecule128|hubbard8x8|...] [--precision mixed|fp64]
 
-Under torchrun (N > 1) every rank advances its own population of the same
-size (walkers are independent between population controls: weak scaling);
-the timed region is bracketed by a barrier and the maximum over ranks is
-reported.  `--impl reference` times the CPU oracle port of the reference's
-algorithm on the host cores (rank 0 only).
+Under torchrun (N > 1) the ranks hold the shards of one population, each
+shard the size of the one-GPU workload (weak scaling): population control
+runs across ranks at the reference's cadence (all-gathered weights, one
+comb, walkers that change rank moved as one NCCL message per peer) and the
+estimator sums are all-reduced at every measurement; the timed region is
+bracketed by a barrier and the maximum over ranks is reported.
+`--impl reference` times the CPU oracle port of the reference's algorithm on
+the host cores (rank 0 only).
 """
 import argparse
 import json
@@ -211,19 +214,26 @@ def cp_phase_model(m, W, precision):
     }
 
 
-def build_engine(capi, inputs, name, precision, seed):
+NO_LOCAL_POP = 1 << 30   # pop_control_step of an engine whose comb runs across ranks
+
+
+def build_engine(capi, inputs, name, precision, seed, local_pop=True):
+    """The workload's engine and population.  With local_pop False the engine
+    never combs on its own (the cross-rank population control does)."""
     m, c = inputs.make_config(name)
     prec = capi.AFQMC_MIXED if precision == "mixed" else capi.AFQMC_FP64
+    pop = c["pop"] if local_pop else NO_LOCAL_POP
     if c["kind"] == "pl":
-        eng = capi.pl_engine(m, c["W"], seed, c["mgs"], c["pop"], precision=prec)
+        eng = capi.pl_engine(m, c["W"], seed, c["mgs"], pop, precision=prec)
         wf, lw, al = inputs.initial_walkers(m.phiTUp, c["W"])
     else:
-        eng = capi.cp_engine(m, c["W"], seed, c["mgs"], c["pop"], precision=prec)
+        eng = capi.cp_engine(m, c["W"], seed, c["mgs"], pop, precision=prec)
         wf, lw, al = inputs.initial_walkers(m.phiT, c["W"])
     eng.set_walkers(wf, lw, al)
     # initialMgsAndPopControl (afqmcPhaselessSetWalker.cpp:140-144)
     eng.modify_gm()
-    eng.pop_control()
+    if local_pop:
+        eng.pop_control()
     return eng, m, c, (wf, lw, al)
 
 
@@ -232,6 +242,37 @@ def run_steps(eng, k, start, measure_skip):
         if (start + i) % measure_skip == 0:
             eng.add_mixed_measurement()
         eng.step(1)
+
+
+class ShardedRunner:
+    """Steps of one population sharded over the ranks (N > 1): the engine
+    steps its own walkers; every pop_step steps the population control runs
+    across ranks (all-gather of the weights, the same comb on every rank,
+    walkers that change rank packed into one message per peer), and every
+    measurement's sums are all-reduced (the reference's MPISum of HNum, den
+    and the per-vector sums).  Every rank takes the same collective steps."""
+
+    def __init__(self, eng, pop_step, measure_skip, device, seed=20240503):
+        from afqmclab_b200 import parallel
+        self.parallel = parallel
+        self.eng, self.pop_step, self.measure_skip = eng, pop_step, measure_skip
+        self.device = device
+        self.pop = parallel.EnginePopulation(eng, device)
+        self.seed, self.counter = seed, 0
+
+    def control(self):
+        _, self.counter = self.parallel.global_pop_control(self.pop, self.seed, self.counter,
+                                                           device=self.device)
+
+    def __call__(self, k, start):
+        for i in range(k):
+            s = start + i
+            if s % self.measure_skip == 0:
+                self.eng.add_mixed_measurement()
+                self.parallel.global_measurement(self.eng, device=self.device)
+            self.eng.step(1)
+            if (s + 1) % self.pop_step == 0:
+                self.control()
 
 
 def energy_check(capi, inputs, name, steps, measure_skip, stream, seed):
@@ -529,21 +570,28 @@ def main():
         return r
 
     precision = default_precision(args)
+    local_pop = world == 1
     try:
-        eng, m, c, init = build_engine(capi, inputs, args.workload, precision, 77 + rank)
+        eng, m, c, init = build_engine(capi, inputs, args.workload, precision, 77 + rank, local_pop)
     except capi.AfqmcError:
         if args.precision != "auto":
             raise
         precision = "fp64"
-        eng, m, c, init = build_engine(capi, inputs, args.workload, precision, 77 + rank)
+        eng, m, c, init = build_engine(capi, inputs, args.workload, precision, 77 + rank, local_pop)
     W = c["W"]
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
     if not args.no_graphs:
         eng.set_graphs(True)
+    if world == 1:
+        def runner(k, start):
+            run_steps(eng, k, start, args.measure_skip)
+    else:
+        runner = ShardedRunner(eng, c["pop"], args.measure_skip, torch.device("cuda", local))
+        runner.control()   # initialMgsAndPopControl's popControl, across ranks
 
     # warm-up
-    run_steps(eng, args.warmup, 0, args.measure_skip)
+    runner(args.warmup, 0)
     eng.synchronize()
 
     def barrier():
@@ -554,11 +602,11 @@ def main():
     # timed region: K steps, inputs resident in HBM (population + model
     # tensors exceed the 126 MB L2 at this size), graphs replayed
     eng.profile(True)
-    run_steps(eng, args.steps, args.warmup, args.measure_skip)
+    runner(args.steps, args.warmup)
     eng.synchronize()
     prof = eng.profile_get()
     eng.profile(False)
-    run_steps(eng, 2, args.warmup + args.steps, args.measure_skip)
+    runner(2, args.warmup + args.steps)
     eng.synchronize()
     launches0 = capi.launch_count()
     clocks = ClockSampler(dev)
@@ -569,7 +617,7 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    run_steps(eng, args.steps, args.warmup + 2 + args.steps, args.measure_skip)
+    runner(args.steps, args.warmup + 2 + args.steps)
     ev1.record(stream)
     ev1.synchronize()
     barrier()
@@ -598,14 +646,14 @@ def main():
     # staging slots: do it, and one step, before the clock starts
     eng.set_walkers_async(h_wf.data_ptr(), h_lw.data_ptr(), h_al.data_ptr())
     eng.upload_wait()
-    run_steps(eng, 1, 1, args.measure_skip)
+    runner(1, 1)
     capi._check(lib.afqmc_get_measurement(eng.h, meas.ctypes.data))
     eng.synchronize()
     barrier()
     t0 = time.perf_counter()
     eng.set_walkers_async(h_wf.data_ptr(), h_lw.data_ptr(), h_al.data_ptr())
     for i in range(e2e_steps):
-        run_steps(eng, 1, i, args.measure_skip)
+        runner(1, i)
         if i + 1 < e2e_steps:
             eng.set_walkers_async(h_wf.data_ptr(), h_lw.data_ptr(), h_al.data_ptr())
         capi._check(lib.afqmc_get_measurement(eng.h, meas.ctypes.data))

@@ -295,6 +295,14 @@ long long afqmc_walker_bytes(afqmc_engine *e);
 /* Copy walker w to / from a device buffer of afqmc_walker_bytes bytes. */
 int afqmc_copy_walker_out(afqmc_engine *e, int w, void *dst_dev);
 int afqmc_copy_walker_in(afqmc_engine *e, int w, const void *src_dev);
+/* Batched transfer records for the walkers that change rank: pack writes
+ * walkers idx[0..count) back to back (afqmc_walker_bytes each) to dst_dev;
+ * unpack fills slots[0..count) (distinct) from src_dev.  One kernel each, so
+ * a whole population control's moves to one peer travel as one message
+ * (the reference sends one walker per MPI message, populationControl.h:55-100).
+ * idx / slots are host arrays. */
+int afqmc_pack_walkers(afqmc_engine *e, int count, const int *idx, void *dst_dev);
+int afqmc_unpack_walkers(afqmc_engine *e, int count, const int *slots, const void *src_dev);
 /* In-place copies walker[i] = walker[table[i]] within this rank (table in
  * local indices; parents keep their own slot). */
 int afqmc_apply_table(afqmc_engine *e, const int *table);

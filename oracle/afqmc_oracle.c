@@ -1131,10 +1131,11 @@ or_gm_ctx c = {e, ws};
 /* popControl (afqmcConstraintPathProjection.cpp:103-156) in the serial
  * build: weights, popConfiguration(1, weight), in-place copies.
  * table/weights outputs may be NULL. */
-void or_pop_control(or_engine *e, int *tableOut, double *weightOut)
+/* The weights half of popControl (afqmcConstraintPathProjection.cpp:106-122):
+ * weight = Re exp(logOverlap), logw -= logOverlap, every walker revived. */
+void or_pop_weights(or_engine *e, double *weight)
 {
     int W = e->W; size_t ws = or_wsize(e);
-    double *weight = (double *)calloc((size_t)W, sizeof(double));
     for (int w = 0; w < W; ++w) {
         if (e->alive[w]) {
             int info;
@@ -1147,6 +1148,13 @@ void or_pop_control(or_engine *e, int *tableOut, double *weightOut)
         }
     }
     for (int w = 0; w < W; ++w) e->alive[w] = 1; /* checkAndResetWalkerIsAlive */
+}
+
+void or_pop_control(or_engine *e, int *tableOut, double *weightOut)
+{
+    int W = e->W; size_t ws = or_wsize(e);
+    double *weight = (double *)calloc((size_t)W, sizeof(double));
+    or_pop_weights(e, weight);
     double *u = (double *)malloc(sizeof(double) * W);
     for (int i = 0; i < W; ++i) u[i] = or_uniform(&e->rng);
     int *table = (int *)malloc(sizeof(int) * W);

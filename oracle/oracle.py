@@ -107,6 +107,7 @@ def _declare(L):
     L.or_green_matrix.argtypes = [P, c_int, c_int, P]
     L.or_modify_gm.argtypes = [P]
     L.or_pop_control.argtypes = [P, P, P]
+    L.or_pop_weights.argtypes = [P, P]
     L.or_project_one_step.argtypes = [P, c_int]
     L.or_set_cadence.argtypes = [P, c_int, c_int]
     L.or_project_half.argtypes = [P, c_int]
@@ -304,6 +305,11 @@ class Engine:
         weight = np.zeros(self.W)
         lib().or_pop_control(self.h, _p(table), _p(weight))
         return table, weight
+
+    def pop_weights(self):
+        w = np.zeros(self.W)
+        lib().or_pop_weights(self.h, _p(w))
+        return w
 
     def project_half(self, which):
         lib().or_project_half(self.h, which)
