@@ -948,6 +948,24 @@ static void or_pl_build_M(const or_engine *e, const zc *aux, zc *M)
     }
 }
 
+/* logw of CholeskyReal::getTwoBodySampleFromAuxForce (choleskyReal.cpp:104-124):
+ * 1/2 sum f^2 - sum x f - sqrt(-dt) sum x bg */
+static zc or_pl_sample_logw(const or_engine *e, const zc *aux, const zc *force)
+{
+    zc f2 = 0, xf = 0, xb = 0;
+    for (int g = 0; g < e->G; ++g) { f2 += force[g] * force[g]; xf += aux[g] * force[g]; xb += aux[g] * e->bg[g]; }
+    return 0.5 * f2 - xf - e->sqrtMinusDt * xb;
+}
+
+/* Stand-alone two-body sample of the engine's Cholesky vectors and
+ * background: M (n x n) and its logw for given aux and force (G each). */
+void or_pl_two_body_sample(const or_engine *e, const double *aux, const double *force, double *M,
+                           double *logw)
+{
+    or_pl_build_M(e, (const zc *)aux, (zc *)M);
+    *(zc *)logw = or_pl_sample_logw(e, (const zc *)aux, (const zc *)force);
+}
+
 static void or_taylor_stats(or_engine *e, int order)
 {
     e->taylorCalls++; e->taylorTotal += order;
@@ -1037,9 +1055,7 @@ static void or_pass2_body(void *c_, int w)
             /* CholeskyReal::sampleAuxFromForce (choleskyReal.cpp:57-65) */
             for (int g = 0; g < G; ++g) aux[g] = or_gaussian(&r) + force[g];
             /* getTwoBodySampleFromAuxForce (:104-124) */
-            zc f2 = 0, xf = 0, xb = 0;
-            for (int g = 0; g < G; ++g) { f2 += force[g] * force[g]; xf += aux[g] * force[g]; xb += aux[g] * e->bg[g]; }
-            zc sampleLogw = 0.5 * f2 - xf - e->sqrtMinusDt * xb;
+            zc sampleLogw = or_pl_sample_logw(e, aux, force);
             /* second cos projection (afqmcPhaselessProjection.cpp:105-111) */
             zc auxForce = 0;
             for (int g = 0; g < G; ++g) auxForce += aux[g] * force[g];

@@ -108,6 +108,7 @@ def _declare(L):
     L.or_modify_gm.argtypes = [P]
     L.or_pop_control.argtypes = [P, P, P]
     L.or_pop_weights.argtypes = [P, P]
+    L.or_pl_two_body_sample.argtypes = [P, P, P, P, P]
     L.or_project_one_step.argtypes = [P, c_int]
     L.or_set_cadence.argtypes = [P, c_int, c_int]
     L.or_project_half.argtypes = [P, c_int]
@@ -305,6 +306,15 @@ class Engine:
         weight = np.zeros(self.W)
         lib().or_pop_control(self.h, _p(table), _p(weight))
         return table, weight
+
+    def two_body_sample(self, aux, force):
+        """(M, logw) of getTwoBodySampleFromAuxForce for explicit aux and force."""
+        a = np.ascontiguousarray(aux, dtype=np.complex128)
+        f = np.ascontiguousarray(force, dtype=np.complex128)
+        M = np.zeros((self.n, self.n), np.complex128, order="F")
+        lw = np.zeros(1, np.complex128)
+        lib().or_pl_two_body_sample(self.h, _p(a), _p(f), _p(M), _p(lw))
+        return M, lw[0]
 
     def pop_weights(self):
         w = np.zeros(self.W)
