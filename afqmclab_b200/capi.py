@@ -252,6 +252,12 @@ class Engine:
         _check(lib().afqmc_get_site_nums(self.h, *[_p(a) for a in out]))
         return out
 
+    def update_background_only(self, bg):
+        """New background for the two-body sampling; the one-body operators
+        stay as they are (updateBackGround without a propagator rebuild)."""
+        b = np.ascontiguousarray(bg, dtype=np.float64)
+        _check(lib().afqmc_pl_update_background(self.h, _p(b), None, 0.0, None, 0.0, None, 0.0))
+
     def update_background(self, m):
         """m: MoleculeInputs after set_background()."""
         a = [_d(m.bg), _z(m.expMinusDtK), _z(m.expHalfDtK), _z(m.expMinusHalfDtK)]

@@ -31,7 +31,7 @@ from . import inputs
 _SEED_COUNTER = struct.Struct("<QQ")
 
 
-def _rank_world():
+def rank_world():
     try:
         import torch.distributed as dist
         if dist.is_available() and dist.is_initialized():
@@ -42,15 +42,15 @@ def _rank_world():
 
 
 def _barrier():
-    rank, world = _rank_world()
+    rank, world = rank_world()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
 
 
-def _sum_over_ranks(a):
+def sum_over_ranks(a):
     """writeThreadSum's MPISum: element-wise sum of a complex array over ranks."""
-    rank, world = _rank_world()
+    rank, world = rank_world()
     a = np.ascontiguousarray(a, dtype=np.complex128)
     if world == 1:
         return a
@@ -67,7 +67,7 @@ def _sum_over_ranks(a):
 def write_walkers(eng, directory=".", walkers_per_rank=None):
     """writeWalkers: rank 0 replaces `directory`/walkers, then every rank
     writes its live walkers as phi_<rank*walkers_per_rank + i>.dat."""
-    rank, _ = _rank_world()
+    rank, _ = rank_world()
     base_dir = os.path.join(directory, "walkers")
     if rank == 0:
         shutil.rmtree(base_dir, ignore_errors=True)
@@ -91,7 +91,7 @@ def read_walkers(eng, directory=".", walkers_per_rank=None, seed=0):
     and is alive; a slot without a file gets a seeded random normalised
     matrix and is dead (fillWalkerRandomly, walkerIsAlive = false), so the
     next population control refills it."""
-    rank, _ = _rank_world()
+    rank, _ = rank_world()
     per = walkers_per_rank or eng.W
     rng = np.random.default_rng(seed + rank)
     wf = np.zeros((eng.n, eng.ncol, eng.W), np.complex128, order="F")
@@ -123,7 +123,7 @@ def read_walkers(eng, directory=".", walkers_per_rank=None, seed=0):
 def save_random(eng, directory="."):
     """randomHaoSave: rank 0 moves random/ to random.bk, then every rank
     writes random/checkpoint_<rank>.dat (int size, then the packed state)."""
-    rank, _ = _rank_world()
+    rank, _ = rank_world()
     rdir = os.path.join(directory, "random")
     bk = os.path.join(directory, "random.bk")
     if rank == 0:
@@ -142,7 +142,7 @@ def save_random(eng, directory="."):
 
 def read_random(eng, directory="."):
     """randomHaoRead: restore this rank's (seed, counter) from its checkpoint."""
-    rank, _ = _rank_world()
+    rank, _ = rank_world()
     with open(os.path.join(directory, "random", f"checkpoint_{rank}.dat"), "rb") as f:
         size = struct.unpack("<i", f.read(4))[0]
         packed = f.read(size)
@@ -165,12 +165,12 @@ def write_measurement(eng, directory="."):
     files (summed over ranks, written by rank 0).  Constrained path: den,
     KNum, VNum, RNum, HNum, NupNum, NdnNum, SplusNum, SminusNum and their
     totals; phaseless: den, TNum, choleskyBgNum, choleskyExNum, HNum."""
-    rank, _ = _rank_world()
+    rank, _ = rank_world()
     m = eng.measurement()
     if eng.kind == "cp":
         site = eng.site_nums()
         parts = np.concatenate([m[:5], *site, [s.sum() for s in site]])
-        tot = _sum_over_ranks(parts)
+        tot = sum_over_ranks(parts)
         L = len(site[0])
         if rank == 0:
             den, H, K, V, R = tot[:5]
@@ -186,7 +186,7 @@ def write_measurement(eng, directory="."):
     else:
         bg, ex = eng.cholesky_nums()
         parts = np.concatenate([m[:3], bg, ex])
-        tot = _sum_over_ranks(parts)
+        tot = sum_over_ranks(parts)
         G = len(bg)
         if rank == 0:
             den, H, T = tot[:3]

@@ -31,3 +31,29 @@ def rel_err(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.abs(a - b).max() / max(1e-300, np.abs(b).max()))
+
+
+def divisors(n):
+    """getDivisors (common/erroranalysisHao): the divisors of n in increasing order."""
+    return [d for d in range(1, n + 1) if n % d == 0]
+
+
+def num_den_block_analysis(num, den, min_blocks=10):
+    """NumDenErrorAnalysis (afqmc/utilities/manipulateMCData/bin/NumDenErrorAnalysis.cpp:36-62)
+    with getMeanError (common/erroranalysisHao/include/serialErrorAnalysis.h:18-47):
+    for each block size b dividing the sample count, the per-block ratios
+    sum(num)/sum(den), their mean and the error sqrt(var/(nb-1)).  Returns
+    (ratio of the totals, the largest error over block sizes that leave at
+    least min_blocks blocks, the per-block-size table)."""
+    num = np.asarray(num)
+    den = np.asarray(den)
+    n = len(num)
+    table = []
+    for b in divisors(n):
+        nb = n // b
+        r = num.reshape(nb, b).sum(1) / den.reshape(nb, b).sum(1)
+        mean = r.mean()
+        err = np.sqrt(np.mean(np.abs(r - mean) ** 2) / (nb - 1)) if nb > 1 else 0.0
+        table.append((b, mean, err))
+    errs = [e for b, _, e in table if n // b >= min_blocks]
+    return num.sum() / den.sum(), max(errs), table
