@@ -15,7 +15,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libafqmc_b200.so")
 SOURCES = ["engine.cu", "zgemm.cu", "walker_kernels.cu", "mixed.cu", "tc_gemm.cu", "exchange_tc.cu",
            "noalloc.cu", "adjoint.cu", "cp_mixed.cu", "overlap_tc.cu", "theta_tc.cu",
-           "exchange_gemm.cu"]
+           "exchange_gemm.cu", "exchange_f64.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 HEADER = os.path.join(os.path.dirname(HERE), "include", "afqmc_b200.h")

@@ -21,6 +21,7 @@
 #include "../../include/afqmc_b200.h"
 #include "common.cuh"
 #include "engine_internal.cuh"
+#include "exchange_f64.cuh"
 #include "mixed.cuh"
 #include "tc_gemm.cuh"
 #include "walker_kernels.cuh"
@@ -214,17 +215,24 @@ void set_blocks(afqmc_engine *e)
 
 // ---------------------------------------------------------------- pieces
 // S_b = phiT_b^H phi (SDSDOperation.cpp:154-164, gmm 'C')
-int overlap_gemm(afqmc_engine *e, const zd *wf, const int *mask)
+// The spin blocks the FP64 step computes: block 0 alone (counted twice) for a
+// closed-shell trial, both otherwise.
+const Blocks &fbl(const afqmc_engine *e)
 {
-    for (int b = 0; b < e->bl.nblk; ++b) {
-        int Ns = e->bl.Ns[b];
+    return (e->exf && e->exf->restricted) ? e->exf->bl1 : e->bl;
+}
+
+int overlap_gemm(afqmc_engine *e, const zd *wf, const int *mask, const Blocks &bl)
+{
+    for (int b = 0; b < bl.nblk; ++b) {
+        int Ns = bl.Ns[b];
         if (Ns == 0) continue;
         ZGemmArgs g;
         g.m = Ns; g.n = Ns; g.k = e->n;
         g.opA = OP_C; g.opB = OP_N;
         g.A = e->phiT[b]; g.lda = e->n; g.strideA = 0;
         g.B = wf; g.ldb = e->n; g.strideB = e->wsize;
-        g.C = e->S + e->bl.sOff[b]; g.ldc = Ns; g.strideC = e->bl.sStride;
+        g.C = e->S + bl.sOff[b]; g.ldc = Ns; g.strideC = bl.sStride;
         g.batch = e->W; g.mask = mask;
         TRY(gemm(g, e->stream));
     }
@@ -232,28 +240,30 @@ int overlap_gemm(afqmc_engine *e, const zd *wf, const int *mask)
 }
 
 // thetaT_b = (S_b^{-1})^T phi_b^T  (zgetrs 'T', SDSDOperation.cpp:166-173)
-int theta_gemm(afqmc_engine *e, const zd *wf, const int *mask)
+int theta_gemm(afqmc_engine *e, const zd *wf, const int *mask, const Blocks &bl)
 {
-    for (int b = 0; b < e->bl.nblk; ++b) {
-        int Ns = e->bl.Ns[b];
+    for (int b = 0; b < bl.nblk; ++b) {
+        int Ns = bl.Ns[b];
         if (Ns == 0) continue;
         ZGemmArgs g;
         g.m = Ns; g.n = e->n; g.k = Ns;
         g.opA = OP_T; g.opB = OP_T;
-        g.A = e->Sinv + e->bl.sOff[b]; g.lda = Ns; g.strideA = e->bl.sStride;
+        g.A = e->Sinv + bl.sOff[b]; g.lda = Ns; g.strideA = bl.sStride;
         g.B = wf; g.ldb = e->n; g.strideB = e->wsize;
-        g.C = e->thetaT + e->bl.tOff[b]; g.ldc = Ns; g.strideC = e->bl.tStride;
+        g.C = e->thetaT + bl.tOff[b]; g.ldc = Ns; g.strideC = bl.tStride;
         g.batch = e->W; g.mask = mask;
         TRY(gemm(g, e->stream));
     }
     return AFQMC_OK;
 }
 
-// phaseless xbar = A^T thetaT for every walker (calculateCholeskyBg, :237-256)
-int xbar_gemm(afqmc_engine *e)
+// phaseless xbar = A^T thetaT for every walker (calculateCholeskyBg, :237-256);
+// a closed-shell block list sums block 0's rows and doubles them
+int xbar_gemm(afqmc_engine *e, const Blocks &bl)
 {
     ZGemmArgs g;
-    g.m = e->G; g.n = e->W; g.k = (int)e->Ktot;
+    g.m = e->G; g.n = e->W; g.k = (int)(bl.mult == 2 ? bl.tOff[1] : e->Ktot);
+    g.alpha = make_double2((double)bl.mult, 0.0);
     g.opA = OP_T; g.opB = OP_N;
     g.A = e->Aall; g.lda = e->Ktot;
     g.B = e->thetaT; g.ldb = e->bl.tStride;
@@ -320,15 +330,16 @@ int project_dtk_dtv(afqmc_engine *e)
     if (e->precision == AFQMC_MIXED) return mixed_project_dtk_dtv(e);
     const bool needTheta = (e->forceType == AFQMC_DYNAMIC_FORCE);
     // overlap, log-determinant, first cos projection
-    { PHASE(AFQMC_PH_OVERLAP); TRY(overlap_gemm(e, e->wf, e->alive)); }
+    const Blocks &bl = fbl(e);
+    { PHASE(AFQMC_PH_OVERLAP); TRY(overlap_gemm(e, e->wf, e->alive, bl)); }
     {
         PHASE(AFQMC_PH_LU);
-        launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, make_double2(0, 0),
+        launch_lu_logdet_inverse(W, bl, e->S, e->Sinv, e->alive, e->logw, make_double2(0, 0),
                                  e->logwT, e->logov, e->alive, e->surv, e->logw, nullptr, e->status,
                                  LU_PROJECT, needTheta, s);
         TRY(check_launch());
     }
-    if (needTheta) { PHASE(AFQMC_PH_THETA); TRY(theta_gemm(e, e->wf, e->surv)); }
+    if (needTheta) { PHASE(AFQMC_PH_THETA); TRY(theta_gemm(e, e->wf, e->surv, bl)); }
     zd hop = one_body_logw(e, 0);
     if (e->kind == KIND_CP) {
         if (needTheta) {
@@ -344,7 +355,7 @@ int project_dtk_dtv(afqmc_engine *e)
         }
         { PHASE(AFQMC_PH_ONEBODY); TRY(one_body(e, 0, e->wfTmp, e->wf, e->surv)); }
     } else {
-        if (needTheta) { PHASE(AFQMC_PH_FORCE); TRY(xbar_gemm(e)); }
+        if (needTheta) { PHASE(AFQMC_PH_FORCE); TRY(xbar_gemm(e, bl)); }
         {
             PHASE(AFQMC_PH_SAMPLE);
             launch_rng_scan(W, e->surv, 2 * e->G, e->counter, e->offs, s);
@@ -386,8 +397,8 @@ int pop_control(afqmc_engine *e)
 {
     PHASE(AFQMC_PH_POPCONTROL);
     if (e->precision == AFQMC_MIXED) return mixed_pop_control(e);
-    TRY(overlap_gemm(e, e->wf, e->alive));
-    launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
+    TRY(overlap_gemm(e, e->wf, e->alive, fbl(e)));
+    launch_lu_logdet_inverse(e->W, fbl(e), e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
                              e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
                              LU_POPWEIGHT, false, e->stream);
     launch_pop_comb(e->W, e->weight, nullptr, e->seed, e->counter, e->number, e->table,
@@ -490,12 +501,12 @@ int add_mixed_measurement_direct(afqmc_engine *e)
     {
         PHASE(AFQMC_PH_MEASURE);
         TRY(one_body(e, 1, e->wf, e->wfTmp, e->alive));
-        TRY(overlap_gemm(e, e->wfTmp, e->alive));
-        launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, one_body_logw(e, 1),
+        TRY(overlap_gemm(e, e->wfTmp, e->alive, fbl(e)));
+        launch_lu_logdet_inverse(W, fbl(e), e->S, e->Sinv, e->alive, e->logw, one_body_logw(e, 1),
                                  e->logwT, e->logov, e->alive, nullptr, nullptr, nullptr,
                                  e->status, LU_PLAIN, true, s);
         TRY(check_launch());
-        TRY(theta_gemm(e, e->wfTmp, e->alive));
+        TRY(theta_gemm(e, e->wfTmp, e->alive, fbl(e)));
     }
     if (e->kind == KIND_CP) {
         PHASE(AFQMC_PH_MEASURE);
@@ -504,18 +515,31 @@ int add_mixed_measurement_direct(afqmc_engine *e)
         launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 3, e->acc, 4 * e->L, e->sites,
                               nullptr, e->siteNum, nullptr, s);
     } else {
-        { PHASE(AFQMC_PH_MEASURE); TRY(xbar_gemm(e)); }
+        const Blocks &bl = fbl(e);
+        const bool exg = e->exf && e->exf->gemm;
+        { PHASE(AFQMC_PH_MEASURE); TRY(xbar_gemm(e, bl)); }
         {
             PHASE(AFQMC_PH_EXCHANGE);
-            if (launch_pl_exchange(W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex, s))
+            if (exg) {
+                // real A: quadratic forms as FP64 GEMMs (exchange_f64.cu); exNum is
+                // accumulated there, the per-walker totals go to the energy
+                bool first = true;
+                for (int b = 0; b < bl.nblk; ++b) {
+                    if (bl.Ns[b] == 0) continue;
+                    TRY(exf64_run(e, e->exf->blk[b], !first, bl.mult));
+                    first = false;
+                }
+            } else if (launch_pl_exchange(W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex, s)) {
                 return fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
+            }
         }
         {
             PHASE(AFQMC_PH_MEASURE);
             launch_pl_energy(W, e->G, e->Ktot, e->wfDaggerT, e->thetaT, e->xbar, e->ex, e->alive,
-                             e->logov, e->eloc, e->den, e->parts, s);
+                             e->logov, e->eloc, e->den, e->parts, s, exg ? e->exf->exTot : nullptr,
+                             bl.mult == 2 ? bl.tOff[1] : e->Ktot, bl.mult);
             launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 1, e->acc, e->G, e->xbar,
-                                  e->ex, e->bgNum, e->exNum, s);
+                                  exg ? nullptr : e->ex, e->bgNum, e->exNum, s);
         }
     }
     return check_launch();
@@ -543,6 +567,8 @@ void free_engine(afqmc_engine *e)
     if (!e) return;
     drop_graphs(e);
     if (e->mx || e->cpm) mixed_destroy(e);
+    delete e->exf;
+    e->exf = nullptr;
     prof_resolve(e);
     for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
     if (e->upStream) cudaStreamSynchronize(e->upStream);
@@ -567,17 +593,53 @@ int engine_pl_local_energy(afqmc_engine *e)
     const int W = e->W;
     cudaStream_t s = e->stream;
     if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
-    TRY(overlap_gemm(e, e->wf, e->alive));
+    TRY(overlap_gemm(e, e->wf, e->alive, e->bl));
     launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, e->logw, make_double2(0, 0),
                              e->logwT, e->logov, e->alive, nullptr, nullptr, nullptr, e->status,
                              LU_PLAIN, true, s);
     TRY(check_launch());
-    TRY(theta_gemm(e, e->wf, e->alive));
-    TRY(xbar_gemm(e));
+    TRY(theta_gemm(e, e->wf, e->alive, e->bl));
+    TRY(xbar_gemm(e, e->bl));
     if (launch_pl_exchange(W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex, s))
         return fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
     launch_pl_energy(W, e->G, e->Ktot, e->wfDaggerT, e->thetaT, e->xbar, e->ex, e->alive, e->logov,
                      e->eloc, e->den, e->parts, s);
+    return check_launch();
+}
+
+// FP64 form, real half-rotated vectors (real trial and Cholesky vectors,
+// tested exactly): the exchange runs as FP64 GEMMs, and a closed-shell trial
+// (equal spin blocks, bit for bit) computes block 0 alone and counts it
+// twice, as the mixed form does.  Complex A keeps the blockwise kernel.
+int fp64_exchange_setup(afqmc_engine *e)
+{
+    std::vector<zd> a((size_t)e->Ktot * e->G);
+    CUDA_TRY(cudaMemcpyAsync(a.data(), e->Aall, sizeof(zd) * a.size(), cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (const zd &v : a)
+        if (v.y != 0.0) return AFQMC_OK;
+    e->exf = new ExF64Scratch();
+    ExF64Scratch &x = *e->exf;
+    if (e->bl.nblk == 2 && e->nup == e->ndn && e->nup > 0) {
+        const size_t cnt = (size_t)e->n * e->nup;
+        std::vector<zd> t0(cnt), t1(cnt);
+        CUDA_TRY(cudaMemcpy(t0.data(), e->phiT[0], sizeof(zd) * cnt, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(t1.data(), e->phiT[1], sizeof(zd) * cnt, cudaMemcpyDeviceToHost));
+        if (std::memcmp(t0.data(), t1.data(), sizeof(zd) * cnt) == 0) {
+            x.restricted = true;
+            x.bl1 = e->bl;
+            x.bl1.nblk = 1;
+            x.bl1.Ns[1] = 0;
+            x.bl1.mult = 2;
+        }
+    }
+    long long Kmax = 0;
+    for (int b = 0; b < e->bl.nblk; ++b) Kmax = std::max(Kmax, (long long)e->bl.Ns[b] * e->n);
+    TRY(exf64_alloc(e, Kmax, x));
+    const Blocks &bl = fbl(e);
+    for (int b = 0; b < bl.nblk; ++b)
+        if (bl.Ns[b] > 0) TRY(exf64_build(e, b, x.blk[b]));
+    x.gemm = true;
     return check_launch();
 }
 
@@ -679,6 +741,7 @@ int afqmc_cp_create(int L, int N, int W, int decomp, int force_type, double dt, 
         CK(gemm(g, e->stream));
     }
     if (precision == AFQMC_MIXED) CK(mixed_create(e));
+    else CK(fp64_exchange_setup(e));
     cudaError_t ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) { free_engine(e); return fail(AFQMC_ERR_CUDA, cudaGetErrorString(ce)); }
 #undef CK
@@ -1032,7 +1095,7 @@ int afqmc_log_overlaps(afqmc_engine *e, double *out)
 {
     if (!e || !out) return fail(AFQMC_ERR_ARG, "null argument");
     if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
-    TRY(overlap_gemm(e, e->wf, nullptr));
+    TRY(overlap_gemm(e, e->wf, nullptr, e->bl));
     launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, nullptr, e->logw, make_double2(0, 0),
                              e->logwT, e->logov, nullptr, nullptr, nullptr, nullptr, nullptr,
                              LU_PLAIN, false, e->stream);
@@ -1047,12 +1110,12 @@ int afqmc_green_matrix(afqmc_engine *e, int walker, int spin, double *out)
     if (!e || !out || walker < 0 || walker >= e->W) return fail(AFQMC_ERR_ARG, "bad argument");
     if (spin < 0 || spin >= e->bl.nblk) return fail(AFQMC_ERR_ARG, "bad spin");
     if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
-    TRY(overlap_gemm(e, e->wf, nullptr));
+    TRY(overlap_gemm(e, e->wf, nullptr, e->bl));
     launch_lu_logdet_inverse(e->W, e->bl, e->S, e->Sinv, nullptr, e->logw, make_double2(0, 0),
                              e->logwT, e->logov, nullptr, nullptr, nullptr, nullptr, nullptr,
                              LU_PLAIN, true, e->stream);
     TRY(check_launch());
-    TRY(theta_gemm(e, e->wf, nullptr));
+    TRY(theta_gemm(e, e->wf, nullptr, e->bl));
     // G^T = thetaT^T phiT^H, i.e. G = conj(phiT) thetaT transposed back on the host
     const int n = e->n, Ns = e->bl.Ns[spin];
     std::vector<zd> h((size_t)n * n);
@@ -1371,8 +1434,8 @@ int afqmc_pop_weights(afqmc_engine *e, double *weight_out)
     if (e->precision == AFQMC_MIXED) {
         TRY(mixed_pop_weights(e));
     } else {
-        TRY(overlap_gemm(e, e->wf, e->alive));
-        launch_lu_logdet_inverse(e->W, e->bl, e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
+        TRY(overlap_gemm(e, e->wf, e->alive, fbl(e)));
+        launch_lu_logdet_inverse(e->W, fbl(e), e->S, nullptr, e->alive, e->logw, make_double2(0, 0),
                                  e->logwT, e->logov, e->alive, nullptr, e->logw, e->weight, e->status,
                                  LU_POPWEIGHT, false, e->stream);
         TRY(check_launch());

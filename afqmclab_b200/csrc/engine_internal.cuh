@@ -12,6 +12,7 @@
 
 struct MixedState;
 struct CpMixedState;
+struct ExF64Scratch;
 
 enum { KIND_CP = 0, KIND_PL = 1 };
 
@@ -66,6 +67,8 @@ struct afqmc_engine {
     // constrained path: per-walker site terms (G_ii up, G_ii down, the two
     // spin-flip off-diagonals; W x 4L) and their den-weighted sums (4L)
     zd *sites = nullptr, *siteNum = nullptr;
+    // FP64 form: closed-shell single block and GEMM exchange (real A)
+    ExF64Scratch *exf = nullptr;
     // mixed-precision state
     MixedState *mx = nullptr;
     CpMixedState *cpm = nullptr;   // constrained-path mixed form

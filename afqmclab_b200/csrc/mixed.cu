@@ -388,18 +388,26 @@ __device__ __forceinline__ void store_b_sw(uint8_t *sB, int a, int i, float v)
 // Taylor series of exp(M) phi (M = sqrt(-dt) sum_g x_g L_g, bf16 operands,
 // fp32 accumulation) for one walker at a time, then the one-body factor:
 //   phi' = S + (E - I) S,  S = sum_k M^k phi / k!
-// Thread i keeps row i of the running sum S in registers; the product
-// accumulators are read back 16 columns at a time and each term is written
-// back as the next bf16 operand.  The
-// order stops at k >= checkFrom once max |term| <= acc (the dynamicOrder
-// rule of the reference's Taylor expansion, CholeskyRealSampleSDOperation /
-// applyToRight with taylor accuracy 1e-10) or at kmax.
-template <int NC>
-__global__ void __launch_bounds__(128, 1)
+// NT = 128 or 256 threads.  Thread t keeps row t % 128 of the running sum S
+// in registers for its share of the NC columns (all of them with 128
+// threads, one half each with 256: warps w and w + 4 read the same TMEM
+// lanes, so the column halves split between them), reads the product
+// accumulators back 16 columns at a time and writes its part of each term
+// back as the next bf16 operand.  The order stops at k >= checkFrom once
+// max |term| <= acc (the dynamicOrder rule of the reference's Taylor
+// expansion, CholeskyRealSampleSDOperation / applyToRight with taylor
+// accuracy 1e-10) or at kmax.
+template <int NC, int NT>
+__global__ void __launch_bounds__(NT, NT == 256 ? 2 : 1)
 taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmE,
                       int W, int n, float *w32, const int *surv, int *order, long long *stats, int kmax,
                       float acc, float relTol, int checkFrom, int doOneBody, int *status, int *err)
 {
+    static_assert(NT == 128 || NT == 256, "128 or 256 threads");
+    constexpr int NG = NT / 128;          // column groups
+    constexpr int NCH = NC / NG;          // columns of one thread
+    constexpr int NW = NT / 32;           // warps
+    static_assert(NCH % 16 == 0, "16-column TMEM reads");
     extern __shared__ uint8_t smem_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int KB = n / 64;
@@ -409,10 +417,11 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     uint8_t *sBi = sBr + (size_t)KB * NC * 128;
     uint64_t *bars = (uint64_t *)(sBi + (size_t)KB * NC * 128);   // [0] M, [1] MMA, [2] E
     uint32_t *tslot = (uint32_t *)(bars + 3);
-    __shared__ float red[4], red0[4];
+    __shared__ float red[NW], red0[NW];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int row = tid;
+    const int row = tid & 127;
+    const int col0 = (tid >> 7) * NCH;    // first column of this thread
     const bool rowOK = row < n;
     if (tid == 0) {
         mbar_init(&bars[0], 1);
@@ -427,7 +436,7 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     __syncthreads();
     tc_fence_after();
     const uint32_t tm = *tslot;
-    const uint32_t lanebase = (uint32_t)(warp * 32) << 16;
+    const uint32_t lanebase = (uint32_t)((warp & 3) * 32) << 16;
     const uint32_t tCr = tm, tCi = tm + 64;
     constexpr uint32_t IDESC = idesc_bf16(128, NC);
     constexpr uint32_t IDESCN = idesc_bf16(128, NC, true);
@@ -452,6 +461,16 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             }
         }
         umma_commit(&bars[1]);
+    };
+    auto block_max = [&](float v, float *buf) {
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) buf[warp] = v;
+    };
+    auto read_max = [&](const float *buf) {
+        float m = buf[0];
+#pragma unroll
+        for (int q = 1; q < NW; ++q) m = fmaxf(m, buf[q]);
+        return m;
     };
 
     // Walkers of this CTA: blockIdx.x, +gridDim.x, ... skipping the dead ones.
@@ -481,29 +500,28 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
         // pulled into L2 while this walker's series runs
         if (tid == 0 && wn < W) bulk_prefetch_l2(w32 + (size_t)wn * 2 * n * NC, (uint32_t)(2 * n * NC * sizeof(float)));
         // order 0: S = phi, operand = bf16(phi); all loads issue before the stores
-        float pr[NC], pi[NC];
+        float pr[NCH], pi[NCH];
 #pragma unroll
-        for (int a = 0; a < NC; ++a) {
-            pr[a] = rowOK ? gw[row + (size_t)n * a] : 0.f;
-            pi[a] = rowOK ? gw[(size_t)n * NC + row + (size_t)n * a] : 0.f;
+        for (int a = 0; a < NCH; ++a) {
+            pr[a] = rowOK ? gw[row + (size_t)n * (col0 + a)] : 0.f;
+            pi[a] = rowOK ? gw[(size_t)n * NC + row + (size_t)n * (col0 + a)] : 0.f;
         }
         float s2 = 0.f;
         if (rowOK) {
 #pragma unroll
-            for (int a = 0; a < NC; ++a) {
-                store_b_sw<NC>(sBr, a, row, pr[a]);
-                store_b_sw<NC>(sBi, a, row, pi[a]);
+            for (int a = 0; a < NCH; ++a) {
+                store_b_sw<NC>(sBr, col0 + a, row, pr[a]);
+                store_b_sw<NC>(sBi, col0 + a, row, pi[a]);
                 s2 = fmaxf(s2, pr[a] * pr[a] + pi[a] * pi[a]);
             }
         }
-        for (int o = 16; o > 0; o >>= 1) s2 = fmaxf(s2, __shfl_xor_sync(0xffffffffu, s2, o));
-        if (lane == 0) red0[warp] = s2;
+        block_max(s2, red0);
         fence_proxy_async();
         tc_fence_before();
         __syncthreads();
         // terms below fp32 resolution of the walker's largest entry cannot
         // change the fp32 sum: the series stops there (or at acc)
-        const float tol = fmaxf(acc, relTol * sqrtf(fmaxf(fmaxf(red0[0], red0[1]), fmaxf(red0[2], red0[3]))));
+        const float tol = fmaxf(acc, relTol * sqrtf(read_max(red0)));
         ok = __syncthreads_and(mbar_wait(&bars[0], phL)) != 0;
         phL ^= 1;
         mPending = false;
@@ -520,14 +538,14 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             float mx = 0.f;
             // Accumulator columns come out of TMEM in chunks of up to 32: all
             // loads of a chunk are issued before the one completion wait.
-            constexpr int CH = (NC % 32 == 0) ? 32 : 16;
+            constexpr int CH = (NCH % 32 == 0) ? 32 : 16;
 #pragma unroll
-            for (int cb = 0; cb < NC; cb += CH) {
+            for (int cb = 0; cb < NCH; cb += CH) {
                 uint32_t cr[CH], ci[CH];
 #pragma unroll
                 for (int c1 = 0; c1 < CH; c1 += 16) {
-                    tmem_ld16_nw(tCr + lanebase + cb + c1, cr + c1);
-                    tmem_ld16_nw(tCi + lanebase + cb + c1, ci + c1);
+                    tmem_ld16_nw(tCr + lanebase + col0 + cb + c1, cr + c1);
+                    tmem_ld16_nw(tCi + lanebase + col0 + cb + c1, ci + c1);
                 }
                 tmem_wait_ld();
 #pragma unroll
@@ -540,19 +558,17 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
                         pi[c0 + a] += ti;
                         if (rowOK) {
                             mx = fmaxf(mx, tr * tr + ti * ti);
-                            store_b_sw<NC>(sBr, c0 + a, row, tr);
-                            store_b_sw<NC>(sBi, c0 + a, row, ti);
+                            store_b_sw<NC>(sBr, col0 + c0 + a, row, tr);
+                            store_b_sw<NC>(sBi, col0 + c0 + a, row, ti);
                         }
                     }
                 }
             }
-            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-            if (lane == 0) red[warp] = mx;
+            block_max(mx, red);
             fence_proxy_async();
             tc_fence_before();
             __syncthreads();
-            const float m4 = fmaxf(fmaxf(red[0], red[1]), fmaxf(red[2], red[3]));
-            const bool conv = (k >= checkFrom) && (sqrtf(m4) <= tol);
+            const bool conv = (k >= checkFrom) && (sqrtf(read_max(red)) <= tol);
             if (conv || k >= kmax) {
                 if (!conv && tid == 0 && status) atomicOr(status + w, (int)ST_TAYLOR_CAP);
                 break;
@@ -581,7 +597,10 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
             }
             if (rowOK) {
 #pragma unroll
-                for (int a = 0; a < NC; ++a) { store_b_sw<NC>(sBr, a, row, pr[a]); store_b_sw<NC>(sBi, a, row, pi[a]); }
+                for (int a = 0; a < NCH; ++a) {
+                    store_b_sw<NC>(sBr, col0 + a, row, pr[a]);
+                    store_b_sw<NC>(sBi, col0 + a, row, pi[a]);
+                }
             }
             fence_proxy_async();
             tc_fence_before();
@@ -599,10 +618,10 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
                 for (int kb = 0; kb < KB; ++kb)
                     tma_load_2d(sMr + kb * 16384, &tmM, &bars[0], kb * 64, (2 * wn) * n);
 #pragma unroll
-            for (int c0 = 0; c0 < NC; c0 += 16) {
+            for (int c0 = 0; c0 < NCH; c0 += 16) {
                 uint32_t vr[16], vi[16];
-                tmem_ld16_nw(tCr + lanebase + c0, vr);
-                tmem_ld16_nw(tCi + lanebase + c0, vi);
+                tmem_ld16_nw(tCr + lanebase + col0 + c0, vr);
+                tmem_ld16_nw(tCi + lanebase + col0 + c0, vi);
                 tmem_wait_ld();
 #pragma unroll
                 for (int a = 0; a < 16; ++a) { pr[c0 + a] += __uint_as_float(vr[a]); pi[c0 + a] += __uint_as_float(vi[a]); }
@@ -610,9 +629,9 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
         }
         if (rowOK) {
 #pragma unroll
-            for (int a = 0; a < NC; ++a) {
-                gw[row + (size_t)n * a] = pr[a];
-                gw[(size_t)n * NC + row + (size_t)n * a] = pi[a];
+            for (int a = 0; a < NCH; ++a) {
+                gw[row + (size_t)n * (col0 + a)] = pr[a];
+                gw[(size_t)n * NC + row + (size_t)n * (col0 + a)] = pi[a];
             }
         }
         if (tid == 0) {
@@ -640,23 +659,40 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     if (warp == 0) tmem_dealloc(tm, 128);
 }
 
+// 256 threads (two per walker row, 16 columns each) for 32-column walkers,
+// whose 256-thread form keeps everything in 128 registers (two CTAs per SM);
+// 128 threads otherwise.  AFQMC_TAYLOR_THREADS=128 selects the 128-thread
+// form for comparison.
+constexpr int taylor_threads(int NC) { return NC == 32 ? 256 : 128; }
+
 template <int NC>
 int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE, int doOneBody)
 {
     const size_t smem = TaylorSmem<NC>::bytes(e->n);
     static std::atomic<unsigned long long> attr{0};
     if (first_on_device(attr)) {
-        cudaFuncSetAttribute(taylor_onebody_kernel<NC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(taylor_onebody_kernel<NC, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TaylorSmem<NC>::bytes(128));
+        cudaFuncSetAttribute(taylor_onebody_kernel<NC, taylor_threads(NC)>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TaylorSmem<NC>::bytes(128));
     }
+    static const bool force128 = [] {
+        const char *v = getenv("AFQMC_TAYLOR_THREADS");
+        return v && atoi(v) == 128;
+    }();
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int perSm = TaylorSmem<NC>::bytes(e->n) <= 112 * 1024 ? 2 : 1;
     int grid = std::min(e->W, perSm * sms);
-    taylor_onebody_kernel<NC><<<grid, 128, smem, e->stream>>>(
-        mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, e->tstats, 30, 1e-10f, 5.9604645e-8f, 4, doOneBody,
-        e->status, e->mx->err);
+    if (taylor_threads(NC) == 256 && !force128)
+        taylor_onebody_kernel<NC, taylor_threads(NC)><<<grid, taylor_threads(NC), smem, e->stream>>>(
+            mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, e->tstats, 30, 1e-10f, 5.9604645e-8f, 4,
+            doOneBody, e->status, e->mx->err);
+    else
+        taylor_onebody_kernel<NC, 128><<<grid, 128, smem, e->stream>>>(
+            mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, e->tstats, 30, 1e-10f, 5.9604645e-8f, 4,
+            doOneBody, e->status, e->mx->err);
     return engine_check_launch();
 }
 

@@ -262,3 +262,34 @@ def test_pl_wide_blocks_step():
     for w in (0, 2):
         for spin in (0, 1):
             assert rel_err(g.green(w, spin), o.green(w, spin)) < STEP_TOL
+
+
+def test_pl_fp64_closed_shell_matches_two_block_form():
+    """With the same trial for both spins the FP64 form computes one spin
+    block and counts it twice, and evaluates the exchange as FP64 GEMMs; a
+    trial whose down block differs from the up block in one last bit takes
+    the two-block path.  Both agree with each other and with the oracle."""
+    m = molecule(n=32, nup=6, ndn=6, G=40)
+    assert np.array_equal(m.phiTUp, m.phiTDn)
+    m2 = molecule(n=32, nup=6, ndn=6, G=40)
+    d = m2.phiTDn.copy()
+    d[0, 0] = np.nextafter(d[0, 0].real, np.inf) + 1j * d[0, 0].imag
+    m2.phiTDn = np.asfortranarray(d)
+    W = 16
+    out = []
+    for mm in (m, m2):
+        g, o = pair_pl(mm, W, 91, 3, 1000, noise=0.05)
+        g.step(4)
+        o.step(4)
+        compare_state(g, o, TRAJ_TOL)
+        for e in (g, o):
+            e.reset_measurement()
+            e.add_mixed_measurement()
+        mg, mo = g.measurement(), o.measurement()
+        assert rel_err(mg[:3], mo[:3]) < STEP_TOL
+        bg, eg = g.cholesky_nums()
+        bo, eo = o.cholesky_nums()
+        assert rel_err(bg, bo) < STEP_TOL and rel_err(eg, eo) < STEP_TOL
+        out.append((g.log_overlaps(), mg))
+    assert logov_close(out[0][0], out[1][0], 1e-9) < 1e-9
+    assert abs(out[0][1][1] / out[0][1][0] - out[1][1][1] / out[1][1][0]) < 1e-9
