@@ -468,13 +468,16 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
         bool sing = false;
         for (int k = 0; k < Ns; ++k) {
             double v = (lane >= k && lane < Ns) ? zcabs1(A[lane * GJ_LD + k]) : -1.0;
+            if (!(v == v)) v = INFINITY;   // a NaN row wins: the comparisons below stay a total order
             int idx = lane;
             for (int o = 16; o > 0; o >>= 1) {
                 double ov = __shfl_xor_sync(0xffffffffu, v, o);
                 int oi = __shfl_xor_sync(0xffffffffu, idx, o);
                 if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
             }
-            const int p = idx;
+            // the pivot row steers the warp-wide branches below (each with a
+            // full-mask __syncwarp): every lane takes lane 0's choice
+            const int p = __shfl_sync(0xffffffffu, idx, 0);
             if (lane == k) myPartner = p;
             if (p != k) {
                 for (int j = lane; j < Ns; j += 32) {
