@@ -34,7 +34,8 @@ SYMBOLS = [
     "afqmc_batch_create", "afqmc_batch_step", "afqmc_batch_synchronize", "afqmc_batch_destroy",
     "afqmc_batch_set_stream",
     "afqmc_set_autotune", "afqmc_bounded_wait_check", "afqmc_get_site_nums",
-    "afqmc_pack_walkers", "afqmc_unpack_walkers",
+    "afqmc_pack_walkers", "afqmc_unpack_walkers", "afqmc_cp_set_observables",
+    "afqmc_get_observables",
 ]
 
 PHASES = ["overlap", "lu", "theta", "force", "sample", "mbuild", "taylor", "onebody", "stabilize",
@@ -108,6 +109,8 @@ def _declare(L):
     L.afqmc_copy_walker_in.argtypes = [P, I, P]
     L.afqmc_apply_table.argtypes = [P, P]
     L.afqmc_pack_walkers.argtypes = [P, I, P, P]
+    L.afqmc_cp_set_observables.argtypes = [P, I]
+    L.afqmc_get_observables.argtypes = [P, P, P, P, P, P]
     L.afqmc_unpack_walkers.argtypes = [P, I, P, P]
     L.afqmc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), I, PP]
     L.afqmc_batch_step.argtypes = [P, I]
@@ -244,6 +247,20 @@ class Engine:
         e = np.zeros(self.G, np.complex128)
         _check(lib().afqmc_get_cholesky_nums(self.h, _p(b), _p(e)))
         return b, e
+
+    def set_observables(self, on=True):
+        _check(lib().afqmc_cp_set_observables(self.h, 1 if on else 0))
+        self.observe = bool(on)
+
+    def observables(self):
+        """greenMatrixNum, densityDensityNum (n x n), splusSminusNum,
+        sminusSplusNum, spairSpairNum (L x L): the observe estimator's sums."""
+        n, L = self.n, self.n // 2
+        out = [np.zeros((n, n), np.complex128, order="F") for _ in range(2)]
+        out += [np.zeros((L, L), np.complex128, order="F") for _ in range(3)]
+        _check(lib().afqmc_get_observables(self.h, *[_p(a) for a in out]))
+        return dict(zip(["greenMatrixNum", "densityDensityNum", "splusSminusNum", "sminusSplusNum",
+                         "spairSpairNum"], out))
 
     def site_nums(self):
         """NupNum, NdnNum, SplusNum, SminusNum (L complex each), CP only."""

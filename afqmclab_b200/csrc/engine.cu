@@ -514,6 +514,18 @@ int add_mixed_measurement_direct(afqmc_engine *e)
                          e->hy, e->hz, e->alive, e->logov, e->eloc, e->den, e->parts, e->sites, s);
         launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 3, e->acc, 4 * e->L, e->sites,
                               nullptr, e->siteNum, nullptr, s);
+        if (e->observe) {
+            // G = conj(phiT) thetaT per walker (SDSDOperation::returnGreenMatrix), then
+            // the observe estimator's sums
+            ZGemmArgs g;
+            g.m = e->n; g.n = e->n; g.k = e->ncol;
+            g.A = e->phiTc; g.lda = e->n; g.strideA = 0;
+            g.B = e->thetaT; g.ldb = e->ncol; g.strideB = e->bl.tStride;
+            g.C = e->Gfull; g.ldc = e->n; g.strideC = (long long)e->n * e->n;
+            g.batch = W; g.mask = e->alive;
+            TRY(gemm(g, s));
+            launch_cp_observe(W, e->L, e->Gfull, e->den, e->alive, e->obs, s);
+        }
     } else {
         const Blocks &bl = fbl(e);
         const bool exg = e->exf && e->exf->gemm;
@@ -741,7 +753,6 @@ int afqmc_cp_create(int L, int N, int W, int decomp, int force_type, double dt, 
         CK(gemm(g, e->stream));
     }
     if (precision == AFQMC_MIXED) CK(mixed_create(e));
-    else CK(fp64_exchange_setup(e));
     cudaError_t ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) { free_engine(e); return fail(AFQMC_ERR_CUDA, cudaGetErrorString(ce)); }
 #undef CK
@@ -828,6 +839,7 @@ int afqmc_pl_create(int n, int Nup, int Ndn, int G, int W, int force_type, doubl
     e->cdv.sqrtDt = std::sqrt(dt);
     e->cdv.constForce = (force_type == AFQMC_CONST_FORCE) ? e->constForcePL : nullptr;
     if (precision == AFQMC_MIXED) CK(mixed_create(e));
+    else CK(fp64_exchange_setup(e));
     cudaError_t ce = cudaStreamSynchronize(e->stream);
     if (ce != cudaSuccess) { free_engine(e); return fail(AFQMC_ERR_CUDA, cudaGetErrorString(ce)); }
 #undef CK
@@ -1015,6 +1027,40 @@ int afqmc_reset_measurement(afqmc_engine *e)
     if (e->bgNum) CUDA_TRY(cudaMemsetAsync(e->bgNum, 0, sizeof(zd) * e->G, e->stream));
     if (e->exNum) CUDA_TRY(cudaMemsetAsync(e->exNum, 0, sizeof(zd) * e->G, e->stream));
     if (e->siteNum) CUDA_TRY(cudaMemsetAsync(e->siteNum, 0, sizeof(zd) * 4 * e->L, e->stream));
+    if (e->obs)
+        CUDA_TRY(cudaMemsetAsync(e->obs, 0, sizeof(zd) * (8LL * e->L * e->L + 3LL * e->L * e->L), e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_cp_set_observables(afqmc_engine *e, int on)
+{
+    if (!e || e->kind != KIND_CP) return fail(AFQMC_ERR_ARG, "constrained-path engine required");
+    drop_graphs(e);
+    if (on && !e->Gfull) {
+        const int n = e->n, N = e->ncol, L = e->L;
+        std::vector<zd> t((size_t)n * N);
+        CUDA_TRY(cudaMemcpyAsync(t.data(), e->phiT[0], sizeof(zd) * t.size(), cudaMemcpyDeviceToHost, e->stream));
+        CUDA_TRY(cudaStreamSynchronize(e->stream));
+        for (zd &v : t) v.y = -v.y;
+        TRY(dupload(e, &e->phiTc, t.data(), t.size()));
+        TRY(dalloc(e, &e->Gfull, (size_t)e->W * n * n));
+        TRY(dalloc(e, &e->obs, (size_t)8 * L * L + (size_t)3 * L * L));
+    }
+    e->observe = on != 0;
+    return AFQMC_OK;
+}
+
+int afqmc_get_observables(afqmc_engine *e, double *greenNum, double *densityDensityNum, double *splusSminusNum,
+                          double *sminusSplusNum, double *spairSpairNum)
+{
+    if (!e || e->kind != KIND_CP || !e->obs) return fail(AFQMC_ERR_STATE, "observables are not enabled");
+    const size_t n2 = 4ULL * e->L * e->L, l2 = (size_t)e->L * e->L;
+    double *dst[5] = {greenNum, densityDensityNum, splusSminusNum, sminusSplusNum, spairSpairNum};
+    const size_t off[5] = {0, n2, 2 * n2, 2 * n2 + l2, 2 * n2 + 2 * l2};
+    const size_t cnt[5] = {n2, n2, l2, l2, l2};
+    for (int k = 0; k < 5; ++k)
+        if (dst[k]) CUDA_TRY(cudaMemcpyAsync(dst[k], e->obs + off[k], sizeof(zd) * cnt[k], cudaMemcpyDeviceToHost, e->stream));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
     return AFQMC_OK;
 }
 

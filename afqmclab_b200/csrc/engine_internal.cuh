@@ -67,6 +67,11 @@ struct afqmc_engine {
     // constrained path: per-walker site terms (G_ii up, G_ii down, the two
     // spin-flip off-diagonals; W x 4L) and their den-weighted sums (4L)
     zd *sites = nullptr, *siteNum = nullptr;
+    // constrained path, observe estimator (off unless enabled): each walker's
+    // full Green's matrix (W x n x n), conj(phiT) and the den-weighted sums
+    // (greenMatrixNum, densityDensityNum: n x n; S+S-, S-S+, pair: L x L)
+    bool observe = false;
+    zd *Gfull = nullptr, *phiTc = nullptr, *obs = nullptr;
     // FP64 form: closed-shell single block and GEMM exchange (real A)
     ExF64Scratch *exf = nullptr;
     // mixed-precision state

@@ -391,7 +391,8 @@ __device__ __forceinline__ void store_b_sw(uint8_t *sB, int a, int i, float v)
 // NT = 128 or 256 threads.  Thread t keeps row t % 128 of the running sum S
 // in registers for its share of the NC columns (all of them with 128
 // threads, one half each with 256: warps w and w + 4 read the same TMEM
-// lanes, so the column halves split between them), reads the product
+// lanes, so the column halves split between them; 256 threads measured
+// 9 % slower at 32 columns and is not launched), reads the product
 // accumulators back 16 columns at a time and writes its part of each term
 // back as the next bf16 operand.  The order stops at k >= checkFrom once
 // max |term| <= acc (the dynamicOrder rule of the reference's Taylor
@@ -659,12 +660,6 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     if (warp == 0) tmem_dealloc(tm, 128);
 }
 
-// 256 threads (two per walker row, 16 columns each) for 32-column walkers,
-// whose 256-thread form keeps everything in 128 registers (two CTAs per SM);
-// 128 threads otherwise.  AFQMC_TAYLOR_THREADS=128 selects the 128-thread
-// form for comparison.
-constexpr int taylor_threads(int NC) { return NC == 32 ? 256 : 128; }
-
 template <int NC>
 int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE, int doOneBody)
 {
@@ -673,26 +668,15 @@ int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE,
     if (first_on_device(attr)) {
         cudaFuncSetAttribute(taylor_onebody_kernel<NC, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TaylorSmem<NC>::bytes(128));
-        cudaFuncSetAttribute(taylor_onebody_kernel<NC, taylor_threads(NC)>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TaylorSmem<NC>::bytes(128));
     }
-    static const bool force128 = [] {
-        const char *v = getenv("AFQMC_TAYLOR_THREADS");
-        return v && atoi(v) == 128;
-    }();
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int perSm = TaylorSmem<NC>::bytes(e->n) <= 112 * 1024 ? 2 : 1;
     int grid = std::min(e->W, perSm * sms);
-    if (taylor_threads(NC) == 256 && !force128)
-        taylor_onebody_kernel<NC, taylor_threads(NC)><<<grid, taylor_threads(NC), smem, e->stream>>>(
-            mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, e->tstats, 30, 1e-10f, 5.9604645e-8f, 4,
-            doOneBody, e->status, e->mx->err);
-    else
-        taylor_onebody_kernel<NC, 128><<<grid, 128, smem, e->stream>>>(
-            mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, e->tstats, 30, 1e-10f, 5.9604645e-8f, 4,
-            doOneBody, e->status, e->mx->err);
+    taylor_onebody_kernel<NC, 128><<<grid, 128, smem, e->stream>>>(
+        mM, mE, e->W, e->n, e->mx->wf32, e->surv, e->order, e->tstats, 30, 1e-10f, 5.9604645e-8f, 4, doOneBody,
+        e->status, e->mx->err);
     return engine_check_launch();
 }
 

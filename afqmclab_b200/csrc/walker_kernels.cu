@@ -1329,6 +1329,58 @@ __global__ void pop_gather_kernel(int W, long long wsize, const int *table, zd *
     if (threadIdx.x == 0) logw[i] = logw[j];
 }
 
+// Observables of HubbardSOCMeasureObserveSDSD::addMeasurement
+// (HubbardSOCMeasureObserveSDSD.cpp:42-185), den-weighted and summed over the
+// alive walkers: greenMatrixNum and densityDensityNum (n x n, n = 2L), and
+// splusSminusNum, sminusSplusNum, spairSpairNum (L x L).  One thread per
+// element (i, j); each sums over the walkers in order, so the sums are
+// reproducible.  G holds each walker's full Green's matrix, column-major.
+__global__ void __launch_bounds__(256)
+cp_observe_kernel(int W, int L, const zd *G, const zd *den, const int *alive, zd *gNum, zd *ddNum,
+                  zd *pmNum, zd *mpNum, zd *pairNum)
+{
+    const int n = 2 * L;
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (e >= (long long)n * n) return;
+    const int i = (int)(e % n), j = (int)(e / n);
+    const bool small = i < L && j < L;
+    zd sg = make_double2(0, 0), sd = make_double2(0, 0), spm = make_double2(0, 0), smp = make_double2(0, 0),
+       spr = make_double2(0, 0);
+    for (int w = 0; w < W; ++w) {
+        if (!alive[w]) continue;
+        const zd d = den[w];
+        const zd *g = G + (size_t)w * n * n;
+        auto at = [&](int r, int c) { return g[r + (size_t)n * c]; };
+        const zd gij = at(i, j);
+        sg = zadd(sg, zmul(gij, d));
+        const zd dd = (i == j) ? at(i, i) : zsub(zmul(at(i, i), at(j, j)), zmul(gij, at(j, i)));
+        sd = zadd(sd, zmul(dd, d));
+        if (small) {
+            zd pm, mp;
+            if (i == j) {
+                const zd both = zsub(zmul(at(i, i), at(i + L, i + L)), zmul(at(i, i + L), at(i + L, i)));
+                pm = zsub(at(i, i), both);
+                mp = zsub(at(i + L, i + L), both);
+            } else {
+                pm = zadd(zneg(zmul(gij, at(j + L, i + L))), zmul(at(i, i + L), at(j + L, j)));
+                mp = zadd(zneg(zmul(at(i + L, j + L), at(j, i))), zmul(at(i + L, i), at(j, j + L)));
+            }
+            const zd pr = zsub(zmul(gij, at(i + L, j + L)), zmul(at(i, j + L), at(i + L, j)));
+            spm = zadd(spm, zmul(pm, d));
+            smp = zadd(smp, zmul(mp, d));
+            spr = zadd(spr, zmul(pr, d));
+        }
+    }
+    gNum[e] = zadd(gNum[e], sg);
+    ddNum[e] = zadd(ddNum[e], sd);
+    if (small) {
+        const long long s = i + (long long)L * j;
+        pmNum[s] = zadd(pmNum[s], spm);
+        mpNum[s] = zadd(mpNum[s], smp);
+        pairNum[s] = zadd(pairNum[s], spr);
+    }
+}
+
 // Walkers idx[k] -> transfer record k of buf (the walker's matrix, then its
 // logw), or back (unpack: record k -> slot idx[k]); one block per record.
 __global__ void walker_xfer_kernel(int count, long long wsize, const int *idx, zd *wf, zd *logw, zd *buf,
@@ -1769,6 +1821,14 @@ void launch_pop_gather(int W, long long wsize, const int *table, zd *wf, zd *log
 {
     g_launch_count++;
     pop_gather_kernel<<<W, 256, 0, s>>>(W, wsize, table, wf, logw);
+}
+
+void launch_cp_observe(int W, int L, const zd *G, const zd *den, const int *alive, zd *obs, cudaStream_t s)
+{
+    g_launch_count++;
+    const long long n2 = 4LL * L * L, l2 = (long long)L * L;
+    cp_observe_kernel<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(W, L, G, den, alive, obs, obs + n2, obs + 2 * n2,
+                                                                  obs + 2 * n2 + l2, obs + 2 * n2 + 2 * l2);
 }
 
 void launch_walker_xfer(int count, long long wsize, const int *idx, zd *wf, zd *logw, zd *buf, bool unpack,

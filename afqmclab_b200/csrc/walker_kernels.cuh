@@ -78,6 +78,9 @@ void launch_mgs(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, z
 void launch_pop_comb(int W, const double *weight, const double *uniforms, uint64_t seed,
                      unsigned long long *counter, int *number, int *table, int *status,
                      cudaStream_t s);
+// Observe-estimator sums (greenMatrixNum, densityDensityNum: n x n each;
+// splusSminusNum, sminusSplusNum, spairSpairNum: L x L each, in that order in obs).
+void launch_cp_observe(int W, int L, const zd *G, const zd *den, const int *alive, zd *obs, cudaStream_t s);
 // Batched walker transfer records (matrix + logw each), walker idx[k] <-> record k.
 void launch_walker_xfer(int count, long long wsize, const int *idx, zd *wf, zd *logw, zd *buf, bool unpack,
                         cudaStream_t s);

@@ -183,6 +183,18 @@ def write_measurement(eng, directory="."):
             for name in ("NupTotNum", "NdnTotNum", "SplusTotNum", "SminusTotNum"):
                 _append_complex(os.path.join(directory, name + ".dat"), tot[off])
                 off += 1
+        if getattr(eng, "observe", False):
+            # HubbardSOCMeasureObserveSDSD::write (HubbardSOCMeasureObserveSDSD.cpp:51-60)
+            obs = eng.observables()
+            names = ["greenMatrixNum", "densityDensityNum", "splusSminusNum", "sminusSplusNum",
+                     "spairSpairNum"]
+            tot = sum_over_ranks(np.concatenate([obs[k].ravel(order="F") for k in names]))
+            off = 0
+            for k in names:
+                size = obs[k].size
+                if rank == 0:
+                    _append_complex(os.path.join(directory, k + ".dat"), tot[off:off + size])
+                off += size
     else:
         bg, ex = eng.cholesky_nums()
         parts = np.concatenate([m[:3], bg, ex])

@@ -737,7 +737,15 @@ def main():
         e1.synchronize()
         ms64 = e0.elapsed_time(e1)
         side = {"value": W * k64 * world / (ms64 / 1e3), "ms_per_step": ms64 / k64, "steps": k64,
-                "speedup_mixed_over_fp64": (ms64 / k64) / (ms / args.steps)}
+                "speedup_mixed_over_fp64": (ms64 / k64) / (ms / args.steps),
+                "algorithm": "same as the mixed form: closed-shell single spin block, exchange as "
+                             "GEMMs (FP64 CUDA-core GEMMs)"}
+        # per-phase times of the FP64 form (direct launches, after the timed steps)
+        f64.profile(True)
+        run_steps(f64, k64, 2 + k64, args.measure_skip)
+        f64.synchronize()
+        side["phases_ms"] = {k: round(v[0], 3) for k, v in f64.profile_get().items() if v[1] > 0}
+        f64.profile(False)
         f64.close()
         if args.energy_steps > 0:
             echeck = energy_check(capi, inputs, args.workload, args.energy_steps, args.measure_skip,

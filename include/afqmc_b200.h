@@ -175,6 +175,17 @@ int afqmc_get_measurement(afqmc_engine *e, double *out);
  * CP only. */
 int afqmc_get_site_nums(afqmc_engine *e, double *NupNum, double *NdnNum, double *SplusNum,
                         double *SminusNum);
+/* Observe estimator of the constrained path (HubbardSOCMeasureObserveSDSD,
+ * HubbardSOCMeasureObserveSDSD.cpp:42-185): with on != 0 every
+ * afqmc_add_mixed_measurement also builds each walker's full Green's matrix
+ * and adds den-weighted greenMatrixNum and densityDensityNum (2L x 2L each)
+ * and splusSminusNum, sminusSplusNum, spairSpairNum (L x L each);
+ * afqmc_reset_measurement clears them.  Off by default (W x 4L^2 complex of
+ * device memory when on).  CP only. */
+int afqmc_cp_set_observables(afqmc_engine *e, int on);
+/* The observe sums, complex column-major (NULL skips one). */
+int afqmc_get_observables(afqmc_engine *e, double *greenNum, double *densityDensityNum,
+                          double *splusSminusNum, double *sminusSplusNum, double *spairSpairNum);
 /* choleskyBgNum / choleskyExNum (G complex each), PL only */
 int afqmc_get_cholesky_nums(afqmc_engine *e, double *bgNum, double *exNum);
 

@@ -645,6 +645,8 @@ typedef struct {
     zc den, HNum, KNum, VNum, RNum, TNum;
     zc *bgNum, *exNum;
     zc *siteNum;       /* CP: NupNum, NdnNum, SplusNum, SminusNum (4 x L) */
+    int observe;       /* CP observe estimator on */
+    zc *obsNum;        /* greenMatrixNum, densityDensityNum (n x n), S+S-, S-S+, pair (L x L) */
     /* taylor statistics */
     long taylorCalls, taylorTotal; int taylorMin, taylorMax;
     int nthreads;
@@ -659,7 +661,7 @@ void or_destroy(or_engine *e)
                     e->expMinusHalfDtK, e->logExpMinusDtK, e->gamma, e->cd00, e->cd01, e->cd10,
                     e->cd11, e->constForceCP, e->U, e->mu, e->hx, e->hy, e->hz, e->wfDaggerK,
                     e->chol, e->bg, e->Aup, e->Adn, e->wfDaggerTUp, e->wfDaggerTDn,
-                    e->constForcePL, e->bgNum, e->exNum, e->siteNum};
+                    e->constForcePL, e->bgNum, e->exNum, e->siteNum, e->obsNum};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
     free(e);
 }
@@ -1222,11 +1224,55 @@ void or_reset_measurement(or_engine *e)
     e->den = e->HNum = e->KNum = e->VNum = e->RNum = e->TNum = 0;
     if (e->bgNum) for (int g = 0; g < e->G; ++g) e->bgNum[g] = e->exNum[g] = 0;
     if (e->siteNum) for (int k = 0; k < 4 * e->L; ++k) e->siteNum[k] = 0;
+    if (e->obsNum) for (int k = 0; k < 11 * e->L * e->L; ++k) e->obsNum[k] = 0;
+}
+
+/* observe estimator switch and sums (greenMatrixNum, densityDensityNum,
+ * splusSminusNum, sminusSplusNum, spairSpairNum, back to back) */
+void or_cp_set_observables(or_engine *e, int on)
+{
+    if (on && !e->obsNum) e->obsNum = (zc *)calloc((size_t)11 * e->L * e->L, sizeof(zc));
+    e->observe = on;
+}
+void or_get_observables(const or_engine *e, double *out)
+{
+    memcpy(out, e->obsNum, sizeof(zc) * 11 * e->L * e->L);
 }
 
 /* per-walker local energy of a propagated walker, accumulated with weight den */
+/* HubbardSOCMeasureObserveSDSD::addGreenMatrix .. addSpairSpair
+ * (HubbardSOCMeasureObserveSDSD.cpp:75-177) for one walker's full G */
+static void or_cp_observables(int L, const zc *G, zc *out)
+{
+    int n = 2 * L;
+    zc *gm = out, *dd = out + (size_t)n * n, *pm = dd + (size_t)n * n, *mp = pm + (size_t)L * L,
+       *pr = mp + (size_t)L * L;
+#define GG(r, c) G[(r) + (size_t)n * (c)]
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+            gm[i + (size_t)n * j] = GG(i, j);
+            dd[i + (size_t)n * j] = (i == j) ? GG(i, i) : GG(i, i) * GG(j, j) - GG(i, j) * GG(j, i);
+        }
+    for (int j = 0; j < L; ++j)
+        for (int i = 0; i < L; ++i) {
+            zc a, b;
+            if (i == j) {
+                zc both = GG(i, i) * GG(i + L, i + L) - GG(i, i + L) * GG(i + L, i);
+                a = GG(i, i) - both;
+                b = GG(i + L, i + L) - both;
+            } else {
+                a = -GG(i, j) * GG(j + L, i + L) + GG(i, i + L) * GG(j + L, j);
+                b = -GG(i + L, j + L) * GG(j, i) + GG(i + L, i) * GG(j, j + L);
+            }
+            pm[i + (size_t)L * j] = a;
+            mp[i + (size_t)L * j] = b;
+            pr[i + (size_t)L * j] = GG(i, j) * GG(i + L, j + L) - GG(i, j + L) * GG(i + L, j);
+        }
+#undef GG
+}
+
 static void or_cp_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut, zc *denOut,
-                                zc *KVR, zc *sites)
+                                zc *KVR, zc *sites, zc *obs)
 {
     int n = e->n, N = e->N, L = e->L;
     zc *th = (zc *)malloc(sizeof(zc) * N * n), *gd = (zc *)malloc(sizeof(zc) * n),
@@ -1246,6 +1292,18 @@ static void or_cp_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut
         R += (e->hx[i] * 0.5 + I * e->hy[i] * 0.5) * god[i + L];
     }
     KVR[0] = K; KVR[1] = V; KVR[2] = R;
+    if (obs) {
+        /* G = conj(phiT) thetaT (SDSDOperation.cpp:74-89) */
+        zc *G = (zc *)malloc(sizeof(zc) * n * n);
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                zc g = 0;
+                for (int a = 0; a < N; ++a) g += conj(e->phiT[IDX(i, a, n)]) * th[IDX(a, j, N)];
+                G[IDX(i, j, n)] = g;
+            }
+        or_cp_observables(L, G, obs);
+        free(G);
+    }
     /* addNupNdn / addSplusSminus (HubbardSOCMeasureFixedSDSD.cpp:221-255) */
     for (int i = 0; i < L; ++i) {
         sites[i] = gd[i];
@@ -1310,12 +1368,13 @@ static void or_pl_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut
     free(thu); free(thd); free(xb); free(ex); free(D);
 }
 
-typedef struct { or_engine *e; size_t ws; int G; zc *el, *dn, *terms, *xb, *ex, *sites; } or_meas_ctx;
+typedef struct { or_engine *e; size_t ws; int G; zc *el, *dn, *terms, *xb, *ex, *sites, *obs; size_t nobs; } or_meas_ctx;
 static void or_meas_body(void *c_, int w)
 {
     or_meas_ctx *c = (or_meas_ctx *)c_;
     or_engine *e = c->e; size_t ws = c->ws; int G = c->G;
     zc *el = c->el, *dn = c->dn, *terms = c->terms, *xb = c->xb, *ex = c->ex, *sites = c->sites;
+    zc *obs = c->obs ? c->obs + (size_t)w * c->nobs : NULL;
         if (!e->alive[w]) return;
         zc *tmp = (zc *)malloc(sizeof(zc) * ws);
         zc lwTmp;
@@ -1329,7 +1388,7 @@ static void or_meas_body(void *c_, int w)
             lwTmp = e->logwExpHalfDtK + e->logw[w];
         }
         if (e->kind == OR_CP) or_cp_walker_energy(e, tmp, lwTmp, el + w, dn + w, terms + 3 * w,
-                                                  sites + (size_t)w * 4 * e->L);
+                                                  sites + (size_t)w * 4 * e->L, obs);
         else or_pl_walker_energy(e, tmp, lwTmp, el + w, dn + w, terms + 3 * w, xb + (size_t)w * G,
                                  ex + (size_t)w * G);
         free(tmp);
@@ -1349,7 +1408,9 @@ void or_add_mixed_measurement(or_engine *e, double *elocOut, double *denOut)
     zc *xb = G ? (zc *)calloc((size_t)W * G, sizeof(zc)) : NULL;
     zc *ex = G ? (zc *)calloc((size_t)W * G, sizeof(zc)) : NULL;
     zc *sites = e->kind == OR_CP ? (zc *)calloc((size_t)W * 4 * e->L, sizeof(zc)) : NULL;
-    or_meas_ctx c = {e, ws, G, el, dn, terms, xb, ex, sites};
+    size_t nobs = (size_t)11 * e->L * e->L;
+    zc *obs = (e->kind == OR_CP && e->observe) ? (zc *)calloc((size_t)W * nobs, sizeof(zc)) : NULL;
+    or_meas_ctx c = {e, ws, G, el, dn, terms, xb, ex, sites, obs, nobs};
     or_parallel_for(W, e->nthreads, or_meas_body, &c);
 
     for (int w = 0; w < W; ++w) {
@@ -1359,6 +1420,8 @@ void or_add_mixed_measurement(or_engine *e, double *elocOut, double *denOut)
         if (e->kind == OR_CP) {
             e->KNum += terms[3 * w] * den; e->VNum += terms[3 * w + 1] * den; e->RNum += terms[3 * w + 2] * den;
             for (int k = 0; k < 4 * e->L; ++k) e->siteNum[k] += sites[(size_t)w * 4 * e->L + k] * den;
+            if (obs)
+                for (size_t k = 0; k < nobs; ++k) e->obsNum[k] += obs[(size_t)w * nobs + k] * den;
         } else {
             e->TNum += terms[3 * w] * den;
             for (int g = 0; g < G; ++g) {
@@ -1370,7 +1433,7 @@ void or_add_mixed_measurement(or_engine *e, double *elocOut, double *denOut)
     }
     if (elocOut) memcpy(elocOut, el, sizeof(zc) * W);
     if (denOut) memcpy(denOut, dn, sizeof(zc) * W);
-    free(el); free(dn); free(terms); free(xb); free(ex); free(sites);
+    free(el); free(dn); free(terms); free(xb); free(ex); free(sites); free(obs);
 }
 
 /* measurement sums: out[0..]= den, HNum, (CP) KNum, VNum, RNum | (PL) TNum */

@@ -108,6 +108,8 @@ def _declare(L):
     L.or_modify_gm.argtypes = [P]
     L.or_pop_control.argtypes = [P, P, P]
     L.or_pop_weights.argtypes = [P, P]
+    L.or_cp_set_observables.argtypes = [P, c_int]
+    L.or_get_observables.argtypes = [P, P]
     L.or_pl_two_body_sample.argtypes = [P, P, P, P, P]
     L.or_project_one_step.argtypes = [P, c_int]
     L.or_set_cadence.argtypes = [P, c_int, c_int]
@@ -337,6 +339,24 @@ class Engine:
         out = np.zeros(5, np.complex128)
         lib().or_get_measurement(self.h, _p(out))
         return out
+
+    def set_observables(self, on=True):
+        lib().or_cp_set_observables(self.h, 1 if on else 0)
+        self.observe = bool(on)
+
+    def observables(self):
+        n, L = self.n, self.n // 2
+        out = np.zeros(11 * L * L, np.complex128)
+        lib().or_get_observables(self.h, _p(out))
+        names = ["greenMatrixNum", "densityDensityNum", "splusSminusNum", "sminusSplusNum",
+                 "spairSpairNum"]
+        sizes = [(n, n), (n, n), (L, L), (L, L), (L, L)]
+        res, off = {}, 0
+        for nm, sh in zip(names, sizes):
+            k = sh[0] * sh[1]
+            res[nm] = out[off:off + k].reshape(sh, order="F")
+            off += k
+        return res
 
     def site_nums(self):
         """NupNum, NdnNum, SplusNum, SminusNum (L complex each), CP only."""
