@@ -38,7 +38,7 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
     zd *sA = (zd *)smem_raw;
     zd *sX = sA + (SMEM ? maxNs * maxNs : 0);
     int *piv = (int *)(sX + (SMEM ? maxNs * maxNs : 0));
-    __shared__ int sFlag;
+    __shared__ int sFlag, sBlk;   // singular anywhere / in the current block
 
     const bool act = (active == nullptr) || active[w] != 0;
     if (!act) {
@@ -60,6 +60,7 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
         zd *X = SMEM ? sX : Xg;
         if (SMEM)
             for (int e = tid; e < Ns * Ns; e += nt) A[e] = Sg[e];
+        if (tid == 0) sBlk = 0;
         __syncthreads();
         for (int j = 0; j < Ns; ++j) {
             if (tid < 32) {
@@ -90,6 +91,7 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
                 for (int i = j + 1 + tid; i < Ns; i += nt) A[i + (size_t)j * Ns] = zmul(A[i + (size_t)j * Ns], inv);
             } else if (tid == 0) {
                 sFlag = 1;
+                sBlk = 1;
             }
             __syncthreads();
             const int r = Ns - j - 1;
@@ -104,10 +106,13 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
             }
             __syncthreads();
         }
-        // log determinant with pivot signs
+        // log determinant with pivot signs; a singular block contributes
+        // lognorm -1e300 and phase 1 (lognormPhaseDeterminant,
+        // tensor_2d_common_fun.cpp:75-84), and the blocks' log-dets add up
+        // (SD2sSD2isOperation.cpp:84-94)
         if (tid == 0) {
-            if (sFlag) {
-                logdetSum = make_double2(-1e300, 0.0);
+            if (sBlk) {
+                logdetSum = zadd(logdetSum, make_double2(-1e300, 0.0));
             } else {
                 double lognorm = 0.0; zd phase = make_double2(1.0, 0.0);
                 for (int j = 0; j < Ns; ++j) {
@@ -118,7 +123,7 @@ lu_kernel(int W, Blocks bl, zd *S, zd *Sinv, const int *active, const zd *logw, 
                     phase = zmul(phase, make_double2(f.x / a, f.y / a));
                 }
                 zd ld = zadd(make_double2(lognorm, 0.0), zlog(phase));
-                if (logdetSum.x > -1e299) logdetSum = zadd(logdetSum, ld);
+                logdetSum = zadd(logdetSum, ld);
             }
         }
         // inverse: X = A^{-1} column by column (P, unit-L forward, U backward)
@@ -384,17 +389,19 @@ gj_cta_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const 
             }
         }
         __syncthreads();
+        // a singular block adds lognorm -1e300 with phase 1
+        // (lognormPhaseDeterminant, tensor_2d_common_fun.cpp:75-84)
         if (sing) {
             singular = true;
+            if (tid == 0) logdetSum = zadd(logdetSum, make_double2(-1e300, 0.0));
         } else if (tid == 0) {
             double lnT = 0.0;
             zd phT = make_double2(1.0, 0.0);
             for (int k = 0; k < NW; ++k) { lnT += redL[k]; phT = zmul(phT, redP[k]); }
             const zd ld = zadd(make_double2(lnT, 0.0), zlog(phT));
-            if (logdetSum.x > -1e299) logdetSum = zadd(logdetSum, ld);
+            logdetSum = zadd(logdetSum, ld);
         }
     }
-    if (singular) logdetSum = make_double2(-1e300, 0.0);
     if (tid == 0) {
         const zd lwR = zadd(logwAdd, logw[w]);
         if (bl.mult == 2) logdetSum = zadd(logdetSum, logdetSum);
@@ -541,11 +548,14 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
             }
         }
         __syncwarp();
+        // a singular block adds lognorm -1e300 with phase 1
+        // (lognormPhaseDeterminant, tensor_2d_common_fun.cpp:75-84)
         if (sing) {
             singular = true;
+            logdetSum = zadd(logdetSum, make_double2(-1e300, 0.0));
         } else {
             zd ld = zadd(make_double2(lognorm, 0.0), zlog(phase));
-            if (logdetSum.x > -1e299) logdetSum = zadd(logdetSum, ld);
+            logdetSum = zadd(logdetSum, ld);
         }
         if (wantInverse && Sinv) {
             zd *Xg = Sinv + (size_t)w * bl.sStride + bl.sOff[b];
@@ -553,7 +563,6 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
         }
         __syncwarp();
     }
-    if (singular) logdetSum = make_double2(-1e300, 0.0);
     if (lane == 0) {
         zd lwR = zadd(logwAdd, logw[w]);
         if (bl.mult == 2) logdetSum = zadd(logdetSum, logdetSum);
@@ -750,11 +759,13 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long 
     }
     bool singular = false;
     zd logdetSum = make_double2(0.0, 0.0);
+    // a singular block adds lognorm -1e300 with phase 1
+    // (lognormPhaseDeterminant, tensor_2d_common_fun.cpp:75-84)
     for (int t = 0; t < nb; ++t) {
-        singular = singular || sgS[warp + t] != 0;
-        logdetSum = zadd(logdetSum, ldS[warp + t]);
+        const bool sb = sgS[warp + t] != 0;
+        singular = singular || sb;
+        logdetSum = zadd(logdetSum, sb ? make_double2(-1e300, 0.0) : ldS[warp + t]);
     }
-    if (singular) logdetSum = make_double2(-1e300, 0.0);
     const zd lwR = zadd(logwAdd, logw[w]);
     if (bl.mult == 2) logdetSum = zadd(logdetSum, logdetSum);
     const zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);

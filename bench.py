@@ -495,6 +495,12 @@ def cpu_measure(name, steps, measure_skip, max_procs=None, walkers_per_proc=None
     if walkers_per_proc is None:
         walkers_per_proc = 2 if c["kind"] == "pl" else max(1, min(16, c["W"] // P))
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    # the oracle build whose GEMM/GEMV-shaped work runs through OpenBLAS, as the
+    # reference's runs through its BLAS (the spawned workers inherit this)
+    from oracle import oracle as O
+    blas = O.scipy_blas()
+    if blas:
+        os.environ["AFQMC_ORACLE_BLAS"], os.environ["AFQMC_ORACLE_BLAS_PREFIX"] = blas
     ctx = mp.get_context("spawn")
     with ctx.Pool(P) as pool:
         res = pool.map(_cpu_worker, [(name, walkers_per_proc, steps, 1000 + i, measure_skip, warmup)
@@ -503,7 +509,8 @@ def cpu_measure(name, steps, measure_skip, max_procs=None, walkers_per_proc=None
     wall = max(r[1] for r in res)
     sample = (f"{P} processes x {walkers_per_proc} walkers x {steps} steps of {name} "
               f"(measurement every {measure_skip} steps, {warmup} untimed warm-up steps), "
-              f"slowest process timed")
+              f"slowest process timed; GEMM/GEMV work through "
+              f"{'OpenBLAS (' + os.path.basename(blas[0]) + ', 1 thread)' if blas else 'plain loops'}")
     return total / wall, P, sample
 
 

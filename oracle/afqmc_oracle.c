@@ -26,6 +26,10 @@
 #include <stdlib.h>
 #include <string.h>
 #include <pthread.h>
+#ifdef OR_BLAS
+#include <dlfcn.h>
+#include <stdio.h>
+#endif
 
 /* ------------------------------------------------------------------ */
 /* Walker-parallel loops.  Walkers are independent within each pass of  */
@@ -118,9 +122,55 @@ static zc opv(char t, const zc *A, int lda, int i, int j)
 }
 
 /* C = alpha op(A) op(B) + beta C; restates gmm_cpu (tensor_2d_bl_cpu.cpp:61-75). */
+#ifdef OR_BLAS
+/* The timed CPU baseline build (liboracle_blas.so): the GEMM- and GEMV-shaped
+ * work goes through an optimised BLAS, as the reference's BL_NAME(gmm) /
+ * BL_NAME(gemv) calls do (common/tensorHao/source/tensor_2d_bl_cpu.cpp:61-75).
+ * The library and its symbol prefix come from AFQMC_ORACLE_BLAS and
+ * AFQMC_ORACLE_BLAS_PREFIX; without them the plain loops below run. */
+typedef void (*or_zgemm_t)(const char *, const char *, const int *, const int *, const int *, const zc *,
+                           const zc *, const int *, const zc *, const int *, const zc *, zc *, const int *);
+typedef void (*or_zgemv_t)(const char *, const int *, const int *, const zc *, const zc *, const int *,
+                           const zc *, const int *, const zc *, zc *, const int *);
+typedef void (*or_dgemv_t)(const char *, const int *, const int *, const double *, const double *,
+                           const int *, const double *, const int *, const double *, double *, const int *);
+static or_zgemm_t p_zgemm;
+static or_zgemv_t p_zgemv;
+static or_dgemv_t p_dgemv;
+static pthread_once_t or_blas_once = PTHREAD_ONCE_INIT;
+static void or_blas_load(void)
+{
+    const char *path = getenv("AFQMC_ORACLE_BLAS");
+    const char *pre = getenv("AFQMC_ORACLE_BLAS_PREFIX");
+    if (!path) return;
+    void *h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+    if (!h) return;
+    char name[128];
+    snprintf(name, sizeof name, "%szgemm_", pre ? pre : "");
+    p_zgemm = (or_zgemm_t)dlsym(h, name);
+    snprintf(name, sizeof name, "%szgemv_", pre ? pre : "");
+    p_zgemv = (or_zgemv_t)dlsym(h, name);
+    snprintf(name, sizeof name, "%sdgemv_", pre ? pre : "");
+    p_dgemv = (or_dgemv_t)dlsym(h, name);
+    if (!p_zgemm || !p_zgemv || !p_dgemv) p_zgemm = NULL, p_zgemv = NULL, p_dgemv = NULL;
+}
+static int or_blas(void)
+{
+    pthread_once(&or_blas_once, or_blas_load);
+    return p_zgemm != NULL;
+}
+int or_blas_available(void) { return or_blas(); }
+#else
+static int or_blas(void) { return 0; }
+int or_blas_available(void) { return 0; }
+#endif
+
 void or_zgemm(char ta, char tb, int m, int n, int k, zc alpha, const zc *A, int lda,
               const zc *B, int ldb, zc beta, zc *C, int ldc)
 {
+#ifdef OR_BLAS
+    if (or_blas()) { p_zgemm(&ta, &tb, &m, &n, &k, &alpha, A, &lda, B, &ldb, &beta, C, &ldc); return; }
+#endif
     if (ta == 'C' && tb == 'N') {
         /* contiguous dot products: C(i,j) = sum_l conj(A(l,i)) B(l,j) */
         for (int j = 0; j < n; ++j)
@@ -145,6 +195,13 @@ void or_zgemm(char ta, char tb, int m, int n, int k, zc alpha, const zc *A, int 
 static void or_zgemm_nn(int m, int n, int k, zc alpha, const zc *A, int lda, const zc *B, int ldb,
                         zc *C, int ldc)
 {
+#ifdef OR_BLAS
+    if (or_blas()) {
+        const zc zero = 0;
+        p_zgemm("N", "N", &m, &n, &k, &alpha, A, &lda, B, &ldb, &zero, C, &ldc);
+        return;
+    }
+#endif
     for (int j = 0; j < n; ++j) {
         zc *c = C + IDX(0, j, ldc);
         for (int i = 0; i < m; ++i) c[i] = 0;
@@ -917,6 +974,16 @@ static zc or_cp_sample_apply(const or_engine *e, const int *aux, const double *f
 static void or_pl_cholesky_bg(const or_engine *e, const zc *thUp, const zc *thDn, zc *xbar)
 {
     int n = e->n, G = e->G, Nu = e->Nup, Nd = e->Ndn;
+#ifdef OR_BLAS
+    if (or_blas()) {
+        /* xbar = A_up^T theta_up + A_dn^T theta_dn (two zgemv, calculateCholeskyBg) */
+        const zc one = 1, zero = 0;
+        const int inc = 1, ku = Nu * n, kd = Nd * n;
+        p_zgemv("T", &ku, &G, &one, e->Aup, &ku, thUp, &inc, &zero, xbar, &inc);
+        if (kd > 0) p_zgemv("T", &kd, &G, &one, e->Adn, &kd, thDn, &inc, &one, xbar, &inc);
+        return;
+    }
+#endif
     for (int g = 0; g < G; ++g) {
         zc s = 0;
         const zc *au = e->Aup + (size_t)g * Nu * n;
@@ -942,6 +1009,21 @@ static void or_pl_force(const or_engine *e, const zc *xbar, zc *force)
 static void or_pl_build_M(const or_engine *e, const zc *aux, zc *M)
 {
     int n2 = e->n * e->n;
+#ifdef OR_BLAS
+    if (or_blas()) {
+        /* real L: M = L c with c = sqrt(-dt) aux, as two dgemv (real, imaginary part) */
+        int G = e->G, inc = 1;
+        double *cr = (double *)malloc(sizeof(double) * G), *ci = (double *)malloc(sizeof(double) * G);
+        double *mr = (double *)malloc(sizeof(double) * n2), *mi = (double *)malloc(sizeof(double) * n2);
+        for (int g = 0; g < G; ++g) { zc c = aux[g] * e->sqrtMinusDt; cr[g] = creal(c); ci[g] = cimag(c); }
+        const double one = 1.0, zero = 0.0;
+        p_dgemv("N", &n2, &G, &one, e->chol, &n2, cr, &inc, &zero, mr, &inc);
+        p_dgemv("N", &n2, &G, &one, e->chol, &n2, ci, &inc, &zero, mi, &inc);
+        for (int i = 0; i < n2; ++i) M[i] = mr[i] + I * mi[i];
+        free(cr); free(ci); free(mr); free(mi);
+        return;
+    }
+#endif
     for (int i = 0; i < n2; ++i) M[i] = 0;
     for (int g = 0; g < e->G; ++g) {
         zc c = aux[g] * e->sqrtMinusDt;
@@ -1345,12 +1427,16 @@ static void or_pl_walker_energy(or_engine *e, const zc *wf, zc logw, zc *elocOut
             const zc *A = (sp == 0 ? e->Aup : e->Adn) + (size_t)g * Ns * n;
             const zc *th = sp == 0 ? thu : thd;
             /* D(a,b) = sum_i A(a,i) theta(i,b), theta(i,b) = thetaT(b,i) */
-            for (int b = 0; b < Ns; ++b)
-                for (int a = 0; a < Ns; ++a) {
-                    zc d = 0;
-                    for (int i = 0; i < n; ++i) d += A[IDX(a, i, Ns)] * th[IDX(b, i, Ns)];
-                    D[IDX(a, b, Ns)] = d;
-                }
+            if (or_blas() && Ns > 0) {
+                or_zgemm('N', 'T', Ns, Ns, n, 1.0, A, Ns, th, Ns, 0.0, D, Ns);
+            } else {
+                for (int b = 0; b < Ns; ++b)
+                    for (int a = 0; a < Ns; ++a) {
+                        zc d = 0;
+                        for (int i = 0; i < n; ++i) d += A[IDX(a, i, Ns)] * th[IDX(b, i, Ns)];
+                        D[IDX(a, b, Ns)] = d;
+                    }
+            }
             for (int i = 0; i < Ns; ++i)
                 for (int j = 0; j < Ns; ++j) s += D[IDX(j, i, Ns)] * D[IDX(i, j, Ns)];
         }

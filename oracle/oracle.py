@@ -13,7 +13,10 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB = os.path.join(_HERE, "liboracle.so")
+# AFQMC_ORACLE_BLAS (a BLAS shared library) selects the build whose GEMM- and
+# GEMV-shaped work runs through that BLAS: the timed CPU baseline.  The
+# checker is the plain build.
+_LIB = os.path.join(_HERE, "liboracle_blas.so" if os.environ.get("AFQMC_ORACLE_BLAS") else "liboracle.so")
 _lib = None
 
 c_int, c_double, c_u64, c_void_p, c_char = (ctypes.c_int, ctypes.c_double, ctypes.c_uint64,
@@ -22,6 +25,18 @@ c_int, c_double, c_u64, c_void_p, c_char = (ctypes.c_int, ctypes.c_double, ctype
 
 def build():
     subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def scipy_blas():
+    """(path, symbol prefix) of the OpenBLAS that scipy bundles, or None."""
+    import glob
+    import scipy
+    libs = glob.glob(os.path.join(os.path.dirname(scipy.__file__) + ".libs", "libscipy_openblas*.so"))
+    return (libs[0], "scipy_") if libs else None
+
+
+def blas_available():
+    return bool(lib().or_blas_available())
 
 
 def lib():
@@ -58,6 +73,7 @@ class C2(ctypes.Structure):
 
 def _declare(L):
     P = c_void_p
+    L.or_blas_available.restype = c_int
     L.or_rng_bits.restype = c_u64
     L.or_rng_bits.argtypes = [c_u64, c_u64]
     L.or_rng_uniform_at.restype = c_double
