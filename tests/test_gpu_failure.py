@@ -1,9 +1,11 @@
 """Failure detection, tested without faulting the GPU.
 
   - Walkers with a zero column (singular overlap) or a NaN entry are injected
-    through the C-ABI.  The singular one must get the reference's log-det of
-    -1e300 (lognormPhaseDeterminant, tensor_2d_common_fun.cpp:75-84) and set
-    status bit 1 in the step; the NaN one sets status bit 2.  The healthy
+    through the C-ABI.  The singular one must get the reference's log-det,
+    lognorm -1e300 for each singular spin block (lognormPhaseDeterminant,
+    tensor_2d_common_fun.cpp:75-84, summed over the blocks as
+    SD2sSD2isOperation.cpp:84-94 does), and set status bit 1 in the step; the
+    NaN one sets status bit 2.  The healthy
     walkers must still match the oracle, and the engine must stay usable.
   - The bounded waits of the tensor-core kernels: a CTA waits, with the same
     wait helpers, on mbarriers that nothing arrives at and a short limit; both
@@ -32,7 +34,9 @@ def _inject(wf):
 def _check_injected(g, o, healthy, seed):
     lg = g.log_overlaps()
     lo = o.log_overlaps()
-    assert lg[1].real == -1e300 and lo[1].real == -1e300
+    # each singular spin block adds -1e300 (one block for SD, two for this
+    # SD2is walker, whose zero column lies in both blocks)
+    assert lg[1].real == lo[1].real and lo[1].real <= -1e300
     assert not np.isfinite(lg[3])
     assert logov_close(lg[healthy], lo[healthy], STEP_TOL) < STEP_TOL
     assert g.status() == 0               # diagnostics record no status
