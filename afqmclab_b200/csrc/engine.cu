@@ -372,7 +372,7 @@ int project_dtk_dtv(afqmc_engine *e)
             g.A = e->chol; g.lda = (long long)e->n * e->n;
             g.B = e->aux; g.ldb = e->G;
             g.C = e->M; g.ldc = (long long)e->n * e->n;
-            g.alpha = make_double2(0.0, e->cdv.sqrtDt);
+            g.alpha = make_double2(0.0, e->cdv.sqrtMinusDtIm);
             TRY(gemm(g, s));
         }
         {
@@ -836,7 +836,7 @@ int afqmc_pl_create(int n, int Nup, int Ndn, int G, int W, int force_type, doubl
     CK(dalloc(e, &e->exNum, G));
     if (precision == AFQMC_FP64) CK(dalloc(e, &e->M, n2 * W));
     e->cdv.n = n; e->cdv.G = G; e->cdv.bg = e->bg; e->cdv.forceCap = force_cap;
-    e->cdv.sqrtDt = std::sqrt(dt);
+    e->cdv.sqrtMinusDtIm = -std::sqrt(dt);
     e->cdv.constForce = (force_type == AFQMC_CONST_FORCE) ? e->constForcePL : nullptr;
     if (precision == AFQMC_MIXED) CK(mixed_create(e));
     else CK(fp64_exchange_setup(e));

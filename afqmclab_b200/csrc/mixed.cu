@@ -299,13 +299,13 @@ mixed_sample_warp_kernel(int W, CholDev c, const float *xbarp, int splits, long 
                     f = cf[u];
                 } else {
                     double a = xr[u] - bgv[u], b = xi[u];
-                    f = make_double2(-b * c.sqrtDt, a * c.sqrtDt);
+                    f = make_double2(-b * c.sqrtMinusDtIm, a * c.sqrtMinusDtIm);
                     double af = zabs(f);
                     if (af > c.forceCap) f = make_double2(f.x * c.forceCap / af, f.y * c.forceCap / af);
                 }
                 zd x = make_double2(gs[u] + f.x, f.y);
-                Y[(size_t)(2 * w) * G + g] = __double2bfloat16(-c.sqrtDt * x.y);
-                Y[(size_t)(2 * w + 1) * G + g] = __double2bfloat16(c.sqrtDt * x.x);
+                Y[(size_t)(2 * w) * G + g] = __double2bfloat16(-c.sqrtMinusDtIm * x.y);
+                Y[(size_t)(2 * w + 1) * G + g] = __double2bfloat16(c.sqrtMinusDtIm * x.x);
                 zfma(f2, f, f);
                 zfma(xf, x, f);
                 zfma(xb, x, make_double2(bgv[u], 0.0));
@@ -324,7 +324,7 @@ mixed_sample_warp_kernel(int W, CholDev c, const float *xbarp, int splits, long 
             zd lw = logw[w];
             lw.x += log(cs);
             zd smp = zsub(zscale(f2, 0.5), xf);
-            smp = zsub(smp, make_double2(-c.sqrtDt * xb.y, c.sqrtDt * xb.x));
+            smp = zsub(smp, make_double2(-c.sqrtMinusDtIm * xb.y, c.sqrtMinusDtIm * xb.x));
             zd t = zadd(smp, lw);
             t.x += dtET;
             logw[w] = zadd(hopLogw, t);

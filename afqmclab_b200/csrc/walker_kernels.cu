@@ -1011,7 +1011,7 @@ pl_sample_kernel(int W, CholDev c, const zd *xbar, int *surv, int *alive,
         } else {
             zd x = xbar[g + (size_t)G * w];
             double a = x.x - c.bg[g], b = x.y;
-            f = make_double2(-b * c.sqrtDt, a * c.sqrtDt);
+            f = make_double2(-b * c.sqrtMinusDtIm, a * c.sqrtMinusDtIm);
             double af = zabs(f);
             if (af > c.forceCap) f = make_double2(f.x * c.forceCap / af, f.y * c.forceCap / af);
         }
@@ -1034,9 +1034,9 @@ pl_sample_kernel(int W, CholDev c, const zd *xbar, int *surv, int *alive,
         } else {
             zd lw = logw[w];
             lw.x += log(cs);
-            // sample logw = 0.5 f.f - x.f - sqrt(-dt) x.bg, sqrt(-dt) = i sqrtDt
+            // sample logw = 0.5 f.f - x.f - sqrt(-dt) x.bg, sqrt(-dt) = i sqrtMinusDtIm
             zd smp = zsub(zscale(f2, 0.5), xf);
-            smp = zsub(smp, make_double2(-c.sqrtDt * xb.y, c.sqrtDt * xb.x));
+            smp = zsub(smp, make_double2(-c.sqrtMinusDtIm * xb.y, c.sqrtMinusDtIm * xb.x));
             zd t = zadd(smp, lw);
             t.x += dtET;
             logw[w] = zadd(hopLogw, t);

@@ -57,7 +57,11 @@ void launch_cp_sample_apply(int W, const HubbardDev &h, const double *force, con
 struct CholDev {
     int n, G;
     const double *bg;
-    double forceCap, sqrtDt;   // sqrt(-dt) = i * sqrtDt
+    // sqrt(-dt) = i * sqrtMinusDtIm.  The reference evaluates it as
+    // sqrt(-dt * complex(1, 0)) (choleskyReal.cpp:17), whose argument has
+    // imaginary part -0.0, so the principal root is -i sqrt(dt):
+    // sqrtMinusDtIm = -sqrt(dt).
+    double forceCap, sqrtMinusDtIm;
     const zd *constForce;      // non-null for constForce
 };
 void launch_pl_sample(int W, const CholDev &c, const zd *xbar, const int *surv_in, int *surv,

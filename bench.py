@@ -17,8 +17,12 @@ runs across ranks at the reference's cadence (all-gathered weights, one
 comb, walkers that change rank moved as one NCCL message per peer) and the
 estimator sums are all-reduced at every measurement; the timed region is
 bracketed by a barrier and the maximum over ranks is reported.
-`--impl reference` times the CPU oracle port of the reference's algorithm on
-the host cores (rank 0 only).
+`--impl reference` times the reference's own tutorial program for the
+workload (built from its sources into oracle/_ref) on the host cores, as
+concurrent single-threaded processes (rank 0 only); where the programs were
+not built it times the CPU oracle port of the same algorithm instead.  The
+cpu_baseline object of the main line is the same measurement on a smaller
+sample.
 """
 import argparse
 import json
@@ -484,6 +488,33 @@ def _cpu_worker(args):
     return nwalk * steps, time.perf_counter() - t0
 
 
+def ref_measure(name, steps, measure_skip, warmup=2, max_procs=None, walkers_per_proc=None):
+    """The reference's own program for the workload (afqmcPhaseless or
+    afqmcConstraintPath, built from the reference's sources into oracle/_ref)
+    on the host cores: P single-threaded processes at once, standing for the
+    MPI ranks of the reference's own build (walkerSizePerThread walkers each;
+    the cross-rank population exchange is not included).  Returns
+    (walker-steps/s, P, sample) or None when the programs were not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref"))
+    import ref_run
+    from afqmclab_b200 import inputs
+    m, c = inputs.make_config(name)
+    kind = c["kind"]
+    if not ref_run.available(kind):
+        return None
+    P = min(os.cpu_count() or 1, max_procs or 64)
+    if walkers_per_proc is None:
+        walkers_per_proc = 4 if kind == "pl" else max(1, min(16, c["W"] // P))
+    v, secs, st = ref_run.timed_sample(kind, m, walkers_per_proc, steps, warmup, measure_skip, P,
+                                       c["mgs"], c["pop"])
+    sample = (f"{P} concurrent single-threaded {ref_run.PROGRAMS[kind]} processes (the reference's "
+              f"tutorial program built from its sources, BLAS/LAPACK through OpenBLAS, 1 thread) x "
+              f"{walkers_per_proc} walkers x {st} steps of {name} (measurement every {measure_skip} "
+              f"steps, after {warmup} steps); projection time = wall time of the run minus that of "
+              f"the same run stopped after the warm-up steps, slowest process ({secs:.2f} s)")
+    return v, P, sample
+
+
 def cpu_measure(name, steps, measure_skip, max_procs=None, walkers_per_proc=None, warmup=0):
     """Oracle port on the host cores: P single-threaded processes, each with
     its own small population (the reference's MPI walker parallelism); each
@@ -525,7 +556,7 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "mixed", "fp64"])
     ap.add_argument("--measure-skip", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-fp64-side", action="store_true")
     ap.add_argument("--no-graphs", action="store_true")
     ap.add_argument("--energy-steps", type=int, default=60)
@@ -537,16 +568,24 @@ def main():
         if rank != 0:
             return 0
         t0 = time.perf_counter()
-        v, P, sample = cpu_measure(args.workload, args.steps, args.measure_skip, warmup=args.warmup)
+        steps = min(args.steps, 200)
+        r = ref_measure(args.workload, steps, args.measure_skip, warmup=args.warmup)
+        if r is not None:
+            (v, P, sample), kind = r, "reference"
+            form = ("the reference's own tutorial program (FP64), built from its sources, "
+                    "single-threaded processes")
+        else:
+            v, P, sample = cpu_measure(args.workload, steps, args.measure_skip, warmup=args.warmup)
+            kind = "port"
+            form = "CPU restatement of the reference's FP64 path (oracle/), single-threaded processes"
         line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": workload_config(args.workload, default_precision(args), args.measure_skip,
                                           args.gpus, not args.no_graphs),
-                "reference_form": "CPU restatement of the reference's FP64 path (oracle/), "
-                                  "single-threaded processes",
-                "cpu_baseline": {"value": v, "unit": UNIT, "cores": P, "kind": "port",
+                "reference_form": form,
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": P, "kind": kind,
                                  "sample": sample},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0},
@@ -761,8 +800,13 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, P, sample = cpu_measure(args.workload, args.cpu_steps, args.measure_skip)
-        cpu = {"value": v, "unit": UNIT, "cores": P, "kind": "port", "sample": sample}
+        r = ref_measure(args.workload, args.cpu_steps, args.measure_skip)
+        if r is not None:
+            v, P, sample = r
+            cpu = {"value": v, "unit": UNIT, "cores": P, "kind": "reference", "sample": sample}
+        else:
+            v, P, sample = cpu_measure(args.workload, args.cpu_steps, args.measure_skip)
+            cpu = {"value": v, "unit": UNIT, "cores": P, "kind": "port", "sample": sample}
 
     if rank == 0:
         line = {

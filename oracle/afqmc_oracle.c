@@ -812,7 +812,9 @@ or_engine *or_pl_create(int n, int Nup, int Ndn, int G, int W, int forceType, do
     e->useLogOneBody = (expMinusDtK == NULL);
     e->chol = ddup(chol, (size_t)n * n * G);
     e->bg = ddup(bg, G);
-    e->sqrtMinusDt = csqrt(-dt + 0.0 * I);
+    /* sqrt(-dt * complex(1, 0)) as choleskyReal.cpp:17 evaluates it: the
+     * product's imaginary part is -0.0, so the principal root is -i sqrt(dt) */
+    e->sqrtMinusDt = -sqrt(dt) * I;
     e->constForcePL = (zc *)calloc((size_t)G, sizeof(zc));
     if (constForce) memcpy(e->constForcePL, constForce, sizeof(zc) * G);
     /* initWfDaggerT (:148-163) and initWfDaggerCholeskyVecs (:165-186) */
@@ -1281,6 +1283,26 @@ void or_project_one_step(or_engine *e, int nsteps)
 }
 
 void or_set_cadence(or_engine *e, int mgsIndex, int popIndex) { e->mgsIndex = mgsIndex; e->popIndex = popIndex; }
+
+/* RealMaterialMolecule::updateBackGround (realMaterialMolecule.cpp:103-115):
+ * the new background reaches the force, the two-body sample weight and the
+ * measurement at once.  With expMinusDtK non-null the one-body operators are
+ * replaced as well, by the dense propagators the driver rebuilds from the new
+ * background (afqmcPhaseless.cpp:145-170), which ends the Taylor form. */
+void or_pl_update_background(or_engine *e, const double *bg, const double *expMinusDtK,
+                             double logwExpMinusDtK, const double *expHalfDtK,
+                             double logwExpHalfDtK, const double *expMinusHalfDtK,
+                             double logwExpMinusHalfDtK)
+{
+    memcpy(e->bg, bg, sizeof(double) * e->G);
+    if (!expMinusDtK) return;
+    size_t n2 = (size_t)e->n * e->n;
+    free(e->expMinusDtK); free(e->expHalfDtK); free(e->expMinusHalfDtK);
+    e->expMinusDtK = zdup(expMinusDtK, n2); e->logwExpMinusDtK = logwExpMinusDtK;
+    e->expHalfDtK = zdup(expHalfDtK, n2); e->logwExpHalfDtK = logwExpHalfDtK;
+    e->expMinusHalfDtK = zdup(expMinusHalfDtK, n2); e->logwExpMinusHalfDtK = logwExpMinusHalfDtK;
+    e->useLogOneBody = 0;
+}
 
 /* projectExpMinusHalfDtK / projectExpHalfDtK: which = -1 (exp(-dt/2 K)) or +1 (exp(+dt/2 K)) */
 void or_project_half(or_engine *e, int which)

@@ -118,6 +118,7 @@ def _declare(L):
     L.or_get_rng_counter.restype = c_u64
     L.or_get_rng_counter.argtypes = [P]
     L.or_set_ET.argtypes = [P, c_double]
+    L.or_pl_update_background.argtypes = [P, P, P, c_double, P, c_double, P, c_double]
     L.or_set_threads.argtypes = [P, c_int]
     L.or_log_overlaps.argtypes = [P, P]
     L.or_green_matrix.argtypes = [P, c_int, c_int, P]
@@ -297,6 +298,19 @@ class Engine:
 
     def set_cadence(self, mgs_index, pop_index):
         lib().or_set_cadence(self.h, mgs_index, pop_index)
+
+    def update_background_only(self, bg):
+        """updateBackGround: new background, one-body operators unchanged."""
+        b = np.ascontiguousarray(bg, dtype=np.float64)
+        lib().or_pl_update_background(self.h, _p(b), None, 0.0, None, 0.0, None, 0.0)
+
+    def update_background(self, m):
+        """New background and the dense propagators rebuilt from it (m: a
+        MoleculeInputs after set_background)."""
+        a = [np.ascontiguousarray(m.bg, dtype=np.float64), _z(m.expMinusDtK), _z(m.expHalfDtK),
+             _z(m.expMinusHalfDtK)]
+        lib().or_pl_update_background(self.h, _p(a[0]), _p(a[1]), float(m.logwDt), _p(a[2]),
+                                      -float(m.logwHalf), _p(a[3]), float(m.logwHalf))
 
     def log_overlaps(self):
         out = np.zeros(self.W, np.complex128)

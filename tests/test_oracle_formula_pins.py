@@ -24,6 +24,15 @@ from tests.helpers import logov_close
 TOL = 1e-12
 
 
+def SQRT_MINUS(dt):
+    """sqrt(-dt * complex(1, 0)) as the reference writes it (choleskyReal.cpp:17,
+    choleskyRealTest.cpp:106): the argument's imaginary part is -0.0, so the
+    principal root is -i sqrt(dt)."""
+    z = np.sqrt(complex(-dt, -0.0))
+    assert z.imag < 0
+    return z
+
+
 def _sym(rng, n):
     a = rng.uniform(-1, 1, (n, n))
     return a + a.T
@@ -81,7 +90,7 @@ def test_molecule_energy_and_force_match_explicit_contractions():
     # force: sqrt(-dt) (xbar - bg), capped in modulus (getForce, :93-116)
     xbar, force = o.pl_force(0)
     assert np.abs(xbar - xg).max() < TOL * max(1.0, np.abs(xg).max())
-    f = (xg - m.bg) * np.sqrt(-dt + 0j)
+    f = (xg - m.bg) * SQRT_MINUS(dt)
     f = np.where(np.abs(f) > cap, f / np.abs(f) * cap, f)
     assert np.abs(force - f).max() < TOL
 
@@ -95,7 +104,7 @@ def test_cholesky_two_body_sample_matches_formula():
     force = _cplx(rng, G)
     aux = rng.standard_normal(G) + force
     M, logw = o.two_body_sample(aux, force)
-    sq = np.sqrt(-dt + 0j)
+    sq = SQRT_MINUS(dt)
     w = np.prod(np.exp(0.5 * force * force - aux * force - aux * sq * m.bg))
     assert abs(np.exp(logw) - w) < TOL * max(1.0, abs(w))
     Mx = sq * np.einsum("g,kjg->kj", aux, m.chol)
