@@ -5,17 +5,48 @@ C-ABI) in place of the oracle.  The reference's own tutorial programs
 same inputs, walkers and seed; the engine follows their random stream, so
 the per-block estimator sums and the final walkers agree to rounding.
 
+The engine's modified Gram-Schmidt gives R_jj > 0 where the reference's
+Householder QR gives signs, so final walkers are compared through
+gauge-invariant quantities: each spin block's projector
+phi (phi^H phi)^-1 phi^H and the log-overlap with the trial (log-weight
+included, phase mod 2 pi).
+
 Tolerance: 1e-8 relative over the whole run (FP64; GPU reductions sum in a
 different order than the reference's serial loops)."""
 import numpy as np
 import pytest
 
 from afqmclab_b200 import capi, driver, inputs
+from oracle import oracle as O
 from tests import test_reference_programs as R
+from tests.helpers import logov_close
 
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-8
+
+
+def _projector(a):
+    return a @ np.linalg.solve(a.conj().T @ a, a.conj().T)
+
+
+def _compare_walkers(eng, out, m, kind):
+    wf_r, lw_r, al_r = out["walkers"]
+    wf, lw, al = eng.get_walkers()
+    assert np.array_equal(al.astype(bool), al_r.astype(bool))
+    blocks = [m.N] if kind == "cp" else [b for b in (m.nup, m.ndn) if b > 0]
+    lo_g, lo_r = [], []
+    for w in np.flatnonzero(al_r):
+        for nb in blocks:
+            assert R._rel(_projector(wf[:, :nb, w]), _projector(wf_r[:, :nb, w])) < TOL
+        if kind == "cp":
+            lo_g.append(O.sdsd(m.phiT, m.logwT, wf[:, :, w], lw[w])[0])
+            lo_r.append(O.sdsd(m.phiT, m.logwT, wf_r[:, :, w], lw_r[w])[0])
+        else:
+            lo_g.append(O.sd2s_sd2is(m.phiTUp, m.phiTDn, m.logwT, wf[:, :, w], lw[w], m.nup, m.ndn)[0])
+            lo_r.append(O.sd2s_sd2is(m.phiTUp, m.phiTDn, m.logwT, wf_r[:, :, w], lw_r[w], m.nup,
+                                     m.ndn)[0])
+    assert logov_close(np.array(lo_g), np.array(lo_r), TOL) < TOL
 
 
 def _streams(sums, out, names):
@@ -34,7 +65,7 @@ def test_engine_follows_constraint_path_program(decomp, force):
     eng, sums, out = R.run_cp_both(m, 8, 1201, meth, mgs=3, pop=7, force_type=force,
                                    make_engine=capi.cp_engine)
     _streams(sums, out, ["den", "HNum", "KNum", "VNum", "RNum"])
-    R.compare_walkers(eng, out, TOL)
+    _compare_walkers(eng, out, m, "cp")
     eng.close()
 
 
@@ -45,7 +76,7 @@ def test_engine_follows_constraint_path_program_100_walkers():
     meth = driver.ConstraintPathMethod(**R.CP_METHOD)
     eng, sums, out = R.run_cp_both(m, 100, 77, meth, mgs=10, pop=40, make_engine=capi.cp_engine)
     _streams(sums, out, ["den", "HNum", "KNum", "VNum", "RNum"])
-    R.compare_walkers(eng, out, TOL)
+    _compare_walkers(eng, out, m, "cp")
     eng.close()
 
 
@@ -62,7 +93,7 @@ def test_engine_follows_phaseless_program(nup, ndn):
     _streams(sums, out, ["den", "HNum", "TNum"])
     assert R._rel(np.array([b for b, _ in nums]), out["choleskyBgNum"]) < TOL
     assert R._rel(np.array([x for _, x in nums]), out["choleskyExNum"]) < TOL
-    R.compare_walkers(eng, out, TOL)
+    _compare_walkers(eng, out, m, "pl")
     eng.close()
 
 
@@ -80,5 +111,5 @@ def test_engine_follows_phaseless_program_adjusting_background():
 
     eng, sums, out = R.run_pl_both(m, 8, 555, meth, mgs=3, pop=5, make_engine=make)
     _streams(sums, out, ["den", "HNum", "TNum"])
-    R.compare_walkers(eng, out, TOL)
+    _compare_walkers(eng, out, m, "pl")
     eng.close()
