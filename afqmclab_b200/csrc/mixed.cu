@@ -448,17 +448,21 @@ taylor_onebody_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_cons
     auto issue = [&](const uint8_t *Ar, const uint8_t *Ai) {
         // C_r (+)= Ar Br - Ai Bi ; C_i (+)= Ai Br + Ar Bi  (Ai absent for the real one-body)
         tc_fence_after();
-        for (int kk = 0; kk < n / 16; ++kk) {
-            const uint32_t kb = kk >> 2, ko = (kk & 3) * 32;
-            const uint64_t aR = desc_k_sw128(smem_u32(Ar + kb * 16384) + ko);
-            const uint64_t bR = desc_k_sw128(smem_u32(sBr + kb * NC * 128) + ko);
-            const uint64_t bI = desc_k_sw128(smem_u32(sBi + kb * NC * 128) + ko);
-            umma_bf16(tCr, aR, bR, IDESC, kk > 0 ? 1u : 0u);
-            umma_bf16(tCi, aR, bI, IDESC, kk > 0 ? 1u : 0u);
-            if (Ai) {
-                const uint64_t aI = desc_k_sw128(smem_u32(Ai + kb * 16384) + ko);
-                umma_bf16(tCr, aI, bI, IDESCN, 1u);
-                umma_bf16(tCi, aI, bR, IDESC, 1u);
+        // descriptors of K step kk = the base descriptor + the step's byte
+        // offset / 16 (the start-address field; no carry for shared addresses)
+        const uint64_t aR0 = desc_k_sw128(smem_u32(Ar)), bR0 = desc_k_sw128(smem_u32(sBr)),
+                       bI0 = desc_k_sw128(smem_u32(sBi)), aI0 = Ai ? desc_k_sw128(smem_u32(Ai)) : 0;
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            if (kk < n / 16) {
+                const uint64_t oa = (uint64_t)(((kk >> 2) * 16384 + (kk & 3) * 32) >> 4);
+                const uint64_t ob = (uint64_t)(((kk >> 2) * NC * 128 + (kk & 3) * 32) >> 4);
+                umma_bf16(tCr, aR0 + oa, bR0 + ob, IDESC, kk > 0 ? 1u : 0u);
+                umma_bf16(tCi, aR0 + oa, bI0 + ob, IDESC, kk > 0 ? 1u : 0u);
+                if (Ai) {
+                    umma_bf16(tCr, aI0 + oa, bI0 + ob, IDESCN, 1u);
+                    umma_bf16(tCi, aI0 + oa, bR0 + ob, IDESC, 1u);
+                }
             }
         }
         umma_commit(&bars[1]);
@@ -680,6 +684,429 @@ int launch_taylor(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE,
     return engine_check_launch();
 }
 
+// Taylor kernel with M in tensor memory (NC = 16 or 32 columns).
+//
+// The A operand of every order's product is the walker's M, the same for all
+// orders; held in shared memory it is re-read by each MMA (4 KB per K step
+// and MMA against 1 KB of the term), and at N = 32 those operand reads, not
+// the multiply, set the MMA rate.  Here M's two bf16 planes live in tensor
+// memory (row i in lane i, 128 columns), loaded once per walker by the
+// threads with tcgen05.st, and each K step is two MMAs with A read from
+// tensor memory and one B window of N = 2 NC rows from shared memory (the
+// term's real rows, then its imaginary rows):
+//   D1 = Re(M) [Re t; Im t],  D2 = Im(M) [Re t; Im t]
+//   Re(M t) = D1[re] - D2[im],  Im(M t) = D1[im] + D2[re].
+// The one-body operator E - I stays resident in shared memory for the
+// kernel's life.  M reaches tensor memory one plane at a time through a
+// shared-memory staging buffer: a TMA load of the plane (128-byte swizzle),
+// then tcgen05.cp of each K step's 128 x 16 slab, all issued by one thread
+// and asynchronous to the others.  The next walker's real plane is loaded
+// while the current series runs and copied in once the series has finished
+// reading M; its imaginary plane is loaded during the one-body product and
+// copied in ahead of the next walker's first MMA.
+// Tensor memory per CTA: M 128 columns, D1 and D2 2 NC each (256 allocated),
+// and shared memory (E, the term, the staging buffer; 81 KB at n = 128)
+// keeps at most two CTAs on an SM, so the allocation never waits.
+template <int NC>
+struct TaylorTsSmem {
+    static constexpr size_t e_bytes(int n) { return (size_t)(n / 64) * 16384; }
+    static constexpr size_t b_bytes(int n) { return (size_t)(n / 64) * 2 * NC * 128; }
+    static constexpr size_t bytes(int n)
+    {
+        return std::max((size_t)80 * 1024, (size_t)1024 + 2 * e_bytes(n) + b_bytes(n) + 64);
+    }
+};
+
+// Fragment access of a 16-lane slab of tensor memory (tcgen05.ld .16x256b):
+// with G column groups of 8, register 4m + q of thread t holds lane
+// (base + t/4 + 8 (q >> 1)), column 8m + 2 (t % 4) + (q & 1) -- the layout
+// stmatrix takes, so a term goes from tensor memory to the next MMA's B
+// operand as bf16 pairs and one transposing stmatrix per four 8x8 tiles.
+template <int G>
+__device__ __forceinline__ void tmem_ld_frag(uint32_t taddr, uint32_t *r);
+template <>
+__device__ __forceinline__ void tmem_ld_frag<2>(uint32_t taddr, uint32_t *r)
+{
+    asm volatile("tcgen05.ld.sync.aligned.16x256b.x2.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr)
+                 : "memory");
+}
+template <>
+__device__ __forceinline__ void tmem_ld_frag<4>(uint32_t taddr, uint32_t *r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
+template <>
+__device__ __forceinline__ void tmem_ld_frag<8>(uint32_t taddr, uint32_t *r)
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.16x256b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+          "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+          "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+          "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+}
+// four 8x8 b16 tiles, each stored transposed: lane 8j + c gives the address
+// of stored row c of tile j, which receives column c of the thread fragment
+__device__ __forceinline__ void stmatrix_x4_trans(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+    asm volatile("stmatrix.sync.aligned.m8n8.x4.trans.shared.b16 [%0], {%1,%2,%3,%4};" ::"r"(addr), "r"(a), "r"(b),
+                 "r"(c), "r"(d)
+                 : "memory");
+}
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
+{
+    __nv_bfloat162 p = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t *>(&p);
+}
+
+template <int NC, int NN>
+__global__ void __launch_bounds__(128, 2)
+taylor_ts_kernel(const __grid_constant__ CUtensorMap tmM, const __grid_constant__ CUtensorMap tmE, int W,
+                 float *w32,
+                 const int *surv, int *order, long long *stats, int kmax, float acc, float relTol,
+                 int checkFrom, int *status, int *err)
+{
+    constexpr int n = NN;        // walker rows: 64 or 128 (all addressing compile-time)
+    constexpr int NB = 2 * NC;   // MMA N: the term's real rows, then its imaginary rows
+    constexpr int G = NC / 8;    // 8-column groups of the real (or imaginary) part
+    constexpr int NE = 8 * G;    // complex elements of a thread: 2 slabs x G groups x 4
+    static_assert(G == 2 || G == 4, "16 or 32 columns");
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    constexpr int KB = n / 64;
+    uint8_t *sE = base;
+    uint8_t *sB = base + KB * 16384;
+    uint8_t *sS = sB + (size_t)KB * NB * 128;                      // M plane staging
+    uint64_t *bars = (uint64_t *)(sS + (size_t)KB * 16384);   // [0] E, [1] MMA, [2] staged, [3] copied
+    uint32_t *tslot = (uint32_t *)(bars + 4);
+    __shared__ float red[4], red0[4];
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // Rows: warp w owns rows 32w..32w+31 (its lane quarter of tensor memory),
+    // as two 16-row slabs h; within slab h thread t holds rows
+    // 32w + 16h + t/4 (+8) and columns 8m + 2 (t % 4) (+1) of each group m.
+    const bool warpOK = 32 * warp < n;   // n = 64 or 128: rows of the warp exist
+    const int r0 = 32 * warp + (lane >> 2), c0 = 2 * (lane & 3);
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1);
+        mbar_init(&bars[3], 1);
+        fence_mbar_init();
+        tma_prefetch_desc(&tmE);
+        tma_prefetch_desc(&tmM);
+    }
+    if (warp == 0) { tmem_alloc(tslot, 256); tmem_relinquish(); }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tm = *tslot;
+    const uint32_t tMr = tm, tMi = tm + 64, tD1 = tm + 128, tD2 = tm + 128 + NB;
+    constexpr uint32_t IDESC = idesc_bf16(128, NB);
+    const uint64_t bB0 = desc_k_sw128(smem_u32(sB));   // K step kk: + its byte offset / 16
+    // stmatrix addresses of this lane for slabs 0 and 1 (real rows; the
+    // imaginary rows are NC B rows further): one stmatrix covers two column
+    // groups of the slab, tile j = lane / 8 = (group 2p + j / 2, slab rows
+    // 8 (j % 2) .. +7), stored row c = lane % 8 = B row 16p + 8 (j / 2) + c,
+    // holding the K chunk of those 8 rows (128-byte swizzle: chunk ^ (row & 7))
+    uint32_t stAddr[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int j = lane >> 3, c = lane & 7;
+        const int brow = 8 * (j >> 1) + c;
+        const int i0 = 32 * warp + 16 * h + 8 * (j & 1);
+        stAddr[h] = smem_u32(sB) + (uint32_t)((i0 >> 6) * NB * 128 + brow * 128 + ((((i0 & 63) >> 3) ^ c) << 4));
+    }
+    if (tid == 0) {
+        mbar_arrive_expect_tx(&bars[0], (uint32_t)(KB * 16384));
+        for (int kb = 0; kb < KB; ++kb) tma_load_2d(sE + kb * 16384, &tmE, &bars[0], kb * 64, 0);
+    }
+    uint32_t phD = 0;
+    bool ok = true, eReady = false;
+
+    auto block_max = [&](float v, float *buf) {
+        for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if (lane == 0) buf[warp] = v;
+    };
+    auto read_max = [&](const float *buf) { return fmaxf(fmaxf(buf[0], buf[1]), fmaxf(buf[2], buf[3])); };
+    auto next_walker = [&](int w) {
+        while (w < W && !surv[w]) w += gridDim.x;
+        return w;
+    };
+    // element e = 4 G h + 4 m + q of this thread: row and column
+    auto erow = [&](int e) { return r0 + 16 * (e / (4 * G)) + 8 * ((e & 3) >> 1); };
+    auto ecol = [&](int e) { return 8 * ((e / 4) % G) + c0 + (e & 1); };
+    // B operand rows of slab h from 4 G values of the slab (one part: real
+    // rows at B row 0, imaginary rows at B row NC)
+    auto stage_part = [&](int h, int part, const float *v) {
+        const uint32_t a0 = stAddr[h] + (uint32_t)(part * NC * 128);
+#pragma unroll
+        for (int p = 0; p < G / 2; ++p)
+            stmatrix_x4_trans(a0 + (uint32_t)(p * 2048), pack_bf16x2(v[8 * p], v[8 * p + 1]),
+                              pack_bf16x2(v[8 * p + 2], v[8 * p + 3]), pack_bf16x2(v[8 * p + 4], v[8 * p + 5]),
+                              pack_bf16x2(v[8 * p + 6], v[8 * p + 7]));
+    };
+    auto stage = [&](const float *vr, const float *vi) {
+        if (!warpOK) return;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            stage_part(h, 0, vr + 4 * G * h);
+            stage_part(h, 1, vi + 4 * G * h);
+        }
+    };
+    // The M staging pipeline (thread 0 only): plane p of walker w into the
+    // staging buffer by TMA, the staged plane into tensor memory by
+    // tcgen05.cp (ordered before the MMAs this thread issues later), and the
+    // wait for the copy to finish reading the buffer.  A failed wait clears
+    // ok0, which the next block-wide check reads.
+    // thread 0's pipeline state, kept in shared memory (no registers for the
+    // other 127 threads): parities of bars[2] and bars[3], loads / copies in
+    // flight, and whether every wait so far succeeded
+    __shared__ uint32_t pipe[5];   // phS, phC, pendS, pendC, ok0
+    if (tid == 0) { pipe[0] = 0; pipe[1] = 0; pipe[2] = 0; pipe[3] = 0; pipe[4] = 1; }
+    auto stage_plane = [&](int w, int p) {
+        mbar_arrive_expect_tx(&bars[2], (uint32_t)(KB * 16384));
+        for (int kb = 0; kb < KB; ++kb) tma_load_2d(sS + kb * 16384, &tmM, &bars[2], kb * 64, (2 * w + p) * n);
+        pipe[2] = 1;
+    };
+    auto copy_plane = [&](uint32_t tDst) {
+        if (!mbar_wait(&bars[2], pipe[0])) pipe[4] = 0;
+        pipe[0] ^= 1;
+        pipe[2] = 0;
+        tc_fence_after();
+        const uint64_t sS0 = desc_k_sw128(smem_u32(sS));
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk) {
+            if (kk < n / 16) {
+                const uint64_t sd = sS0 + (uint64_t)(((kk >> 2) * 16384 + (kk & 3) * 32) >> 4);
+                asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;" ::"r"(tDst + kk * 8), "l"(sd) : "memory");
+            }
+        }
+        umma_commit(&bars[3]);
+        pipe[3] = 1;
+    };
+    auto staging_free = [&]() {
+        if (!mbar_wait(&bars[3], pipe[1])) pipe[4] = 0;
+        pipe[1] ^= 1;
+        pipe[3] = 0;
+    };
+
+    int w = next_walker(blockIdx.x);
+    if (tid == 0 && w < W) {
+        stage_plane(w, 0);
+        copy_plane(tMr);
+        staging_free();
+        stage_plane(w, 1);
+    }
+    while (w < W) {
+        const int wn = next_walker(w + gridDim.x);
+        float *gw = w32 + (size_t)w * 2 * n * NC;
+        if (tid == 0 && wn < W) {
+            bulk_prefetch_l2(w32 + (size_t)wn * 2 * n * NC, (uint32_t)(2 * n * NC * sizeof(float)));
+        }
+        // order 0: S = phi, operand = bf16(phi)
+        float pr[NE], pi[NE];
+        float s2 = 0.f;
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const size_t off = (size_t)erow(e) + (size_t)n * ecol(e);
+            pr[e] = warpOK ? gw[off] : 0.f;
+            pi[e] = warpOK ? gw[(size_t)n * NC + off] : 0.f;
+            s2 = fmaxf(s2, pr[e] * pr[e] + pi[e] * pi[e]);
+        }
+        stage(pr, pi);
+        block_max(s2, red0);
+        fence_proxy_async();
+        tc_fence_before();
+        __syncthreads();
+        const float tol = fmaxf(acc, relTol * sqrtf(read_max(red0)));
+        if (!eReady) {
+            ok = __syncthreads_and(mbar_wait(&bars[0], 0)) != 0;
+            eReady = ok;
+            if (!ok) break;
+        }
+        int k = 0;
+        while (true) {
+            ++k;
+            if (tid == 0) {
+                if (k == 1) copy_plane(tMi);   // this walker's imaginary plane, staged meanwhile
+                tc_fence_after();
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk) {
+                    if (kk < n / 16) {
+                        const uint64_t bd = bB0 + (uint64_t)(((kk >> 2) * NB * 128 + (kk & 3) * 32) >> 4);
+                        umma_bf16_ts(tD1, tMr + kk * 8, bd, IDESC, kk > 0 ? 1u : 0u);
+                        umma_bf16_ts(tD2, tMi + kk * 8, bd, IDESC, kk > 0 ? 1u : 0u);
+                    }
+                }
+                umma_commit(&bars[1]);
+                if (k == 1) {
+                    // the next walker's real plane goes into the freed staging buffer
+                    staging_free();
+                    if (wn < W) stage_plane(wn, 0);
+                }
+            }
+            ok = __syncthreads_and(mbar_wait(&bars[1], phD) && (tid != 0 || pipe[4])) != 0;
+            phD ^= 1;
+            if (!ok) break;
+            tc_fence_after();
+            const float inv = 1.0f / (float)k;
+            float mx = 0.f;
+            if (warpOK) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    // D1 = Re M [Re t; Im t], D2 = Im M [Re t; Im t] over this slab:
+                    // Re t' = (D1 re - D2 im) / k first, then Im t' = (D1 im + D2 re) / k
+                    const uint32_t lo = (uint32_t)(32 * warp + 16 * h) << 16;
+                    float tr[4 * G];
+                    {
+                        uint32_t a[4 * G], b[4 * G];
+                        tmem_ld_frag<G>(tD1 + lo, a);
+                        tmem_ld_frag<G>(tD2 + lo + NC, b);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int x = 0; x < 4 * G; ++x) {
+                            tr[x] = (__uint_as_float(a[x]) - __uint_as_float(b[x])) * inv;
+                            pr[4 * G * h + x] += tr[x];
+                        }
+                    }
+                    stage_part(h, 0, tr);
+                    float ti[4 * G];
+                    {
+                        uint32_t a[4 * G], b[4 * G];
+                        tmem_ld_frag<G>(tD1 + lo + NC, a);
+                        tmem_ld_frag<G>(tD2 + lo, b);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int x = 0; x < 4 * G; ++x) {
+                            ti[x] = (__uint_as_float(a[x]) + __uint_as_float(b[x])) * inv;
+                            pi[4 * G * h + x] += ti[x];
+                            mx = fmaxf(mx, fmaf(tr[x], tr[x], ti[x] * ti[x]));
+                        }
+                    }
+                    stage_part(h, 1, ti);
+                }
+            }
+            block_max(mx, red);
+            fence_proxy_async();
+            tc_fence_before();
+            __syncthreads();
+            const bool conv = (k >= checkFrom) && (sqrtf(read_max(red)) <= tol);
+            if (conv || k >= kmax) {
+                if (!conv && tid == 0 && status) atomicOr(status + w, (int)ST_TAYLOR_CAP);
+                break;
+            }
+        }
+        if (!ok) break;
+        // one-body: phi' = S + (E - I) S, the operand = bf16(S)
+        stage(pr, pi);
+        fence_proxy_async();
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint64_t bE0 = desc_k_sw128(smem_u32(sE));
+#pragma unroll
+            for (int kk = 0; kk < 8; ++kk) {
+                if (kk < n / 16) {
+                    const uint64_t oe = (uint64_t)(((kk >> 2) * 16384 + (kk & 3) * 32) >> 4);
+                    const uint64_t ob = (uint64_t)(((kk >> 2) * NB * 128 + (kk & 3) * 32) >> 4);
+                    umma_bf16(tD1, bE0 + oe, bB0 + ob, IDESC, kk > 0 ? 1u : 0u);
+                }
+            }
+            umma_commit(&bars[1]);
+            // the series has finished reading M: the next walker's real plane goes in
+            if (wn < W) copy_plane(tMr);
+        }
+        ok = __syncthreads_and(mbar_wait(&bars[1], phD) && (tid != 0 || pipe[4])) != 0;
+        phD ^= 1;
+        if (!ok) break;
+        tc_fence_after();
+        if (warpOK) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint32_t a[4 * G], b[4 * G];
+                const uint32_t lo = (uint32_t)(32 * warp + 16 * h) << 16;
+                tmem_ld_frag<G>(tD1 + lo, a);
+                tmem_ld_frag<G>(tD1 + lo + NC, b);
+                tmem_wait_ld();
+#pragma unroll
+                for (int x = 0; x < 4 * G; ++x) {
+                    pr[4 * G * h + x] += __uint_as_float(a[x]);
+                    pi[4 * G * h + x] += __uint_as_float(b[x]);
+                }
+            }
+#pragma unroll
+            for (int e = 0; e < NE; ++e) {
+                const size_t off = (size_t)erow(e) + (size_t)n * ecol(e);
+                gw[off] = pr[e];
+                gw[(size_t)n * NC + off] = pi[e];
+            }
+        }
+        if (tid == 0) {
+            if (wn < W) {
+                // the next walker's imaginary plane, copied in before its first MMA
+                staging_free();
+                stage_plane(wn, 1);
+            }
+            order[w] = k;
+            if (stats) {
+                atomicAdd((unsigned long long *)&stats[0], 1ULL);
+                atomicAdd((unsigned long long *)&stats[1], (unsigned long long)k);
+                atomicMin(&stats[2], (long long)k);
+                atomicMax(&stats[3], (long long)k);
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+        w = wn;
+    }
+    // a failed wait: let the loads and copies this CTA issued finish before it exits
+    if (!ok && !eReady) (void)mbar_wait(&bars[0], 0);
+    if (tid == 0) {
+        if (pipe[2]) (void)mbar_wait(&bars[2], pipe[0]);
+        if (pipe[3]) (void)mbar_wait(&bars[3], pipe[1]);
+    }
+    if (!ok && err) atomicExch(err, 2);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tm, 256);
+}
+
+template <int NC>
+int launch_taylor_ts(afqmc_engine *e, const CUtensorMap &mM, const CUtensorMap &mE)
+{
+    const size_t smem = TaylorTsSmem<NC>::bytes(e->n);
+    static std::atomic<unsigned long long> attr{0};
+    if (first_on_device(attr)) {
+        cudaFuncSetAttribute(taylor_ts_kernel<NC, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TaylorTsSmem<NC>::bytes(128));
+        cudaFuncSetAttribute(taylor_ts_kernel<NC, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TaylorTsSmem<NC>::bytes(64));
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = std::min(e->W, 2 * sms);
+    auto kern = e->n == 128 ? taylor_ts_kernel<NC, 128> : taylor_ts_kernel<NC, 64>;
+    kern<<<grid, 128, smem, e->stream>>>(
+        mM, mE, e->W, e->mx->wf32, e->surv, e->order, e->tstats, 30, 1e-10f, 5.9604645e-8f, 4,
+        e->status, e->mx->err);
+    return engine_check_launch();
+}
+
 int run_taylor(afqmc_engine *e)
 {
     MixedState *m = e->mx;
@@ -689,8 +1116,8 @@ int run_taylor(afqmc_engine *e)
     r = tc_make_map_bf16(&mE, m->Et, e->n, e->n, e->n, 128);
     if (r) return engine_fail(AFQMC_ERR_CUDA, "tensor map (E): " + std::to_string(r));
     switch (e->ncol) {
-    case 16: return launch_taylor<16>(e, mM, mE, 1);
-    case 32: return launch_taylor<32>(e, mM, mE, 1);
+    case 16: return launch_taylor_ts<16>(e, mM, mE);
+    case 32: return launch_taylor_ts<32>(e, mM, mE);
     case 48: return launch_taylor<48>(e, mM, mE, 1);
     case 64: return launch_taylor<64>(e, mM, mE, 1);
     default: return engine_fail(AFQMC_ERR_UNSUPPORTED, "mixed Taylor kernel needs 16, 32, 48 or 64 columns");
