@@ -35,6 +35,7 @@ SYMBOLS = [
     "afqmc_batch_set_stream",
     "afqmc_set_autotune", "afqmc_bounded_wait_check", "afqmc_get_site_nums",
     "afqmc_pack_walkers", "afqmc_unpack_walkers", "afqmc_cp_set_observables",
+    "afqmc_cp_bp_begin", "afqmc_cp_bp_measure", "afqmc_cp_bp_state",
     "afqmc_get_observables",
 ]
 
@@ -110,6 +111,9 @@ def _declare(L):
     L.afqmc_apply_table.argtypes = [P, P]
     L.afqmc_pack_walkers.argtypes = [P, I, P, P]
     L.afqmc_cp_set_observables.argtypes = [P, I]
+    L.afqmc_cp_bp_begin.argtypes = [P, I, I]
+    L.afqmc_cp_bp_measure.argtypes = [P]
+    L.afqmc_cp_bp_state.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(I)]
     L.afqmc_get_observables.argtypes = [P, P, P, P, P, P]
     L.afqmc_unpack_walkers.argtypes = [P, I, P, P]
     L.afqmc_batch_create.argtypes = [ctypes.POINTER(ctypes.c_void_p), I, PP]
@@ -251,6 +255,21 @@ class Engine:
     def set_observables(self, on=True):
         _check(lib().afqmc_cp_set_observables(self.h, 1 if on else 0))
         self.observe = bool(on)
+
+    # back-propagation (constrained path, FP64 form, observe estimator on)
+    def bp_begin(self, steps, measure_skip):
+        """prepareBackPropagation: open a window of `steps` recorded steps."""
+        _check(lib().afqmc_cp_bp_begin(self.h, int(steps), int(measure_skip)))
+
+    def bp_measure(self):
+        """addMeasurement of the back-propagation driver (window full)."""
+        _check(lib().afqmc_cp_bp_measure(self.h))
+
+    def bp_state(self):
+        """(window open, BPIndex)."""
+        a, i = ctypes.c_int(), ctypes.c_int()
+        _check(lib().afqmc_cp_bp_state(self.h, ctypes.byref(a), ctypes.byref(i)))
+        return bool(a.value), i.value
 
     def observables(self):
         """greenMatrixNum, densityDensityNum (n x n), splusSminusNum,

@@ -120,6 +120,22 @@ int device_error_word(int **out)
 
 }  // namespace
 
+// Back-propagation state of a constrained-path engine
+// (tutorials/afqmcConstraintPathBP: afqmcConstraintPath.h members
+// walkerBackup, walkerBPMeasure, twoBodyAuxBackup, twoBodyAuxBPMeasure,
+// tablePerThreadBackup, isBP, BPIndex).  Field records are [step][walker][site]
+// ints, validity flags [step][walker] (the walker was sampled at that step),
+// tables [step][walker]; tableValid[i] says a population control ran at step i.
+struct BPState {
+    int steps = 0, skip = 0, index = 0, cap = 0;
+    bool active = false;
+    int *aux = nullptr, *auxMeas = nullptr, *valid = nullptr, *validMeas = nullptr, *table = nullptr;
+    int *ones = nullptr;
+    std::vector<char> tableValid;
+    zd *wfBackup = nullptr, *logwBackup = nullptr, *wfMeas = nullptr, *logwMeas = nullptr;
+    zd *left = nullptr, *leftTmp = nullptr, *right = nullptr, *logwL = nullptr, *logovBP = nullptr;
+};
+
 namespace {
 
 template <class T>
@@ -349,9 +365,16 @@ int project_dtk_dtv(afqmc_engine *e)
         {
             PHASE(AFQMC_PH_SAMPLE);
             launch_rng_scan(W, e->surv, e->L, e->counter, e->offs, s);
+            BPState *bp = (e->bp && e->bp->active) ? e->bp : nullptr;
+            // back-propagation: this step's fields and which walkers drew them
+            // (twoBodyAuxBackup[i][BPIndex], afqmcConstraintPathProjection.cpp:73)
+            int *auxOut = bp ? bp->aux + (size_t)bp->index * W * e->L : nullptr;
             launch_cp_sample_apply(W, e->hd, e->forceCP, e->surv, e->offs, e->seed, e->wf, e->wfTmp,
-                                   e->logw, e->dt * e->ET, hop, nullptr, s);
+                                   e->logw, e->dt * e->ET, hop, auxOut, s);
             TRY(check_launch());
+            if (bp)
+                CUDA_TRY(cudaMemcpyAsync(bp->valid + (size_t)bp->index * W, e->surv, sizeof(int) * W,
+                                         cudaMemcpyDeviceToDevice, s));
         }
         { PHASE(AFQMC_PH_ONEBODY); TRY(one_body(e, 0, e->wfTmp, e->wf, e->surv)); }
     } else {
@@ -404,6 +427,13 @@ int pop_control(afqmc_engine *e)
     launch_pop_comb(e->W, e->weight, nullptr, e->seed, e->counter, e->number, e->table,
                     e->status + e->W, e->stream);
     launch_pop_gather(e->W, e->wsize, e->table, e->wf, e->logw, e->stream);
+    if (e->bp && e->bp->active) {
+        // tablePerThreadBackup[BPIndex] (afqmcConstraintPathProjection.cpp:161-170)
+        BPState *bp = e->bp;
+        CUDA_TRY(cudaMemcpyAsync(bp->table + (size_t)bp->index * e->W, e->table, sizeof(int) * e->W,
+                                 cudaMemcpyDeviceToDevice, e->stream));
+        bp->tableValid[bp->index] = 1;
+    }
     return check_launch();
 }
 
@@ -452,6 +482,17 @@ int capture(afqmc_engine *e, cudaGraphExec_t *out, long long *kernels, F body)
 // capture; the profiler needs direct launches.
 int project_one_step(afqmc_engine *e)
 {
+    if (e->bp && e->bp->active) {
+        // recording a back-propagation window: direct launches (the record
+        // offsets move every step), BPIndex++ after the step
+        BPState *bp = e->bp;
+        if (bp->index >= bp->steps)
+            return fail(AFQMC_ERR_STATE, "back-propagation window is full: measure it first");
+        bp->tableValid[bp->index] = 0;
+        TRY(project_one_step_direct(e));
+        bp->index++;
+        return AFQMC_OK;
+    }
     if (!e->useGraphs || e->prof || !e->graphWarm) {
         int r = project_one_step_direct(e);
         if (r == AFQMC_OK && e->useGraphs) e->graphWarm = true;
@@ -581,6 +622,8 @@ void free_engine(afqmc_engine *e)
     if (e->mx || e->cpm) mixed_destroy(e);
     delete e->exf;
     e->exf = nullptr;
+    delete e->bp;
+    e->bp = nullptr;
     prof_resolve(e);
     for (cudaEvent_t ev : e->evpool) cudaEventDestroy(ev);
     if (e->upStream) cudaStreamSynchronize(e->upStream);
@@ -745,6 +788,7 @@ int afqmc_cp_create(int L, int N, int W, int decomp, int force_type, double dt, 
     // wfDaggerK = phiT^H K (HubbardSOCMeasureFixedSDSD::initWfDaggerK, :160-167)
     zd *Kd = nullptr;
     CK(dupload(e, &Kd, K, (size_t)n * n));
+    e->Kmat = Kd;
     CK(dalloc(e, &e->wfDaggerK, (size_t)N * n));
     {
         ZGemmArgs g;
@@ -1062,6 +1106,219 @@ int afqmc_get_observables(afqmc_engine *e, double *greenNum, double *densityDens
         if (dst[k]) CUDA_TRY(cudaMemcpyAsync(dst[k], e->obs + off[k], sizeof(zd) * cnt[k], cudaMemcpyDeviceToHost, e->stream));
     CUDA_TRY(cudaStreamSynchronize(e->stream));
     return AFQMC_OK;
+}
+
+// ------------------------------------------------------------ back-propagation
+// The back-propagated estimator of tutorials/afqmcConstraintPathBP
+// (afqmcConstraintPathBackPropagation.cpp, afqmcConstraintPathMeasure.cpp:
+// addMeasurement): the fields and population-control tables of a window of
+// `steps` steps are recorded; at measurement the window-start walkers are
+// resampled by the recorded tables, the trial is propagated leftwards through
+// each walker's recorded fields, and the observe estimator (energies from the
+// full Green's matrix, HubbardSOCMeasureCommuteSDSD::addEnergy, and the
+// observables) is accumulated for the pair (left: back-propagated trial,
+// right: window-start walker), weighted by the current walker's overlap.
+
+int afqmc_cp_bp_begin(afqmc_engine *e, int steps, int measure_skip)
+{
+    if (!e || e->kind != KIND_CP) return fail(AFQMC_ERR_ARG, "constrained-path engine required");
+    if (e->precision != AFQMC_FP64) return fail(AFQMC_ERR_UNSUPPORTED, "back-propagation runs in the FP64 form");
+    if (steps <= 0 || measure_skip <= 0) return fail(AFQMC_ERR_ARG, "steps and measure_skip must be positive");
+    if (!e->observe) return fail(AFQMC_ERR_STATE, "back-propagation measures the observe estimator: enable it first");
+    const int W = e->W, L = e->L;
+    const size_t ws = (size_t)e->wsize;
+    if (!e->bp) e->bp = new BPState();
+    BPState *bp = e->bp;
+    if (!bp->wfBackup) {
+        TRY(dalloc(e, &bp->wfBackup, ws * W)); TRY(dalloc(e, &bp->wfMeas, ws * W));
+        TRY(dalloc(e, &bp->left, ws * W)); TRY(dalloc(e, &bp->leftTmp, ws * W)); TRY(dalloc(e, &bp->right, ws * W));
+        TRY(dalloc(e, &bp->logwBackup, W)); TRY(dalloc(e, &bp->logwMeas, W)); TRY(dalloc(e, &bp->logwL, W));
+        TRY(dalloc(e, &bp->logovBP, W));
+        TRY(dalloc(e, &bp->ones, W));
+        launch_set_int(bp->ones, 1, W, e->stream);
+    }
+    if (steps > bp->cap) {
+        TRY(dalloc(e, &bp->aux, (size_t)steps * W * L)); TRY(dalloc(e, &bp->auxMeas, (size_t)steps * W * L));
+        TRY(dalloc(e, &bp->valid, (size_t)steps * W)); TRY(dalloc(e, &bp->validMeas, (size_t)steps * W));
+        TRY(dalloc(e, &bp->table, (size_t)steps * W));
+        bp->cap = steps;
+    }
+    drop_graphs(e);
+    // prepareBackPropagation: the window starts from the current walkers
+    CUDA_TRY(cudaMemcpyAsync(bp->wfBackup, e->wf, sizeof(zd) * ws * W, cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(bp->logwBackup, e->logw, sizeof(zd) * W, cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemsetAsync(bp->valid, 0, sizeof(int) * (size_t)steps * W, e->stream));
+    bp->steps = steps;
+    bp->skip = measure_skip;
+    bp->index = 0;
+    bp->tableValid.assign((size_t)steps, 0);
+    bp->active = true;
+    return check_launch();
+}
+
+int afqmc_cp_bp_state(afqmc_engine *e, int *active, int *index)
+{
+    if (!e) return fail(AFQMC_ERR_ARG, "null engine");
+    const bool on = e->bp && e->bp->active;
+    if (active) *active = on ? 1 : 0;
+    if (index) *index = on ? e->bp->index : 0;
+    return AFQMC_OK;
+}
+
+namespace {
+
+// generateWalkerBackupFromWalkerBPMeasure
+// (afqmcConstraintPathBackPropagation.cpp:78-97): the next window's start
+// walkers = the resampled window-start walkers propagated over the first
+// measure_skip recorded steps (walkers without a record at a step are not
+// propagated at it), normalised (logw reset to 0) at every step j with
+// j % mgsStep == 0.
+int bp_regenerate_backup(afqmc_engine *e)
+{
+    BPState *bp = e->bp;
+    const int W = e->W, L = e->L;
+    const size_t ws = (size_t)e->wsize;
+    cudaStream_t s = e->stream;
+    CUDA_TRY(cudaMemcpyAsync(bp->wfBackup, bp->wfMeas, sizeof(zd) * ws * W, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(bp->logwBackup, bp->logwMeas, sizeof(zd) * W, cudaMemcpyDeviceToDevice, s));
+    for (int j = 0; j < bp->skip; ++j) {
+        const int *valid = bp->validMeas + (size_t)j * W;
+        launch_cp_aux_apply(W, e->hd, bp->auxMeas + (size_t)j * W * L, valid, bp->wfBackup, bp->leftTmp,
+                            bp->logwBackup, false, e->expLogw[0], s);
+        ZGemmArgs g;
+        g.m = e->n; g.n = e->ncol; g.k = e->n;
+        g.A = e->expK[0]; g.lda = e->n;
+        g.B = bp->leftTmp; g.ldb = e->n; g.strideB = e->wsize;
+        g.C = bp->wfBackup; g.ldc = e->n; g.strideC = e->wsize;
+        g.batch = W; g.mask = valid;
+        TRY(gemm(g, s));
+        if (j % e->mgsStep == 0) {
+            launch_mgs(W, e->n, e->ncol, e->nup, e->ndn, 0, bp->wfBackup, bp->logwBackup, bp->ones, e->status, s);
+            CUDA_TRY(cudaMemsetAsync(bp->logwBackup, 0, sizeof(zd) * W, s));
+        }
+    }
+    return check_launch();
+}
+
+// one-body operator k applied from the left, K^H phi (HopSDOperation::
+// applyToLeft, hopSDOperation.cpp:21-26), to every alive walker of src
+// (srcStride 0: the same matrix for all) into dst
+int left_one_body(afqmc_engine *e, int k, const zd *src, long long srcStride, zd *dst)
+{
+    ZGemmArgs g;
+    g.m = e->n; g.n = e->ncol; g.k = e->n;
+    g.opA = OP_C;
+    g.A = e->expK[k]; g.lda = e->n;
+    g.B = src; g.ldb = e->n; g.strideB = srcStride;
+    g.C = dst; g.ldc = e->n; g.strideC = e->wsize;
+    g.batch = e->W; g.mask = e->alive;
+    return gemm(g, e->stream);
+}
+
+}  // namespace
+
+int afqmc_cp_bp_measure(afqmc_engine *e)
+{
+    if (!e || e->kind != KIND_CP) return fail(AFQMC_ERR_ARG, "constrained-path engine required");
+    BPState *bp = e->bp;
+    if (!bp || !bp->active || bp->index != bp->steps)
+        return fail(AFQMC_ERR_STATE, "no complete back-propagation window to measure");
+    const int W = e->W, L = e->L, steps = bp->steps, skip = bp->skip;
+    const size_t ws = (size_t)e->wsize;
+    cudaStream_t s = e->stream;
+    PHASE(AFQMC_PH_MEASURE);
+    // prepareBackPropagationMeasAndNextBackup (afqmcConstraintPathBackPropagation.cpp:22-76)
+    std::swap(bp->wfMeas, bp->wfBackup);
+    std::swap(bp->logwMeas, bp->logwBackup);
+    if (steps >= skip) {
+        CUDA_TRY(cudaMemcpyAsync(bp->auxMeas, bp->aux, sizeof(int) * (size_t)steps * W * L, cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(bp->validMeas, bp->valid, sizeof(int) * (size_t)steps * W, cudaMemcpyDeviceToDevice, s));
+    } else {
+        std::swap(bp->auxMeas, bp->aux);
+        std::swap(bp->validMeas, bp->valid);
+    }
+    for (int i = 0; i < steps; ++i) {
+        if (bp->tableValid[i]) {
+            const int *tab = bp->table + (size_t)i * W;
+            launch_pop_gather(W, e->wsize, tab, bp->wfMeas, bp->logwMeas, s);
+            launch_bp_gather_rows(W, L, i + 1, tab, bp->auxMeas, s);
+            launch_bp_gather_rows(W, 1, i + 1, tab, bp->validMeas, s);
+        }
+        if (i + 1 == skip) TRY(bp_regenerate_backup(e));
+    }
+    if (steps >= skip) {
+        // the window slides by measure_skip steps: records skip..steps-1 move
+        // to 0..steps-skip-1 (in increasing order, so no source is overwritten
+        // before it is read), their old slots are left without a table
+        for (int i = 0; i + skip < steps; ++i) {
+            CUDA_TRY(cudaMemcpyAsync(bp->aux + (size_t)i * W * L, bp->aux + (size_t)(i + skip) * W * L,
+                                     sizeof(int) * (size_t)W * L, cudaMemcpyDeviceToDevice, s));
+            CUDA_TRY(cudaMemcpyAsync(bp->valid + (size_t)i * W, bp->valid + (size_t)(i + skip) * W,
+                                     sizeof(int) * W, cudaMemcpyDeviceToDevice, s));
+            CUDA_TRY(cudaMemcpyAsync(bp->table + (size_t)i * W, bp->table + (size_t)(i + skip) * W,
+                                     sizeof(int) * W, cudaMemcpyDeviceToDevice, s));
+            bp->tableValid[i] = bp->tableValid[i + skip];
+            bp->tableValid[i + skip] = 0;
+        }
+        bp->index = steps - skip;
+    } else {
+        bp->active = false;
+    }
+
+    // addMeasurement (afqmcConstraintPathMeasure.cpp:47-78) for the alive walkers.
+    // The weight: the current walker's overlap with the trial after exp(dt/2 K).
+    TRY(one_body(e, 1, e->wf, e->wfTmp, e->alive));
+    TRY(overlap_gemm(e, e->wfTmp, e->alive, fbl(e)));
+    launch_lu_logdet_inverse(W, fbl(e), e->S, nullptr, e->alive, e->logw, one_body_logw(e, 1), e->logwT,
+                             e->logov, e->alive, nullptr, nullptr, nullptr, e->status, LU_PLAIN, false, s);
+    // left: exp(-dt/2 K)^H phiT, then for j = steps..1 the recorded fields and
+    // exp(-dt K) from the left, normalised when (steps - j + 1) % mgsStep == 0,
+    // then exp(dt/2 K)^H
+    TRY(left_one_body(e, 2, e->phiT[0], 0, bp->left));
+    CUDA_TRY(cudaMemsetAsync(bp->logwL, 0, sizeof(zd) * W, s));
+    const zd noLogw = make_double2(0.0, 0.0);
+    for (int j = steps; j > 0; --j) {
+        launch_cp_aux_apply(W, e->hd, bp->auxMeas + (size_t)(j - 1) * W * L, e->alive, bp->left, bp->leftTmp,
+                            bp->logwL, true, noLogw, s);
+        TRY(left_one_body(e, 0, bp->leftTmp, e->wsize, bp->left));
+        if ((steps - j + 1) % e->mgsStep == 0)
+            launch_mgs(W, e->n, e->ncol, e->nup, e->ndn, 0, bp->left, bp->logwL, e->alive, e->status, s);
+    }
+    TRY(left_one_body(e, 1, bp->left, e->wsize, bp->leftTmp));
+    // right: exp(dt/2 K) times the window-start walker
+    TRY(one_body(e, 1, bp->wfMeas, bp->right, e->alive));
+    // S = left^H right, its inverse, thetaT = S^-T right^T, G = conj(left) thetaT
+    // (SDSDOperation.cpp:52-186 for the pair)
+    {
+        ZGemmArgs g;
+        g.m = e->ncol; g.n = e->ncol; g.k = e->n;
+        g.opA = OP_C;
+        g.A = bp->leftTmp; g.lda = e->n; g.strideA = e->wsize;
+        g.B = bp->right; g.ldb = e->n; g.strideB = e->wsize;
+        g.C = e->S; g.ldc = e->ncol; g.strideC = e->bl.sStride;
+        g.batch = W; g.mask = e->alive;
+        TRY(gemm(g, s));
+    }
+    CUDA_TRY(cudaMemsetAsync(bp->logwL, 0, sizeof(zd) * W, s));
+    launch_lu_logdet_inverse(W, e->bl, e->S, e->Sinv, e->alive, bp->logwL, noLogw, noLogw, bp->logovBP, e->alive,
+                             nullptr, nullptr, nullptr, e->status, LU_PLAIN, true, s);
+    TRY(theta_gemm(e, bp->right, e->alive, e->bl));
+    launch_zconj((long long)ws * W, bp->leftTmp, bp->left, s);
+    {
+        ZGemmArgs g;
+        g.m = e->n; g.n = e->n; g.k = e->ncol;
+        g.A = bp->left; g.lda = e->n; g.strideA = e->wsize;
+        g.B = e->thetaT; g.ldb = e->ncol; g.strideB = e->bl.tStride;
+        g.C = e->Gfull; g.ldc = e->n; g.strideC = (long long)e->n * e->n;
+        g.batch = W; g.mask = e->alive;
+        TRY(gemm(g, s));
+    }
+    launch_cp_commute_energy(W, L, e->Gfull, e->Kmat, e->U, e->mu, e->hx, e->hy, e->hz, e->alive, e->logov,
+                             e->eloc, e->den, e->parts, s);
+    launch_measure_reduce(W, e->alive, e->eloc, e->den, e->parts, 3, e->acc, 0, nullptr, nullptr, nullptr,
+                          nullptr, s);
+    launch_cp_observe(W, L, e->Gfull, e->den, e->alive, e->obs, s);
+    return check_launch();
 }
 
 int afqmc_add_mixed_measurement(afqmc_engine *e)

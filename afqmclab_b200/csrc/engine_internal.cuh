@@ -13,6 +13,7 @@
 struct MixedState;
 struct CpMixedState;
 struct ExF64Scratch;
+struct BPState;
 
 enum { KIND_CP = 0, KIND_PL = 1 };
 
@@ -72,6 +73,10 @@ struct afqmc_engine {
     // (greenMatrixNum, densityDensityNum: n x n; S+S-, S-S+, pair: L x L)
     bool observe = false;
     zd *Gfull = nullptr, *phiTc = nullptr, *obs = nullptr;
+    // back-propagation (constrained path, FP64 form; off unless begun) and the
+    // model's K (2L x 2L), which the back-propagated estimator needs
+    BPState *bp = nullptr;
+    zd *Kmat = nullptr;
     // FP64 form: closed-shell single block and GEMM exchange (real A)
     ExF64Scratch *exf = nullptr;
     // mixed-precision state

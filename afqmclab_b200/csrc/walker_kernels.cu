@@ -899,6 +899,52 @@ __device__ __forceinline__ zd zsin(zd z)
     return make_double2(s * cosh(z.y), c * sinh(z.y));
 }
 
+// The 2x2 block of site i of a NiupNidn two-body sample with auxiliary
+// field x (setTwoBodySampleMatrix, NiupNidn.cpp:252-322): the field part
+// exp(gamma_i x) (or its cosh/sinh, cos/sin form for the hopping
+// decompositions) times the constant one-site factor constDiag.
+__device__ __forceinline__ void cp_site_matrix(const HubbardDev &h, int i, int x, zd &a00, zd &a01, zd &a10,
+                                               zd &a11)
+{
+    const zd ga = zscale(h.gamma[i], (double)x);
+    if (h.decomp == 0) {
+        const zd e = zexp(ga);
+        a00 = zmul(e, h.cd00[i]); a10 = zmul(e, h.cd10[i]); a01 = zmul(e, h.cd01[i]); a11 = zmul(e, h.cd11[i]);
+    } else if (h.decomp == 1) {
+        const zd e = zexp(ga), ei = zdiv(make_double2(1.0, 0.0), e);
+        a00 = zmul(e, h.cd00[i]); a10 = zmul(ei, h.cd10[i]); a01 = zmul(e, h.cd01[i]); a11 = zmul(ei, h.cd11[i]);
+    } else if (h.decomp == 2) {
+        const zd c = zcosh(ga), s = zsinh(ga);
+        a00 = zadd(zmul(c, h.cd00[i]), zmul(s, h.cd10[i]));
+        a10 = zadd(zmul(s, h.cd00[i]), zmul(c, h.cd10[i]));
+        a01 = zadd(zmul(c, h.cd01[i]), zmul(s, h.cd11[i]));
+        a11 = zadd(zmul(s, h.cd01[i]), zmul(c, h.cd11[i]));
+    } else {
+        const zd c = zcos(ga), s = zsin(ga);
+        a00 = zadd(zmul(c, h.cd00[i]), zmul(s, h.cd10[i]));
+        a10 = zadd(zmul(zneg(s), h.cd00[i]), zmul(c, h.cd10[i]));
+        a01 = zadd(zmul(c, h.cd01[i]), zmul(s, h.cd11[i]));
+        a11 = zadd(zmul(zneg(s), h.cd01[i]), zmul(c, h.cd11[i]));
+    }
+}
+
+// The force-independent log-weight of a sample (getTwoBodySampleFromAux,
+// NiupNidn.cpp:100-130): L log(1/2), plus for densityCharge dt U_sum / 2 and
+// minus the Kahan sum of aux_i gamma_i (erroranalysisHao/include/kahan.h).
+__device__ __forceinline__ zd cp_sample_logw(const HubbardDev &h, const int *aux)
+{
+    const int L = h.L;
+    if (h.decomp != 0) return make_double2(log(0.5) * L, 0.0);
+    zd sum = make_double2(0.0, 0.0), comp = make_double2(0.0, 0.0);
+    for (int i = 0; i < L; ++i) {
+        const zd y = zsub(zscale(h.gamma[i], (double)aux[i]), comp);
+        const zd t = zadd(sum, y);
+        comp = zsub(zsub(t, sum), y);
+        sum = t;
+    }
+    return zsub(make_double2(log(0.5) * L + h.dtUSum * 0.5, 0.0), sum);
+}
+
 // ---------------------------------------------------------------------------
 // Hubbard aux-field sampling + two-body sample + its application:
 // NiupNidn::sampleAuxFromForce (NiupNidn.cpp:66-84),
@@ -928,45 +974,11 @@ cp_sample_apply_kernel(int W, HubbardDev h, const double *force, const int *surv
         int x = (rng_uniform(seed, offs[w] + (unsigned long long)i) < prob) ? -1 : 1;
         aux[i] = x;
         if (auxOut) auxOut[(size_t)w * L + i] = x;
-        zd ga = zscale(h.gamma[i], (double)x);
-        zd a00, a01, a10, a11;
-        if (h.decomp == 0) {
-            zd e = zexp(ga);
-            a00 = zmul(e, h.cd00[i]); a10 = zmul(e, h.cd10[i]); a01 = zmul(e, h.cd01[i]); a11 = zmul(e, h.cd11[i]);
-        } else if (h.decomp == 1) {
-            zd e = zexp(ga), ei = zdiv(make_double2(1.0, 0.0), e);
-            a00 = zmul(e, h.cd00[i]); a10 = zmul(ei, h.cd10[i]); a01 = zmul(e, h.cd01[i]); a11 = zmul(ei, h.cd11[i]);
-        } else if (h.decomp == 2) {
-            zd c = zcosh(ga), s = zsinh(ga);
-            a00 = zadd(zmul(c, h.cd00[i]), zmul(s, h.cd10[i]));
-            a10 = zadd(zmul(s, h.cd00[i]), zmul(c, h.cd10[i]));
-            a01 = zadd(zmul(c, h.cd01[i]), zmul(s, h.cd11[i]));
-            a11 = zadd(zmul(s, h.cd01[i]), zmul(c, h.cd11[i]));
-        } else {
-            zd c = zcos(ga), s = zsin(ga);
-            a00 = zadd(zmul(c, h.cd00[i]), zmul(s, h.cd10[i]));
-            a10 = zadd(zmul(zneg(s), h.cd00[i]), zmul(c, h.cd10[i]));
-            a01 = zadd(zmul(c, h.cd01[i]), zmul(s, h.cd11[i]));
-            a11 = zadd(zmul(zneg(s), h.cd01[i]), zmul(c, h.cd11[i]));
-        }
-        d00[i] = a00; d01[i] = a01; d10[i] = a10; d11[i] = a11;
+        cp_site_matrix(h, i, x, d00[i], d01[i], d10[i], d11[i]);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        zd lw;
-        if (h.decomp == 0) {
-            // KahanData<complex<double>> sum of aux*gamma (erroranalysisHao/include/kahan.h)
-            zd sum = make_double2(0.0, 0.0), comp = make_double2(0.0, 0.0);
-            for (int i = 0; i < L; ++i) {
-                zd y = zsub(zscale(h.gamma[i], (double)aux[i]), comp);
-                zd t = zadd(sum, y);
-                comp = zsub(zsub(t, sum), y);
-                sum = t;
-            }
-            lw = zsub(make_double2(log(0.5) * L + h.dtUSum * 0.5, 0.0), sum);
-        } else {
-            lw = make_double2(log(0.5) * L, 0.0);
-        }
+        zd lw = cp_sample_logw(h, aux);
         double lp = 0.0;
         for (int i = 0; i < L; ++i) lp += aux[i] * fs[i] - log(exp(fs[i]) + exp(-fs[i]));
         lw.x -= lp;
@@ -985,6 +997,114 @@ cp_sample_apply_kernel(int W, HubbardDev h, const double *force, const int *surv
         dst[i + (size_t)n * j] = r0;
         dst[i + L + (size_t)n * j] = r1;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Back-propagation pieces (afqmcConstraintPathBP: afqmcConstraintPathMeasure.cpp
+// addMeasurement, afqmcConstraintPathBackPropagation.cpp).
+//
+// A recorded field sample applied to every walker whose record is valid
+// (getTwoBodySampleFromAux, NiupNidn.cpp:100-130): to the right
+// (NiupNidnSampleSDOperation::applyToRight, NiupNidnSDOperation.cpp:15-41,
+// logw += sample logw) or to the left (applyToLeft, :43-68: the 2x2 blocks
+// conjugated and their off-diagonals exchanged, logw += conj(sample logw)),
+// plus extraLogw (the log-weight of a one-body factor applied after it).
+// One block per walker; aux holds L fields per walker.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+cp_aux_apply_kernel(int W, HubbardDev h, const int *aux, const int *valid, const zd *wf, zd *wfOut, zd *logw,
+                    int left, zd extraLogw)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int w = blockIdx.x;
+    if (!valid[w]) return;
+    const int L = h.L, N = h.N, n = h.n;
+    zd *d00 = (zd *)smem_raw, *d01 = d00 + L, *d10 = d00 + 2 * L, *d11 = d00 + 3 * L;
+    const int *x = aux + (size_t)w * L;
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        zd a00, a01, a10, a11;
+        cp_site_matrix(h, i, x[i], a00, a01, a10, a11);
+        if (left) {
+            d00[i] = zconj(a00); d01[i] = zconj(a10); d10[i] = zconj(a01); d11[i] = zconj(a11);
+        } else {
+            d00[i] = a00; d01[i] = a01; d10[i] = a10; d11[i] = a11;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const zd lw = cp_sample_logw(h, x);
+        logw[w] = zadd(extraLogw, zadd(left ? zconj(lw) : lw, logw[w]));
+    }
+    const zd *src = wf + (size_t)w * n * N;
+    zd *dst = wfOut + (size_t)w * n * N;
+    for (int e = threadIdx.x; e < L * N; e += blockDim.x) {
+        const int i = e % L, j = e / L;
+        const zd a = src[i + (size_t)n * j], b = src[i + L + (size_t)n * j];
+        zd r0 = zmul(d00[i], a), r1 = zmul(d10[i], a);
+        zfma(r0, d01[i], b);
+        zfma(r1, d11[i], b);
+        dst[i + (size_t)n * j] = r0;
+        dst[i + L + (size_t)n * j] = r1;
+    }
+}
+
+// The population-control table applied to recorded rows: for steps
+// s < nsteps, row (s, w) takes row (s, table[w]) when table[w] != w
+// (AfqmcBackPropagationPop::operator=, the first BPNumber field records of
+// the parent).  Parents keep their own slot, so the copies are independent.
+__global__ void bp_gather_rows_kernel(int W, int rowlen, int nsteps, const int *table, int *data)
+{
+    const int w = blockIdx.x, st = blockIdx.y;
+    if (w >= W || st >= nsteps) return;
+    const int p = table[w];
+    if (p == w || p < 0 || p >= W) return;
+    const int *src = data + ((size_t)st * W + p) * rowlen;
+    int *dst = data + ((size_t)st * W + w) * rowlen;
+    for (int i = threadIdx.x; i < rowlen; i += blockDim.x) dst[i] = src[i];
+}
+
+// The commute estimator's energies from a walker's full Green's matrix
+// (HubbardSOCMeasureCommuteSDSD::addEnergy, :143-188): K = sum K(j,i) G(j,i),
+// V = sum_i U_i (G_ii G_{i+L,i+L} - G_{i,i+L} G_{i+L,i}), and the chemical
+// potential and field terms; den = exp(logov), as the mixed estimator's.
+// One block per walker, fixed-order block reductions.
+__global__ void __launch_bounds__(256)
+cp_commute_energy_kernel(int W, int L, const zd *G, const zd *K, const double *U, const double *mu,
+                         const double *hx, const double *hy, const double *hz, const int *alive,
+                         const zd *logov, zd *eloc, zd *den, zd *parts)
+{
+    __shared__ double red[32];
+    const int w = blockIdx.x;
+    if (w >= W || !alive[w]) return;
+    const int n = 2 * L;
+    const zd *g = G + (size_t)w * n * n;
+    zd kE = make_double2(0, 0), vE = make_double2(0, 0), rE = make_double2(0, 0);
+    for (long long e = threadIdx.x; e < (long long)n * n; e += blockDim.x) kE = zadd(kE, zmul(K[e], g[e]));
+    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+        auto at = [&](int r, int c) { return g[r + (size_t)n * c]; };
+        vE = zadd(vE, zscale(zsub(zmul(at(i, i), at(i + L, i + L)), zmul(at(i, i + L), at(i + L, i))), U[i]));
+        rE = zadd(rE, zscale(at(i, i), -mu[i] + hz[i] * 0.5));
+        rE = zadd(rE, zscale(at(i + L, i + L), -mu[i] - hz[i] * 0.5));
+        rE = zadd(rE, zmul(make_double2(hx[i] * 0.5, -hy[i] * 0.5), at(i, i + L)));
+        rE = zadd(rE, zmul(make_double2(hx[i] * 0.5, hy[i] * 0.5), at(i + L, i)));
+    }
+    kE = block_zsum(kE, red);
+    vE = block_zsum(vE, red);
+    rE = block_zsum(rE, red);
+    if (threadIdx.x == 0) {
+        eloc[w] = zadd(zadd(kE, vE), rE);
+        den[w] = zexp(logov[w]);
+        parts[3 * (size_t)w + 0] = kE;
+        parts[3 * (size_t)w + 1] = vE;
+        parts[3 * (size_t)w + 2] = rE;
+    }
+}
+
+__global__ void zconj_kernel(long long count, const zd *src, zd *dst)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+         e += (long long)gridDim.x * blockDim.x)
+        dst[e] = zconj(src[e]);
 }
 
 // ---------------------------------------------------------------------------
@@ -1840,6 +1960,36 @@ void launch_cp_observe(int W, int L, const zd *G, const zd *den, const int *aliv
     const long long n2 = 4LL * L * L, l2 = (long long)L * L;
     cp_observe_kernel<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(W, L, G, den, alive, obs, obs + n2, obs + 2 * n2,
                                                                   obs + 2 * n2 + l2, obs + 2 * n2 + 2 * l2);
+}
+
+void launch_cp_aux_apply(int W, const HubbardDev &h, const int *aux, const int *valid, const zd *wf, zd *wfOut,
+                         zd *logw, bool left, zd extraLogw, cudaStream_t s)
+{
+    g_launch_count++;
+    cp_aux_apply_kernel<<<W, 256, (size_t)4 * h.L * sizeof(zd), s>>>(W, h, aux, valid, wf, wfOut, logw, left ? 1 : 0,
+                                                                      extraLogw);
+}
+
+void launch_bp_gather_rows(int W, int rowlen, int nsteps, const int *table, int *data, cudaStream_t s)
+{
+    if (nsteps <= 0) return;
+    g_launch_count++;
+    bp_gather_rows_kernel<<<dim3((unsigned)W, (unsigned)nsteps), 64, 0, s>>>(W, rowlen, nsteps, table, data);
+}
+
+void launch_cp_commute_energy(int W, int L, const zd *G, const zd *K, const double *U, const double *mu,
+                              const double *hx, const double *hy, const double *hz, const int *alive,
+                              const zd *logov, zd *eloc, zd *den, zd *parts, cudaStream_t s)
+{
+    g_launch_count++;
+    cp_commute_energy_kernel<<<W, 256, 0, s>>>(W, L, G, K, U, mu, hx, hy, hz, alive, logov, eloc, den, parts);
+}
+
+void launch_zconj(long long count, const zd *src, zd *dst, cudaStream_t s)
+{
+    g_launch_count++;
+    const long long blocks = std::min<long long>((count + 255) / 256, 4096);
+    zconj_kernel<<<(unsigned)blocks, 256, 0, s>>>(count, src, dst);
 }
 
 void launch_walker_xfer(int count, long long wsize, const int *idx, zd *wf, zd *logw, zd *buf, bool unpack,

@@ -85,6 +85,17 @@ void launch_pop_comb(int W, const double *weight, const double *uniforms, uint64
 // Observe-estimator sums (greenMatrixNum, densityDensityNum: n x n each;
 // splusSminusNum, sminusSplusNum, spairSpairNum: L x L each, in that order in obs).
 void launch_cp_observe(int W, int L, const zd *G, const zd *den, const int *alive, zd *obs, cudaStream_t s);
+// back-propagation: a recorded field sample applied to the right or the
+// left of the walkers whose record is valid; recorded rows gathered by a
+// population-control table; the commute estimator's energies from full G;
+// an elementwise conjugate copy
+void launch_cp_aux_apply(int W, const HubbardDev &h, const int *aux, const int *valid, const zd *wf, zd *wfOut,
+                         zd *logw, bool left, zd extraLogw, cudaStream_t s);
+void launch_bp_gather_rows(int W, int rowlen, int nsteps, const int *table, int *data, cudaStream_t s);
+void launch_cp_commute_energy(int W, int L, const zd *G, const zd *K, const double *U, const double *mu,
+                              const double *hx, const double *hy, const double *hz, const int *alive,
+                              const zd *logov, zd *eloc, zd *den, zd *parts, cudaStream_t s);
+void launch_zconj(long long count, const zd *src, zd *dst, cudaStream_t s);
 // Batched walker transfer records (matrix + logw each), walker idx[k] <-> record k.
 void launch_walker_xfer(int count, long long wsize, const int *idx, zd *wf, zd *logw, zd *buf, bool unpack,
                         cudaStream_t s);

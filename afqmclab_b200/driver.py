@@ -35,6 +35,14 @@ class ConstraintPathMethod:
 
 
 @dataclass
+class ConstraintPathBPMethod(ConstraintPathMethod):
+    """AfqmcConstraintPathMethod of the back-propagation tutorial: the
+    constrained-path parameters plus backPropagationStep
+    (tutorials/afqmcConstraintPathBP/source/afqmcConstraintPathMethod.cpp:19-46)."""
+    backPropagationStep: int = 40
+
+
+@dataclass
 class PhaselessMethod:
     """AfqmcPhaselessMethod's loop parameters and their defaults
     (afqmcPhaselessMethod.cpp:160-183)."""
@@ -112,6 +120,53 @@ def run_constraint_path(eng, method, out_dir=None, on_block=None):
     sums = _blocks(eng, method, out_dir, on_block)
     eng.project_half(+1)
     return sums
+
+
+def run_constraint_path_bp(eng, method, out_dir=None, on_block=None):
+    """measureWithProjection of the back-propagation driver
+    (tutorials/afqmcConstraintPathBP/source/afqmcConstraintPath.cpp:115-172):
+    thermalise with E_T adjustment, open a back-propagation window, and in the
+    blocks measure the back-propagated observe estimator whenever the window
+    is full.  The engine must have the observe estimator on.  Returns the
+    block sums (writeNumber x 5: den, HNum, KNum, VNum, RNum)."""
+    bp, skip = method.backPropagationStep, method.measureSkipStep
+    eng.set_cadence(0, 0)
+    eng.reset_measurement()
+    eng.project_half(-1)
+    for i in range(method.thermalSize):
+        if i < method.ETAdjustMaxSize and i % method.ETAdjustStep == 0:
+            eng.add_mixed_measurement()
+            eng.set_ET(float(mixed_energy(eng).real))
+            eng.reset_measurement()
+        eng.step(1)
+    eng.bp_begin(bp, skip)                        # prepareBackPropagation
+    if bp >= skip:
+        for _ in range(bp):
+            eng.step(1)
+    sums = []
+    for i in range(method.writeNumber):
+        for _ in range(method.measureNumberPerWrite):
+            for _ in range(method.measureSkipStep):
+                active, index = eng.bp_state()
+                if active and index == bp:
+                    eng.bp_measure()
+                eng.step(1)
+            if bp < skip:
+                eng.bp_begin(bp, skip)
+        sums.append(eng.measurement())
+        if out_dir is not None:
+            rank, _ = records.rank_world()
+            beta = (method.thermalSize + (i + 0.5) * method.measureNumberPerWrite * method.measureSkipStep
+                    - 0.5) * method.dt
+            if rank == 0:
+                with open(os.path.join(out_dir, "beta.dat"), "a") as f:
+                    f.write(f"{beta:26.16e}\n")
+            records.write_measurement(eng, out_dir)
+        if on_block is not None:
+            on_block(i, eng)
+        eng.reset_measurement()
+    eng.project_half(+1)
+    return np.array(sums)
 
 
 def run_phaseless(eng, model, method, out_dir=None, on_block=None):

@@ -186,6 +186,25 @@ int afqmc_cp_set_observables(afqmc_engine *e, int on);
 /* The observe sums, complex column-major (NULL skips one). */
 int afqmc_get_observables(afqmc_engine *e, double *greenNum, double *densityDensityNum,
                           double *splusSminusNum, double *sminusSplusNum, double *spairSpairNum);
+/* Back-propagated estimator of the constrained path (tutorials/
+ * afqmcConstraintPathBP: prepareBackPropagation,
+ * afqmcConstraintPathBackPropagation.cpp:11-20; addMeasurement,
+ * afqmcConstraintPathMeasure.cpp:47-78).  afqmc_cp_bp_begin starts a window of
+ * `steps` steps from the current walkers (measure_skip: the driver's
+ * measureSkipStep); every step then records its auxiliary fields and any
+ * population-control table.  Once `steps` steps are recorded,
+ * afqmc_cp_bp_measure resamples the window-start walkers by the recorded
+ * tables, propagates the trial leftwards through each walker's recorded
+ * fields, and adds the observe estimator (den, HNum/KNum/VNum/RNum from the
+ * full Green's matrix, greenMatrixNum, ...) for the pair, weighted by the
+ * current walker's overlap; with steps >= measure_skip the window then slides
+ * by measure_skip steps, otherwise back-propagation stops until the next
+ * afqmc_cp_bp_begin.  FP64 form, observe estimator on
+ * (afqmc_cp_set_observables); a step past a full window is an error.
+ * afqmc_cp_bp_state reports whether a window is open and its BPIndex. */
+int afqmc_cp_bp_begin(afqmc_engine *e, int steps, int measure_skip);
+int afqmc_cp_bp_measure(afqmc_engine *e);
+int afqmc_cp_bp_state(afqmc_engine *e, int *active, int *index);
 /* choleskyBgNum / choleskyExNum (G complex each), PL only */
 int afqmc_get_cholesky_nums(afqmc_engine *e, double *bgNum, double *exNum);
 

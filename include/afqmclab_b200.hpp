@@ -384,6 +384,28 @@ public:
               "afqmc_pl_update_background");
     }
 
+    // Back-propagation of the constrained path (tutorials/afqmcConstraintPathBP):
+    // prepareBackPropagation, the full-window test of the driver loop
+    // (BPIndex == backPropagationStep) and addMeasurement.  FP64 form with the
+    // observe estimator on (setObservables).
+    void setObservables(bool on)
+    {
+        requireKind(0);
+        check(afqmc_cp_set_observables(e_, on ? 1 : 0), "afqmc_cp_set_observables");
+    }
+    void prepareBackPropagation(int backPropagationStep, int measureSkipStep)
+    {
+        requireKind(0);
+        check(afqmc_cp_bp_begin(e_, backPropagationStep, measureSkipStep), "afqmc_cp_bp_begin");
+    }
+    bool backPropagationReady(int backPropagationStep) const
+    {
+        int active = 0, index = 0;
+        check(afqmc_cp_bp_state(e_, &active, &index), "afqmc_cp_bp_state");
+        return active != 0 && index == backPropagationStep;
+    }
+    void addBackPropagationMeasurement() { check(afqmc_cp_bp_measure(e_), "afqmc_cp_bp_measure"); }
+
     // OR of the per-walker status bits (1 singular overlap, 2 non-finite,
     // 4 Taylor order cap, 8 zero column norm, 16 comb, 32 tensor-core wait)
     int status() const

@@ -37,7 +37,7 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.normpath(os.path.join(_HERE, "..", "_ref"))
-PROGRAMS = {"cp": "afqmcConstraintPath", "pl": "afqmcPhaseless"}
+PROGRAMS = {"cp": "afqmcConstraintPath", "pl": "afqmcPhaseless", "bp": "afqmcConstraintPathBP"}
 
 sys.path.insert(0, os.path.normpath(os.path.join(_HERE, "..", "..")))
 from afqmclab_b200 import inputs  # noqa: E402
@@ -62,7 +62,7 @@ def build(reference="/root/reference"):
 def rng_offset(kind, m):
     """Uniforms the program draws in estimateMemory, before its first
     projection step."""
-    return m.L if kind == "cp" else 2 * m.G
+    return m.L if kind in ("cp", "bp") else 2 * m.G
 
 
 def start_like_program(eng, kind, m, seed):
@@ -244,6 +244,37 @@ def run_cp(m, method, wf, logw, seed, mgs_step=10, pop_step=40, force_type="dyna
         prepare("cp", m, method, wf, logw, seed, mgs_step, pop_step, force_type, workdir)
         log = _run("cp", workdir, threads, timeout)
         out = _streams(workdir, ["den", "HNum", "KNum", "VNum", "RNum"])
+        out["walkers"] = _final_walkers(workdir, "cp", wf.shape)
+        return out, log
+    finally:
+        if own:
+            shutil.rmtree(workdir, ignore_errors=True)
+
+
+OBSERVE_STREAMS = ["greenMatrixNum", "densityDensityNum", "splusSminusNum", "sminusSplusNum",
+                   "spairSpairNum"]
+
+
+def run_cp_bp(m, method, bp_steps, wf, logw, seed, mgs_step=10, pop_step=40, force_type="dynamicForce",
+              threads=1, workdir=None, timeout=600):
+    """One run of afqmcConstraintPathBP (back-propagation, observe estimator)
+    on the Hubbard inputs `m` with backPropagationStep = bp_steps.  Returns the
+    streams den, HNum, KNum, VNum, RNum (one row per block) and the observe
+    streams (one 2L x 2L or L x L matrix per block, column-major rows), the
+    final walkers and the program's stdout."""
+    own = workdir is None
+    workdir = workdir or tempfile.mkdtemp(prefix="afqmc_ref_bp_")
+    try:
+        prepare("cp", m, method, wf, logw, seed, mgs_step, pop_step, force_type, workdir)
+        with open(os.path.join(workdir, "afqmc_param"), "a") as f:
+            f.write(f"backPropagationStep {bp_steps}\n")
+        log = _run("bp", workdir, threads, timeout)
+        out = _streams(workdir, ["den", "HNum", "KNum", "VNum", "RNum"])
+        nb = len(out["den"])
+        for name in OBSERVE_STREAMS:
+            v = _streams(workdir, [name]).get(name)
+            if v is not None:
+                out[name] = v.reshape(nb, -1)
         out["walkers"] = _final_walkers(workdir, "cp", wf.shape)
         return out, log
     finally:
