@@ -7,7 +7,10 @@
 std::atomic<long long> g_launch_count{0};
 
 #include <stdio.h>
+#include <cooperative_groups.h>
 #include "once.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -624,6 +627,54 @@ __device__ __forceinline__ zd zrcp(zd b)
     return make_double2(r * d, -d);
 }
 
+// Per-walker finish of the block log-determinants: the overlap's log and,
+// by mode, the constraint or the population weight.  ldB/sgB hold the
+// walker's nb block log-determinants and singular flags.
+__device__ void lu_walker_finish(int w, bool act, int nb, int mult, const zd *ldB, const int *sgB,
+                                 const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv,
+                                 zd *logwOut, double *weight, int *status, int mode)
+{
+    if (!act) {
+        if (mode == LU_PROJECT) surv[w] = 0;
+        if (mode == LU_POPWEIGHT) { weight[w] = 0.0; alive[w] = 1; }
+        return;
+    }
+    bool singular = false;
+    zd logdetSum = make_double2(0.0, 0.0);
+    // a singular block adds lognorm -1e300 with phase 1
+    // (lognormPhaseDeterminant, tensor_2d_common_fun.cpp:75-84)
+    for (int t = 0; t < nb; ++t) {
+        const bool sb = sgB[t] != 0;
+        singular = singular || sb;
+        logdetSum = zadd(logdetSum, sb ? make_double2(-1e300, 0.0) : ldB[t]);
+    }
+    const zd lwR = zadd(logwAdd, logw[w]);
+    if (mult == 2) logdetSum = zadd(logdetSum, logdetSum);
+    const zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
+    logov[w] = lo;
+    if (singular && status) atomicOr(status + w, (int)ST_SINGULAR);
+    if (!(isfinite(lo.x) && isfinite(lo.y)) && status && !singular) atomicOr(status + w, (int)ST_NONFINITE);
+    if (mode == LU_PROJECT) {
+        const double ph = lo.y;
+        const double c = cos(ph);
+        if (c <= 0.0) {
+            alive[w] = 0; surv[w] = 0;
+        } else {
+            logwOut[w] = zadd(logw[w], make_double2(log(c), -ph));
+            surv[w] = 1;
+        }
+    } else if (mode == LU_POPWEIGHT) {
+        const zd e = zexp(lo);
+        if (e.x <= 0.0) {
+            weight[w] = 0.0;
+        } else {
+            weight[w] = e.x;
+            logwOut[w] = zsub(logw[w], lo);
+        }
+        alive[w] = 1;
+    }
+}
+
 __global__ void __launch_bounds__(GR_WARPS * 32, 3)
 gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
               const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
@@ -752,44 +803,286 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long 
     if (lane == 0) { ldS[warp] = ld; sgS[warp] = sing ? 1 : 0; }
     __syncthreads();
     if (lane != 0 || b != 0 || !inW) return;
-    if (!act) {
-        if (mode == LU_PROJECT) surv[w] = 0;
-        if (mode == LU_POPWEIGHT) { weight[w] = 0.0; alive[w] = 1; }
-        return;
-    }
-    bool singular = false;
-    zd logdetSum = make_double2(0.0, 0.0);
-    // a singular block adds lognorm -1e300 with phase 1
-    // (lognormPhaseDeterminant, tensor_2d_common_fun.cpp:75-84)
-    for (int t = 0; t < nb; ++t) {
-        const bool sb = sgS[warp + t] != 0;
-        singular = singular || sb;
-        logdetSum = zadd(logdetSum, sb ? make_double2(-1e300, 0.0) : ldS[warp + t]);
-    }
-    const zd lwR = zadd(logwAdd, logw[w]);
-    if (bl.mult == 2) logdetSum = zadd(logdetSum, logdetSum);
-    const zd lo = zadd(zadd(zconj(logwT), lwR), logdetSum);
-    logov[w] = lo;
-    if (singular && status) atomicOr(status + w, (int)ST_SINGULAR);
-    if (!(isfinite(lo.x) && isfinite(lo.y)) && status && !singular) atomicOr(status + w, (int)ST_NONFINITE);
-    if (mode == LU_PROJECT) {
-        const double ph = lo.y;
-        const double c = cos(ph);
-        if (c <= 0.0) {
-            alive[w] = 0; surv[w] = 0;
-        } else {
-            logwOut[w] = zadd(logw[w], make_double2(log(c), -ph));
-            surv[w] = 1;
+    lu_walker_finish(w, act, nb, bl.mult, ldS + warp, sgS + warp, logw, logwAdd, logwT,
+                     logov, alive, surv, logwOut, weight, status, mode);
+}
+
+// ---------------------------------------------------------------------------
+// The same rotated Gauss-Jordan for blocks of 33-64 columns, one CTA of four
+// warps per matrix.  Warp (rh, ch) holds rows rh*32+lane and half ch of a
+// 64-column window that moves by one column per step.  The half-0 warps hold
+// the current column in slot 0; while they update step k they already search
+// the pivot of step k+1 in their new slot 0 (max |re|+|im|, ties to the lower
+// position, NaN first), and each warp's winning lane publishes its row, its
+// position and the reciprocal of its pivot.  After one CTA barrier per step:
+//   - half 0 updates from the published half-0 row of the winner; the last
+//     slot of every row (and of the pivot row) is the updated slot 0 of half
+//     1 from the step before, passed through shared memory;
+//   - half 1 takes its factor f = a_k * (1/piv) from the published column k,
+//     the pivot row's lane writes its half-1 row, a barrier of the two half-1
+//     warps, then half 1 updates and takes the new inverse column in its last
+//     slot.
+// Shared buffers alternate between even and odd steps, so the only CTA-wide
+// barrier per step is the one that publishes step k+1's inputs.
+// Only Ns steps run and the padding is zero: padding rows stay zero in every
+// real column and are never chosen, and after step Ns the window holds the
+// inverse columns 0..Ns-1 in its last Ns slots.  Row r's final position is
+// the image of r under the interchanges applied first to last, so column j
+// of the interchanged inverse is column r of the inverse for the row r whose
+// final position is j.  The two blocks of a two-block walker run as a
+// cluster of two CTAs; rank 0 combines them through distributed shared
+// memory.
+// ---------------------------------------------------------------------------
+struct GR64Cand {
+    unsigned long long u;   // rank of the candidate: bits of |re|+|im| plus one, 0 if not eligible
+    int key;                // its position
+    int row;                // its row (rh*32+lane)
+    zd a0;                  // its value in the current column
+    zd q;                   // 1 / a0, zero when a0 is zero
+};
+
+// A rank that orders candidates like the pivot search: for values >= +0 the
+// IEEE bits are monotonic; NaN ranks as infinity; ineligible rows rank 0.
+__device__ __forceinline__ unsigned long long gr64_rank(zd a0, bool eligible)
+{
+    double v = zcabs1(a0);
+    if (!(v == v)) v = INFINITY;
+    return eligible ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
+}
+
+// 1 / b without a division, so that it schedules between other arithmetic:
+// b is scaled by a power of two (exact) so that max(|re|, |im|) lies in
+// [1, 2), the real reciprocal y of d = |b|^2 in [1, 8) starts from the
+// single-precision approximation and takes two Newton-Raphson steps
+// y <- y + y (1 - d y), each of which doubles the correct bits (about 21 ->
+// 42 -> full precision), and 1/b = s conj(b s) y.  Within a few ulp of the
+// rounded quotient; a NaN or infinite b gives NaN (callers test zero first).
+__device__ __forceinline__ zd zrcp_nr(zd b)
+{
+    const double m = fmax(fabs(b.x), fabs(b.y));
+    const long long e = (__double_as_longlong(m) >> 52) & 0x7ff;
+    const double s = __longlong_as_double((2046 - e) << 52);   // 2^(1023 - e)
+    const double xs = b.x * s, ys = b.y * s;
+    const double d = fma(xs, xs, ys * ys);
+    double y = (double)__fdividef(1.0f, (float)d);
+    y = fma(y, fma(-d, y, 1.0), y);
+    y = fma(y, fma(-d, y, 1.0), y);
+    const double t = y * s;
+    return make_double2(xs * t, -ys * t);
+}
+
+// Position of the warp's best candidate: largest rank, then lowest position.
+__device__ __forceinline__ int gr64_warp_best(unsigned long long u, int pos)
+{
+    const unsigned hi = (unsigned)(u >> 32), lo = (unsigned)u;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    const unsigned key = (hi == mhi && lo == mlo) ? (unsigned)pos : 0xffffffffu;
+    return (int)__reduce_min_sync(0xffffffffu, key);
+}
+
+__device__ __forceinline__ void gr64_half_bar()
+{
+    asm volatile("bar.sync 1, 64;" ::: "memory");
+}
+
+template <int NB>
+__global__ void __launch_bounds__(128, 3)
+gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
+                const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
+                double *weight, int *status, int mode, int wantInverse)
+{
+    __shared__ __align__(16) zd prowC[2][2][32];   // [step parity][rh]: half 0 of each warp's candidate
+    __shared__ __align__(16) zd prow1[32];         // half 1 of the pivot row
+    __shared__ __align__(16) zd colS[2][64];       // [step parity][row]: the current column
+    __shared__ __align__(16) zd xS[2][64];         // [step parity][row]: half 1's updated slot 0
+    __shared__ __align__(16) GR64Cand cand[2][2];  // [step parity][rh]
+    __shared__ __align__(16) zd pivS[64];
+    __shared__ __align__(16) zd phS[2];
+    __shared__ double lnS[2];
+    __shared__ int pvS[64];
+    __shared__ int jxS[64];
+    __shared__ zd ldS;
+    __shared__ int sgS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rh = warp >> 1, ch = warp & 1;
+    const int r = rh * 32 + lane;
+    const int w = NB == 1 ? (int)blockIdx.x : (int)(blockIdx.x >> 1);
+    const int b = NB == 1 ? 0 : (int)(blockIdx.x & 1);
+    const bool act = (active == nullptr) || active[w] != 0;
+    const int Ns = b == 0 ? bl.Ns[0] : bl.Ns[1];
+    const long long sOff = b == 0 ? bl.sOff[0] : bl.sOff[1];
+    const bool inv = wantInverse && (Sinv || Sinv32);
+    bool sing = false;
+    zd ld = make_double2(0.0, 0.0);
+    if (act && Ns > 0) {   // uniform over the CTA
+        const zd *Sg = S + (size_t)w * bl.sStride + sOff;
+        zd a[32];
+#pragma unroll
+        for (int s = 0; s < 32; ++s) {
+            const int c = ch * 32 + s;
+            a[s] = (r < Ns && c < Ns) ? Sg[r + (size_t)Ns * c] : make_double2(0.0, 0.0);
         }
-    } else if (mode == LU_POPWEIGHT) {
-        const zd e = zexp(lo);
-        if (e.x <= 0.0) {
-            weight[w] = 0.0;
-        } else {
-            weight[w] = e.x;
-            logwOut[w] = zsub(logw[w], lo);
+        int pos = r;
+        if (ch == 0) {
+            // step 0's inputs, as if a step -1 had produced them
+            xS[1][r] = a[31];
+            colS[0][r] = a[0];
+            const unsigned long long u = gr64_rank(a[0], true);
+            if (pos == gr64_warp_best(u, pos)) {
+                GR64Cand c;
+                c.u = u; c.key = pos; c.row = r; c.a0 = a[0];
+                c.q = zeq0(a[0]) ? make_double2(0.0, 0.0) : zrcp_nr(a[0]);
+                cand[0][rh] = c;
+#pragma unroll
+                for (int s = 0; s < 31; ++s) prowC[0][rh][s] = a[s];
+            }
         }
-        alive[w] = 1;
+#pragma unroll 1
+        for (int k = 0; k < Ns; ++k) {
+            __syncthreads();   // step k's candidates, column, half-0 rows and half 1's last slots
+            const int cb = k & 1, pb = cb ^ 1;
+            const unsigned long long u0 = cand[cb][0].u, u1 = cand[cb][1].u;
+            const int k0 = cand[cb][0].key, k1 = cand[cb][1].key;
+            const int second = (u1 > u0 || (u1 == u0 && k1 < k0)) ? 1 : 0;
+            const int p = second ? k1 : k0;
+            const zd q = cand[cb][second].q;
+            if (threadIdx.x == 0) {
+                const zd piv = cand[cb][second].a0;
+                pvS[k] = p;
+                pivS[k] = piv;
+                sing = sing || zeq0(piv);
+            }
+            const bool isP = (pos == p);
+            if (pos == k) pos = p;
+            if (isP) pos = k;
+            if (ch == 0) {
+                a[31] = xS[pb][r];
+                const zd *pr = prowC[cb][second];
+                const zd p31 = xS[pb][cand[cb][second].row];
+                const zd f = isP ? make_double2(0.0, 0.0) : zmul(a[0], q);
+                {
+                    const zd pv = pr[1];
+                    a[0].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[1].x));
+                    a[0].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[1].y));
+                }
+                // the pivot search of step k+1 on the new slot 0
+                bool win = false;
+                unsigned long long u = 0;
+                zd qn = make_double2(0.0, 0.0);
+                if (k + 1 < Ns) {
+                    colS[pb][r] = a[0];
+                    u = gr64_rank(a[0], pos > k);
+                    win = (pos == gr64_warp_best(u, pos));
+                    if (!zeq0(a[0])) qn = zrcp_nr(a[0]);
+                }
+#pragma unroll
+                for (int s = 2; s < 32; ++s) {
+                    const zd pv = s < 31 ? pr[s] : p31;
+                    a[s - 1].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[s].x));
+                    a[s - 1].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[s].y));
+                }
+                if (win) {
+                    GR64Cand c;
+                    c.u = u; c.key = pos; c.row = r; c.a0 = a[0];
+                    c.q = qn;
+                    cand[pb][rh] = c;
+#pragma unroll
+                    for (int s = 0; s < 31; ++s) prowC[pb][rh][s] = a[s];
+                }
+            } else {
+                const zd f = isP ? make_double2(0.0, 0.0) : zmul(colS[cb][r], q);
+                if (isP) {
+#pragma unroll
+                    for (int s = 0; s < 32; ++s) prow1[s] = a[s];
+                }
+                gr64_half_bar();
+                zd x;
+                x.x = fma(-f.x, prow1[0].x, fma(f.y, prow1[0].y, a[0].x));
+                x.y = fma(-f.x, prow1[0].y, fma(-f.y, prow1[0].x, a[0].y));
+                xS[cb][r] = x;
+#pragma unroll
+                for (int s = 1; s < 32; ++s) {
+                    const zd pv = prow1[s];
+                    a[s - 1].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[s].x));
+                    a[s - 1].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[s].y));
+                }
+                a[31] = isP ? make_double2(1.0, 0.0) : zneg(f);
+            }
+        }
+        if (threadIdx.x == 0) sgS = sing ? 1 : 0;
+        __syncthreads();   // last slots of step Ns-1, all pivots
+        sing = sgS != 0;
+        if (ch == 0) a[31] = xS[(Ns - 1) & 1][r];
+        const bool real = r < Ns;   // padding rows keep positions >= Ns
+        const zd myD = real ? pivS[pos] : make_double2(1.0, 0.0);
+        if (ch == 0) {
+            // log-determinant: every real row supplied exactly one pivot
+            double ln = 0.0;
+            zd ph = make_double2(1.0, 0.0);
+            if (real && !sing) {
+                const double ad = zabs(myD);
+                ln = log(ad);
+                ph = make_double2(myD.x / ad, myD.y / ad);
+                if (pvS[pos] != pos) ph = zneg(ph);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                ln += __shfl_xor_sync(0xffffffffu, ln, o);
+                zd t;
+                t.x = __shfl_xor_sync(0xffffffffu, ph.x, o);
+                t.y = __shfl_xor_sync(0xffffffffu, ph.y, o);
+                ph = zmul(ph, t);
+            }
+            if (lane == 0) { lnS[rh] = ln; phS[rh] = ph; }
+            if (real) jxS[pos] = r;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && !sing) ld = zadd(make_double2(lnS[0] + lnS[1], 0.0), zlog(zmul(phS[0], phS[1])));
+        if (inv && real) {
+            // window slot t = 32 ch + s holds interchanged column j = t - (64 - Ns)
+            const zd sc = sing ? make_double2(0.0, 0.0) : zrcp(myD);
+            const int j0 = ch * 32 - (64 - Ns);
+            if (Sinv32) {
+                // fp32 planes [re | im], each Ns x Ns column-major
+                float *Xr = Sinv32 + (size_t)w * s32 + 2 * sOff, *Xi = Xr + (size_t)Ns * Ns;
+#pragma unroll
+                for (int s = 0; s < 32; ++s) {
+                    const int j = j0 + s;
+                    if (j >= 0) {
+                        const int c = jxS[j];
+                        const zd v = zmul(sc, a[s]);
+                        Xr[pos + (size_t)Ns * c] = (float)v.x;
+                        Xi[pos + (size_t)Ns * c] = (float)v.y;
+                    }
+                }
+            } else {
+                zd *Xg = Sinv + (size_t)w * bl.sStride + sOff;
+#pragma unroll
+                for (int s = 0; s < 32; ++s) {
+                    const int j = j0 + s;
+                    if (j >= 0) Xg[pos + (size_t)Ns * jxS[j]] = zmul(sc, a[s]);
+                }
+            }
+        }
+    }
+    if (threadIdx.x == 0) { ldS = ld; sgS = sing ? 1 : 0; }
+    if constexpr (NB == 2) {
+        cg::cluster_group cl = cg::this_cluster();
+        cl.sync();
+        if (threadIdx.x == 0 && b == 0) {
+            const zd ldB[2] = {ldS, *cl.map_shared_rank(&ldS, 1)};
+            const int sgB[2] = {sgS, *cl.map_shared_rank(&sgS, 1)};
+            lu_walker_finish(w, act, 2, bl.mult, ldB, sgB, logw, logwAdd, logwT, logov, alive, surv, logwOut,
+                             weight, status, mode);
+        }
+        cl.sync();   // rank 1's shared memory stays until rank 0 has read it
+    } else {
+        if (threadIdx.x == 0) {
+            const int sg = sing ? 1 : 0;
+            lu_walker_finish(w, act, 1, bl.mult, &ld, &sg, logw, logwAdd, logwT, logov, alive, surv, logwOut,
+                             weight, status, mode);
+        }
     }
 }
 
@@ -1801,6 +2094,30 @@ void launch_lu_logdet_inverse32(int W, const Blocks &bl, zd *S, zd *Sinv, float 
         gj_reg_kernel<<<(unsigned)((mats + GR_WARPS - 1) / GR_WARPS), GR_WARPS * 32, 0, s>>>(
             W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov, alive, surv,
             logwOut, weight, status, mode, wantInverse ? 1 : 0);
+        return;
+    }
+    if (maxNs > 32 && maxNs <= 64 && (bl.nblk == 1 || bl.nblk == 2)) {
+        g_launch_count++;
+        zd *X64 = Sinv32 ? nullptr : Sinv;
+        const int inv = wantInverse ? 1 : 0;
+        if (bl.nblk == 1) {
+            gj_reg64_kernel<1><<<W, 128, 0, s>>>(W, bl, S, X64, Sinv32, s32, active, logw, logwAdd, logwT, logov,
+                                                 alive, surv, logwOut, weight, status, mode, inv);
+            return;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(2 * W));
+        cfg.blockDim = dim3(128);
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 2;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, gj_reg64_kernel<2>, W, bl, (const zd *)S, X64, Sinv32, s32, active, logw,
+                           logwAdd, logwT, logov, alive, surv, logwOut, weight, status, mode, inv);
         return;
     }
     launch_lu_fp64(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov, alive, surv, logwOut, weight, status,
