@@ -598,10 +598,14 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
 // ---------------------------------------------------------------------------
 // Same contract as gj_warp_kernel for one or two blocks of 17..32 columns, one
 // warp per (walker, block) and the matrix in registers: lane i holds row i
-// (padded to 32 x 32 with the identity, which adds no interchange and a unit
-// pivot).  The column loop is not unrolled; instead every lane's row rotates
-// by one slot per step, so the current column is always register slot 0 and
-// every register index is static.
+// (padded to 32 x 32 with zeros; only Ns steps run, after which the last Ns
+// register slots hold the inverse columns).  The column loop is not
+// unrolled; instead every lane's row rotates by one slot per step, so the
+// current column is always register slot 0 and every register index is
+// static.  While it updates step k the warp already searches the pivot of
+// step k+1 in its new slot 0 (redux over a rank of |re|+|im|), and the
+// winning lane publishes its row, position and a division-free reciprocal of
+// its pivot, so a step starts with one warp barrier and no search.
 //   - pivot: zgetf2's choice, first position >= k of maximal |re|+|im| in the
 //     column; rows are not moved, each lane keeps the position its row has in
 //     the interchanged matrix (ties go to the lower position, as in izamax);
@@ -625,6 +629,46 @@ __device__ __forceinline__ zd zrcp(zd b)
     }
     const double r = b.x / b.y, d = 1.0 / (b.y + b.x * r);
     return make_double2(r * d, -d);
+}
+
+// A rank that orders candidates like the pivot search: for values >= +0 the
+// IEEE bits are monotonic; NaN ranks as infinity; ineligible rows rank 0.
+__device__ __forceinline__ unsigned long long gr_rank(zd a0, bool eligible)
+{
+    double v = zcabs1(a0);
+    if (!(v == v)) v = INFINITY;
+    return eligible ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
+}
+
+// 1 / b without a division, so that it schedules between other arithmetic:
+// b is scaled by a power of two (exact) so that max(|re|, |im|) lies in
+// [1, 2), the real reciprocal y of d = |b|^2 in [1, 8) starts from the
+// single-precision approximation and takes two Newton-Raphson steps
+// y <- y + y (1 - d y), each of which doubles the correct bits (about 21 ->
+// 42 -> full precision), and 1/b = s conj(b s) y.  Within a few ulp of the
+// rounded quotient; a NaN or infinite b gives NaN (callers test zero first).
+__device__ __forceinline__ zd zrcp_nr(zd b)
+{
+    const double m = fmax(fabs(b.x), fabs(b.y));
+    const long long e = (__double_as_longlong(m) >> 52) & 0x7ff;
+    const double s = __longlong_as_double((2046 - e) << 52);   // 2^(1023 - e)
+    const double xs = b.x * s, ys = b.y * s;
+    const double d = fma(xs, xs, ys * ys);
+    double y = (double)__fdividef(1.0f, (float)d);
+    y = fma(y, fma(-d, y, 1.0), y);
+    y = fma(y, fma(-d, y, 1.0), y);
+    const double t = y * s;
+    return make_double2(xs * t, -ys * t);
+}
+
+// Position of the warp's best candidate: largest rank, then lowest position.
+__device__ __forceinline__ int gr_warp_best(unsigned long long u, int pos)
+{
+    const unsigned hi = (unsigned)(u >> 32), lo = (unsigned)u;
+    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+    const unsigned key = (hi == mhi && lo == mlo) ? (unsigned)pos : 0xffffffffu;
+    return (int)__reduce_min_sync(0xffffffffu, key);
 }
 
 // Per-walker finish of the block log-determinants: the overlap's log and,
@@ -675,14 +719,17 @@ __device__ void lu_walker_finish(int w, bool act, int nb, int mult, const zd *ld
     }
 }
 
-__global__ void __launch_bounds__(GR_WARPS * 32, 3)
+__global__ void __launch_bounds__(GR_WARPS * 32, 2)
 gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
               const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
               double *weight, int *status, int mode, int wantInverse)
 {
-    __shared__ __align__(16) zd prow[GR_WARPS][2][32];
+    __shared__ __align__(16) zd prow[GR_WARPS][2][32];   // [warp][step parity]: the pivot row
+    __shared__ __align__(16) zd candQ[GR_WARPS][2];      // 1 / pivot
+    __shared__ __align__(16) zd candA[GR_WARPS][2];      // pivot
+    __shared__ int candKey[GR_WARPS][2];                 // pivot position
     __shared__ int pvS[GR_WARPS][32];
-    __shared__ int ixS[GR_WARPS][32];
+    __shared__ int jxS[GR_WARPS][32];
     __shared__ zd pivS[GR_WARPS][32];
     __shared__ zd ldS[GR_WARPS];
     __shared__ int sgS[GR_WARPS];
@@ -702,53 +749,74 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long 
         zd a[32];
 #pragma unroll
         for (int j = 0; j < 32; ++j)
-            a[j] = (lane < Ns && j < Ns) ? Sg[lane + (size_t)Ns * j] : make_double2(lane == j ? 1.0 : 0.0, 0.0);
+            a[j] = (lane < Ns && j < Ns) ? Sg[lane + (size_t)Ns * j] : make_double2(0.0, 0.0);
         // A row chosen at step k keeps position k for good, so a lane's final
         // position names the step whose pivot it supplied (and its row scale).
         int pos = lane;
-#pragma unroll 1
-        for (int k = 0; k < 32; ++k) {
-            double v = pos >= k ? zcabs1(a[0]) : -1.0;
-            if (!(v == v)) v = INFINITY;   // a NaN row wins, so every lane agrees on p
-            int key = pos;
+        {
+            const unsigned long long u = gr_rank(a[0], true);
+            if (pos == gr_warp_best(u, pos)) {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ov = __shfl_xor_sync(0xffffffffu, v, o);
-                const int ok = __shfl_xor_sync(0xffffffffu, key, o);
-                if (ov > v || (ov == v && ok < key)) { v = ov; key = ok; }
+                for (int s = 0; s < 32; ++s) prow[warp][0][s] = a[s];
+                candKey[warp][0] = pos;
+                candA[warp][0] = a[0];
+                candQ[warp][0] = zeq0(a[0]) ? make_double2(0.0, 0.0) : zrcp_nr(a[0]);
             }
-            const int p = key;
+        }
+#pragma unroll 2
+        for (int k = 0; k < Ns; ++k) {
+            __syncwarp();   // step k's pivot row, position and reciprocal
+            const int cb = k & 1, pb = cb ^ 1;
+            const int p = candKey[warp][cb];
+            const zd q = candQ[warp][cb];
+            if (lane == 0) {
+                const zd piv = candA[warp][cb];
+                pvS[warp][k] = p;
+                pivS[warp][k] = piv;
+                sing = sing || zeq0(piv);
+            }
             const bool isP = (pos == p);
-            zd *pr = prow[warp][k & 1];
-            if (isP) {
-#pragma unroll
-                for (int s = 0; s < 32; ++s) pr[s] = a[s];
-            }
-            if (lane == 0) pvS[warp][k] = p;
-            __syncwarp();
-            const zd piv = pr[0];
-            if (lane == 0) pivS[warp][k] = piv;
             if (pos == k) pos = p;
             if (isP) pos = k;
-            const bool z = zeq0(piv);
-            sing = sing || z;
-            const zd q = z ? make_double2(0.0, 0.0) : zrcp(piv);
             const zd f = isP ? make_double2(0.0, 0.0) : zmul(a[0], q);
             const zd nk = isP ? make_double2(1.0, 0.0) : zneg(f);
+            const zd *pr = prow[warp][cb];
+            {
+                const zd pv = pr[1];
+                a[0].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[1].x));
+                a[0].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[1].y));
+            }
+            // the pivot search of step k+1 on the new slot 0 (also after the
+            // last step, where nothing reads it, so the step stays one
+            // straight-line block the compiler can interleave)
+            const unsigned long long u = gr_rank(a[0], pos > k);
+            const bool win = (pos == gr_warp_best(u, pos));
+            const zd qr = zrcp_nr(a[0]);
+            const zd qn = zeq0(a[0]) ? make_double2(0.0, 0.0) : qr;
 #pragma unroll
-            for (int s = 1; s < 32; ++s) {
+            for (int s = 2; s < 32; ++s) {
                 const zd pv = pr[s];
                 a[s - 1].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[s].x));
                 a[s - 1].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[s].y));
             }
             a[31] = nk;
+            if (win) {
+#pragma unroll
+                for (int s = 0; s < 32; ++s) prow[warp][pb][s] = a[s];
+                candKey[warp][pb] = pos;
+                candA[warp][pb] = a[0];
+                candQ[warp][pb] = qn;
+            }
         }
-        // log-determinant: every lane supplied exactly one pivot
+        // log-determinant: every real row supplied exactly one pivot (the
+        // zero padding rows keep positions >= Ns and are never chosen)
+        sing = __any_sync(0xffffffffu, sing);
         __syncwarp();
-        const zd myD = pivS[warp][pos];
+        const bool real = lane < Ns;
+        const zd myD = real ? pivS[warp][pos] : make_double2(1.0, 0.0);
         double ln = 0.0;
         zd ph = make_double2(1.0, 0.0);
-        if (!sing) {
+        if (real && !sing) {
             const double ad = zabs(myD);
             ln = log(ad);
             ph = make_double2(myD.x / ad, myD.y / ad);
@@ -764,38 +832,33 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long 
         }
         if (!sing) ld = zadd(make_double2(ln, 0.0), zlog(ph));
         if (inv) {
-            // columns of the inverse: undo the interchanges as column swaps,
-            // last first; row slot j of this lane lands in column ixS^-1[j]
-            if (lane == 0) {
-                int *ix = ixS[warp], *pv = pvS[warp];
-                for (int c = 0; c < Ns; ++c) ix[c] = c;
-                for (int k = Ns - 1; k >= 0; --k) {
-                    const int q2 = pv[k];
-                    if (q2 < 0 || q2 >= Ns) continue;   // only a non-finite matrix
-                    const int t = ix[k]; ix[k] = ix[q2]; ix[q2] = t;
-                }
-                for (int c = 0; c < Ns; ++c) pv[ix[c]] = c;
-            }
+            // Row r's final position is the image of r under the interchanges
+            // applied first to last, so interchanged column j (register slot
+            // j + 32 - Ns) is column r of the inverse for the row r whose
+            // final position is j.
+            if (real) jxS[warp][pos] = lane;
             __syncwarp();
             const zd sc = sing ? make_double2(0.0, 0.0) : zrcp(myD);
-            if (pos < Ns && Sinv32) {
+            const int j0 = Ns - 32;
+            if (real && Sinv32) {
                 // fp32 planes [re | im], each Ns x Ns column-major
                 float *Xr = Sinv32 + (size_t)w * s32 + 2 * sOff, *Xi = Xr + (size_t)Ns * Ns;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int c = pvS[warp][j];
-                    if (j < Ns && c >= 0 && c < Ns) {
-                        const zd v = zmul(sc, a[j]);
+                for (int s = 0; s < 32; ++s) {
+                    const int j = j0 + s;
+                    if (j >= 0) {
+                        const int c = jxS[warp][j];
+                        const zd v = zmul(sc, a[s]);
                         Xr[pos + (size_t)Ns * c] = (float)v.x;
                         Xi[pos + (size_t)Ns * c] = (float)v.y;
                     }
                 }
-            } else if (pos < Ns) {
+            } else if (real) {
                 zd *Xg = Sinv + (size_t)w * bl.sStride + sOff;
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int c = pvS[warp][j];
-                    if (j < Ns && c >= 0 && c < Ns) Xg[pos + (size_t)Ns * c] = zmul(sc, a[j]);
+                for (int s = 0; s < 32; ++s) {
+                    const int j = j0 + s;
+                    if (j >= 0) Xg[pos + (size_t)Ns * jxS[warp][j]] = zmul(sc, a[s]);
                 }
             }
         }
@@ -841,53 +904,13 @@ struct GR64Cand {
     zd q;                   // 1 / a0, zero when a0 is zero
 };
 
-// A rank that orders candidates like the pivot search: for values >= +0 the
-// IEEE bits are monotonic; NaN ranks as infinity; ineligible rows rank 0.
-__device__ __forceinline__ unsigned long long gr64_rank(zd a0, bool eligible)
-{
-    double v = zcabs1(a0);
-    if (!(v == v)) v = INFINITY;
-    return eligible ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
-}
-
-// 1 / b without a division, so that it schedules between other arithmetic:
-// b is scaled by a power of two (exact) so that max(|re|, |im|) lies in
-// [1, 2), the real reciprocal y of d = |b|^2 in [1, 8) starts from the
-// single-precision approximation and takes two Newton-Raphson steps
-// y <- y + y (1 - d y), each of which doubles the correct bits (about 21 ->
-// 42 -> full precision), and 1/b = s conj(b s) y.  Within a few ulp of the
-// rounded quotient; a NaN or infinite b gives NaN (callers test zero first).
-__device__ __forceinline__ zd zrcp_nr(zd b)
-{
-    const double m = fmax(fabs(b.x), fabs(b.y));
-    const long long e = (__double_as_longlong(m) >> 52) & 0x7ff;
-    const double s = __longlong_as_double((2046 - e) << 52);   // 2^(1023 - e)
-    const double xs = b.x * s, ys = b.y * s;
-    const double d = fma(xs, xs, ys * ys);
-    double y = (double)__fdividef(1.0f, (float)d);
-    y = fma(y, fma(-d, y, 1.0), y);
-    y = fma(y, fma(-d, y, 1.0), y);
-    const double t = y * s;
-    return make_double2(xs * t, -ys * t);
-}
-
-// Position of the warp's best candidate: largest rank, then lowest position.
-__device__ __forceinline__ int gr64_warp_best(unsigned long long u, int pos)
-{
-    const unsigned hi = (unsigned)(u >> 32), lo = (unsigned)u;
-    const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
-    const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
-    const unsigned key = (hi == mhi && lo == mlo) ? (unsigned)pos : 0xffffffffu;
-    return (int)__reduce_min_sync(0xffffffffu, key);
-}
-
 __device__ __forceinline__ void gr64_half_bar()
 {
     asm volatile("bar.sync 1, 64;" ::: "memory");
 }
 
 template <int NB>
-__global__ void __launch_bounds__(128, 3)
+__global__ void __launch_bounds__(128, 2)
 gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
                 const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
                 double *weight, int *status, int mode, int wantInverse)
@@ -928,8 +951,8 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
             // step 0's inputs, as if a step -1 had produced them
             xS[1][r] = a[31];
             colS[0][r] = a[0];
-            const unsigned long long u = gr64_rank(a[0], true);
-            if (pos == gr64_warp_best(u, pos)) {
+            const unsigned long long u = gr_rank(a[0], true);
+            if (pos == gr_warp_best(u, pos)) {
                 GR64Cand c;
                 c.u = u; c.key = pos; c.row = r; c.a0 = a[0];
                 c.q = zeq0(a[0]) ? make_double2(0.0, 0.0) : zrcp_nr(a[0]);
@@ -966,16 +989,14 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
                     a[0].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[1].x));
                     a[0].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[1].y));
                 }
-                // the pivot search of step k+1 on the new slot 0
-                bool win = false;
-                unsigned long long u = 0;
-                zd qn = make_double2(0.0, 0.0);
-                if (k + 1 < Ns) {
-                    colS[pb][r] = a[0];
-                    u = gr64_rank(a[0], pos > k);
-                    win = (pos == gr64_warp_best(u, pos));
-                    if (!zeq0(a[0])) qn = zrcp_nr(a[0]);
-                }
+                // the pivot search of step k+1 on the new slot 0 (also after
+                // the last step, where nothing reads it, so the step stays
+                // one straight-line block the compiler can interleave)
+                colS[pb][r] = a[0];
+                const unsigned long long u = gr_rank(a[0], pos > k);
+                const bool win = (pos == gr_warp_best(u, pos));
+                const zd qr = zrcp_nr(a[0]);
+                const zd qn = zeq0(a[0]) ? make_double2(0.0, 0.0) : qr;
 #pragma unroll
                 for (int s = 2; s < 32; ++s) {
                     const zd pv = s < 31 ? pr[s] : p31;
