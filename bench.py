@@ -195,6 +195,8 @@ def phase_flops(c, m, taylor_avg):
 # dram__bytes_write.sum, summed over the phase's launches).
 NCU_TRAFFIC = {
     ("molecule128", "mixed", "taylor"): (201.41e6 + 35.22e6, "1 taylor_ts_kernel<32,128> launch"),
+    ("molecule128", "mixed", "mbuild"): (27.56e6 + 80.28e6,
+                                         "1 tc_gemm_t_kernel<1> launch (M-build; its writes partly still in L2 at the end)"),
 }
 
 
