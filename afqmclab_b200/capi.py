@@ -25,7 +25,7 @@ SYMBOLS = [
     "afqmc_set_rng", "afqmc_get_rng", "afqmc_set_ET", "afqmc_set_cadence",
     "afqmc_project_one_step", "afqmc_project_half", "afqmc_modify_gm", "afqmc_pop_control",
     "afqmc_reset_measurement", "afqmc_add_mixed_measurement", "afqmc_get_measurement",
-    "afqmc_get_cholesky_nums", "afqmc_pl_update_background", "afqmc_log_overlaps",
+    "afqmc_get_cholesky_nums", "afqmc_pl_update_background", "afqmc_pl_rebuild_propagators", "afqmc_log_overlaps",
     "afqmc_green_matrix", "afqmc_taylor_stats", "afqmc_status", "afqmc_pop_configuration_dev",
     "afqmc_profile_enable", "afqmc_profile_get", "afqmc_launch_count", "afqmc_gemm_bf16_dev",
     "afqmc_pop_configuration_noalloc_dev", "afqmc_set_graphs", "afqmc_pl_adjoint",
@@ -90,6 +90,7 @@ def _declare(L):
     L.afqmc_get_cholesky_nums.argtypes = [P, P, P]
     L.afqmc_get_site_nums.argtypes = [P, P, P, P, P]
     L.afqmc_pl_update_background.argtypes = [P, P, P, D, P, D, P, D]
+    L.afqmc_pl_rebuild_propagators.argtypes = [P, P]
     L.afqmc_log_overlaps.argtypes = [P, P]
     L.afqmc_green_matrix.argtypes = [P, I, I, P]
     L.afqmc_taylor_stats.argtypes = [P, ctypes.POINTER(ctypes.c_longlong),
@@ -293,6 +294,13 @@ class Engine:
         stay as they are (updateBackGround without a propagator rebuild)."""
         b = np.ascontiguousarray(bg, dtype=np.float64)
         _check(lib().afqmc_pl_update_background(self.h, _p(b), None, 0.0, None, 0.0, None, 0.0))
+
+    def rebuild_propagators(self, K):
+        """expMinusDtK, expHalfDtK and expMinusHalfDtK rebuilt on the GPU from
+        the engine's current background and the model's one-body K
+        (RealMaterialMolecule::returnExpMinusAlphaK)."""
+        k = np.asfortranarray(K, dtype=np.float64)
+        _check(lib().afqmc_pl_rebuild_propagators(self.h, _p(k)))
 
     def update_background(self, m):
         """m: MoleculeInputs after set_background()."""

@@ -1394,6 +1394,137 @@ int afqmc_pl_update_background(afqmc_engine *e, const double *bg, const double *
     return AFQMC_OK;
 }
 
+namespace {
+
+// RealMaterialMolecule::setKp (realMaterialMolecule.cpp:155-166): Kp = K +
+// sum_g bg_g L_g (the gemv of the reference, accumulated over g in order),
+// one thread per matrix entry.
+__global__ void kp_build_kernel(long long n2, int G, const double *K, const double *chol, const double *bg,
+                                zd *Kp)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2;
+         i += (long long)gridDim.x * blockDim.x) {
+        double s = K[i];
+        for (int g = 0; g < G; ++g) s = fma(chol[i + n2 * g], bg[g], s);
+        Kp[i] = make_double2(s, 0.0);
+    }
+}
+
+// out[0] = max_j sum_i |Kp(i, j)| (the 1-norm, for the scaling of the series),
+// out[1] = sum_g bg_g^2 in the reference's order (the propagators' logw).
+__global__ void kp_norms_kernel(int n, const zd *Kp, int G, const double *bg, double *out)
+{
+    __shared__ double red[256];
+    double m = 0.0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double c = 0.0;
+        for (int i = 0; i < n; ++i) c += fabs(Kp[i + (size_t)n * j].x);
+        m = fmax(m, c);
+    }
+    red[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double b = 0.0;
+        for (int g = 0; g < G; ++g) b += bg[g] * bg[g];
+        out[0] = red[0];
+        out[1] = b;
+    }
+}
+
+// dst = scale * src + diag * I (n x n, column-major); src may be null (zero)
+__global__ void scaled_plus_identity_kernel(int n, const zd *src, double scale, double diag, zd *dst)
+{
+    const long long n2 = (long long)n * n;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n2;
+         i += (long long)gridDim.x * blockDim.x) {
+        zd v = src ? make_double2(scale * src[i].x, scale * src[i].y) : make_double2(0.0, 0.0);
+        if (i % (n + 1) == 0) v.x += diag;
+        dst[i] = v;
+    }
+}
+
+// exp(-alpha Kp) into dst: the series of B = -alpha Kp / 2^s to order 16 by
+// Horner's rule (X <- I + B X / j), then s squarings, with s the smallest
+// power that brings ||B||_1 to 0.5 or below, where the truncated term is
+// below 1e-19 relative.  The same matrix function as the reference's
+// V exp(-alpha lambda) V^T from the eigensystem of Kp (returnExpMinusAlphaK,
+// realMaterialMolecule.cpp:117-131), computed with GEMMs instead of an
+// eigensolver.
+int expm_series(afqmc_engine *e, const zd *Kp, double alpha, double kpNorm1, zd *dst, zd *B, zd *X, zd *Y)
+{
+    const int n = e->n;
+    cudaStream_t s = e->stream;
+    int sq = 0;
+    while (std::fabs(alpha) * kpNorm1 > 0.5 * std::ldexp(1.0, sq) && sq < 60) ++sq;
+    const int blocks = (int)std::min<long long>(1024, ((long long)n * n + 255) / 256);
+    constexpr int ORDER = 16;
+    g_launch_count += 2;
+    scaled_plus_identity_kernel<<<blocks, 256, 0, s>>>(n, Kp, -alpha / std::ldexp(1.0, sq), 0.0, B);
+    scaled_plus_identity_kernel<<<blocks, 256, 0, s>>>(n, B, 1.0 / ORDER, 1.0, X);
+    TRY(check_launch());
+    for (int j = ORDER - 1; j >= 1; --j) {
+        g_launch_count++;
+        scaled_plus_identity_kernel<<<blocks, 256, 0, s>>>(n, nullptr, 0.0, 1.0, Y);
+        TRY(check_launch());
+        ZGemmArgs g;
+        g.m = n; g.n = n; g.k = n;
+        g.alpha = make_double2(1.0 / j, 0.0); g.beta = make_double2(1.0, 0.0);
+        g.A = B; g.lda = n; g.B = X; g.ldb = n; g.C = Y; g.ldc = n;
+        TRY(gemm(g, s));
+        std::swap(X, Y);
+    }
+    for (int q = 0; q < sq; ++q) {
+        ZGemmArgs g;
+        g.m = n; g.n = n; g.k = n;
+        g.A = X; g.lda = n; g.B = X; g.ldb = n; g.C = Y; g.ldc = n;
+        TRY(gemm(g, s));
+        std::swap(X, Y);
+    }
+    CUDA_TRY(cudaMemcpyAsync(dst, X, sizeof(zd) * n * n, cudaMemcpyDeviceToDevice, s));
+    return AFQMC_OK;
+}
+
+}  // namespace
+
+int afqmc_pl_rebuild_propagators(afqmc_engine *e, const double *K)
+{
+    if (!e || e->kind != KIND_PL || !K) return fail(AFQMC_ERR_ARG, "phaseless engine and K required");
+    const int n = e->n, G = e->G;
+    const size_t n2 = (size_t)n * n;
+    if (!e->kin) TRY(dalloc(e, &e->kin, n2));
+    if (!e->propScratch) TRY(dalloc(e, &e->propScratch, 4 * n2));
+    if (!e->propNorms) TRY(dalloc(e, &e->propNorms, 2));
+    if (!e->expK[0]) TRY(dalloc(e, &e->expK[0], n2));
+    drop_graphs(e);
+    cudaStream_t s = e->stream;
+    CUDA_TRY(cudaMemcpyAsync(e->kin, K, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+    zd *Kp = e->propScratch, *B = Kp + n2, *X = B + n2, *Y = X + n2;
+    g_launch_count += 2;
+    kp_build_kernel<<<(int)std::min<size_t>(1024, (n2 + 255) / 256), 256, 0, s>>>((long long)n2, G, e->kin,
+                                                                                  e->chol, e->bg, Kp);
+    kp_norms_kernel<<<1, 256, 0, s>>>(n, Kp, G, e->bg, e->propNorms);
+    TRY(check_launch());
+    double h[2] = {0.0, 0.0};
+    CUDA_TRY(cudaMemcpyAsync(h, e->propNorms, sizeof(h), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (!std::isfinite(h[0]) || !std::isfinite(h[1])) return fail(AFQMC_ERR_ARG, "non-finite K + sum_g bg_g L_g");
+    // afqmcPhaseless.cpp:151-177: expMinusDtK, expMinusHalfDtK and expHalfDtK,
+    // each with logw = alpha * 0.5 * sum bg^2
+    const double alphas[3] = {e->dt, -0.5 * e->dt, 0.5 * e->dt};   // slots 0, 1 (expHalfDtK), 2
+    for (int k = 0; k < 3; ++k) {
+        TRY(expm_series(e, Kp, alphas[k], h[0], e->expK[k], B, X, Y));
+        e->expLogw[k] = make_double2(alphas[k] * 0.5 * h[1], 0.0);
+    }
+    e->useLog = false;
+    if (e->precision == AFQMC_MIXED) TRY(mixed_update_operators(e));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return AFQMC_OK;
+}
+
 int afqmc_log_overlaps(afqmc_engine *e, double *out)
 {
     if (!e || !out) return fail(AFQMC_ERR_ARG, "null argument");

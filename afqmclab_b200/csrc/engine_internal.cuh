@@ -49,6 +49,10 @@ struct afqmc_engine {
     zd expLogw[3] = {{0, 0}, {0, 0}, {0, 0}};
     bool useLog = false;
     zd *logK = nullptr;
+    // propagator rebuild on the GPU: K (n x n), scratch Kp and three Taylor
+    // matrices (n x n each), the 1-norm of Kp and sum bg^2
+    double *kin = nullptr, *propNorms = nullptr;
+    zd *propScratch = nullptr;
     zd logKLogw{0, 0};
     // Hubbard
     HubbardDev hd{};

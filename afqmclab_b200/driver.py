@@ -172,10 +172,11 @@ def run_constraint_path_bp(eng, method, out_dir=None, on_block=None):
 def run_phaseless(eng, model, method, out_dir=None, on_block=None):
     """measureWithProjection of the phaseless driver.  `model` is the host
     RealMaterialMolecule (inputs.MoleculeInputs): the background it holds is
-    updated at each adjustment, and its propagators are rebuilt (host eigen
-    decomposition, as returnExpMinusAlphaK does) where the reference rebuilds
-    them.  An adjustable run must start the engine in the Taylor one-body
-    form; the rebuild switches it to the dense propagators."""
+    updated at each adjustment, and the engine rebuilds its propagators on
+    the GPU from that background and the model's K where the reference
+    rebuilds them (returnExpMinusAlphaK).  An adjustable run must start the
+    engine in the Taylor one-body form; the rebuild switches it to the dense
+    propagators."""
     growth = method.growth_measurements()
     adj_max = method.ETAndBackGroundAdjustMaxSize
 
@@ -186,8 +187,7 @@ def run_phaseless(eng, model, method, out_dir=None, on_block=None):
         eng.reset_measurement()
 
     def rebuild():
-        model.set_background(model.bg)
-        eng.update_background(model)
+        eng.rebuild_propagators(model.K)
 
     eng.set_cadence(0, 0)
     eng.reset_measurement()

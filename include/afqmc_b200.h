@@ -216,6 +216,17 @@ int afqmc_pl_update_background(afqmc_engine *e, const double *bg, const double *
                                double logwExpHalfDtK, const double *expMinusHalfDtK,
                                double logwExpMinusHalfDtK);
 
+/* Propagator rebuild on the GPU from the engine's current background:
+ * RealMaterialMolecule::setKp (Kp = K + sum_g bg_g L_g,
+ * realMaterialMolecule.cpp:155-166) and the three returnExpMinusAlphaK
+ * calls of afqmcPhaseless.cpp:151-177 (alpha = dt, -dt/2, dt/2 into
+ * expMinusDtK, expHalfDtK, expMinusHalfDtK; logw = alpha * 0.5 * sum bg^2,
+ * realMaterialMolecule.cpp:117-131).  K: the model's one-body K, n x n
+ * column-major.  exp(-alpha Kp) is a scaled Taylor series evaluated with
+ * FP64 GEMMs (the reference diagonalises Kp; same matrix function).  The
+ * engine leaves the Taylor one-body form, as after a dense update. */
+int afqmc_pl_rebuild_propagators(afqmc_engine *e, const double *K);
+
 /* Adjoint of the mixed local energy E = sum_w den_w E_w / sum_w den_w and of
  * the mean log-overlap at the current walkers (no one-body half step), with
  * respect to the one-body matrix t (RealMaterialMolecule::t), the Cholesky

@@ -383,6 +383,21 @@ public:
                                          dbl(expMinusHalfDtK.matrix), expMinusHalfDtK.logw.real()),
               "afqmc_pl_update_background");
     }
+    // New background only (updateBackGround); the propagators stay
+    void updateBackGround(const std::vector<double> &bg)
+    {
+        requireKind(1);
+        check(afqmc_pl_update_background(e_, bg.data(), nullptr, 0.0, nullptr, 0.0, nullptr, 0.0),
+              "afqmc_pl_update_background");
+    }
+    // expMinusDtK, expMinusHalfDtK, expHalfDtK = model.returnExpMinusAlphaK(dt, dt/2, -dt/2)
+    // (afqmcPhaseless.cpp:151-177), built on the GPU from the current
+    // background and the model's K (n x n, column-major)
+    void rebuildPropagators(const std::vector<double> &K)
+    {
+        requireKind(1);
+        check(afqmc_pl_rebuild_propagators(e_, K.data()), "afqmc_pl_rebuild_propagators");
+    }
 
     // Back-propagation of the constrained path (tutorials/afqmcConstraintPathBP):
     // prepareBackPropagation, the full-window test of the driver loop

@@ -303,6 +303,7 @@ class Engine:
         """updateBackGround: new background, one-body operators unchanged."""
         b = np.ascontiguousarray(bg, dtype=np.float64)
         lib().or_pl_update_background(self.h, _p(b), None, 0.0, None, 0.0, None, 0.0)
+        self.bg = b.copy()
 
     def update_background(self, m):
         """New background and the dense propagators rebuilt from it (m: a
@@ -311,6 +312,26 @@ class Engine:
              _z(m.expMinusHalfDtK)]
         lib().or_pl_update_background(self.h, _p(a[0]), _p(a[1]), float(m.logwDt), _p(a[2]),
                                       -float(m.logwHalf), _p(a[3]), float(m.logwHalf))
+        self.bg = a[0].copy()
+
+    def rebuild_propagators(self, K):
+        """expMinusDtK, expMinusHalfDtK, expHalfDtK = returnExpMinusAlphaK(dt,
+        dt/2, -dt/2) from the current background, by the reference's route
+        (realMaterialMolecule.cpp:117-131, 155-178): Kp = K + sum_g bg_g L_g,
+        its eigensystem, V exp(-alpha lambda) V^T, logw = alpha/2 sum bg^2."""
+        n, G = self.n, self.G
+        Kp = np.asarray(K, dtype=np.float64) + (self.chol.reshape(n * n, G, order="F") @ self.bg).reshape(
+            n, n, order="F")
+        lam, V = np.linalg.eigh(Kp)
+        bg2 = float(sum(b * b for b in self.bg))
+
+        def ex(alpha):
+            return _z((V * np.exp(-alpha * lam)) @ V.T)
+
+        a = [ex(self.dt), ex(-0.5 * self.dt), ex(0.5 * self.dt)]
+        b = np.ascontiguousarray(self.bg, dtype=np.float64)
+        lib().or_pl_update_background(self.h, _p(b), _p(a[0]), self.dt * 0.5 * bg2, _p(a[1]),
+                                      -0.5 * self.dt * 0.5 * bg2, _p(a[2]), 0.5 * self.dt * 0.5 * bg2)
 
     def log_overlaps(self):
         out = np.zeros(self.W, np.complex128)
@@ -472,4 +493,8 @@ def pl_engine(m, W, seed, mgs_step=10, pop_step=10, force_type="dynamicForce", l
                            float(np.imag(m.logwT)), seed)
     eng = Engine(h, "pl", m.n, max(m.nup, m.ndn), W, G=m.G, nup=m.nup, ndn=m.ndn)
     eng.seed = seed
+    # the model arrays the propagator rebuild reads
+    eng.chol = np.asfortranarray(m.chol, dtype=np.float64)
+    eng.bg = np.array(m.bg, dtype=np.float64)
+    eng.dt = float(m.dt)
     return eng

@@ -102,3 +102,79 @@ def test_mixed_form_follows_fp64_through_update():
     mf, mx = f.measurement(), x.measurement()
     assert abs(mf[1] / mf[0] - mx[1] / mx[0]) < 2e-3 * abs(mf[1] / mf[0])
     assert x.status() == 0
+
+
+# ---------------------------------------------------------------------------
+# The propagator rebuild on the GPU (afqmc_pl_rebuild_propagators) against
+# the eigensystem route of the reference (returnExpMinusAlphaK,
+# realMaterialMolecule.cpp:117-131, here host numpy eigh of Kp): the two
+# engines hold the same background, one receives the operators built on the
+# host, the other rebuilds them itself from K.  project_half(+1 / -1)
+# applies expHalfDtK / expMinusHalfDtK with no random numbers; steps then
+# exercise expMinusDtK and the log-weights.  dt = 0.4 makes ||dt Kp|| large
+# enough that the series is scaled and squared.
+
+def _rebuilt_pair(m, m2, W, seed, log_one_body, precision):
+    host = capi.pl_engine(m, W, seed, 1000, 1000, log_one_body=log_one_body, precision=precision)
+    dev = capi.pl_engine(m, W, seed, 1000, 1000, log_one_body=log_one_body, precision=precision)
+    host.update_background(m2)
+    dev.update_background_only(m2.bg)
+    dev.rebuild_propagators(m2.K)
+    return host, dev
+
+
+def _same_walkers(a, b, tol):
+    wa, la, aa = a.get_walkers()
+    wb, lb, ab = b.get_walkers()
+    assert (aa == ab).all()
+    assert rel_err(wb, wa) < tol
+    assert np.abs(lb - la).max() < tol * max(1.0, np.abs(la).max())
+
+
+@pytest.mark.parametrize("log_one_body,dt", [(False, 0.01), (True, 0.01), (False, 0.4)])
+def test_gpu_rebuild_matches_eigensystem_route(log_one_body, dt):
+    m = molecule()
+    m.dt = dt
+    m.set_background(m.bg)
+    m2 = molecule()
+    m2.dt = dt
+    m2.set_background(0.02 * np.cos(np.arange(m2.G)))
+    m2.ET = m.ET
+    W, seed = 10, 91
+    host, dev = _rebuilt_pair(m, m2, W, seed, log_one_body, capi.AFQMC_FP64)
+    wf, lw, al = inputs.initial_walkers(m.phiTUp, W, seed=seed + 1, noise=0.05)
+    for which in (+1, -1):
+        for e in (host, dev):
+            e.set_walkers(wf, lw, al)
+            e.project_half(which)
+        _same_walkers(host, dev, 1e-12)
+    if dt > 0.1:
+        return
+    for e in (host, dev):
+        e.set_walkers(wf, lw, al)
+        e.set_rng(seed, 0)
+        e.step(3)
+    assert host.rng_counter() == dev.rng_counter()
+    _same_walkers(host, dev, 1e-10)
+    for e in (host, dev):
+        e.reset_measurement()
+        e.add_mixed_measurement()
+    assert rel_err(dev.measurement()[:3], host.measurement()[:3]) < STEP_TOL
+
+
+def test_gpu_rebuild_mixed_form():
+    m = inputs.molecule_inputs(64, 16, 16, 128, dt=0.005, decay=30.0, seed=7)
+    m.ET = -5.0
+    m2 = inputs.molecule_inputs(64, 16, 16, 128, dt=0.005, decay=30.0, seed=7)
+    m2.set_background(0.05 * np.cos(np.arange(m2.G)))
+    m2.ET = m.ET
+    W, seed = 48, 83
+    host, dev = _rebuilt_pair(m, m2, W, seed, False, capi.AFQMC_MIXED)
+    wf, lw, al = inputs.initial_walkers(m.phiTUp, W, seed=seed + 1, noise=0.02)
+    for e in (host, dev):
+        e.set_walkers(wf, lw, al)
+        e.set_rng(seed, 0)
+        e.step(2)
+    # the same tf32/bf16 operators up to the last bits of exp(-dt Kp)
+    _same_walkers(host, dev, 1e-5)
+    assert dev.status() == 0
