@@ -1459,6 +1459,10 @@ int mixed_project_dtk_dtv(afqmc_engine *e)
 int mixed_modify_gm(afqmc_engine *e)
 {
     if (e->kind == KIND_CP) return cp_mixed_modify_gm(e);
+    // columns in registers (FP64) where the shape fits one CTA of 512 lanes
+    if (launch_mgs_col(e->W, e->n, e->ncol, e->nup, e->ndn, 1, e->mx->wf32, true, e->logw, e->alive,
+                       e->status, e->stream))
+        return engine_check_launch();
     const size_t bytes = (size_t)e->n * e->ncol * sizeof(float2);
     static std::atomic<unsigned long long> attr{0};
     if (first_on_device(attr)) {

@@ -1577,6 +1577,132 @@ mgs_kernel(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, zd *lo
 }
 
 // ---------------------------------------------------------------------------
+// The same Gram-Schmidt with each column in registers: column c belongs to
+// TPC adjacent lanes, lane k of the group holding rows k + TPC r (r < 16), so
+// a column's reductions are log2(TPC) shuffles inside the group and its
+// loads are coalesced.  Step j: the owners of column j form its norm,
+// normalise it and publish it as q_j in shared memory (alternate buffers for
+// odd and even j); one CTA barrier; every later column c takes
+// d = q_j^H a_c and a_c -= d q_j.  Columns and the log R_jj sum keep the
+// order of mgs_kernel.  One CTA of ncol * TPC threads per walker.  F32: the
+// walkers of the mixed form, fp32 planes [re n x ncol | im n x ncol]; the
+// columns stay FP64 in registers through the sweep and are rounded to fp32
+// once at the end.
+// ---------------------------------------------------------------------------
+constexpr int MGSC_RB = 16;   // rows per lane
+
+template <int TPC, bool F32>
+__global__ void __launch_bounds__(512, 1)
+mgs_col_kernel(int W, int n, int ncol, int nup, int ndn, int isSD2is, void *wfv, zd *logw, const int *alive,
+               int *status)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    zd *q = (zd *)smem_raw;                          // [2][n]
+    double *logr = (double *)(q + 2 * (size_t)n);    // [ncol]
+    __shared__ int badS;
+    const int w = blockIdx.x;
+    if (alive && !alive[w]) return;   // uniform over the CTA
+    const int tid = threadIdx.x, c = tid / TPC, k = tid % TPC;
+    const bool col = c < ncol;
+    // the shuffles run inside branches taken by whole lane groups only
+    const unsigned gmask = (TPC == 32 ? 0xffffffffu : ((1u << TPC) - 1u)) << ((tid & 31) & ~(TPC - 1));
+    const size_t ws = (size_t)n * ncol;
+    zd *g = F32 ? nullptr : (zd *)wfv + (size_t)w * ws;
+    float *g32 = F32 ? (float *)wfv + (size_t)w * 2 * ws : nullptr;
+    zd a[MGSC_RB];
+#pragma unroll
+    for (int r = 0; r < MGSC_RB; ++r) {
+        const int i = k + TPC * r;
+        const size_t e = i + (size_t)n * c;
+        if (!(col && i < n)) a[r] = make_double2(0.0, 0.0);
+        else if (F32) a[r] = make_double2(g32[e], g32[ws + e]);
+        else a[r] = g[e];
+    }
+    if (tid == 0) badS = 0;
+    for (int j = 0; j < ncol; ++j) {
+        zd *qj = q + (size_t)(j & 1) * n;
+        if (c == j) {
+            double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+            for (int r = 0; r < MGSC_RB; r += 2) {
+                s0 = fma(a[r].x, a[r].x, fma(a[r].y, a[r].y, s0));
+                s1 = fma(a[r + 1].x, a[r + 1].x, fma(a[r + 1].y, a[r + 1].y, s1));
+            }
+            double s = s0 + s1;
+#pragma unroll
+            for (int o = 1; o < TPC; o <<= 1) s += __shfl_xor_sync(gmask, s, o, TPC);
+            const double rj = sqrt(s);
+            const double inv = rj > 0.0 ? 1.0 / rj : 0.0;
+#pragma unroll
+            for (int r = 0; r < MGSC_RB; ++r) {
+                a[r] = zscale(a[r], inv);
+                const int i = k + TPC * r;
+                if (i < n) qj[i] = a[r];
+            }
+            if (k == 0) {
+                logr[j] = log(rj);
+                if (rj == 0.0) badS = 1;
+            }
+        }
+        __syncthreads();   // q_j published
+        if (col && c > j) {
+            zd d0 = make_double2(0.0, 0.0), d1 = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int r = 0; r < MGSC_RB; r += 2) {
+                const int i0 = k + TPC * r, i1 = i0 + TPC;
+                if (i0 < n) zfma(d0, zconj(qj[i0]), a[r]);
+                if (i1 < n) zfma(d1, zconj(qj[i1]), a[r + 1]);
+            }
+            zd d = zadd(d0, d1);
+#pragma unroll
+            for (int o = 1; o < TPC; o <<= 1) {
+                d.x += __shfl_xor_sync(gmask, d.x, o, TPC);
+                d.y += __shfl_xor_sync(gmask, d.y, o, TPC);
+            }
+#pragma unroll
+            for (int r = 0; r < MGSC_RB; ++r) {
+                const int i = k + TPC * r;
+                if (i < n) {
+                    const zd qv = qj[i];
+                    a[r].x -= d.x * qv.x - d.y * qv.y;
+                    a[r].y -= d.x * qv.y + d.y * qv.x;
+                }
+            }
+        }
+    }
+    if (col) {
+#pragma unroll
+        for (int r = 0; r < MGSC_RB; ++r) {
+            const int i = k + TPC * r;
+            const size_t e = i + (size_t)n * c;
+            if (i < n) {
+                if (F32) {
+                    g32[e] = (float)a[r].x;
+                    g32[ws + e] = (float)a[r].y;
+                } else {
+                    g[e] = a[r];
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const int nmin = nup < ndn ? nup : ndn;
+        double logR = 0.0, logRmin = 0.0;
+        for (int jj = 0; jj < ncol; ++jj) {
+            logR += logr[jj];
+            if (jj < nmin) logRmin += logr[jj];
+        }
+        zd lw = logw[w];
+        if (!isSD2is) lw.x += logR;
+        else if (nup == ndn) lw.x += 2.0 * logR;
+        else lw.x += logR + logRmin;
+        logw[w] = lw;
+        if (badS && status) atomicOr(status + w, (int)ST_ZERO_NORM);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // popConfiguration (populationControlConfiguration.cpp:24-101) for one
 // process: W uniforms from the stream, the comb over the normalised weights
 // accumulated in the reference's serial order (bit-exact tables), then the
@@ -2247,10 +2373,37 @@ void launch_taylor_accum(int W, long long wsize, const zd *term, zd *wfNew, cons
                                            acc, isLast, status);
 }
 
+// Gram-Schmidt with the columns in registers (mgs_col_kernel) where
+// ncol * TPC lanes fit one CTA of 512; false where the shape does not fit.
+bool launch_mgs_col(int W, int n, int ncol, int nup, int ndn, int isSD2is, void *wf, bool f32, zd *logw,
+                    const int *alive, int *status, cudaStream_t s)
+{
+    int tpc = 1;
+    while (tpc * MGSC_RB < n && tpc < 32) tpc <<= 1;
+    if (!(tpc * MGSC_RB >= n && tpc <= 16 && ncol * tpc <= 512 && ncol > 0)) return false;
+    const int threads = (ncol * tpc + 31) / 32 * 32;
+    const size_t smem = (size_t)2 * n * sizeof(zd) + (size_t)ncol * sizeof(double);
+#define MGSC_LAUNCH(T)                                                                                     \
+    (f32 ? mgs_col_kernel<T, true><<<W, threads, smem, s>>>(W, n, ncol, nup, ndn, isSD2is, wf, logw, alive, \
+                                                             status)                                        \
+         : mgs_col_kernel<T, false><<<W, threads, smem, s>>>(W, n, ncol, nup, ndn, isSD2is, wf, logw, alive, \
+                                                              status))
+    switch (tpc) {
+    case 1: MGSC_LAUNCH(1); break;
+    case 2: MGSC_LAUNCH(2); break;
+    case 4: MGSC_LAUNCH(4); break;
+    case 8: MGSC_LAUNCH(8); break;
+    default: MGSC_LAUNCH(16); break;
+    }
+#undef MGSC_LAUNCH
+    return true;
+}
+
 void launch_mgs(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, zd *logw,
                 const int *alive, int *status, cudaStream_t s)
 {
     g_launch_count++;
+    if (launch_mgs_col(W, n, ncol, nup, ndn, isSD2is, wf, false, logw, alive, status, s)) return;
     size_t bytes = (size_t)n * ncol * sizeof(zd);
     if (bytes <= 160 * 1024) {
         static std::atomic<unsigned long long> attr{0};

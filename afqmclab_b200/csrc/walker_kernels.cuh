@@ -74,6 +74,11 @@ void launch_taylor_accum(int W, long long wsize, const zd *term, zd *wfNew, cons
                          int *status, cudaStream_t s);
 
 // Modified Gram-Schmidt stabilisation (replaces SD::stabilize / SD2is::stabilize)
+// Gram-Schmidt with the columns in registers; wf is zd (f32 false) or the
+// mixed form's fp32 planes (f32 true).  Returns false (nothing launched)
+// where the shape does not fit one CTA of 512 lanes.
+bool launch_mgs_col(int W, int n, int ncol, int nup, int ndn, int isSD2is, void *wf, bool f32, zd *logw,
+                    const int *alive, int *status, cudaStream_t s);
 void launch_mgs(int W, int n, int ncol, int nup, int ndn, int isSD2is, zd *wf, zd *logw,
                 const int *alive, int *status, cudaStream_t s);
 
