@@ -80,7 +80,7 @@ struct CpTcArgs {
 //   warp 0 lane 0 : TMA producer      warp 1 : TMEM owner, lane 0 issues the UMMAs
 //   warps 2..5    : epilogue (TMEM lane quarter = warp % 4)
 template <int MODE>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(192, 2)
 cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
               const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1, CpTcArgs p)
 {
@@ -171,32 +171,39 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
         const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
         const int row = m0 + q * 32 + lane;
         if (ok && MODE == CPM_ONEBODY) {
-            const long long n = p.n;
+            // 32 columns per chunk: the residual loads of a chunk are all in
+            // flight before the accumulator is read; row-based pointers with
+            // 32-bit column offsets keep the registers for two CTAs per SM
+            const int n = p.n;
+            const long long col0 = (long long)tile * BN;
+            const int ncols = (int)(p.cols - col0 < BN ? p.cols - col0 : BN);
+            const size_t rbase = (size_t)row + (size_t)n * col0;
+            const float *rh = p.rhi + rbase, *rl = p.rlo + rbase;
+            float *oh = p.ohi + rbase;
+            float *ol = p.olo ? p.olo + rbase : nullptr;
+            const bool rowOK = row < n;
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 16) {
-                // residuals first (independent loads in flight), then the accumulator
-                float res[16];
+            for (int c0 = 0; c0 < BN; c0 += 32) {
+                float res[32];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const long long col = (long long)tile * BN + c0 + j;
-                    const size_t idx = (size_t)row + (size_t)n * col;
-                    res[j] = (row < p.n && col < p.cols) ? p.rhi[idx] + p.rlo[idx] : 0.f;
+                for (int j = 0; j < 32; ++j) {
+                    const int c = c0 + j;
+                    res[j] = (rowOK && c < ncols) ? rh[n * c] + rl[n * c] : 0.f;
                 }
-                float v[16];
-                tmem_ld16(trow + c0, v);
-                if (row < p.n) {
+                float v[32];
+                tmem_ld32(trow + c0, v);
+                if (rowOK) {
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const long long col = (long long)tile * BN + c0 + j;
-                        if (col < p.cols) {
-                            const size_t idx = (size_t)row + (size_t)n * col;
+                    for (int j = 0; j < 32; ++j) {
+                        const int c = c0 + j;
+                        if (c < ncols) {
                             const float x = v[j] + res[j];
-                            if (p.olo) {
+                            if (ol) {
                                 const float h = tf32_round(x);
-                                p.ohi[idx] = h;
-                                p.olo[idx] = x - h;
+                                oh[n * c] = h;
+                                ol[n * c] = x - h;
                             } else {
-                                p.ohi[idx] = x;
+                                oh[n * c] = x;
                             }
                         }
                     }
@@ -230,26 +237,38 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
             int cur = 0;
 #pragma unroll 1
             for (int c0 = 0; c0 < ncols; c0 += 32) {
+                // this chunk's walker entries first, all loads in flight
+                // before the accumulator is read (and ahead of the stores)
+                float fr[16], fi[16];
+#pragma unroll
+                for (int t = 0; t < 16; ++t) {
+                    const int col = c0 + 2 * t;
+                    const int j = col / two, a = (col - j * two) >> 1;
+                    const int w = tile * p.wpt + j;
+                    if (col < ncols && row < n && w < p.W) {
+                        const float *ph = p.phi + (size_t)w * 2 * n * N + prow + (size_t)n * a;
+                        fr[t] = ph[0];
+                        fi[t] = ph[(size_t)n * N];
+                    } else {
+                        fr[t] = 0.f;
+                        fi[t] = 0.f;
+                    }
+                }
                 float v[32];
                 tmem_ld32(trow + c0, v);
 #pragma unroll
                 for (int t = 0; t < 16; ++t) {
                     const int col = c0 + 2 * t;
                     if (col < ncols) {
-                        const int j = col / two, a = (col - j * two) >> 1;
+                        const int j = col / two;
                         if (j != cur) {
                             const int w = tile * p.wpt + cur;
                             if (row < n && w < p.W) p.gd[(size_t)w * n + row] = make_float2(gr, gi);
                             gr = gi = 0.f;
                             cur = j;
                         }
-                        const int w = tile * p.wpt + j;
-                        if (row < n && w < p.W) {
-                            const float *ph = p.phi + (size_t)w * 2 * n * N + prow + (size_t)n * a;
-                            const float fr = ph[0], fi = ph[(size_t)n * N];
-                            gr += fr * v[2 * t] - fi * v[2 * t + 1];
-                            gi += fr * v[2 * t + 1] + fi * v[2 * t];
-                        }
+                        gr += fr[t] * v[2 * t] - fi[t] * v[2 * t + 1];
+                        gi += fr[t] * v[2 * t + 1] + fi[t] * v[2 * t];
                     }
                 }
             }
