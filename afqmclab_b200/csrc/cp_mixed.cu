@@ -58,6 +58,9 @@ constexpr int STAGES = 2;   // two CTAs per SM: one epilogue overlaps the other'
 constexpr int A_BYTES = BM * BK * 4;
 constexpr int B_BYTES = BN * BK * 4;
 constexpr size_t SMEM = 1024 + (size_t)STAGES * (A_BYTES + B_BYTES) + 256;
+constexpr int RES_BUFS = 3;
+constexpr int RES_BYTES = 2 * BM * 32 * 4;   // hi and lo of 32 columns
+static_assert(RES_BUFS * RES_BYTES <= STAGES * (A_BYTES + B_BYTES), "residual buffers exceed the stages");
 
 enum { CPM_ONEBODY = 0, CPM_OVERLAP = 1, CPM_GDIAG = 2 };
 
@@ -82,7 +85,8 @@ struct CpTcArgs {
 template <int MODE>
 __global__ void __launch_bounds__(192, 2)
 cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ CUtensorMap tA1,
-              const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1, CpTcArgs p)
+              const __grid_constant__ CUtensorMap tB0, const __grid_constant__ CUtensorMap tB1,
+              const __grid_constant__ CUtensorMap tR0, const __grid_constant__ CUtensorMap tR1, CpTcArgs p)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *base = (uint8_t *)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -91,7 +95,10 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
     uint64_t *full = (uint64_t *)(sB + STAGES * B_BYTES);
     uint64_t *empty = full + STAGES;
     uint64_t *tmemFull = empty + STAGES;
-    uint32_t *tmemSlot = (uint32_t *)(tmemFull + 1);
+    // one-body: the residual columns in three 32 KB buffers over the freed stages
+    uint64_t *resFull = tmemFull + 1;
+    uint64_t *resEmpty = resFull + RES_BUFS;
+    uint32_t *tmemSlot = (uint32_t *)(resEmpty + RES_BUFS);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * BM;
@@ -105,6 +112,7 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
         mbar_init(tmemFull, 1);
+        for (int b = 0; b < RES_BUFS; ++b) { mbar_init(&resFull[b], 1); mbar_init(&resEmpty[b], 4); }
         fence_mbar_init();
         tma_prefetch_desc(&tA0);
         tma_prefetch_desc(&tB0);
@@ -145,6 +153,24 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
                 const int s = kt % STAGES;
                 ok = mbar_wait(&empty[s], ((kt / STAGES) - 1) & 1);
             }
+            if (MODE == CPM_ONEBODY) {
+                // the MMAs have read the stages: the residual phi = hi + lo of
+                // the tile's columns, 32 at a time, by TMA into the freed space
+                int issued = 0;
+                for (int ch = 0; ch < BN / 32 && ok; ++ch) {
+                    const int b = ch % RES_BUFS;
+                    if (ch >= RES_BUFS) ok = mbar_wait(&resEmpty[b], ((ch / RES_BUFS) - 1) & 1);
+                    if (!ok) break;
+                    uint8_t *buf = base + b * RES_BYTES;
+                    mbar_arrive_expect_tx(&resFull[b], RES_BYTES);
+                    tma_load_2d(buf, &tR0, &resFull[b], m0, tile * BN + ch * 32);
+                    tma_load_2d(buf + RES_BYTES / 2, &tR1, &resFull[b], m0, tile * BN + ch * 32);
+                    ++issued;
+                }
+                // the copies land before this CTA can leave
+                for (int ch = issued - RES_BUFS < 0 ? 0 : issued - RES_BUFS; ch < issued; ++ch)
+                    (void)mbar_wait(&resFull[ch % RES_BUFS], (ch / RES_BUFS) & 1);
+            }
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -171,33 +197,31 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
         const uint32_t trow = tmem + ((uint32_t)(q * 32) << 16);
         const int row = m0 + q * 32 + lane;
         if (ok && MODE == CPM_ONEBODY) {
-            // 32 columns per chunk: the residual loads of a chunk are all in
-            // flight before the accumulator is read; row-based pointers with
-            // 32-bit column offsets keep the registers for two CTAs per SM
+            // phi' = (E - I) phi + phi: the residual phi = hi + lo comes by
+            // TMA, 32 columns per buffer, smem [column][row]
             const int n = p.n;
             const long long col0 = (long long)tile * BN;
             const int ncols = (int)(p.cols - col0 < BN ? p.cols - col0 : BN);
             const size_t rbase = (size_t)row + (size_t)n * col0;
-            const float *rh = p.rhi + rbase, *rl = p.rlo + rbase;
             float *oh = p.ohi + rbase;
             float *ol = p.olo ? p.olo + rbase : nullptr;
             const bool rowOK = row < n;
+            const int rl = q * 32 + lane;
 #pragma unroll 1
-            for (int c0 = 0; c0 < BN; c0 += 32) {
-                float res[32];
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int c = c0 + j;
-                    res[j] = (rowOK && c < ncols) ? rh[n * c] + rl[n * c] : 0.f;
-                }
+            for (int ch = 0; ch < BN / 32; ++ch) {
+                const int b = ch % RES_BUFS;
+                ok = __all_sync(0xffffffffu, mbar_wait(&resFull[b], (ch / RES_BUFS) & 1)) != 0;
+                if (!ok) break;
                 float v[32];
-                tmem_ld32(trow + c0, v);
+                tmem_ld32(trow + ch * 32, v);
+                const float *hb = (const float *)(base + b * RES_BYTES), *lb = hb + BM * 32;
                 if (rowOK) {
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
-                        const int c = c0 + j;
+                        const int c = ch * 32 + j;
                         if (c < ncols) {
-                            const float x = v[j] + res[j];
+                            const float res = hb[j * BM + rl] + lb[j * BM + rl];
+                            const float x = v[j] + res;
                             if (ol) {
                                 const float h = tf32_round(x);
                                 oh[n * c] = h;
@@ -208,6 +232,8 @@ cpm_tc_kernel(const __grid_constant__ CUtensorMap tA0, const __grid_constant__ C
                         }
                     }
                 }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&resEmpty[b]);
             }
         } else if (ok && MODE == CPM_OVERLAP) {
             const int N = p.N;
@@ -300,7 +326,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder()
 
 // fp32 tensor map, 128-byte swizzle, box of 32 elements along dim 0.
 int make_map_f32(CUtensorMap *map, const float *base, int rank, const long long *dims,
-                 const long long *pitchBytes, const int *box)
+                 const long long *pitchBytes, const int *box, bool swizzle128 = true)
 {
     auto enc = encoder();
     if (!enc) return (int)cudaErrorNotSupported;
@@ -314,29 +340,40 @@ int make_map_f32(CUtensorMap *map, const float *base, int rank, const long long 
         st[i] = (cuuint64_t)pitchBytes[i];
     }
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, rank, const_cast<float *>(base), d, st, bx, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? 0 : (int)r + 10000;
 }
 
+// the one-body's residual walker columns: box of BM rows x 32 columns, no
+// swizzle (smem [column][row])
+int make_res_map(CUtensorMap *map, const float *base, int n, long long cols)
+{
+    long long d[2] = {n, cols}, pch[1] = {(long long)n * 4};
+    int box[2] = {BM, 32};
+    return make_map_f32(map, base, 2, d, pch, box, false);
+}
+
 template <int MODE>
 int launch_tc_stream(cudaStream_t s, dim3 grid, const CUtensorMap &a0, const CUtensorMap &a1,
-                     const CUtensorMap &b0, const CUtensorMap &b1, const CpTcArgs &args)
+                     const CUtensorMap &b0, const CUtensorMap &b1, const CUtensorMap &r0, const CUtensorMap &r1,
+                     const CpTcArgs &args)
 {
     static std::atomic<unsigned long long> attr{0};
     if (first_on_device(attr)) {
         cudaFuncSetAttribute(cpm_tc_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
     }
     g_launch_count++;
-    cpm_tc_kernel<MODE><<<grid, 192, SMEM, s>>>(a0, a1, b0, b1, args);
+    cpm_tc_kernel<MODE><<<grid, 192, SMEM, s>>>(a0, a1, b0, b1, r0, r1, args);
     return (int)cudaGetLastError();
 }
 
 template <int MODE>
 int launch_tc(afqmc_engine *e, dim3 grid, const CUtensorMap &a0, const CUtensorMap &a1, const CUtensorMap &b0,
-              const CUtensorMap &b1, const CpTcArgs &args)
+              const CUtensorMap &b1, const CUtensorMap &r0, const CUtensorMap &r1, const CpTcArgs &args)
 {
-    launch_tc_stream<MODE>(e->stream, grid, a0, a1, b0, b1, args);
+    launch_tc_stream<MODE>(e->stream, grid, a0, a1, b0, b1, r0, r1, args);
     return engine_check_launch();
 }
 
@@ -370,7 +407,7 @@ int overlap_tc(afqmc_engine *e, const float *hi, const float *lo)
     a.idesc = idesc_tf32(BM, m->wptO * m->bnw);
     a.S = (double *)e->S; a.sStride = e->bl.sStride;
     dim3 grid((2 * N + BM - 1) / BM, (W + m->wptO - 1) / m->wptO);
-    return launch_tc<CPM_OVERLAP>(e, grid, a0, a1, b0, b1, a);
+    return launch_tc<CPM_OVERLAP>(e, grid, a0, a1, b0, b1, a0, a1, a);
 }
 
 // Green's function entries for the force: gd[w][q] = G(partner(q), q)
@@ -391,7 +428,7 @@ int gdiag_tc(afqmc_engine *e)
     a.idesc = idesc_tf32(BM, (m->wptG * 2 * N + 15) / 16 * 16);
     a.phi = m->hi; a.gd = m->gd;
     dim3 grid((n + BM - 1) / BM, (W + m->wptG - 1) / m->wptG);
-    return launch_tc<CPM_GDIAG>(e, grid, a0, a0, b0, b0, a);
+    return launch_tc<CPM_GDIAG>(e, grid, a0, a0, b0, b0, a0, a0, a);
 }
 
 // phi <- phi + (exp(-dtK) - I) phi from (thi, tlo) into (hi, lo)
@@ -409,13 +446,16 @@ int onebody_tc(afqmc_engine *e)
     int boxB[2] = {BK, BN};
     CTRY(make_map_f32(&b0, m->thi, 2, db, pb, boxB));
     CTRY(make_map_f32(&b1, m->tlo, 2, db, pb, boxB));
+    CUtensorMap r0, r1;
+    CTRY(make_res_map(&r0, m->thi, n, cols));
+    CTRY(make_res_map(&r1, m->tlo, n, cols));
     CpTcArgs a = base_args(e);
     a.kbA = (n + BK - 1) / BK; a.nseg = 3;
     a.cols = cols;
     a.idesc = idesc_tf32(BM, BN);
     a.rhi = m->thi; a.rlo = m->tlo; a.ohi = m->hi; a.olo = m->lo;
     dim3 grid((n + BM - 1) / BM, (unsigned)((cols + BN - 1) / BN));
-    return launch_tc<CPM_ONEBODY>(e, grid, a0, a1, b0, b1, a);
+    return launch_tc<CPM_ONEBODY>(e, grid, a0, a1, b0, b1, r0, r1, a);
 }
 
 // Bg rows of walker w: row 2a = [Re Sinv(a, :) | Im Sinv(a, :)],
@@ -652,6 +692,9 @@ int onebody_tf32_launch(cudaStream_t s, int n, int ncol, int W, const float *Ehi
     int boxB[2] = {BK, BN};
     if (!r) r = make_map_f32(&b0, rhi, 2, db, pb, boxB);
     if (!r) r = make_map_f32(&b1, rlo, 2, db, pb, boxB);
+    CUtensorMap r0, r1;
+    if (!r) r = make_res_map(&r0, rhi, n, cols);
+    if (!r) r = make_res_map(&r1, rlo, n, cols);
     if (r) return r;
     CpTcArgs a{};
     a.n = n; a.N = ncol; a.W = W;
@@ -661,7 +704,7 @@ int onebody_tf32_launch(cudaStream_t s, int n, int ncol, int W, const float *Ehi
     a.rhi = rhi; a.rlo = rlo; a.ohi = ohi; a.olo = olo;
     a.err = err;
     dim3 grid((n + BM - 1) / BM, (unsigned)((cols + BN - 1) / BN));
-    return launch_tc_stream<CPM_ONEBODY>(s, grid, a0, a1, b0, b1, a);
+    return launch_tc_stream<CPM_ONEBODY>(s, grid, a0, a1, b0, b1, r0, r1, a);
 }
 
 bool cp_mixed_supported(int L, int N, std::string *why)
