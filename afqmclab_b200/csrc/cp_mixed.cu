@@ -12,8 +12,10 @@
 //             G(p, q) = sum_a phi(p, a) D(q, a) with D = conj(phiT) S^{-T},
 //             one tf32 product (the force only steers importance sampling).
 // The aux-field sampling, the weight/phase bookkeeping, the modified
-// Gram-Schmidt re-orthonormalisation (on an FP64 copy), population control
-// and the measurement (on an FP64 copy) stay in FP64.
+// Gram-Schmidt re-orthonormalisation (on an FP64 copy) and population
+// control stay in FP64.  The measurement takes its half step exp(+dtK/2) and
+// the overlap on the tensor cores (as the propagation) and the LU, Green's
+// function and energy in FP64 on a copy of the half-stepped walkers.
 //
 // Reference step being replaced: afqmcConstraintPathProjection.cpp:40-86
 // (projectExpMinusDtKExpMinusDtV) with HubbardSOCSDOperation /
@@ -38,6 +40,7 @@ struct CpMixedState {
     float *hi = nullptr, *lo = nullptr;     // walkers
     float *thi = nullptr, *tlo = nullptr;   // after the two-body sample
     float *Ehi = nullptr, *Elo = nullptr;   // exp(-dtK) - I, n x n row-major
+    float *Hhi = nullptr, *Hlo = nullptr;   // exp(+dtK/2) - I (the measurement's half step), when real
     float *Ohi = nullptr, *Olo = nullptr;   // overlap operator, 2N x 2n row-major
     float *Ag = nullptr;                    // [Re phiT | Im phiT], n x K2 row-major
     float *Bg = nullptr;                    // per walker 2N x K2: S^{-1} rows, re/im interleaved
@@ -431,31 +434,38 @@ int gdiag_tc(afqmc_engine *e)
     return launch_tc<CPM_GDIAG>(e, grid, a0, a0, b0, b0, a0, a0, a);
 }
 
-// phi <- phi + (exp(-dtK) - I) phi from (thi, tlo) into (hi, lo)
-int onebody_tc(afqmc_engine *e)
+// out <- in + (O - I) in for a one-body operator given as O - I (hi, lo)
+int onebody_tc_op(afqmc_engine *e, const float *Ohi, const float *Olo, const float *inHi, const float *inLo,
+                  float *outHi, float *outLo)
 {
-    CpMixedState *m = e->cpm;
     const int n = e->n, N = e->ncol, W = e->W;
     CUtensorMap a0, a1, b0, b1;
     long long da[2] = {n, n}, pa[1] = {(long long)n * 4};
     int boxA[2] = {BK, BM};
-    CTRY(make_map_f32(&a0, m->Ehi, 2, da, pa, boxA));
-    CTRY(make_map_f32(&a1, m->Elo, 2, da, pa, boxA));
+    CTRY(make_map_f32(&a0, Ohi, 2, da, pa, boxA));
+    CTRY(make_map_f32(&a1, Olo, 2, da, pa, boxA));
     const long long cols = 2LL * N * W;
     long long db[2] = {n, cols}, pb[1] = {(long long)n * 4};
     int boxB[2] = {BK, BN};
-    CTRY(make_map_f32(&b0, m->thi, 2, db, pb, boxB));
-    CTRY(make_map_f32(&b1, m->tlo, 2, db, pb, boxB));
+    CTRY(make_map_f32(&b0, inHi, 2, db, pb, boxB));
+    CTRY(make_map_f32(&b1, inLo, 2, db, pb, boxB));
     CUtensorMap r0, r1;
-    CTRY(make_res_map(&r0, m->thi, n, cols));
-    CTRY(make_res_map(&r1, m->tlo, n, cols));
+    CTRY(make_res_map(&r0, inHi, n, cols));
+    CTRY(make_res_map(&r1, inLo, n, cols));
     CpTcArgs a = base_args(e);
     a.kbA = (n + BK - 1) / BK; a.nseg = 3;
     a.cols = cols;
     a.idesc = idesc_tf32(BM, BN);
-    a.rhi = m->thi; a.rlo = m->tlo; a.ohi = m->hi; a.olo = m->lo;
+    a.rhi = inHi; a.rlo = inLo; a.ohi = outHi; a.olo = outLo;
     dim3 grid((n + BM - 1) / BM, (unsigned)((cols + BN - 1) / BN));
     return launch_tc<CPM_ONEBODY>(e, grid, a0, a1, b0, b1, r0, r1, a);
+}
+
+// phi <- phi + (exp(-dtK) - I) phi from (thi, tlo) into (hi, lo)
+int onebody_tc(afqmc_engine *e)
+{
+    CpMixedState *m = e->cpm;
+    return onebody_tc_op(e, m->Ehi, m->Elo, m->thi, m->tlo, m->hi, m->lo);
 }
 
 // Bg rows of walker w: row 2a = [Re Sinv(a, :) | Im Sinv(a, :)],
@@ -720,8 +730,9 @@ int cp_mixed_create(afqmc_engine *e)
     std::string why;
     if (!cp_mixed_supported(e->L, e->ncol, &why)) return engine_fail(AFQMC_ERR_UNSUPPORTED, why);
     const int n = e->n, N = e->ncol, W = e->W;
-    std::vector<zd> E((size_t)n * n), T((size_t)n * N);
+    std::vector<zd> E((size_t)n * n), T((size_t)n * N), H((size_t)n * n);
     if (cudaMemcpy(E.data(), e->expK[0], sizeof(zd) * E.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(H.data(), e->expK[1], sizeof(zd) * H.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
         cudaMemcpy(T.data(), e->phiT[0], sizeof(zd) * T.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
         return engine_fail(AFQMC_ERR_CUDA, "reading operators for the mixed form");
     for (const zd &v : E)
@@ -769,6 +780,20 @@ int cp_mixed_create(afqmc_engine *e)
             ag[(size_t)q * m->K2 + b] = tf32_host((float)t.x);
             ag[(size_t)q * m->K2 + N + b] = tf32_host((float)t.y);
         }
+    // the measurement's half step exp(+dtK/2) - I on the tensor cores when it is real
+    bool hReal = true;
+    for (const zd &v : H) hReal = hReal && v.y == 0.0;
+    if (hReal) {
+        std::vector<float> hh((size_t)n * n), hl((size_t)n * n);
+        for (int i = 0; i < n; ++i)
+            for (int k = 0; k < n; ++k)
+                split_host(H[i + (size_t)n * k].x - (i == k ? 1.0 : 0.0), hh[(size_t)i * n + k], hl[(size_t)i * n + k]);
+        CM(engine_dalloc(e, &m->Hhi, (size_t)n * n));
+        CM(engine_dalloc(e, &m->Hlo, (size_t)n * n));
+        if (cudaMemcpy(m->Hhi, hh.data(), 4 * hh.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(m->Hlo, hl.data(), 4 * hl.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            return engine_fail(AFQMC_ERR_CUDA, "uploading the mixed-form half-step operator");
+    }
     if (cudaMemcpy(m->Ehi, eh.data(), 4 * eh.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(m->Elo, el.data(), 4 * el.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(m->Ohi, oh.data(), 4 * oh.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -799,6 +824,25 @@ int cp_mixed_sync_from_fp64(afqmc_engine *e)
     g_launch_count++;
     split_kernel<<<e->W, 256, 0, e->stream>>>(e->W, e->n, e->ncol, e->wf, e->cpm->hi, e->cpm->lo);
     return engine_check_launch();
+}
+
+// The measurement's half step and overlap on the tensor cores: (thi, tlo) <-
+// the walkers after exp(+dtK/2) (compensated tf32, as the propagation),
+// S = phiT^H of them (FP64 result in e->S), and their FP64 copy in e->wfTmp
+// for the Green's function.  *done is false (nothing launched) where the
+// half-step operator is not real; the FP64 measurement runs then.
+int cp_mixed_measure_prep(afqmc_engine *e, bool *done)
+{
+    CpMixedState *m = e->cpm;
+    *done = false;
+    if (!m->Hhi) return AFQMC_OK;
+    CM(onebody_tc_op(e, m->Hhi, m->Hlo, m->hi, m->lo, m->thi, m->tlo));
+    CM(overlap_tc(e, m->thi, m->tlo));
+    g_launch_count++;
+    combine_kernel<<<e->W, 256, 0, e->stream>>>(e->W, e->n, e->ncol, m->thi, m->tlo, e->wfTmp);
+    CM(engine_check_launch());
+    *done = true;
+    return AFQMC_OK;
 }
 
 int cp_mixed_status(afqmc_engine *e)

@@ -1,6 +1,8 @@
 // Mixed-precision form of the constrained-path (Hubbard) walker step:
-// tcgen05 kind::tf32 contractions with compensated (hi + lo) operands,
-// FP64 LU/log-determinant, weights, re-orthonormalisation and measurement.
+// tcgen05 kind::tf32 contractions with compensated (hi + lo) operands
+// (propagation, and the measurement's half step and overlap), FP64
+// LU/log-determinant, weights, re-orthonormalisation and the rest of the
+// measurement.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -22,6 +24,10 @@ int cp_mixed_pop_weights(afqmc_engine *e);
 int cp_mixed_sync_to_fp64(afqmc_engine *e);
 int cp_mixed_sync_from_fp64(afqmc_engine *e);
 int cp_mixed_status(afqmc_engine *e);
+// the measurement's half step and overlap on the tensor cores (S in e->S,
+// the FP64 walkers after the half step in e->wfTmp); *done false when the
+// half-step operator is not real (the FP64 measurement runs then)
+int cp_mixed_measure_prep(afqmc_engine *e, bool *done);
 
 // Shared tf32 tensor-core pieces (also used by the phaseless mixed form):
 // (E - I) of a real n x n operator E (host, column-major) as tf32 high/low

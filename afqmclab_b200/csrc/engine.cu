@@ -20,6 +20,7 @@
 
 #include "../../include/afqmc_b200.h"
 #include "common.cuh"
+#include "cp_mixed.cuh"
 #include "engine_internal.cuh"
 #include "exchange_f64.cuh"
 #include "mixed.cuh"
@@ -535,14 +536,20 @@ int add_mixed_measurement(afqmc_engine *e)
 int add_mixed_measurement_direct(afqmc_engine *e)
 {
     if (e->precision == AFQMC_MIXED && e->kind == KIND_PL) return mixed_add_measurement(e);
-    // constrained-path mixed form: the measurement runs on an FP64 copy
-    if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
     const int W = e->W;
     cudaStream_t s = e->stream;
     {
         PHASE(AFQMC_PH_MEASURE);
-        TRY(one_body(e, 1, e->wf, e->wfTmp, e->alive));
-        TRY(overlap_gemm(e, e->wfTmp, e->alive, fbl(e)));
+        // constrained-path mixed form: the half step and the overlap on the
+        // tensor cores, the rest on an FP64 copy of the half-stepped walkers;
+        // the FP64 form (or a complex half-step operator) runs both in FP64
+        bool tcPrep = false;
+        if (e->precision == AFQMC_MIXED) TRY(cp_mixed_measure_prep(e, &tcPrep));
+        if (!tcPrep) {
+            if (e->precision == AFQMC_MIXED) TRY(mixed_sync_to_fp64(e));
+            TRY(one_body(e, 1, e->wf, e->wfTmp, e->alive));
+            TRY(overlap_gemm(e, e->wfTmp, e->alive, fbl(e)));
+        }
         launch_lu_logdet_inverse(W, fbl(e), e->S, e->Sinv, e->alive, e->logw, one_body_logw(e, 1),
                                  e->logwT, e->logov, e->alive, nullptr, nullptr, nullptr,
                                  e->status, LU_PLAIN, true, s);

@@ -1,14 +1,18 @@
 """Constrained-path mixed-precision form (tcgen05 kind::tf32 contractions
-with compensated hi/lo operands; FP64 LU/log-det, weights, re-orthonormalisation,
-population control and measurement) against the plain FP64 form on the same
+with compensated hi/lo operands, also for the measurement's half step and
+overlap; FP64 LU/log-det, weights, re-orthonormalisation, population control
+and the rest of the measurement) against the plain FP64 form on the same
 walkers and random stream.
 
 Tolerances: with a constant force (identical aux fields) walkers and
 log-weights agree to 2e-5 relative after several steps (fp32 walkers,
 3-term tf32 products); with the dynamic force (tf32 Green's function entries)
 at least 90% of walkers take the same aux fields in the first step; the mixed
-estimator on identical walkers agrees to 1e-6 relative (FP64 measurement of
-the fp32-rounded walkers) and, along a run, to 2e-3 relative."""
+estimator on identical walkers agrees to 2e-5 relative in the energy and to
+1e-4 in the normalisation sum_w overlap_w (the half step and the overlap as
+3-term tf32 products, about 1e-7 per entry, amplified in each walker's
+overlap determinant; the ratio cancels most of it), and, along a run, to
+2e-3 relative."""
 import numpy as np
 import pytest
 
@@ -93,8 +97,9 @@ def test_measurement_on_same_walkers(name):
         e.reset_measurement()
         e.add_mixed_measurement()
     mf, mx = f.measurement(), x.measurement()
-    assert abs(mf[0] - mx[0]) < 1e-6 * abs(mf[0])
-    assert abs(mf[1] / mf[0] - mx[1] / mx[0]) < 1e-6 * abs(mf[1] / mf[0])
+    assert abs(mf[0] - mx[0]) < 1e-4 * abs(mf[0])
+    assert abs(mf[1] / mf[0] - mx[1] / mx[0]) < 2e-5 * abs(mf[1] / mf[0])
+    print(name, "den", abs(mf[0] - mx[0]) / abs(mf[0]), "E", abs(mf[1] / mf[0] - mx[1] / mx[0]) / abs(mf[1] / mf[0]))
 
 
 def test_cadence_and_population_control():
