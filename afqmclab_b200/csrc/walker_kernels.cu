@@ -596,21 +596,18 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
 }
 
 // ---------------------------------------------------------------------------
-// Same contract as gj_warp_kernel for one or two blocks of 17..32 columns, one
-// warp per (walker, block) and the matrix in registers: lane i holds row i
-// (padded to 32 x 32 with zeros; only Ns steps run, after which the last Ns
-// register slots hold the inverse columns).  The column loop is not
-// unrolled; instead every lane's row rotates by one slot per step, so the
-// current column is always register slot 0 and every register index is
-// static.  While it updates step k the warp already searches the pivot of
-// step k+1 in its new slot 0 (redux over a rank of |re|+|im|), and the
-// winning lane publishes its row, position and a division-free reciprocal of
-// its pivot, so a step starts with one warp barrier and no search.
+// Gauss-Jordan with the matrix in registers (gj_regw_kernel below), same
+// contract as gj_warp_kernel for one or two blocks of 17..64 columns: each
+// row lives in registers (padded with zeros to the window; only Ns steps
+// run, after which the last Ns window slots hold the inverse columns).  The
+// column loop is not unrolled; instead every row rotates by one slot per
+// step, so the current column is always register slot 0 and every register
+// index is static.
 //   - pivot: zgetf2's choice, first position >= k of maximal |re|+|im| in the
 //     column; rows are not moved, each lane keeps the position its row has in
 //     the interchanged matrix (ties go to the lower position, as in izamax);
-//   - the chosen lane writes its row to shared memory (a broadcast source for
-//     the warp); every other row i takes a_ij -= (a_ik / piv) a_pj and
+//   - the chosen row is published in shared memory (a broadcast source);
+//     every other row i takes a_ij -= (a_ik / piv) a_pj and
 //     a_ik = -a_ik / piv (in-place Gauss-Jordan, which leaves the inverse of the
 //     interchanged matrix); the pivot row is not rescaled but keeps a row scale
 //     1/piv, applied once at the end.
@@ -618,8 +615,6 @@ gj_warp_kernel(int W, Blocks bl, const zd *S, zd *Sinv, const int *active, const
 // their logs and the phase their product with one sign flip per interchange
 // (logDeterminant, tensor_2d_common_fun.cpp:75-105).
 // ---------------------------------------------------------------------------
-constexpr int GR_WARPS = 4;
-
 // 1 / b by Smith's scaling (one ratio, one reciprocal)
 __device__ __forceinline__ zd zrcp(zd b)
 {
@@ -719,161 +714,12 @@ __device__ void lu_walker_finish(int w, bool act, int nb, int mult, const zd *ld
     }
 }
 
-__global__ void __launch_bounds__(GR_WARPS * 32, 2)
-gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
-              const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
-              double *weight, int *status, int mode, int wantInverse)
-{
-    __shared__ __align__(16) zd prow[GR_WARPS][2][32];   // [warp][step parity]: the pivot row
-    __shared__ __align__(16) zd candQ[GR_WARPS][2];      // 1 / pivot
-    __shared__ __align__(16) zd candA[GR_WARPS][2];      // pivot
-    __shared__ int candKey[GR_WARPS][2];                 // pivot position
-    __shared__ int pvS[GR_WARPS][32];
-    __shared__ int jxS[GR_WARPS][32];
-    __shared__ zd pivS[GR_WARPS][32];
-    __shared__ zd ldS[GR_WARPS];
-    __shared__ int sgS[GR_WARPS];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nb = bl.nblk;   // 1 or 2, so a walker's warps share this CTA
-    const int mIdx = blockIdx.x * GR_WARPS + warp;
-    const int w = mIdx / nb, b = mIdx - w * nb;
-    const bool inW = w < W;
-    const bool act = inW && ((active == nullptr) || active[w] != 0);
-    const int Ns = b == 0 ? bl.Ns[0] : bl.Ns[1];
-    const long long sOff = b == 0 ? bl.sOff[0] : bl.sOff[1];
-    const bool inv = wantInverse && (Sinv || Sinv32);
-    bool sing = false;
-    zd ld = make_double2(0.0, 0.0);
-    if (act && Ns > 0) {
-        const zd *Sg = S + (size_t)w * bl.sStride + sOff;
-        zd a[32];
-#pragma unroll
-        for (int j = 0; j < 32; ++j)
-            a[j] = (lane < Ns && j < Ns) ? Sg[lane + (size_t)Ns * j] : make_double2(0.0, 0.0);
-        // A row chosen at step k keeps position k for good, so a lane's final
-        // position names the step whose pivot it supplied (and its row scale).
-        int pos = lane;
-        {
-            const unsigned long long u = gr_rank(a[0], true);
-            if (pos == gr_warp_best(u, pos)) {
-#pragma unroll
-                for (int s = 0; s < 32; ++s) prow[warp][0][s] = a[s];
-                candKey[warp][0] = pos;
-                candA[warp][0] = a[0];
-                candQ[warp][0] = zeq0(a[0]) ? make_double2(0.0, 0.0) : zrcp_nr(a[0]);
-            }
-        }
-#pragma unroll 2
-        for (int k = 0; k < Ns; ++k) {
-            __syncwarp();   // step k's pivot row, position and reciprocal
-            const int cb = k & 1, pb = cb ^ 1;
-            const int p = candKey[warp][cb];
-            const zd q = candQ[warp][cb];
-            if (lane == 0) {
-                const zd piv = candA[warp][cb];
-                pvS[warp][k] = p;
-                pivS[warp][k] = piv;
-                sing = sing || zeq0(piv);
-            }
-            const bool isP = (pos == p);
-            if (pos == k) pos = p;
-            if (isP) pos = k;
-            const zd f = isP ? make_double2(0.0, 0.0) : zmul(a[0], q);
-            const zd nk = isP ? make_double2(1.0, 0.0) : zneg(f);
-            const zd *pr = prow[warp][cb];
-            {
-                const zd pv = pr[1];
-                a[0].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[1].x));
-                a[0].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[1].y));
-            }
-            // the pivot search of step k+1 on the new slot 0 (also after the
-            // last step, where nothing reads it, so the step stays one
-            // straight-line block the compiler can interleave)
-            const unsigned long long u = gr_rank(a[0], pos > k);
-            const bool win = (pos == gr_warp_best(u, pos));
-            const zd qr = zrcp_nr(a[0]);
-            const zd qn = zeq0(a[0]) ? make_double2(0.0, 0.0) : qr;
-#pragma unroll
-            for (int s = 2; s < 32; ++s) {
-                const zd pv = pr[s];
-                a[s - 1].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[s].x));
-                a[s - 1].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[s].y));
-            }
-            a[31] = nk;
-            if (win) {
-#pragma unroll
-                for (int s = 0; s < 32; ++s) prow[warp][pb][s] = a[s];
-                candKey[warp][pb] = pos;
-                candA[warp][pb] = a[0];
-                candQ[warp][pb] = qn;
-            }
-        }
-        // log-determinant: every real row supplied exactly one pivot (the
-        // zero padding rows keep positions >= Ns and are never chosen)
-        sing = __any_sync(0xffffffffu, sing);
-        __syncwarp();
-        const bool real = lane < Ns;
-        const zd myD = real ? pivS[warp][pos] : make_double2(1.0, 0.0);
-        double ln = 0.0;
-        zd ph = make_double2(1.0, 0.0);
-        if (real && !sing) {
-            const double ad = zabs(myD);
-            ln = log(ad);
-            ph = make_double2(myD.x / ad, myD.y / ad);
-            if (pvS[warp][pos] != pos) ph = zneg(ph);
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            ln += __shfl_xor_sync(0xffffffffu, ln, o);
-            zd t;
-            t.x = __shfl_xor_sync(0xffffffffu, ph.x, o);
-            t.y = __shfl_xor_sync(0xffffffffu, ph.y, o);
-            ph = zmul(ph, t);
-        }
-        if (!sing) ld = zadd(make_double2(ln, 0.0), zlog(ph));
-        if (inv) {
-            // Row r's final position is the image of r under the interchanges
-            // applied first to last, so interchanged column j (register slot
-            // j + 32 - Ns) is column r of the inverse for the row r whose
-            // final position is j.
-            if (real) jxS[warp][pos] = lane;
-            __syncwarp();
-            const zd sc = sing ? make_double2(0.0, 0.0) : zrcp(myD);
-            const int j0 = Ns - 32;
-            if (real && Sinv32) {
-                // fp32 planes [re | im], each Ns x Ns column-major
-                float *Xr = Sinv32 + (size_t)w * s32 + 2 * sOff, *Xi = Xr + (size_t)Ns * Ns;
-#pragma unroll
-                for (int s = 0; s < 32; ++s) {
-                    const int j = j0 + s;
-                    if (j >= 0) {
-                        const int c = jxS[warp][j];
-                        const zd v = zmul(sc, a[s]);
-                        Xr[pos + (size_t)Ns * c] = (float)v.x;
-                        Xi[pos + (size_t)Ns * c] = (float)v.y;
-                    }
-                }
-            } else if (real) {
-                zd *Xg = Sinv + (size_t)w * bl.sStride + sOff;
-#pragma unroll
-                for (int s = 0; s < 32; ++s) {
-                    const int j = j0 + s;
-                    if (j >= 0) Xg[pos + (size_t)Ns * jxS[warp][j]] = zmul(sc, a[s]);
-                }
-            }
-        }
-    }
-    if (lane == 0) { ldS[warp] = ld; sgS[warp] = sing ? 1 : 0; }
-    __syncthreads();
-    if (lane != 0 || b != 0 || !inW) return;
-    lu_walker_finish(w, act, nb, bl.mult, ldS + warp, sgS + warp, logw, logwAdd, logwT,
-                     logov, alive, surv, logwOut, weight, status, mode);
-}
-
 // ---------------------------------------------------------------------------
-// The same rotated Gauss-Jordan for blocks of 33-64 columns, one CTA of four
-// warps per matrix.  Warp (rh, ch) holds rows rh*32+lane and half ch of a
-// 64-column window that moves by one column per step.  The half-0 warps hold
+// The same rotated Gauss-Jordan with the window split between two column
+// halves, one CTA per matrix: RH row halves x 2 column halves of SL slots
+// (RH = 2, SL = 32 for blocks of 33-64 columns, four warps; RH = 1, SL = 16
+// for 17-32 columns, two warps).  Warp (rh, ch) holds rows rh*32+lane and
+// half ch of a 2 SL-column window that moves by one column per step.  The half-0 warps hold
 // the current column in slot 0; while they update step k they already search
 // the pivot of step k+1 in their new slot 0 (max |re|+|im|, ties to the lower
 // position, NaN first), and each warp's winning lane publishes its row, its
@@ -882,7 +728,7 @@ gj_reg_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long 
 //     slot of every row (and of the pivot row) is the updated slot 0 of half
 //     1 from the step before, passed through shared memory;
 //   - half 1 takes its factor f = a_k * (1/piv) from the published column k,
-//     the pivot row's lane writes its half-1 row, a barrier of the two half-1
+//     the pivot row's lane writes its half-1 row, a barrier of the half-1
 //     warps, then half 1 updates and takes the new inverse column in its last
 //     slot.
 // Shared buffers alternate between even and odd steps, so the only CTA-wide
@@ -909,22 +755,23 @@ __device__ __forceinline__ void gr64_half_bar()
     asm volatile("bar.sync 1, 64;" ::: "memory");
 }
 
-template <int NB>
-__global__ void __launch_bounds__(128, 2)
-gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
+template <int NB, int SL, int RH>
+__global__ void __launch_bounds__(64 * RH, RH == 2 ? 2 : 8)
+gj_regw_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
                 const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
                 double *weight, int *status, int mode, int wantInverse)
 {
-    __shared__ __align__(16) zd prowC[2][2][32];   // [step parity][rh]: half 0 of each warp's candidate
-    __shared__ __align__(16) zd prow1[32];         // half 1 of the pivot row
-    __shared__ __align__(16) zd colS[2][64];       // [step parity][row]: the current column
-    __shared__ __align__(16) zd xS[2][64];         // [step parity][row]: half 1's updated slot 0
-    __shared__ __align__(16) GR64Cand cand[2][2];  // [step parity][rh]
-    __shared__ __align__(16) zd pivS[64];
-    __shared__ __align__(16) zd phS[2];
-    __shared__ double lnS[2];
-    __shared__ int pvS[64];
-    __shared__ int jxS[64];
+    constexpr int NR = 32 * RH;                      // rows of the window
+    __shared__ __align__(16) zd prowC[2][RH][SL];   // [step parity][rh]: half 0 of each warp's candidate
+    __shared__ __align__(16) zd prow1[SL];          // half 1 of the pivot row
+    __shared__ __align__(16) zd colS[2][NR];        // [step parity][row]: the current column
+    __shared__ __align__(16) zd xS[2][NR];          // [step parity][row]: half 1's updated slot 0
+    __shared__ __align__(16) GR64Cand cand[2][RH];  // [step parity][rh]
+    __shared__ __align__(16) zd pivS[NR];
+    __shared__ __align__(16) zd phS[RH];
+    __shared__ double lnS[RH];
+    __shared__ int pvS[NR];
+    __shared__ int jxS[NR];
     __shared__ zd ldS;
     __shared__ int sgS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -940,16 +787,16 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
     zd ld = make_double2(0.0, 0.0);
     if (act && Ns > 0) {   // uniform over the CTA
         const zd *Sg = S + (size_t)w * bl.sStride + sOff;
-        zd a[32];
+        zd a[SL];
 #pragma unroll
-        for (int s = 0; s < 32; ++s) {
-            const int c = ch * 32 + s;
+        for (int s = 0; s < SL; ++s) {
+            const int c = ch * SL + s;
             a[s] = (r < Ns && c < Ns) ? Sg[r + (size_t)Ns * c] : make_double2(0.0, 0.0);
         }
         int pos = r;
         if (ch == 0) {
             // step 0's inputs, as if a step -1 had produced them
-            xS[1][r] = a[31];
+            xS[1][r] = a[SL - 1];
             colS[0][r] = a[0];
             const unsigned long long u = gr_rank(a[0], true);
             if (pos == gr_warp_best(u, pos)) {
@@ -958,17 +805,20 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
                 c.q = zeq0(a[0]) ? make_double2(0.0, 0.0) : zrcp_nr(a[0]);
                 cand[0][rh] = c;
 #pragma unroll
-                for (int s = 0; s < 31; ++s) prowC[0][rh][s] = a[s];
+                for (int s = 0; s < SL - 1; ++s) prowC[0][rh][s] = a[s];
             }
         }
 #pragma unroll 1
         for (int k = 0; k < Ns; ++k) {
             __syncthreads();   // step k's candidates, column, half-0 rows and half 1's last slots
             const int cb = k & 1, pb = cb ^ 1;
-            const unsigned long long u0 = cand[cb][0].u, u1 = cand[cb][1].u;
-            const int k0 = cand[cb][0].key, k1 = cand[cb][1].key;
-            const int second = (u1 > u0 || (u1 == u0 && k1 < k0)) ? 1 : 0;
-            const int p = second ? k1 : k0;
+            int second = 0;
+            if constexpr (RH == 2) {
+                const unsigned long long u0 = cand[cb][0].u, u1 = cand[cb][1].u;
+                const int k0 = cand[cb][0].key, k1 = cand[cb][1].key;
+                second = (u1 > u0 || (u1 == u0 && k1 < k0)) ? 1 : 0;
+            }
+            const int p = cand[cb][second].key;
             const zd q = cand[cb][second].q;
             if (threadIdx.x == 0) {
                 const zd piv = cand[cb][second].a0;
@@ -980,9 +830,9 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
             if (pos == k) pos = p;
             if (isP) pos = k;
             if (ch == 0) {
-                a[31] = xS[pb][r];
+                a[SL - 1] = xS[pb][r];
                 const zd *pr = prowC[cb][second];
-                const zd p31 = xS[pb][cand[cb][second].row];
+                const zd pLast = xS[pb][cand[cb][second].row];
                 const zd f = isP ? make_double2(0.0, 0.0) : zmul(a[0], q);
                 {
                     const zd pv = pr[1];
@@ -998,8 +848,8 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
                 const zd qr = zrcp_nr(a[0]);
                 const zd qn = zeq0(a[0]) ? make_double2(0.0, 0.0) : qr;
 #pragma unroll
-                for (int s = 2; s < 32; ++s) {
-                    const zd pv = s < 31 ? pr[s] : p31;
+                for (int s = 2; s < SL; ++s) {
+                    const zd pv = s < SL - 1 ? pr[s] : pLast;
                     a[s - 1].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[s].x));
                     a[s - 1].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[s].y));
                 }
@@ -1009,32 +859,33 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
                     c.q = qn;
                     cand[pb][rh] = c;
 #pragma unroll
-                    for (int s = 0; s < 31; ++s) prowC[pb][rh][s] = a[s];
+                    for (int s = 0; s < SL - 1; ++s) prowC[pb][rh][s] = a[s];
                 }
             } else {
                 const zd f = isP ? make_double2(0.0, 0.0) : zmul(colS[cb][r], q);
                 if (isP) {
 #pragma unroll
-                    for (int s = 0; s < 32; ++s) prow1[s] = a[s];
+                    for (int s = 0; s < SL; ++s) prow1[s] = a[s];
                 }
-                gr64_half_bar();
+                if constexpr (RH == 2) gr64_half_bar();
+                else __syncwarp();
                 zd x;
                 x.x = fma(-f.x, prow1[0].x, fma(f.y, prow1[0].y, a[0].x));
                 x.y = fma(-f.x, prow1[0].y, fma(-f.y, prow1[0].x, a[0].y));
                 xS[cb][r] = x;
 #pragma unroll
-                for (int s = 1; s < 32; ++s) {
+                for (int s = 1; s < SL; ++s) {
                     const zd pv = prow1[s];
                     a[s - 1].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[s].x));
                     a[s - 1].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[s].y));
                 }
-                a[31] = isP ? make_double2(1.0, 0.0) : zneg(f);
+                a[SL - 1] = isP ? make_double2(1.0, 0.0) : zneg(f);
             }
         }
         if (threadIdx.x == 0) sgS = sing ? 1 : 0;
         __syncthreads();   // last slots of step Ns-1, all pivots
         sing = sgS != 0;
-        if (ch == 0) a[31] = xS[(Ns - 1) & 1][r];
+        if (ch == 0) a[SL - 1] = xS[(Ns - 1) & 1][r];
         const bool real = r < Ns;   // padding rows keep positions >= Ns
         const zd myD = real ? pivS[pos] : make_double2(1.0, 0.0);
         if (ch == 0) {
@@ -1059,16 +910,19 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
             if (real) jxS[pos] = r;
         }
         __syncthreads();
-        if (threadIdx.x == 0 && !sing) ld = zadd(make_double2(lnS[0] + lnS[1], 0.0), zlog(zmul(phS[0], phS[1])));
+        if (threadIdx.x == 0 && !sing) {
+            if constexpr (RH == 2) ld = zadd(make_double2(lnS[0] + lnS[1], 0.0), zlog(zmul(phS[0], phS[1])));
+            else ld = zadd(make_double2(lnS[0], 0.0), zlog(phS[0]));
+        }
         if (inv && real) {
-            // window slot t = 32 ch + s holds interchanged column j = t - (64 - Ns)
+            // window slot t = SL ch + s holds interchanged column j = t - (2 SL - Ns)
             const zd sc = sing ? make_double2(0.0, 0.0) : zrcp(myD);
-            const int j0 = ch * 32 - (64 - Ns);
+            const int j0 = ch * SL - (2 * SL - Ns);
             if (Sinv32) {
                 // fp32 planes [re | im], each Ns x Ns column-major
                 float *Xr = Sinv32 + (size_t)w * s32 + 2 * sOff, *Xi = Xr + (size_t)Ns * Ns;
 #pragma unroll
-                for (int s = 0; s < 32; ++s) {
+                for (int s = 0; s < SL; ++s) {
                     const int j = j0 + s;
                     if (j >= 0) {
                         const int c = jxS[j];
@@ -1080,7 +934,7 @@ gj_reg64_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long lon
             } else {
                 zd *Xg = Sinv + (size_t)w * bl.sStride + sOff;
 #pragma unroll
-                for (int s = 0; s < 32; ++s) {
+                for (int s = 0; s < SL; ++s) {
                     const int j = j0 + s;
                     if (j >= 0) Xg[pos + (size_t)Ns * jxS[j]] = zmul(sc, a[s]);
                 }
@@ -2227,6 +2081,33 @@ void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const in
                                logwOut, weight, status, mode, wantInverse, s);
 }
 
+// the split-window register LU: one CTA per block, the two blocks of a
+// two-block walker as a cluster of two CTAs
+template <int SL, int RH>
+static void launch_regw(int W, const Blocks &bl, zd *S, zd *X64, float *Sinv32, long long s32, const int *active,
+                        const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
+                        double *weight, int *status, int mode, int inv, cudaStream_t s)
+{
+    if (bl.nblk == 1) {
+        gj_regw_kernel<1, SL, RH><<<W, 64 * RH, 0, s>>>(W, bl, S, X64, Sinv32, s32, active, logw, logwAdd, logwT,
+                                                        logov, alive, surv, logwOut, weight, status, mode, inv);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(2 * W));
+    cfg.blockDim = dim3(64 * RH);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, gj_regw_kernel<2, SL, RH>, W, bl, (const zd *)S, X64, Sinv32, s32, active, logw,
+                       logwAdd, logwT, logov, alive, surv, logwOut, weight, status, mode, inv);
+}
+
 void launch_lu_logdet_inverse32(int W, const Blocks &bl, zd *S, zd *Sinv, float *Sinv32, const int *active,
                                 const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv,
                                 zd *logwOut, double *weight, int *status, int mode, bool wantInverse,
@@ -2235,36 +2116,14 @@ void launch_lu_logdet_inverse32(int W, const Blocks &bl, zd *S, zd *Sinv, float 
     int maxNs = 0;
     for (int b = 0; b < bl.nblk; ++b) maxNs = bl.Ns[b] > maxNs ? bl.Ns[b] : maxNs;
     const long long s32 = sinv32_stride(bl);
-    if (maxNs > 16 && maxNs <= 32 && (bl.nblk == 1 || bl.nblk == 2)) {
+    if (maxNs > 16 && maxNs <= 64 && (bl.nblk == 1 || bl.nblk == 2)) {
         g_launch_count++;
-        const long long mats = (long long)W * bl.nblk;
-        gj_reg_kernel<<<(unsigned)((mats + GR_WARPS - 1) / GR_WARPS), GR_WARPS * 32, 0, s>>>(
-            W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov, alive, surv,
-            logwOut, weight, status, mode, wantInverse ? 1 : 0);
-        return;
-    }
-    if (maxNs > 32 && maxNs <= 64 && (bl.nblk == 1 || bl.nblk == 2)) {
-        g_launch_count++;
-        zd *X64 = Sinv32 ? nullptr : Sinv;
-        const int inv = wantInverse ? 1 : 0;
-        if (bl.nblk == 1) {
-            gj_reg64_kernel<1><<<W, 128, 0, s>>>(W, bl, S, X64, Sinv32, s32, active, logw, logwAdd, logwT, logov,
-                                                 alive, surv, logwOut, weight, status, mode, inv);
-            return;
-        }
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(2 * W));
-        cfg.blockDim = dim3(128);
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = 2;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        cudaLaunchKernelEx(&cfg, gj_reg64_kernel<2>, W, bl, (const zd *)S, X64, Sinv32, s32, active, logw,
-                           logwAdd, logwT, logov, alive, surv, logwOut, weight, status, mode, inv);
+        if (maxNs <= 32)
+            launch_regw<16, 1>(W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov,
+                               alive, surv, logwOut, weight, status, mode, wantInverse ? 1 : 0, s);
+        else
+            launch_regw<32, 2>(W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov,
+                               alive, surv, logwOut, weight, status, mode, wantInverse ? 1 : 0, s);
         return;
     }
     launch_lu_fp64(W, bl, S, Sinv, active, logw, logwAdd, logwT, logov, alive, surv, logwOut, weight, status,
