@@ -750,22 +750,23 @@ struct GR64Cand {
     zd q;                   // 1 / a0, zero when a0 is zero
 };
 
-__device__ __forceinline__ void gr64_half_bar()
+// named barrier 1 of the column groups other than 0
+__device__ __forceinline__ void upper_groups_bar(int threads)
 {
-    asm volatile("bar.sync 1, 64;" ::: "memory");
+    asm volatile("bar.sync 1, %0;" ::"r"(threads) : "memory");
 }
 
-template <int NB, int SL, int RH>
-__global__ void __launch_bounds__(64 * RH, RH == 2 ? 2 : 8)
+template <int NB, int SL, int RH, int NQ>
+__global__ void __launch_bounds__(32 * RH * NQ, SL == 16 ? 65536 / (32 * RH * NQ * 128) : 2)
 gj_regw_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long s32, const int *active,
                 const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
                 double *weight, int *status, int mode, int wantInverse)
 {
     constexpr int NR = 32 * RH;                      // rows of the window
     __shared__ __align__(16) zd prowC[2][RH][SL];   // [step parity][rh]: half 0 of each warp's candidate
-    __shared__ __align__(16) zd prow1[SL];          // half 1 of the pivot row
+    __shared__ __align__(16) zd prowQ[NQ][SL];      // [cq >= 1]: column group cq of the pivot row
     __shared__ __align__(16) zd colS[2][NR];        // [step parity][row]: the current column
-    __shared__ __align__(16) zd xS[2][NR];          // [step parity][row]: half 1's updated slot 0
+    __shared__ __align__(16) zd xS[NQ][2][NR];      // [cq >= 1][step parity][row]: group cq's updated slot 0
     __shared__ __align__(16) GR64Cand cand[2][RH];  // [step parity][rh]
     __shared__ __align__(16) zd pivS[NR];
     __shared__ __align__(16) zd phS[RH];
@@ -775,7 +776,7 @@ gj_regw_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long
     __shared__ zd ldS;
     __shared__ int sgS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rh = warp >> 1, ch = warp & 1;
+    const int rh = warp / NQ, ch = warp % NQ;   // ch: the column group
     const int r = rh * 32 + lane;
     const int w = NB == 1 ? (int)blockIdx.x : (int)(blockIdx.x >> 1);
     const int b = NB == 1 ? 0 : (int)(blockIdx.x & 1);
@@ -794,9 +795,10 @@ gj_regw_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long
             a[s] = (r < Ns && c < Ns) ? Sg[r + (size_t)Ns * c] : make_double2(0.0, 0.0);
         }
         int pos = r;
+        // step 0's inputs, as if a step -1 had produced them: each group's
+        // last slot as the next group's "updated slot 0"
+        if (ch < NQ - 1) xS[ch + 1][1][r] = a[SL - 1];
         if (ch == 0) {
-            // step 0's inputs, as if a step -1 had produced them
-            xS[1][r] = a[SL - 1];
             colS[0][r] = a[0];
             const unsigned long long u = gr_rank(a[0], true);
             if (pos == gr_warp_best(u, pos)) {
@@ -830,9 +832,9 @@ gj_regw_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long
             if (pos == k) pos = p;
             if (isP) pos = k;
             if (ch == 0) {
-                a[SL - 1] = xS[pb][r];
+                a[SL - 1] = xS[1][pb][r];
                 const zd *pr = prowC[cb][second];
-                const zd pLast = xS[pb][cand[cb][second].row];
+                const zd pLast = xS[1][pb][cand[cb][second].row];
                 const zd f = isP ? make_double2(0.0, 0.0) : zmul(a[0], q);
                 {
                     const zd pv = pr[1];
@@ -862,30 +864,35 @@ gj_regw_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long
                     for (int s = 0; s < SL - 1; ++s) prowC[pb][rh][s] = a[s];
                 }
             } else {
+                // a middle group's last slot: its right neighbour's slot 0 of step k-1
+                if (ch < NQ - 1) a[SL - 1] = xS[ch + 1][pb][r];
                 const zd f = isP ? make_double2(0.0, 0.0) : zmul(colS[cb][r], q);
+                zd *pq = prowQ[ch];
                 if (isP) {
 #pragma unroll
-                    for (int s = 0; s < SL; ++s) prow1[s] = a[s];
+                    for (int s = 0; s < SL; ++s) pq[s] = a[s];
                 }
-                if constexpr (RH == 2) gr64_half_bar();
+                if constexpr (RH * (NQ - 1) > 1) upper_groups_bar(32 * RH * (NQ - 1));
                 else __syncwarp();
                 zd x;
-                x.x = fma(-f.x, prow1[0].x, fma(f.y, prow1[0].y, a[0].x));
-                x.y = fma(-f.x, prow1[0].y, fma(-f.y, prow1[0].x, a[0].y));
-                xS[cb][r] = x;
+                x.x = fma(-f.x, pq[0].x, fma(f.y, pq[0].y, a[0].x));
+                x.y = fma(-f.x, pq[0].y, fma(-f.y, pq[0].x, a[0].y));
+                xS[ch][cb][r] = x;
 #pragma unroll
                 for (int s = 1; s < SL; ++s) {
-                    const zd pv = prow1[s];
+                    const zd pv = pq[s];
                     a[s - 1].x = fma(-f.x, pv.x, fma(f.y, pv.y, a[s].x));
                     a[s - 1].y = fma(-f.x, pv.y, fma(-f.y, pv.x, a[s].y));
                 }
-                a[SL - 1] = isP ? make_double2(1.0, 0.0) : zneg(f);
+                // the last group takes the new inverse column; the others
+                // take their neighbour's slot 0 at the next step
+                if (ch == NQ - 1) a[SL - 1] = isP ? make_double2(1.0, 0.0) : zneg(f);
             }
         }
         if (threadIdx.x == 0) sgS = sing ? 1 : 0;
         __syncthreads();   // last slots of step Ns-1, all pivots
         sing = sgS != 0;
-        if (ch == 0) a[SL - 1] = xS[(Ns - 1) & 1][r];
+        if (ch < NQ - 1) a[SL - 1] = xS[ch + 1][(Ns - 1) & 1][r];
         const bool real = r < Ns;   // padding rows keep positions >= Ns
         const zd myD = real ? pivS[pos] : make_double2(1.0, 0.0);
         if (ch == 0) {
@@ -915,9 +922,9 @@ gj_regw_kernel(int W, Blocks bl, const zd *S, zd *Sinv, float *Sinv32, long long
             else ld = zadd(make_double2(lnS[0], 0.0), zlog(phS[0]));
         }
         if (inv && real) {
-            // window slot t = SL ch + s holds interchanged column j = t - (2 SL - Ns)
+            // window slot t = SL ch + s holds interchanged column j = t - (NQ SL - Ns)
             const zd sc = sing ? make_double2(0.0, 0.0) : zrcp(myD);
-            const int j0 = ch * SL - (2 * SL - Ns);
+            const int j0 = ch * SL - (NQ * SL - Ns);
             if (Sinv32) {
                 // fp32 planes [re | im], each Ns x Ns column-major
                 float *Xr = Sinv32 + (size_t)w * s32 + 2 * sOff, *Xi = Xr + (size_t)Ns * Ns;
@@ -2083,19 +2090,20 @@ void launch_lu_logdet_inverse(int W, const Blocks &bl, zd *S, zd *Sinv, const in
 
 // the split-window register LU: one CTA per block, the two blocks of a
 // two-block walker as a cluster of two CTAs
-template <int SL, int RH>
+template <int SL, int RH, int NQ>
 static void launch_regw(int W, const Blocks &bl, zd *S, zd *X64, float *Sinv32, long long s32, const int *active,
                         const zd *logw, zd logwAdd, zd logwT, zd *logov, int *alive, int *surv, zd *logwOut,
                         double *weight, int *status, int mode, int inv, cudaStream_t s)
 {
+    constexpr int T = 32 * RH * NQ;
     if (bl.nblk == 1) {
-        gj_regw_kernel<1, SL, RH><<<W, 64 * RH, 0, s>>>(W, bl, S, X64, Sinv32, s32, active, logw, logwAdd, logwT,
-                                                        logov, alive, surv, logwOut, weight, status, mode, inv);
+        gj_regw_kernel<1, SL, RH, NQ><<<W, T, 0, s>>>(W, bl, S, X64, Sinv32, s32, active, logw, logwAdd, logwT,
+                                                      logov, alive, surv, logwOut, weight, status, mode, inv);
         return;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(2 * W));
-    cfg.blockDim = dim3(64 * RH);
+    cfg.blockDim = dim3(T);
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -2104,7 +2112,7 @@ static void launch_regw(int W, const Blocks &bl, zd *S, zd *X64, float *Sinv32, 
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, gj_regw_kernel<2, SL, RH>, W, bl, (const zd *)S, X64, Sinv32, s32, active, logw,
+    cudaLaunchKernelEx(&cfg, gj_regw_kernel<2, SL, RH, NQ>, W, bl, (const zd *)S, X64, Sinv32, s32, active, logw,
                        logwAdd, logwT, logov, alive, surv, logwOut, weight, status, mode, inv);
 }
 
@@ -2119,10 +2127,10 @@ void launch_lu_logdet_inverse32(int W, const Blocks &bl, zd *S, zd *Sinv, float 
     if (maxNs > 16 && maxNs <= 64 && (bl.nblk == 1 || bl.nblk == 2)) {
         g_launch_count++;
         if (maxNs <= 32)
-            launch_regw<16, 1>(W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov,
+            launch_regw<16, 1, 2>(W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov,
                                alive, surv, logwOut, weight, status, mode, wantInverse ? 1 : 0, s);
         else
-            launch_regw<32, 2>(W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov,
+            launch_regw<32, 2, 2>(W, bl, S, Sinv32 ? nullptr : Sinv, Sinv32, s32, active, logw, logwAdd, logwT, logov,
                                alive, surv, logwOut, weight, status, mode, wantInverse ? 1 : 0, s);
         return;
     }
