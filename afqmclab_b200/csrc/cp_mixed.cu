@@ -510,9 +510,11 @@ cpm_sample_apply_kernel(int W, HubbardDev h, const float2 *gd, const int *surv, 
     const int w = blockIdx.x;
     if (!surv[w]) return;
     const int L = h.L, N = h.N, n = h.n;
-    float2 *d = (float2 *)smem_raw;                  // 4 L entries: d00, d01, d10, d11
+    // layout: 16-byte entries first, so every array is aligned for any L
+    zd *gxS = (zd *)smem_raw;                        // per site: gamma x
+    float2 *d = (float2 *)(gxS + L);                 // 4 L entries: d00, d01, d10, d11
     int *aux = (int *)(d + 4 * L);
-    double *fs = (double *)(aux + L + (L & 1));
+    double *lpS = (double *)(aux + L + (L & 1));     // per site: x f - log(e^f + e^-f)
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
         double f;
         if (h.constForce) {
@@ -526,12 +528,13 @@ cpm_sample_apply_kernel(int W, HubbardDev h, const float2 *gd, const int *surv, 
             f = zmul(h.gamma[i], bgv).x;
             f = fmin(fmax(f, -h.forceCap), h.forceCap);
         }
-        fs[i] = f;
         const double em = exp(-f), ep = exp(f);
         const int x = (rng_uniform(seed, offs[w] + (unsigned long long)i) < em / (em + ep)) ? -1 : 1;
         aux[i] = x;
         if (auxOut) auxOut[(size_t)w * L + i] = x;
+        lpS[i] = x * f - log(ep + em);
         const zd ga = zscale(h.gamma[i], (double)x);
+        gxS[i] = ga;
         zd a00, a01, a10, a11;
         if (h.decomp == 0) {
             const zd ex = zexp_d(ga);
@@ -563,26 +566,31 @@ cpm_sample_apply_kernel(int W, HubbardDev h, const float2 *gd, const int *surv, 
         d[3 * L + i] = make_float2((float)a11.x, (float)a11.y);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        zd lw;
-        if (h.decomp == 0) {
-            zd sum = make_double2(0.0, 0.0), comp = make_double2(0.0, 0.0);
-            for (int i = 0; i < L; ++i) {
-                const zd y = zsub(zscale(h.gamma[i], (double)aux[i]), comp);
-                const zd t = zadd(sum, y);
-                comp = zsub(zsub(t, sum), y);
-                sum = t;
-            }
-            lw = zsub(make_double2(log(0.5) * L + h.dtUSum * 0.5, 0.0), sum);
-        } else {
-            lw = make_double2(log(0.5) * L, 0.0);
-        }
+    if (threadIdx.x < 32) {
+        // the walker's sample log-weight: the per-site terms summed by warp 0
+        // in a fixed order (lane-strided partial sums, then a shuffle tree)
+        const int lane = threadIdx.x;
         double lp = 0.0;
-        for (int i = 0; i < L; ++i) lp += aux[i] * fs[i] - log(exp(fs[i]) + exp(-fs[i]));
-        lw.x -= lp;
-        zd t = zadd(lw, logw[w]);
-        t.x += dtET;
-        logw[w] = zadd(hopLogw, t);
+        zd gsum = make_double2(0.0, 0.0);
+        for (int i = lane; i < L; i += 32) {
+            lp += lpS[i];
+            gsum = zadd(gsum, gxS[i]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lp += __shfl_xor_sync(0xffffffffu, lp, o);
+            gsum.x += __shfl_xor_sync(0xffffffffu, gsum.x, o);
+            gsum.y += __shfl_xor_sync(0xffffffffu, gsum.y, o);
+        }
+        if (lane == 0) {
+            zd lw;
+            if (h.decomp == 0) lw = zsub(make_double2(log(0.5) * L + h.dtUSum * 0.5, 0.0), gsum);
+            else lw = make_double2(log(0.5) * L, 0.0);
+            lw.x -= lp;
+            zd t = zadd(lw, logw[w]);
+            t.x += dtET;
+            logw[w] = zadd(hopLogw, t);
+        }
     }
     const size_t base = (size_t)w * 2 * n * N, plane = (size_t)n * N;
     for (int e = threadIdx.x; e < L * N; e += blockDim.x) {
@@ -877,7 +885,7 @@ int cp_mixed_project_dtk_dtv(afqmc_engine *e)
         PHASE(AFQMC_PH_SAMPLE);
         launch_rng_scan(W, e->surv, e->L, e->counter, e->offs, s);
         const int L = e->L;
-        const size_t smem = sizeof(float2) * 4 * L + sizeof(int) * (L + (L & 1)) + sizeof(double) * L;
+        const size_t smem = sizeof(float2) * 4 * L + sizeof(int) * (L + (L & 1)) + sizeof(double) * L + sizeof(zd) * L;
         g_launch_count++;
         cpm_sample_apply_kernel<<<W, 256, smem, s>>>(W, e->hd, m->gd, e->surv, e->offs, e->seed, m->hi, m->lo,
                                                      m->thi, m->tlo, e->logw, e->dt * e->ET,
