@@ -1143,23 +1143,31 @@ cp_sample_apply_kernel(int W, HubbardDev h, const double *force, const int *surv
     const double *fw = h.constForce ? h.constForce : force + (size_t)w * L;
     for (int i = threadIdx.x; i < L; i += blockDim.x) {
         double f = fw[i];
-        fs[i] = f;
         double em = exp(-f), ep = exp(f);
         double prob = em / (em + ep);
         int x = (rng_uniform(seed, offs[w] + (unsigned long long)i) < prob) ? -1 : 1;
         aux[i] = x;
         if (auxOut) auxOut[(size_t)w * L + i] = x;
+        fs[i] = x * f - log(ep + em);   // the site's term of the force's log-probability
         cp_site_matrix(h, i, x, d00[i], d01[i], d10[i], d11[i]);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        zd lw = cp_sample_logw(h, aux);
+    if (threadIdx.x < 32) {
+        // the site terms summed by warp 0 in a fixed order (lane-strided
+        // partial sums, then a shuffle tree); the sample's own log-weight keeps
+        // the reference's in-order compensated sum
+        const int lane = threadIdx.x;
         double lp = 0.0;
-        for (int i = 0; i < L; ++i) lp += aux[i] * fs[i] - log(exp(fs[i]) + exp(-fs[i]));
-        lw.x -= lp;
-        zd t = zadd(lw, logw[w]);
-        t.x += dtET;
-        logw[w] = zadd(hopLogw, t);
+        for (int i = lane; i < L; i += 32) lp += fs[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lp += __shfl_xor_sync(0xffffffffu, lp, o);
+        if (lane == 0) {
+            zd lw = cp_sample_logw(h, aux);
+            lw.x -= lp;
+            zd t = zadd(lw, logw[w]);
+            t.x += dtET;
+            logw[w] = zadd(hopLogw, t);
+        }
     }
     const zd *src = wf + (size_t)w * n * N;
     zd *dst = wfTmp + (size_t)w * n * N;
