@@ -21,7 +21,7 @@ FORCE = {"dynamicForce": 0, "constForce": 1}
 SYMBOLS = [
     "afqmc_last_error", "afqmc_version", "afqmc_cp_create", "afqmc_pl_create", "afqmc_destroy",
     "afqmc_set_stream", "afqmc_synchronize", "afqmc_set_walkers", "afqmc_get_walkers",
-    "afqmc_set_walkers_async", "afqmc_upload_wait",
+    "afqmc_set_walkers_f32_async", "afqmc_set_walkers_async", "afqmc_upload_wait",
     "afqmc_set_rng", "afqmc_get_rng", "afqmc_set_ET", "afqmc_set_cadence",
     "afqmc_project_one_step", "afqmc_project_half", "afqmc_modify_gm", "afqmc_pop_control",
     "afqmc_reset_measurement", "afqmc_add_mixed_measurement", "afqmc_get_measurement",
@@ -78,6 +78,7 @@ def _declare(L):
     L.afqmc_set_walkers.argtypes = [P, P, P, P]
     L.afqmc_get_walkers.argtypes = [P, P, P, P]
     L.afqmc_set_walkers_async.argtypes = [P, P, P, P]
+    L.afqmc_set_walkers_f32_async.argtypes = [P, P, P, P]
     L.afqmc_upload_wait.argtypes = [P]
     L.afqmc_set_rng.argtypes = [P, U64, U64]
     L.afqmc_get_rng.argtypes = [P, ctypes.POINTER(U64), ctypes.POINTER(U64)]
@@ -182,6 +183,13 @@ class Engine:
         must stay unchanged until upload_wait() or a synchronizing call)."""
         _check(lib().afqmc_set_walkers_async(self.h, ctypes.c_void_p(wf_ptr), ctypes.c_void_p(logw_ptr),
                                              ctypes.c_void_p(alive_ptr)))
+
+    def set_walkers_f32_async(self, wf32_ptr, logw_ptr, alive_ptr):
+        """Asynchronous upload of fp32 walkers in the phaseless mixed form's
+        layout (per walker: real plane then imaginary plane, n x ncol each,
+        column-major) from host pointers (pinned)."""
+        _check(lib().afqmc_set_walkers_f32_async(self.h, ctypes.c_void_p(wf32_ptr), ctypes.c_void_p(logw_ptr),
+                                                 ctypes.c_void_p(alive_ptr)))
 
     def upload_wait(self):
         _check(lib().afqmc_upload_wait(self.h))

@@ -933,20 +933,32 @@ int afqmc_set_walkers(afqmc_engine *e, const double *wf, const double *logw, con
     return AFQMC_OK;
 }
 
+namespace {
+
+// the copy stream, its events and the log-weight / alive staging slots,
+// made by the first asynchronous upload
+int upload_init(afqmc_engine *e)
+{
+    if (e->upStream) return AFQMC_OK;
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->upStream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+        CUDA_TRY(cudaEventCreateWithFlags(&e->upReady[k], cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&e->upFree[k], cudaEventDisableTiming));
+        CUDA_TRY(cudaEventRecord(e->upFree[k], e->stream));
+        TRY(dalloc(e, &e->stgLw[k], (size_t)e->W));
+        TRY(dalloc(e, &e->stgAl[k], (size_t)e->W));
+    }
+    return AFQMC_OK;
+}
+
+}  // namespace
+
 int afqmc_set_walkers_async(afqmc_engine *e, const double *wf, const double *logw, const int *alive)
 {
     if (!e || !wf || !logw || !alive) return fail(AFQMC_ERR_ARG, "null argument");
-    if (!e->upStream) {
-        CUDA_TRY(cudaStreamCreateWithFlags(&e->upStream, cudaStreamNonBlocking));
-        for (int k = 0; k < 2; ++k) {
-            CUDA_TRY(cudaEventCreateWithFlags(&e->upReady[k], cudaEventDisableTiming));
-            CUDA_TRY(cudaEventCreateWithFlags(&e->upFree[k], cudaEventDisableTiming));
-            CUDA_TRY(cudaEventRecord(e->upFree[k], e->stream));
-            TRY(dalloc(e, &e->stgWf[k], (size_t)e->wsize * e->W));
-            TRY(dalloc(e, &e->stgLw[k], (size_t)e->W));
-            TRY(dalloc(e, &e->stgAl[k], (size_t)e->W));
-        }
-    }
+    TRY(upload_init(e));
+    if (!e->stgWf[0])
+        for (int k = 0; k < 2; ++k) TRY(dalloc(e, &e->stgWf[k], (size_t)e->wsize * e->W));
     const int k = e->upNext;
     e->upNext ^= 1;
     // the slot's previous contents must have been installed first
@@ -966,6 +978,30 @@ int afqmc_set_walkers_async(afqmc_engine *e, const double *wf, const double *log
                                  e->stream));
         if (e->precision == AFQMC_MIXED) TRY(mixed_sync_from_fp64(e));
     }
+    CUDA_TRY(cudaEventRecord(e->upFree[k], e->stream));
+    return AFQMC_OK;
+}
+
+int afqmc_set_walkers_f32_async(afqmc_engine *e, const float *wf32, const double *logw, const int *alive)
+{
+    if (!e || !wf32 || !logw || !alive) return fail(AFQMC_ERR_ARG, "null argument");
+    if (e->precision != AFQMC_MIXED || !mixed_can_load_direct(e))
+        return fail(AFQMC_ERR_UNSUPPORTED, "fp32 walker upload is for the phaseless mixed form");
+    TRY(upload_init(e));
+    const size_t count = (size_t)2 * e->wsize * e->W;   // [re | im] planes per walker
+    if (!e->stgWf32[0])
+        for (int k = 0; k < 2; ++k) TRY(dalloc(e, &e->stgWf32[k], count));
+    const int k = e->upNext;
+    e->upNext ^= 1;
+    CUDA_TRY(cudaStreamWaitEvent(e->upStream, e->upFree[k], 0));
+    CUDA_TRY(cudaMemcpyAsync(e->stgWf32[k], wf32, sizeof(float) * count, cudaMemcpyHostToDevice, e->upStream));
+    CUDA_TRY(cudaMemcpyAsync(e->stgLw[k], logw, sizeof(zd) * e->W, cudaMemcpyHostToDevice, e->upStream));
+    CUDA_TRY(cudaMemcpyAsync(e->stgAl[k], alive, sizeof(int) * e->W, cudaMemcpyHostToDevice, e->upStream));
+    CUDA_TRY(cudaEventRecord(e->upReady[k], e->upStream));
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->upReady[k], 0));
+    CUDA_TRY(cudaMemcpyAsync(e->logw, e->stgLw[k], sizeof(zd) * e->W, cudaMemcpyDeviceToDevice, e->stream));
+    CUDA_TRY(cudaMemcpyAsync(e->alive, e->stgAl[k], sizeof(int) * e->W, cudaMemcpyDeviceToDevice, e->stream));
+    TRY(mixed_load_f32(e, e->stgWf32[k]));
     CUDA_TRY(cudaEventRecord(e->upFree[k], e->stream));
     return AFQMC_OK;
 }

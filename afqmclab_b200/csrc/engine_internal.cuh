@@ -30,6 +30,7 @@ struct afqmc_engine {
     cudaStream_t upStream = nullptr;
     cudaEvent_t upReady[2] = {nullptr, nullptr}, upFree[2] = {nullptr, nullptr};
     zd *stgWf[2] = {nullptr, nullptr}, *stgLw[2] = {nullptr, nullptr};
+    float *stgWf32[2] = {nullptr, nullptr};   // fp32 walkers of the phaseless mixed form
     int *stgAl[2] = {nullptr, nullptr};
     int upNext = 0;
     Blocks bl{};

@@ -1398,6 +1398,14 @@ int mixed_sync_from_fp64(afqmc_engine *e)
 
 bool mixed_can_load_direct(const afqmc_engine *e) { return e->kind != KIND_CP; }
 
+int mixed_load_f32(afqmc_engine *e, const float *src)
+{
+    const cudaError_t r = cudaMemcpyAsync(e->mx->wf32, src, sizeof(float) * (size_t)e->W * e->mx->ws32,
+                                          cudaMemcpyDeviceToDevice, e->stream);
+    if (r != cudaSuccess) return engine_fail(AFQMC_ERR_CUDA, std::string("installing fp32 walkers: ") + cudaGetErrorString(r));
+    return AFQMC_OK;
+}
+
 int mixed_load_direct(afqmc_engine *e, const zd *src)
 {
     wf_to_f32p_kernel<<<e->W, 256, 0, e->stream>>>(e->W, e->wsize, src, e->mx->wf32, nullptr);

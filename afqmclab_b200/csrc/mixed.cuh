@@ -17,6 +17,9 @@ int mixed_sync_from_fp64(afqmc_engine *e);
 // its fp32 walkers directly from another device buffer; the FP64 copy is
 // refreshed from the fp32 walkers before any FP64 use.
 bool mixed_can_load_direct(const afqmc_engine *e);
+// the walkers from a device buffer already in the phaseless mixed form's
+// fp32 planar layout (2 n ncol floats per walker: real plane, imaginary plane)
+int mixed_load_f32(afqmc_engine *e, const float *src);
 int mixed_load_direct(afqmc_engine *e, const zd *src);
 int mixed_status(afqmc_engine *e);
 int mixed_pop_control(afqmc_engine *e);

@@ -122,6 +122,14 @@ int afqmc_get_walkers(afqmc_engine *e, double *wf, double *logw, int *alive);
  * (afqmc_upload_wait, or any call that synchronizes the engine's stream after
  * the install).  The first call allocates two device staging slots. */
 int afqmc_set_walkers_async(afqmc_engine *e, const double *wf, const double *logw, const int *alive);
+/* The same asynchronous upload for the phaseless mixed form with the walkers
+ * already in its fp32 layout: per walker 2 n Ncol floats, the real parts
+ * (n x Ncol, column-major) then the imaginary parts; the form keeps its
+ * walkers in that layout, so this moves half the bytes of the FP64 upload.
+ * Other engines return AFQMC_ERR_UNSUPPORTED.  The first call allocates two
+ * fp32 staging slots.  (SD2is::read/write carry complex doubles; the
+ * difference is only the upload format.) */
+int afqmc_set_walkers_f32_async(afqmc_engine *e, const float *wf32, const double *logw, const int *alive);
 int afqmc_upload_wait(afqmc_engine *e);
 
 /* Counter-based random stream: replaces randomHaoInit/randomHaoSave/Read

@@ -79,3 +79,51 @@ def test_async_upload_overlaps_running_step():
     assert np.array_equal(got[2], al)
     # the mixed form keeps fp32 walkers: the round trip is exact to fp32
     np.testing.assert_allclose(got[0], wf, rtol=0, atol=1e-6)
+
+
+def _fp32_planes(wf):
+    """The phaseless mixed form's walker layout: per walker the real parts of
+    the n x ncol matrix (column-major), then the imaginary parts, as fp32."""
+    n, ncol, nw = wf.shape
+    out = np.empty((nw, 2, n * ncol), np.float32)
+    for w in range(nw):
+        flat = wf[:, :, w].reshape(-1, order="F")
+        out[w, 0] = flat.real.astype(np.float32)
+        out[w, 1] = flat.imag.astype(np.float32)
+    return out.reshape(-1)
+
+
+def test_fp32_upload_installs_the_same_population():
+    """afqmc_set_walkers_f32_async with the walkers in the mixed form's fp32
+    layout installs bit for bit what afqmc_set_walkers installs from complex
+    doubles (the same fp32 rounding), and the steps that follow agree exactly;
+    the FP64 form rejects it."""
+    pops = [_pinned_population(_engine(capi.AFQMC_FP64)[1], seed) for seed in (6, 7)]
+    ref = []
+    e, _ = _engine(capi.AFQMC_MIXED)
+    for (wf, lw, al), _h in pops:
+        e.set_walkers(wf, lw, al)
+        e.step(2)
+        ref.append((e.get_walkers(), e.log_overlaps()))
+    e.close()
+
+    got = []
+    e, _ = _engine(capi.AFQMC_MIXED)
+    for (wf, lw, al), h in pops:
+        h32 = torch.from_numpy(_fp32_planes(wf)).pin_memory()
+        e.set_walkers_f32_async(h32.data_ptr(), h[1].data_ptr(), h[2].data_ptr())
+        e.step(2)
+        got.append((e.get_walkers(), e.log_overlaps()))
+        e.upload_wait()
+    e.close()
+    for (w_ref, lo_ref), (w_got, lo_got) in zip(ref, got):
+        for a, b in zip(w_ref, w_got):
+            assert np.array_equal(a, b)
+        assert np.array_equal(lo_ref, lo_got)
+
+    f, m = _engine(capi.AFQMC_FP64)
+    (wf, lw, al), h = pops[0]
+    h32 = torch.from_numpy(_fp32_planes(wf)).pin_memory()
+    with pytest.raises(capi.AfqmcError):
+        f.set_walkers_f32_async(h32.data_ptr(), h[1].data_ptr(), h[2].data_ptr())
+    f.close()
