@@ -1873,15 +1873,32 @@ cp_energy_kernel(int W, HubbardDev h, const zd *wfDaggerK, const zd *thetaT, lon
     zd *st = sites + (size_t)w * 4 * L;
     zd K = make_double2(0, 0), V = make_double2(0, 0), R = make_double2(0, 0);
     for (int e = threadIdx.x; e < N * n; e += blockDim.x) zfma(K, wfDaggerK[e], th[e]);
-    for (int i = threadIdx.x; i < L; i += blockDim.x) {
+    // P adjacent lanes per site, lane p taking j = p, p + P, ...: the loads of a
+    // site come in runs of P entries and each sum is N / P long; the P
+    // partial sums meet in a shuffle tree
+    const int P = L >= 256 ? 1 : L >= 128 ? 2 : L >= 64 ? 4 : 8;
+    const int part = threadIdx.x % P;
+    const int sitesPerPass = blockDim.x / P;
+    for (int i0 = 0; i0 < L; i0 += sitesPerPass) {
+        const int i = i0 + threadIdx.x / P;
+        const bool site = i < L;   // uniform over each lane group of P
         zd gi = make_double2(0, 0), gL = make_double2(0, 0), oi = make_double2(0, 0), oL = make_double2(0, 0);
-        for (int j = 0; j < N; ++j) {
-            zd pi = zconj(h.phiT[i + (size_t)n * j]), pL = zconj(h.phiT[i + L + (size_t)n * j]);
-            zfma(gi, pi, th[j + (size_t)N * i]);
-            zfma(gL, pL, th[j + (size_t)N * (i + L)]);
-            zfma(oi, pi, th[j + (size_t)N * (i + L)]);
-            zfma(oL, pL, th[j + (size_t)N * i]);
+        if (site) {
+            for (int j = part; j < N; j += P) {
+                zd pi = zconj(h.phiT[i + (size_t)n * j]), pL = zconj(h.phiT[i + L + (size_t)n * j]);
+                zfma(gi, pi, th[j + (size_t)N * i]);
+                zfma(gL, pL, th[j + (size_t)N * (i + L)]);
+                zfma(oi, pi, th[j + (size_t)N * (i + L)]);
+                zfma(oL, pL, th[j + (size_t)N * i]);
+            }
         }
+        for (int o = 1; o < P; o <<= 1) {
+            gi.x += __shfl_xor_sync(0xffffffffu, gi.x, o); gi.y += __shfl_xor_sync(0xffffffffu, gi.y, o);
+            gL.x += __shfl_xor_sync(0xffffffffu, gL.x, o); gL.y += __shfl_xor_sync(0xffffffffu, gL.y, o);
+            oi.x += __shfl_xor_sync(0xffffffffu, oi.x, o); oi.y += __shfl_xor_sync(0xffffffffu, oi.y, o);
+            oL.x += __shfl_xor_sync(0xffffffffu, oL.x, o); oL.y += __shfl_xor_sync(0xffffffffu, oL.y, o);
+        }
+        if (!site || part != 0) continue;
         st[i] = gi;
         st[i + L] = gL;
         st[i + 2 * L] = oi;
