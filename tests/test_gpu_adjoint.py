@@ -3,7 +3,9 @@
 (n=64, 16+16 electrons): the energy and the one-body derivative against the
 oracle (the den-weighted mixed Green's function of the reference's
 SD2sSD2isOperation), every derivative against central finite differences
-(step 1e-6, FP64) along random directions.
+(step 1e-6, FP64) along random directions; a small population after 3 steps,
+and the configuration's own size (L=320 Cholesky vectors, 512 walkers after
+200 steps).
 
 Tolerances: 1e-10 relative against the oracle; 1e-6 relative against the
 finite differences."""
@@ -112,3 +114,61 @@ def test_autograd_wrapper_backward(setup):
     fdz, _ = _fd(actx, [m.t, m.chol, m.phiTUp, m.phiTDn], 2, dz)
     got = float(np.real(np.sum(np.conj(pu.grad.numpy()) * dz)))
     assert abs(np.real(fdz) - got) <= FD_TOL * abs(np.real(fdz))
+
+
+
+def _fd_richardson(actx, base, which, direction, h=1e-4):
+    """Central differences at h and h/2 combined as (4 D(h/2) - D(h)) / 3:
+    truncation O(h^4), rounding about eps |f| / h."""
+    def central(step):
+        plus = [a.copy() for a in base]
+        minus = [a.copy() for a in base]
+        plus[which] = plus[which] + step * direction
+        minus[which] = minus[which] - step * direction
+        ep = actx.evaluate(*plus, want_chol=False)
+        em = actx.evaluate(*minus, want_chol=False)
+        return np.array([(ep["E"] - em["E"]) / (2 * step), (ep["mean_logov"] - em["mean_logov"]) / (2 * step)])
+
+    d1, d2 = central(h), central(h / 2)
+    return (4 * d2 - d1) / 3
+
+
+def test_adjoint_at_the_configuration_size():
+    """The adjoint configuration as stated: n=64, 16+16 electrons, 320
+    Cholesky vectors, 512 walkers after 200 steps (Gram-Schmidt and
+    population control every 10): energy and density matrix against the
+    oracle (1e-10), every derivative class against Richardson-extrapolated
+    central differences (1e-6).  After 200 steps the weights have spread and
+    the estimator's curvature along a random direction makes a plain central
+    difference at step 1e-6 err by about 1e-6 relative; the extrapolation
+    removes that truncation error."""
+    m = inputs.molecule_inputs(64, 16, 16, 320, dt=0.005, decay=60.0, seed=13)
+    m.ET = -20.0
+    W = 512
+    eng = capi.pl_engine(m, W, 17, 10, 10)
+    eng.set_walkers(*inputs.initial_walkers(m.phiTUp, W, seed=19, noise=0.03))
+    eng.step(200)
+    assert eng.status() == 0
+    walkers = eng.get_walkers()
+    eng.close()
+    actx = adjoint.AdjointContext(m, walkers)
+    test_energy_and_density_matrix_match_oracle((m, walkers, actx))
+
+    base = [m.t.copy(), m.chol.copy(), m.phiTUp.copy(), m.phiTDn.copy()]
+    out = actx.evaluate(*base)
+    rng = np.random.default_rng(101)
+    d = rng.standard_normal(m.t.shape)
+    fdE, _ = _fd_richardson(actx, base, 0, d)
+    an = np.sum(out["dE_dt"] * d)
+    assert abs(fdE - an) <= FD_TOL * abs(an)
+    d = rng.standard_normal(m.chol.shape)
+    fdE, _ = _fd_richardson(actx, base, 1, d)
+    an = np.sum(out["dE_dchol"] * d)
+    assert abs(fdE - an) <= FD_TOL * abs(an)
+    for s in (0, 1):
+        d = rng.standard_normal(base[2 + s].shape) + 1j * rng.standard_normal(base[2 + s].shape)
+        fdE, fdL = _fd_richardson(actx, base, 2 + s, d)
+        anE = np.sum(out["dE_dconj_phiT"][s] * np.conj(d))
+        anL = np.sum(out["dlogov_dconj_phiT"][s] * np.conj(d))
+        assert abs(fdE - anE) <= FD_TOL * abs(anE), (s, fdE, anE)
+        assert abs(fdL - anL) <= FD_TOL * abs(anL), (s, fdL, anL)
