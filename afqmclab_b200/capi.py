@@ -344,18 +344,28 @@ class Engine:
         _check(lib().afqmc_profile_get(self.h, _p(ms), _p(cnt)))
         return {PHASES[i]: (float(ms[i]), int(cnt[i])) for i in range(len(PHASES))}
 
-    def adjoint(self, want_chol=True):
-        """Mixed local energy, mean log-overlap and their gradients (afqmc_pl_adjoint)."""
+    def adjoint(self, want_chol=True, chol_out=None):
+        """Mixed local energy, mean log-overlap and their gradients (afqmc_pl_adjoint).
+        chol_out: optional complex128 torch tensor of n*n*G elements on the
+        engine's GPU that receives dE/dL_g (column-major n x n x G) in place of
+        a host array; the result's "dE_dchol" is then that tensor."""
         n, G, nu, nd = self.n, self.G, self.nup, self.ndn
         E = np.zeros(1, np.complex128)
         L = np.zeros(1, np.complex128)
         dt = np.zeros((n, n), np.complex128, order="F")
-        dc = np.zeros((n, n, G), np.complex128, order="F") if want_chol else None
+        if chol_out is not None:
+            if not chol_out.is_cuda or chol_out.numel() != n * n * G or not chol_out.is_contiguous() \
+                    or str(chol_out.dtype) != "torch.complex128":
+                raise AfqmcError("chol_out must be a contiguous complex128 CUDA tensor of n*n*G elements")
+            dc = chol_out
+        else:
+            dc = np.zeros((n, n, G), np.complex128, order="F") if want_chol else None
         du = np.zeros((n, nu), np.complex128, order="F")
         dd = np.zeros((n, max(nd, 1)), np.complex128, order="F")
         lu = np.zeros((n, nu), np.complex128, order="F")
         ld = np.zeros((n, max(nd, 1)), np.complex128, order="F")
-        _check(lib().afqmc_pl_adjoint(self.h, _p(E), _p(L), _p(dt), _p(dc), _p(du),
+        dcp = ctypes.c_void_p(dc.data_ptr()) if chol_out is not None else _p(dc)
+        _check(lib().afqmc_pl_adjoint(self.h, _p(E), _p(L), _p(dt), dcp, _p(du),
                                       _p(dd) if nd else None, _p(lu), _p(ld) if nd else None))
         return {"E": E[0], "mean_logov": L[0], "dE_dt": dt, "dE_dchol": dc,
                 "dE_dconj_phiT": (du, dd[:, :nd]), "dlogov_dconj_phiT": (lu, ld[:, :nd])}

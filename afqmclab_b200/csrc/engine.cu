@@ -650,7 +650,10 @@ void free_engine(afqmc_engine *e)
 // half step of addMixedMeasurement: logov, Sinv, thetaT, xbar, ex, eloc, den
 // (FP64 arithmetic; the mixed form's fp32 walkers are read through the FP64
 // copy).  Used by the adjoint.
-int engine_pl_local_energy(afqmc_engine *e)
+// exchange: PL_EX_BLOCKWISE the per-walker kernel over both spin blocks;
+// PL_EX_GEMM_ONE the FP64 GEMM form over block 0 counted twice (a restricted
+// trial); PL_EX_GEMM_ALL the GEMM form over every block.
+int engine_pl_local_energy(afqmc_engine *e, int exchange)
 {
     const int W = e->W;
     cudaStream_t s = e->stream;
@@ -662,6 +665,21 @@ int engine_pl_local_energy(afqmc_engine *e)
     TRY(check_launch());
     TRY(theta_gemm(e, e->wf, e->alive, e->bl));
     TRY(xbar_gemm(e, e->bl));
+    if (exchange != PL_EX_BLOCKWISE) {
+        if (!e->exf || !e->exf->gemm) return fail(AFQMC_ERR_STATE, "GEMM exchange not set up");
+        const bool one = exchange == PL_EX_GEMM_ONE;
+        if (one && !e->exf->restricted) return fail(AFQMC_ERR_STATE, "trial is not spin-restricted");
+        const int nb = one ? 1 : e->bl.nblk, mult = one ? 2 : 1;
+        bool first = true;
+        for (int b = 0; b < nb; ++b) {
+            if (e->bl.Ns[b] == 0) continue;
+            TRY(exf64_walker_totals(e, exf64_block(e, b), !first, mult));
+            first = false;
+        }
+        launch_pl_energy(W, e->G, e->Ktot, e->wfDaggerT, e->thetaT, e->xbar, e->ex, e->alive, e->logov,
+                         e->eloc, e->den, e->parts, s, e->exf->exTot, one ? e->bl.tOff[1] : e->Ktot, mult);
+        return check_launch();
+    }
     if (launch_pl_exchange(W, e->n, e->G, e->bl, e->Aall, e->Ktot, e->thetaT, e->alive, e->ex, s))
         return fail(AFQMC_ERR_UNSUPPORTED, "exchange kernel supports at most 64 electrons per spin");
     launch_pl_energy(W, e->G, e->Ktot, e->wfDaggerT, e->thetaT, e->xbar, e->ex, e->alive, e->logov,

@@ -145,3 +145,7 @@ int engine_check_launch();
 int engine_gemm(const ZGemmArgs &a, cudaStream_t s);
 template <class T> int engine_dalloc(afqmc_engine *e, T **p, size_t count);
 zd engine_one_body_logw(afqmc_engine *e, int which);
+// Local energy of the phaseless engine at the current walkers (logov, Sinv,
+// thetaT, xbar, eloc, den); the exchange form is one of PL_EX_*.
+enum { PL_EX_BLOCKWISE = 0, PL_EX_GEMM_ONE = 1, PL_EX_GEMM_ALL = 2 };
+int engine_pl_local_energy(afqmc_engine *e, int exchange);

@@ -150,11 +150,18 @@ int exf64_alloc(afqmc_engine *e, long long Kmax, ExF64Scratch &s)
     return AFQMC_OK;
 }
 
-int exf64_run(afqmc_engine *e, const ExF64 &x, bool accumulate, int mult)
+ExF64 exf64_block(const afqmc_engine *e, int b)
+{
+    ExF64 x = e->exf->blk[e->exf->restricted ? 0 : b];
+    x.b = b;
+    return x;
+}
+
+int exf64_walker_totals(afqmc_engine *e, const ExF64 &x, bool accumulate, int mult)
 {
     ExF64Scratch &s = *e->exf;
     const long long K = x.K;
-    const int W = e->W, G = e->G;
+    const int W = e->W;
     const zd *U = e->thetaT + e->bl.tOff[x.b];
     const long long ldu = e->bl.tStride;
     cudaStream_t st = e->stream;
@@ -166,6 +173,33 @@ int exf64_run(afqmc_engine *e, const ExF64 &x, bool accumulate, int mult)
     if ((r = gemm_check(z, st))) return r;
     g_launch_count++;
     ex_walker_dot_kernel<<<W, 256, 0, st>>>(K, U, ldu, s.Z, e->alive, mult, accumulate ? 1 : 0, s.exTot);
+    return engine_check_launch();
+}
+
+int exf64_pair_matrix(afqmc_engine *e, const ExF64 &x, const zd *Uden, const zd *Um)
+{
+    ExF64Scratch &s = *e->exf;
+    const long long K = x.K;
+    ZGemmArgs m;
+    m.m = (int)K; m.n = (int)K; m.k = e->W; m.opA = OP_N; m.opB = OP_T;
+    m.A = Uden; m.lda = K; m.B = Um; m.ldb = K; m.C = s.M; m.ldc = K;
+    int r = gemm_check(m, e->stream);
+    if (r) return r;
+    g_launch_count++;
+    ex_exchange_kernel<<<1184, 256, 0, e->stream>>>(K, x.Ns, s.M, s.R);
+    return engine_check_launch();
+}
+
+int exf64_run(afqmc_engine *e, const ExF64 &x, bool accumulate, int mult)
+{
+    ExF64Scratch &s = *e->exf;
+    const long long K = x.K;
+    const int W = e->W, G = e->G;
+    const zd *U = e->thetaT + e->bl.tOff[x.b];
+    const long long ldu = e->bl.tStride;
+    cudaStream_t st = e->stream;
+    int r;
+    if ((r = exf64_walker_totals(e, x, accumulate, mult))) return r;
     // M = U_den U^T  (U_den into Z)
     g_launch_count++;
     ex_scale_kernel<<<W, 256, 0, st>>>(K, U, ldu, e->logov, e->alive, s.Z);

@@ -28,3 +28,11 @@ int exf64_alloc(afqmc_engine *e, long long Kmax, ExF64Scratch &s);
 int exf64_build(afqmc_engine *e, int b, ExF64 &x);
 // Adds block x's exchange: exTot[w] (+)= mult u^T V u, exNum[g] += mult x_g^T R x_g.
 int exf64_run(afqmc_engine *e, const ExF64 &x, bool accumulate, int mult);
+// The operands of spin block b (block 0's X and V when restricted, which are
+// block 1's too: both blocks carry the same trial).
+ExF64 exf64_block(const afqmc_engine *e, int b);
+// Z = V U (Z(b + Ns i, w) = sum_g (D_gw A_g)(b, i)) and exTot[w] (+)= mult u_w^T Z_w.
+int exf64_walker_totals(afqmc_engine *e, const ExF64 &x, bool accumulate, int mult);
+// M = Uden Um^T (K x K) and its exchange permutation R, R(a + Ns i, b + Ns j) =
+// M(b + Ns i, a + Ns j); Uden, Um are K x W with leading dimension K.
+int exf64_pair_matrix(afqmc_engine *e, const ExF64 &x, const zd *Uden, const zd *Um);

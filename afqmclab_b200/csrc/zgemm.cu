@@ -33,8 +33,11 @@ __device__ __forceinline__ zd load_op(const void *P, long long ld, int i, int l,
     return v;
 }
 
-template <int BM, int BN, int TM, int TN, int OPA, int OPB>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN))
+// REAL: 0 both operands complex (a real operand is loaded as complex with a
+// zero imaginary part), 1 A real, 2 B real, 3 both real; a real operand
+// takes one FP64 multiply-add per real product instead of the complex four.
+template <int BM, int BN, int TM, int TN, int OPA, int OPB, int REAL>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), 2)
 zgemm_kernel(ZGemmArgs a)
 {
     constexpr int NTX = BM / TM;           // threads along rows
@@ -63,6 +66,53 @@ zgemm_kernel(ZGemmArgs a)
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = make_double2(0.0, 0.0);
 
+    // real-operand forms (half the multiply-adds per K-step) fetch the next
+    // K-step's tiles into registers before this step's products and store them
+    // to shared memory after, so the global loads' latency overlaps the
+    // multiply-adds; the complex form has the registers for neither and
+    // stores them before its products
+    constexpr bool STAGE = REAL != 0;
+    constexpr int LA = (BM * BK + NT - 1) / NT, LB = (BN * BK + NT - 1) / NT;
+    zd pa[LA], pb[LB];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int t = 0; t < LA; ++t) {
+            const int e = tid + t * NT;
+            int i, l;
+            if (OPA == OP_N) { i = e % BM; l = e / BM; } else { l = e % BK; i = e / BK; }
+            const int gi = tileM + i, gl = k0 + l;
+            zd v = make_double2(0.0, 0.0);
+            if (e < BM * BK && gi < a.m && gl < a.k) v = load_op<OPA>(Ab, a.lda, gi, gl, a.a_real, a.planeA);
+            pa[t] = v;
+        }
+#pragma unroll
+        for (int t = 0; t < LB; ++t) {
+            const int e = tid + t * NT;
+            int l, j;
+            if (OPB == OP_N) { l = e % BK; j = e / BK; } else { j = e % BN; l = e / BN; }
+            const int gl = k0 + l, gj = tileN + j;
+            zd v = make_double2(0.0, 0.0);
+            if (e < BN * BK && gl < a.k && gj < a.n) v = load_op<OPB>(Bb, a.ldb, gl, gj, a.b_real, a.planeB);
+            pb[t] = v;
+        }
+    };
+    auto commit = [&](int buf) {
+#pragma unroll
+        for (int t = 0; t < LA; ++t) {
+            const int e = tid + t * NT;
+            int i, l;
+            if (OPA == OP_N) { i = e % BM; l = e / BM; } else { l = e % BK; i = e / BK; }
+            if (e < BM * BK) As[buf][l][i] = pa[t];
+        }
+#pragma unroll
+        for (int t = 0; t < LB; ++t) {
+            const int e = tid + t * NT;
+            int l, j;
+            if (OPB == OP_N) { l = e % BK; j = e / BK; } else { j = e % BN; l = e / BN; }
+            if (e < BN * BK) Bs[buf][l][j] = pb[t];
+        }
+    };
+
     auto load_tiles = [&](int buf, int k0) {
         for (int e = tid; e < BM * BK; e += NT) {
             int i, l;
@@ -83,10 +133,17 @@ zgemm_kernel(ZGemmArgs a)
     };
 
     int buf = 0;
-    load_tiles(0, 0);
+    if (STAGE) {
+        fetch(0);
+        commit(0);
+    } else {
+        load_tiles(0, 0);
+    }
     __syncthreads();
     for (int k0 = 0; k0 < a.k; k0 += BK) {
-        if (k0 + BK < a.k) load_tiles(buf ^ 1, k0 + BK);
+        const bool more = k0 + BK < a.k;
+        if (STAGE && more) fetch(k0 + BK);
+        if (!STAGE && more) load_tiles(buf ^ 1, k0 + BK);
 #pragma unroll
         for (int l = 0; l < BK; ++l) {
             zd ra[TM], rb[TN];
@@ -97,8 +154,21 @@ zgemm_kernel(ZGemmArgs a)
 #pragma unroll
             for (int i = 0; i < TM; ++i)
 #pragma unroll
-                for (int j = 0; j < TN; ++j) zfma(acc[i][j], ra[i], rb[j]);
+                for (int j = 0; j < TN; ++j) {
+                    if (REAL == 0) {
+                        zfma(acc[i][j], ra[i], rb[j]);
+                    } else if (REAL == 1) {
+                        acc[i][j].x = fma(ra[i].x, rb[j].x, acc[i][j].x);
+                        acc[i][j].y = fma(ra[i].x, rb[j].y, acc[i][j].y);
+                    } else if (REAL == 2) {
+                        acc[i][j].x = fma(ra[i].x, rb[j].x, acc[i][j].x);
+                        acc[i][j].y = fma(ra[i].y, rb[j].x, acc[i][j].y);
+                    } else {
+                        acc[i][j].x = fma(ra[i].x, rb[j].x, acc[i][j].x);
+                    }
+                }
         }
+        if (STAGE && more) commit(buf ^ 1);
         __syncthreads();
         buf ^= 1;
     }
@@ -132,18 +202,32 @@ zgemm_kernel(ZGemmArgs a)
     }
 }
 
-template <int BM, int BN, int TM, int TN, int OPA, int OPB>
+template <int BM, int BN, int TM, int TN, int OPA, int OPB, int REAL = 0>
 cudaError_t launch3(const ZGemmArgs &a, cudaStream_t s)
 {
     dim3 grid((a.m + BM - 1) / BM, (a.n + BN - 1) / BN, a.batch);
     dim3 block((BM / TM) * (BN / TN));
-    zgemm_kernel<BM, BN, TM, TN, OPA, OPB><<<grid, block, 0, s>>>(a);
+    zgemm_kernel<BM, BN, TM, TN, OPA, OPB, REAL><<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int BM, int BN, int TM, int TN, int OPA, int OPB>
+cudaError_t launch_real(const ZGemmArgs &a, cudaStream_t s)
+{
+    const int real = (a.a_real == ST_R64 ? 1 : 0) | (a.b_real == ST_R64 ? 2 : 0);
+    if (real == 1) return launch3<BM, BN, TM, TN, OPA, OPB, 1>(a, s);
+    if (real == 2) return launch3<BM, BN, TM, TN, OPA, OPB, 2>(a, s);
+    if (real == 3) return launch3<BM, BN, TM, TN, OPA, OPB, 3>(a, s);
+    return launch3<BM, BN, TM, TN, OPA, OPB, 0>(a, s);
 }
 
 template <int BM, int BN, int TM, int TN>
 cudaError_t launch2(const ZGemmArgs &a, cudaStream_t s)
 {
+    // the operator pairs that real operands come with take the real forms
+    if (a.opA == OP_N && a.opB == OP_N) return launch_real<BM, BN, TM, TN, OP_N, OP_N>(a, s);
+    if (a.opA == OP_N && a.opB == OP_T) return launch_real<BM, BN, TM, TN, OP_N, OP_T>(a, s);
+    if (a.opA == OP_C && a.opB == OP_N) return launch_real<BM, BN, TM, TN, OP_C, OP_N>(a, s);
 #define ZG_CASE(OA, OB) \
     if (a.opA == OA && a.opB == OB) return launch3<BM, BN, TM, TN, OA, OB>(a, s);
     ZG_CASE(OP_N, OP_N) ZG_CASE(OP_N, OP_T) ZG_CASE(OP_N, OP_C)

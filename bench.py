@@ -415,7 +415,11 @@ def bench_adjoint(args, capi, inputs, torch, rank, world):
     eng.step(3)
     eng.synchronize()
     reps = max(1, args.steps // 50)
-    eng.adjoint()           # warm-up (allocations, first launches)
+    n, G, N = m.n, m.G, m.nup + m.ndn
+    # dE/dL_g (n x n x G complex, 1.3 GB at n=256) stays in HBM as a torch
+    # tensor; the other outputs are host arrays
+    dchol = torch.empty(n * n * G, dtype=torch.complex128, device="cuda")
+    eng.adjoint(chol_out=dchol)   # warm-up (allocations, first launches)
     eng.synchronize()
     clocks = ClockSampler(torch.cuda.current_device())
     clocks.start()
@@ -423,20 +427,20 @@ def bench_adjoint(args, capi, inputs, torch, rank, world):
     t0 = time.perf_counter()
     out = None
     for _ in range(reps):
-        out = eng.adjoint()
+        out = eng.adjoint(chol_out=dchol)
     eng.synchronize()
     dt = time.perf_counter() - t0
     clk = clocks.stop()
-    n, G, N = m.n, m.G, m.nup + m.ndn
     line = {"metric": "walker adjoint evaluations/s (E, dE/dt, dE/dL_g, dE/dconj(phiT)), FP64",
             "value": W * reps / dt, "unit": "walker-evaluations/s", "n_gpus": world, "steps": reps,
             "warmup": 1, "ms_per_step": dt / reps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "adjoint", "model": name, "n_orbitals": n, "electrons": [m.nup, m.ndn],
-                       "cholesky": G, "walkers": W, "timing": "host wall clock around synchronous calls"},
+                       "cholesky": G, "walkers": W, "timing": "host wall clock around synchronous calls",
+                       "outputs": "dE/dL_g into a CUDA tensor, the rest to host arrays"},
             "energy": [float(out["E"].real), float(out["E"].imag)],
             "gradient_norms": {"dE_dt": float(np.abs(out["dE_dt"]).max()),
-                               "dE_dchol": float(np.abs(out["dE_dchol"]).max())},
+                               "dE_dchol": float(dchol.abs().max())},
             "clocks": clk}
     if rank == 0:
         print(json.dumps(line), flush=True)

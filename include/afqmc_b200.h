@@ -245,6 +245,9 @@ int afqmc_pl_rebuild_propagators(afqmc_engine *e, const double *K);
  * Outputs (host, complex, column-major, any may be NULL): energy (1),
  * mean_logov (1), dE_dt (n x n), dE_dchol (n x n x G), dE_dconj_phiT_up
  * (n x Nup), dE_dconj_phiT_dn (n x Ndn), dLogov_dconj_phiT_up/dn.
+ * dE_dchol may instead be device memory of the engine's GPU (found by
+ * cudaPointerGetAttributes): the gradient is then written there directly,
+ * with no copy to the host.
  * FP64; determinants and D_g are recomputed per walker, nothing is stored. */
 int afqmc_pl_adjoint(afqmc_engine *e, double *energy, double *mean_logov, double *dE_dt,
                      double *dE_dchol, double *dE_dconj_phiT_up, double *dE_dconj_phiT_dn,

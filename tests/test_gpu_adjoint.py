@@ -117,6 +117,59 @@ def test_autograd_wrapper_backward(setup):
 
 
 
+def _compare_forms(actx_real, actx_phase, m, phase):
+    """The GEMM form (real trial) against the per-walker form (the same trial
+    times a global phase c, which makes the half-rotated vectors complex): E,
+    dE/dt and dE/dL_g are invariant under the phase and the orbital gradient
+    rotates by c (dE/dconj(c phiT) = c dE/dconj(phiT))."""
+    base = [m.t.copy(), m.chol.copy(), m.phiTUp.copy(), m.phiTDn.copy()]
+    a = actx_real.evaluate(*base)
+    b = actx_phase.evaluate(base[0], base[1], phase * base[2], phase * base[3])
+    assert abs(a["E"] - b["E"]) < 1e-10 * abs(a["E"])
+    for key in ("dE_dt", "dE_dchol"):
+        assert np.abs(a[key] - b[key]).max() < 1e-9 * np.abs(a[key]).max(), key
+    for s in (0, 1):
+        ga, gb = phase * a["dE_dconj_phiT"][s], b["dE_dconj_phiT"][s]
+        assert np.abs(ga - gb).max() < 1e-9 * np.abs(ga).max(), s
+        la, lb = phase * a["dlogov_dconj_phiT"][s], b["dlogov_dconj_phiT"][s]
+        assert np.abs(la - lb).max() < 1e-9 * np.abs(la).max(), s
+
+
+def test_gemm_and_per_walker_forms_agree(setup):
+    """Every evaluation form on the same walkers: a restricted trial (block 0
+    counted twice) and an unrestricted real trial (each block its own
+    operands), each against the per-walker form."""
+    m, walkers, actx = setup
+    phase = np.exp(0.3j)
+    _compare_forms(actx, actx, m, phase)
+    rng = np.random.default_rng(7)
+    m3 = inputs.molecule_inputs(64, 16, 16, 64, dt=0.005, decay=20.0, seed=11)
+    m3.ET = -20.0
+    q, _ = np.linalg.qr(m3.phiTDn.real + 0.1 * rng.standard_normal(m3.phiTDn.shape))
+    m3.phiTDn = np.asfortranarray(q.astype(np.complex128))
+    assert not np.allclose(m3.phiTDn, m3.phiTUp)
+    actx3 = adjoint.AdjointContext(m3, walkers)
+    _compare_forms(actx3, actx3, m3, phase)
+
+
+def test_chol_gradient_into_device_memory(setup):
+    """dE/dL_g written straight into a CUDA tensor equals the host copy."""
+    m, walkers, actx = setup
+    eng = capi.pl_engine(m, walkers[0].shape[2], 1, precision=capi.AFQMC_FP64)
+    try:
+        eng.set_walkers(*walkers)
+        host = eng.adjoint()
+        dev = torch.zeros(m.n * m.n * m.G, dtype=torch.complex128, device="cuda")
+        out = eng.adjoint(chol_out=dev)
+        got = dev.cpu().numpy().reshape((m.n, m.n, m.G), order="F")
+        assert np.array_equal(got, host["dE_dchol"])
+        assert out["E"] == host["E"]
+        with pytest.raises(capi.AfqmcError):
+            eng.adjoint(chol_out=torch.zeros(3, dtype=torch.complex128, device="cuda"))
+    finally:
+        eng.close()
+
+
 def _fd_richardson(actx, base, which, direction, h=1e-4):
     """Central differences at h and h/2 combined as (4 D(h/2) - D(h)) / 3:
     truncation O(h^4), rounding about eps |f| / h."""
