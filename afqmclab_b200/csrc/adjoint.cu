@@ -568,38 +568,40 @@ extern "C" int afqmc_pl_adjoint(afqmc_engine *e, double *energy, double *mean_lo
     else if (form == PL_EX_GEMM_ONE) r = adjoint_gemm(c, 1, 2);
     else r = adjoint_gemm(c, e->bl.nblk, 1);
     if (r) return r;
+    // dE/dt = sum_s conj(phiT_s) R_s^T / sum den (n x n; R_s^T is Rt's block)
+    zd *dEdt = nullptr;
+    if (dE_dt) {
+        zd *cT;
+        ACK(bufs.get(&dEdt, (size_t)n * n));
+        ACK(bufs.get(&cT, (size_t)n * std::max(e->bl.Ns[0], e->bl.Ns[1])));
+        bool first = true;
+        for (int sb = 0; sb < e->bl.nblk; ++sb) {
+            const int Ns = e->bl.Ns[sb];
+            if (Ns == 0) continue;
+            adj_conj_kernel<<<64, 256, 0, s>>>((long long)n * Ns, e->phiT[sb], cT);
+            ACK(cudaGetLastError());
+            ZGemmArgs g;
+            g.m = n; g.n = n; g.k = Ns;
+            g.A = cT; g.lda = n; g.B = Rt + e->bl.tOff[sb]; g.ldb = Ns; g.C = dEdt; g.ldc = n;
+            g.alpha = invDen;
+            g.beta = first ? make_double2(0.0, 0.0) : make_double2(1.0, 0.0);
+            r = engine_gemm(g, s);
+            if (r) return r;
+            first = false;
+        }
+        if (first) ACK(cudaMemsetAsync(dEdt, 0, sizeof(zd) * (size_t)n * n, s));
+    }
 
     // gradients to the host
-    std::vector<zd> hR(Ktot), hS(Ktot), hpT0((size_t)n * e->bl.Ns[0]), hpT1;
+    std::vector<zd> hS(Ktot);
     std::vector<double> hG(2 * Ktot);
-    ACK(cudaMemcpyAsync(hR.data(), Rt, sizeof(zd) * Ktot, cudaMemcpyDeviceToHost, s));
     ACK(cudaMemcpyAsync(hS.data(), St, sizeof(zd) * Ktot, cudaMemcpyDeviceToHost, s));
     ACK(cudaMemcpyAsync(hG.data(), gradT, sizeof(double) * 2 * Ktot, cudaMemcpyDeviceToHost, s));
-    ACK(cudaMemcpyAsync(hpT0.data(), e->phiT[0], sizeof(zd) * hpT0.size(), cudaMemcpyDeviceToHost, s));
-    if (e->bl.nblk > 1) {
-        hpT1.resize((size_t)n * e->bl.Ns[1]);
-        ACK(cudaMemcpyAsync(hpT1.data(), e->phiT[1], sizeof(zd) * hpT1.size(), cudaMemcpyDeviceToHost, s));
-    }
+    if (dEdt) ACK(cudaMemcpyAsync(dE_dt, dEdt, sizeof(zd) * (size_t)n * n, cudaMemcpyDeviceToHost, s));
     if (dchol && !cholDev)
         ACK(cudaMemcpyAsync(dE_dchol, dchol, sizeof(zd) * (size_t)n * n * G, cudaMemcpyDeviceToHost, s));
     ACK(cudaStreamSynchronize(s));
 #undef ACK
-    const std::vector<zd> *pT[2] = {&hpT0, &hpT1};
-    // dE/dt(i,j) = sum_s sum_b R_s(j,b) conj(phiT_s(i,b)) / sum den   (R_s(j,b) = Rt(b,j))
-    if (dE_dt) {
-        for (int j = 0; j < n; ++j)
-            for (int i = 0; i < n; ++i) {
-                zd v = make_double2(0, 0);
-                for (int sb = 0; sb < e->bl.nblk; ++sb) {
-                    const int Ns = e->bl.Ns[sb];
-                    for (int b = 0; b < Ns; ++b)
-                        zfma(v, hR[e->bl.tOff[sb] + b + (size_t)Ns * j], zconj((*pT[sb])[i + (size_t)n * b]));
-                }
-                v = zmul(v, invDen);
-                dE_dt[2 * (i + (size_t)n * j)] = v.x;
-                dE_dt[2 * (i + (size_t)n * j) + 1] = v.y;
-            }
-    }
     // orbital gradients: transpose the (N x n) accumulators to n x N; with
     // block 0 counted twice, block 1's energy gradient is block 0's
     double *outE[2] = {dE_dconj_phiT_up, dE_dconj_phiT_dn};
