@@ -58,7 +58,12 @@ zgemm_kernel(ZGemmArgs a)
     __shared__ zd Bs[2][BK][BN];
 
     const int tid = threadIdx.x;
-    const int tx = tid % NTX, ty = tid / NTX;
+    // a warp covers 8 row and 4 column positions of the 16 x 16 thread grid,
+    // so each operand fragment load touches 8 (A) or 4 (B) distinct 16-byte
+    // words: one shared-memory wavefront each
+    static_assert(NTX == 16 && NT == 256, "16 x 16 thread grid");
+    const int warp = tid >> 5, lane = tid & 31;
+    const int tx = (warp & 1) * 8 + (lane & 7), ty = (warp >> 1) * 4 + (lane >> 3);
 
     zd acc[TM][TN];
 #pragma unroll
