@@ -80,14 +80,16 @@ ex_scale_kernel(long long K, const zd *U, long long ldu, const zd *logov, const 
     for (long long q = threadIdx.x; q < K; q += blockDim.x) o[q] = zmul(d, u[q]);
 }
 
-// R(a + Ns i, b + Ns j) = M(b + Ns i, a + Ns j)
+// R(a + Ns i, b + Ns j) = M(b + Ns i, a + Ns j); M is symmetric and only its
+// lower triangle (row >= column) is read
 __global__ void ex_exchange_kernel(long long K, int Ns, const zd *M, zd *R)
 {
     for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < K * K;
          e += (long long)gridDim.x * blockDim.x) {
         const long long q1 = e % K, q2 = e / K;
         const long long a = q1 % Ns, i = q1 / Ns, b = q2 % Ns, j = q2 / Ns;
-        R[e] = M[(size_t)(b + Ns * i) + (size_t)K * (a + Ns * j)];
+        const long long r = b + Ns * i, c = a + Ns * j;
+        R[e] = r >= c ? M[(size_t)r + (size_t)K * c] : M[(size_t)c + (size_t)K * r];
     }
 }
 
@@ -183,6 +185,7 @@ int exf64_pair_matrix(afqmc_engine *e, const ExF64 &x, const zd *Uden, const zd 
     ZGemmArgs m;
     m.m = (int)K; m.n = (int)K; m.k = e->W; m.opA = OP_N; m.opB = OP_T;
     m.A = Uden; m.lda = K; m.B = Um; m.ldb = K; m.C = s.M; m.ldc = K;
+    m.lower = 1;   // M = sum_w den_w u_w u_w^T is symmetric
     int r = gemm_check(m, e->stream);
     if (r) return r;
     g_launch_count++;
@@ -206,6 +209,7 @@ int exf64_run(afqmc_engine *e, const ExF64 &x, bool accumulate, int mult)
     ZGemmArgs m;
     m.m = (int)K; m.n = (int)K; m.k = W; m.opA = OP_N; m.opB = OP_T;
     m.A = s.Z; m.lda = K; m.B = U; m.ldb = ldu; m.C = s.M; m.ldc = K;
+    m.lower = 1;   // M = sum_w den_w u_w u_w^T is symmetric
     if ((r = gemm_check(m, st))) return r;
     g_launch_count++;
     ex_exchange_kernel<<<1184, 256, 0, st>>>(K, x.Ns, s.M, s.R);

@@ -47,6 +47,7 @@ zgemm_kernel(ZGemmArgs a)
     if (a.skip && a.skip[b] != 0) return;
     const int tileM = blockIdx.x * BM, tileN = blockIdx.y * BN;
     if (tileM >= a.m || tileN >= a.n) return;
+    if (a.lower && tileM + BM <= tileN) return;
 
     const size_t esA = a.a_real == ST_R64 ? sizeof(double) : a.a_real == ST_C32P ? sizeof(float) : sizeof(zd);
     const size_t esB = a.b_real == ST_R64 ? sizeof(double) : a.b_real == ST_C32P ? sizeof(float) : sizeof(zd);

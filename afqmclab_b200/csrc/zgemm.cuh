@@ -24,6 +24,9 @@ struct ZGemmArgs {
     int batch = 1;
     const int *mask = nullptr;     // skip batch b when mask[b] == 0
     const int *skip = nullptr;     // skip batch b when skip[b] != 0
+    // symmetric product (m = n): only output tiles that meet the lower
+    // triangle (row >= column) are computed; tiles above it are not written
+    int lower = 0;
     // complex f32 planar operands: imaginary plane at +planeA/+planeB floats
     // (set a_real/b_real = 2 to select them; 1 = real f64 as before)
     long long planeA = 0, planeB = 0;
