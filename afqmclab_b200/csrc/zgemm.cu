@@ -37,7 +37,7 @@ __device__ __forceinline__ zd load_op(const void *P, long long ld, int i, int l,
 // zero imaginary part), 1 A real, 2 B real, 3 both real; a real operand
 // takes one FP64 multiply-add per real product instead of the complex four.
 template <int BM, int BN, int TM, int TN, int OPA, int OPB, int REAL>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN), 2)
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), TM * TN > 16 ? 1 : 2)
 zgemm_kernel(ZGemmArgs a)
 {
     constexpr int NTX = BM / TM;           // threads along rows
@@ -252,7 +252,31 @@ cudaError_t launch2(const ZGemmArgs &a, cudaStream_t s)
 // outside stream capture; captured launches reuse the cached choice.
 namespace {
 
-constexpr int NCAND = 4;
+constexpr int NCAND = 5;
+
+int real_form(const ZGemmArgs &a)
+{
+    if (a.opA != OP_N || (a.opB != OP_N && a.opB != OP_T)) return 0;
+    return (a.a_real == ST_R64 ? 1 : 0) | (a.b_real == ST_R64 ? 2 : 0);
+}
+
+// Wide thread tiles for one real operand: a thread's A (B) values cost four
+// shared-memory wavefronts per complex and two per real value and K-column,
+// so 4 x 8 (complex A, real B) and 8 x 4 (real A, complex B) give 64 FP64
+// FMAs per 32 wavefronts, twice the 4 x 4 form's 32 per 24.
+cudaError_t launch_wide_real(const ZGemmArgs &a, cudaStream_t s)
+{
+    const int real = real_form(a);
+    if (real == 2) {
+        if (a.opB == OP_N) return launch3<64, 128, 4, 8, OP_N, OP_N, 2>(a, s);
+        return launch3<64, 128, 4, 8, OP_N, OP_T, 2>(a, s);
+    }
+    if (real == 1) {
+        if (a.opB == OP_N) return launch3<128, 64, 8, 4, OP_N, OP_N, 1>(a, s);
+        return launch3<128, 64, 8, 4, OP_N, OP_T, 1>(a, s);
+    }
+    return launch2<64, 64, 4, 4>(a, s);
+}
 
 cudaError_t launch_cand(int c, const ZGemmArgs &a, cudaStream_t s)
 {
@@ -260,7 +284,8 @@ cudaError_t launch_cand(int c, const ZGemmArgs &a, cudaStream_t s)
     case 0: return launch2<32, 32, 2, 2>(a, s);
     case 1: return launch2<32, 64, 2, 4>(a, s);
     case 2: return launch2<64, 64, 4, 4>(a, s);
-    default: return launch2<128, 32, 8, 2>(a, s);
+    case 3: return launch2<128, 32, 8, 2>(a, s);
+    default: return launch_wide_real(a, s);
     }
 }
 
@@ -268,6 +293,8 @@ int default_cand(const ZGemmArgs &a)
 {
     if (a.m <= 32 && a.n <= 32) return 0;
     if (a.m <= 32) return 1;
+    const int real = real_form(a);
+    if ((real == 1 || real == 2) && a.m >= 128 && a.n >= 128) return 4;
     return 2;
 }
 
