@@ -234,6 +234,7 @@ cudaError_t launch2(const ZGemmArgs &a, cudaStream_t s)
     if (a.opA == OP_N && a.opB == OP_N) return launch_real<BM, BN, TM, TN, OP_N, OP_N>(a, s);
     if (a.opA == OP_N && a.opB == OP_T) return launch_real<BM, BN, TM, TN, OP_N, OP_T>(a, s);
     if (a.opA == OP_C && a.opB == OP_N) return launch_real<BM, BN, TM, TN, OP_C, OP_N>(a, s);
+    if (a.opA == OP_T && a.opB == OP_N) return launch_real<BM, BN, TM, TN, OP_T, OP_N>(a, s);
 #define ZG_CASE(OA, OB) \
     if (a.opA == OA && a.opB == OB) return launch3<BM, BN, TM, TN, OA, OB>(a, s);
     ZG_CASE(OP_N, OP_N) ZG_CASE(OP_N, OP_T) ZG_CASE(OP_N, OP_C)
