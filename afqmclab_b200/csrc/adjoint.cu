@@ -550,10 +550,13 @@ extern "C" int afqmc_pl_adjoint(afqmc_engine *e, double *energy, double *mean_lo
         cudaPointerAttributes pa{};
         int dev = -1;
         ACK(cudaGetDevice(&dev));
-        if (cudaPointerGetAttributes(&pa, dE_dchol) == cudaSuccess)
-            cholDev = pa.type == cudaMemoryTypeDevice && pa.device == dev;
-        else
+        if (cudaPointerGetAttributes(&pa, dE_dchol) == cudaSuccess) {
+            if (pa.type == cudaMemoryTypeDevice && pa.device != dev)
+                return engine_fail(AFQMC_ERR_ARG, "dE_dchol is device memory of another GPU");
+            cholDev = pa.type == cudaMemoryTypeDevice;
+        } else {
             cudaGetLastError();
+        }
         if (cholDev) dchol = (zd *)dE_dchol;
         else ACK(bufs.get(&dchol, (size_t)n * n * G));
     }

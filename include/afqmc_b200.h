@@ -247,7 +247,7 @@ int afqmc_pl_rebuild_propagators(afqmc_engine *e, const double *K);
  * (n x Nup), dE_dconj_phiT_dn (n x Ndn), dLogov_dconj_phiT_up/dn.
  * dE_dchol may instead be device memory of the engine's GPU (found by
  * cudaPointerGetAttributes): the gradient is then written there directly,
- * with no copy to the host.
+ * with no copy to the host (device memory of another GPU: AFQMC_ERR_ARG).
  * FP64; determinants and D_g are recomputed per walker, nothing is stored. */
 int afqmc_pl_adjoint(afqmc_engine *e, double *energy, double *mean_logov, double *dE_dt,
                      double *dE_dchol, double *dE_dconj_phiT_up, double *dE_dconj_phiT_dn,
