@@ -278,26 +278,9 @@ int theta_gemm(afqmc_engine *e, const zd *wf, const int *mask, const Blocks &bl)
 // a closed-shell block list sums block 0's rows and doubles them
 int xbar_gemm(afqmc_engine *e, const Blocks &bl)
 {
-    if (e->exf && e->exf->gemm) {
-        // real half-rotated vectors: the exchange's real X (K x G per block)
-        // in place of the complex-typed Aall, one real x complex GEMM per block
-        bool first = true;
-        for (int b = 0; b < bl.nblk; ++b) {
-            if (bl.Ns[b] == 0) continue;
-            const ExF64 x = exf64_block(e, b);
-            ZGemmArgs g;
-            g.m = e->G; g.n = e->W; g.k = (int)x.K;
-            g.alpha = make_double2((double)bl.mult, 0.0);
-            g.beta = first ? make_double2(0.0, 0.0) : make_double2(1.0, 0.0);
-            g.opA = OP_T; g.opB = OP_N; g.a_real = ST_R64;
-            g.A = x.X; g.lda = x.K;
-            g.B = e->thetaT + e->bl.tOff[b]; g.ldb = e->bl.tStride;
-            g.C = e->xbar; g.ldc = e->G;
-            TRY(gemm(g, e->stream));
-            first = false;
-        }
-        return AFQMC_OK;
-    }
+    // real half-rotated vectors: the exchange's real X (K x G per block) in
+    // place of the complex-typed Aall, one real x complex product per block
+    if (e->exf && e->exf->gemm) return exf64_force(e, bl);
     ZGemmArgs g;
     g.m = e->G; g.n = e->W; g.k = (int)(bl.mult == 2 ? bl.tOff[1] : e->Ktot);
     g.alpha = make_double2((double)bl.mult, 0.0);

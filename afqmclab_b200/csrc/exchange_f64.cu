@@ -110,6 +110,18 @@ ex_vector_dot_kernel(long long K, const double *X, const zd *Y, int mult, zd *ex
     if (threadIdx.x == 0) exNum[g] = zadd(exNum[g], zscale(s, (double)mult));
 }
 
+// xbar = alpha sum_s P_s (+ xbar when accumulating); P_s consecutive G x W blocks
+__global__ void ex_force_sum_kernel(long long count, int S, const zd *P, zd alpha, int accumulate, zd *xbar)
+{
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < count;
+         e += (long long)gridDim.x * blockDim.x) {
+        zd v = P[e];
+        for (int s = 1; s < S; ++s) v = zadd(v, P[(size_t)s * count + e]);
+        v = zmul(alpha, v);
+        xbar[e] = accumulate ? zadd(xbar[e], v) : v;
+    }
+}
+
 int gemm_check(const ZGemmArgs &a, cudaStream_t s)
 {
     cudaError_t r = zgemm_batched(a, s);
@@ -149,6 +161,49 @@ int exf64_alloc(afqmc_engine *e, long long Kmax, ExF64Scratch &s)
     if ((r = engine_dalloc(e, &s.R, (size_t)Kmax * Kmax))) return r;
     if ((r = engine_dalloc(e, &s.Y, (size_t)Kmax * e->G))) return r;
     if ((r = engine_dalloc(e, &s.exTot, (size_t)e->W))) return r;
+    // the force's output (G x W) may be too few 64 x 64 tiles for the SMs:
+    // about four CTA slots' worth of work in partial products over K
+    const long long tiles = (long long)((e->G + 63) / 64) * ((e->W + 63) / 64);
+    int S = 1;
+    while (S < 8 && tiles * S < 592) S *= 2;
+    s.xsplit = S;
+    if (S > 1 && (r = engine_dalloc(e, &s.xp, (size_t)S * e->G * e->W))) return r;
+    return AFQMC_OK;
+}
+
+int exf64_force(afqmc_engine *e, const Blocks &bl)
+{
+    ExF64Scratch &s = *e->exf;
+    const int G = e->G, W = e->W;
+    bool first = true;
+    int r;
+    for (int b = 0; b < bl.nblk; ++b) {
+        if (bl.Ns[b] == 0) continue;
+        const ExF64 x = exf64_block(e, b);
+        int S = s.xsplit;
+        while (S > 1 && x.K % S) S /= 2;
+        ZGemmArgs g;
+        g.m = G; g.n = W; g.k = (int)(x.K / S);
+        g.opA = OP_T; g.opB = OP_N; g.a_real = ST_R64;
+        g.A = x.X; g.lda = x.K; g.strideA = x.K / S;
+        g.B = e->thetaT + e->bl.tOff[b]; g.ldb = e->bl.tStride; g.strideB = x.K / S;
+        const zd mult = make_double2((double)bl.mult, 0.0);
+        if (S == 1) {
+            g.C = e->xbar; g.ldc = G;
+            g.alpha = mult;
+            g.beta = first ? make_double2(0.0, 0.0) : make_double2(1.0, 0.0);
+            if ((r = gemm_check(g, e->stream))) return r;
+        } else {
+            g.C = s.xp; g.ldc = G; g.strideC = (long long)G * W;
+            g.batch = S;
+            if ((r = gemm_check(g, e->stream))) return r;
+            g_launch_count++;
+            ex_force_sum_kernel<<<296, 256, 0, e->stream>>>((long long)G * W, S, s.xp, mult, first ? 0 : 1,
+                                                           e->xbar);
+            if ((r = engine_check_launch())) return r;
+        }
+        first = false;
+    }
     return AFQMC_OK;
 }
 

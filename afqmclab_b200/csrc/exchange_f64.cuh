@@ -19,6 +19,9 @@ struct ExF64 {
 // bit for bit (bl1 lists block 0 with multiplicity 2).
 struct ExF64Scratch {
     zd *Z = nullptr, *M = nullptr, *R = nullptr, *Y = nullptr, *exTot = nullptr;
+    // the force's K split: xsplit partial products (G x W each) in xp
+    zd *xp = nullptr;
+    int xsplit = 1;
     ExF64 blk[2];
     bool gemm = false, restricted = false;
     Blocks bl1{};
@@ -36,3 +39,5 @@ int exf64_walker_totals(afqmc_engine *e, const ExF64 &x, bool accumulate, int mu
 // M = Uden Um^T (K x K) and its exchange permutation R, R(a + Ns i, b + Ns j) =
 // M(b + Ns i, a + Ns j); Uden, Um are K x W with leading dimension K.
 int exf64_pair_matrix(afqmc_engine *e, const ExF64 &x, const zd *Uden, const zd *Um);
+// Force xbar(g, w) = mult sum_b x_g^T u_w over the blocks of bl, on the real X.
+int exf64_force(afqmc_engine *e, const Blocks &bl);
